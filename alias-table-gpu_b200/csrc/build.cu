@@ -1,0 +1,188 @@
+// build.cu — C ABI of the weight total and the single-table alias build.
+//
+// wrs_sum_f32          <- Adder::addGpuCub (utils/Adder.cu:144-157)
+// wrs_alias_build_f32  <- AliasTableSplitGpu<TableStorage>::build()
+//                         (construction/aliasTable/buildMethod/AliasTableSplitGpu.cu:388-468)
+//
+// Unlike the reference build (>= 5 blocking device-to-host copies and >= 3 cudaMalloc/cudaFree
+// pairs inside build()), the whole build is four stream-ordered operations on caller memory:
+// a 128-byte memset of the scratch header, then the wsum, tile_scan and split_pack kernels.
+#include <cuda_runtime.h>
+
+#include <mutex>
+#include <vector>
+
+#include "build_kernels.cuh"
+#include "host_util.h"
+
+namespace wrs {
+
+DeviceInfo device_info() {
+    static std::mutex mu;
+    static std::vector<DeviceInfo> cache;
+    static std::vector<bool> have;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)cache.size() <= dev) {
+        cache.resize(dev + 1);
+        have.resize(dev + 1, false);
+    }
+    if (!have[dev]) {
+        DeviceInfo d{};
+        cudaDeviceGetAttribute(&d.sm_count, cudaDevAttrMultiProcessorCount, dev);
+        cudaDeviceGetAttribute(&d.major, cudaDevAttrComputeCapabilityMajor, dev);
+        cudaDeviceGetAttribute(&d.minor, cudaDevAttrComputeCapabilityMinor, dev);
+        int optin = 0;
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        d.smem_optin = (size_t)optin;
+        if (d.sm_count <= 0) d.sm_count = 148;
+        cache[dev] = d;
+        have[dev] = true;
+    }
+    return cache[dev];
+}
+
+wrs_status read_device_status(const uint32_t* d_status, cudaStream_t stream) {
+    uint32_t h = 0;
+    cudaError_t e = cudaMemcpyAsync(&h, d_status, sizeof(h), cudaMemcpyDeviceToHost, stream);
+    if (e != cudaSuccess) return WRS_ERR_CUDA;
+    e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return WRS_ERR_CUDA;
+    return (wrs_status)h;
+}
+
+uint32_t wsum_grid(uint64_t n) {
+    const DeviceInfo d = device_info();
+    uint64_t g = (n + 2047) / 2048;
+    const uint64_t cap = (uint64_t)d.sm_count * 8;
+    if (g > cap) g = cap;
+    if (g > kWsumMaxGrid) g = kWsumMaxGrid;
+    if (g < 1) g = 1;
+    return (uint32_t)g;
+}
+
+namespace {
+
+constexpr int64_t kMaxItems = (int64_t)0x7fffffff - 8192;
+
+int ipt_for(const wrs_build_opts* opts) {
+    const uint32_t t = opts ? opts->tile_items : 0u;
+    switch (t) {
+        case 0:
+        case 2048: return 8;
+        case 1024: return 4;
+        case 4096: return 16;
+        default: return -1;
+    }
+}
+
+struct BuildLayout {
+    BuildHeader* hdr;
+    double2* partials;
+    uint32_t* flags;
+    TileVals* agg;
+    TileVals* incl;
+    size_t bytes;
+};
+
+BuildLayout carve_build(void* scratch, uint64_t num_tiles, bool psa) {
+    (void)psa;
+    Carver c(scratch);
+    BuildLayout L;
+    L.hdr = c.take<BuildHeader>(1);
+    L.partials = c.take<double2>(kWsumMaxGrid);
+    L.flags = c.take<uint32_t>(num_tiles);
+    L.agg = c.take<TileVals>(num_tiles);
+    L.incl = c.take<TileVals>(num_tiles);
+    L.bytes = c.off;
+    return L;
+}
+
+template <int IPT>
+wrs_status launch_build(const float* d_w, uint64_t n, uint32_t method, wrs_alias_row* d_table, double* d_W,
+                        const BuildLayout& L, uint64_t num_tiles, cudaStream_t stream) {
+    constexpr int T = kBuildThreads * IPT;
+    (void)method;
+    cudaError_t e = cudaMemsetAsync(L.hdr, 0, sizeof(BuildHeader), stream);
+    if (e != cudaSuccess) return WRS_ERR_CUDA;
+    const uint32_t g = wsum_grid(n);
+    const uint64_t zero_words = num_tiles;
+    wsum_kernel<kWsumBlock><<<g, kWsumBlock, 0, stream>>>(d_w, n, L.hdr, L.partials, L.flags, zero_words, d_W);
+    tile_scan_kernel<IPT><<<(uint32_t)num_tiles, kBuildThreads, 0, stream>>>(d_w, n, L.hdr, L.agg, L.incl, L.flags,
+                                                                              (uint32_t)num_tiles);
+    {
+        const size_t smem = (size_t)T * (2 * sizeof(u128) + 2 * sizeof(uint32_t));
+        e = cudaFuncSetAttribute(split_pack_kernel<IPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return WRS_ERR_CUDA;
+        split_pack_kernel<IPT><<<(uint32_t)num_tiles, kBuildThreads, smem, stream>>>(d_w, n, L.hdr, L.agg, L.incl,
+                                                                                     (uint32_t)num_tiles, d_table);
+    }
+    return launch_status();
+}
+
+}  // namespace
+}  // namespace wrs
+
+using namespace wrs;
+
+extern "C" size_t wrs_sum_scratch_bytes(int64_t n) {
+    (void)n;
+    Carver c(nullptr);
+    c.take<BuildHeader>(1);
+    c.take<double2>(kWsumMaxGrid);
+    return c.off;
+}
+
+extern "C" wrs_status wrs_sum_f32(const float* d_w, int64_t n, double* d_total, void* d_scratch,
+                                  size_t scratch_bytes, void* stream_) {
+    if (!d_w || !d_total || !d_scratch || n < 1 || n > kMaxItems) return WRS_ERR_INVALID_ARGUMENT;
+    if (scratch_bytes < wrs_sum_scratch_bytes(n)) return WRS_ERR_SCRATCH_TOO_SMALL;
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+    Carver c(d_scratch);
+    BuildHeader* hdr = c.take<BuildHeader>(1);
+    double2* partials = c.take<double2>(kWsumMaxGrid);
+    if (cudaMemsetAsync(hdr, 0, sizeof(BuildHeader), stream) != cudaSuccess) return WRS_ERR_CUDA;
+    wsum_kernel<kWsumBlock><<<wsum_grid((uint64_t)n), kWsumBlock, 0, stream>>>(d_w, (uint64_t)n, hdr, partials,
+                                                                               nullptr, 0, d_total);
+    return launch_status();
+}
+
+extern "C" size_t wrs_alias_build_scratch_bytes(int64_t n, const wrs_build_opts* opts) {
+    const int ipt = ipt_for(opts);
+    if (n < 1 || ipt < 0) return 0;
+    const uint64_t T = (uint64_t)kBuildThreads * ipt;
+    const uint64_t nt = ((uint64_t)n + T - 1) / T;
+    const bool psa = opts && opts->method == WRS_METHOD_PSA_PLUS;
+    return carve_build(nullptr, nt, psa).bytes;
+}
+
+extern "C" wrs_status wrs_alias_build_f32(const float* d_w, int64_t n, const wrs_build_opts* opts,
+                                          wrs_alias_row* d_table, double* d_W, void* d_scratch,
+                                          size_t scratch_bytes, void* stream_) {
+    if (!d_w || !d_table || !d_scratch || n < 1 || n > kMaxItems) return WRS_ERR_INVALID_ARGUMENT;
+    const int ipt = ipt_for(opts);
+    const uint32_t method = opts ? opts->method : WRS_METHOD_SPLIT;
+    if (ipt < 0 || method > WRS_METHOD_PSA_PLUS) return WRS_ERR_INVALID_ARGUMENT;
+    if (method == WRS_METHOD_PSA_PLUS) return WRS_ERR_UNSUPPORTED;
+    const uint64_t T = (uint64_t)kBuildThreads * ipt;
+    const uint64_t nt = ((uint64_t)n + T - 1) / T;
+    const bool psa = method == WRS_METHOD_PSA_PLUS;
+    if (scratch_bytes < carve_build(nullptr, nt, psa).bytes) return WRS_ERR_SCRATCH_TOO_SMALL;
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+    const BuildLayout L = carve_build(d_scratch, nt, psa);
+    wrs_status st;
+    switch (ipt) {
+        case 4: st = launch_build<4>(d_w, (uint64_t)n, method, d_table, d_W, L, nt, stream); break;
+        case 16: st = launch_build<16>(d_w, (uint64_t)n, method, d_table, d_W, L, nt, stream); break;
+        default: st = launch_build<8>(d_w, (uint64_t)n, method, d_table, d_W, L, nt, stream); break;
+    }
+    if (st != WRS_SUCCESS) return st;
+    if (opts && (opts->flags & WRS_FLAG_SYNC)) return read_device_status(&L.hdr->status, stream);
+    return WRS_SUCCESS;
+}
+
+extern "C" wrs_status wrs_scratch_status(const void* d_scratch, void* stream) {
+    if (!d_scratch) return WRS_ERR_INVALID_ARGUMENT;
+    return read_device_status(&static_cast<const BuildHeader*>(d_scratch)->status, static_cast<cudaStream_t>(stream));
+}

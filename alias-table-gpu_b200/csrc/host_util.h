@@ -1,0 +1,50 @@
+// host_util.h — host helpers shared by the C ABI translation units.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "wrs.h"
+
+namespace wrs {
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+struct DeviceInfo {
+    int sm_count;
+    int major;
+    int minor;
+    size_t smem_optin;
+};
+
+// Cached per device ordinal.
+DeviceInfo device_info();
+
+inline wrs_status cuda_status(cudaError_t e) { return e == cudaSuccess ? WRS_SUCCESS : WRS_ERR_CUDA; }
+
+// Launch-error check after a kernel launch.
+inline wrs_status launch_status() { return cuda_status(cudaGetLastError()); }
+
+// Synchronise `stream` and read a device status word.
+wrs_status read_device_status(const uint32_t* d_status, cudaStream_t stream);
+
+// Simple linear carve of a scratch buffer.
+struct Carver {
+    unsigned char* base;
+    size_t off;
+    explicit Carver(void* p) : base(static_cast<unsigned char*>(p)), off(0) {}
+    template <typename T>
+    T* take(size_t count, size_t align = 256) {
+        off = align_up(off, align);
+        T* p = base ? reinterpret_cast<T*>(base + off) : nullptr;
+        off += count * sizeof(T);
+        return p;
+    }
+};
+
+constexpr int kWsumBlock = 256;
+constexpr uint32_t kWsumMaxGrid = 2048;
+uint32_t wsum_grid(uint64_t n);
+
+}  // namespace wrs

@@ -1,0 +1,154 @@
+// sample.cu — C ABI of the alias samplers and of rejection sampling.
+//
+// wrs_alias_sample        <- SamplerGpuBasic / SamplerGpuSectioned[Shared]::executeBenchmarkSampling
+//                            (sampling/aliasTable/SamplerGpuBasic.cu:109-133,
+//                             SamplerGpuSectioned.cu:138-166, SamplerGpuSectionedShared.cu:90-111)
+// wrs_rejection_build_f32 <- RejectionSampling::build + fillA
+//                            (construction/rejectionSampling/RejectionSampling.cu:35-56)
+// wrs_rejection_sample    <- SamplerRejection[GiveUp]::executeBenchmarkSampling
+//                            (sampling/rejectionSampling/SamplerRejection.cu:63-72)
+#include <cuda_runtime.h>
+
+#include "host_util.h"
+#include "rejection_kernels.cuh"
+#include "sample_kernels.cuh"
+
+using namespace wrs;
+
+namespace {
+constexpr int64_t kMaxItems = (int64_t)0x7fffffff - 8192;
+constexpr uint32_t kDefaultSection = 65536;
+constexpr size_t kStageMaxBytes = 96 * 1024;  // sections up to this size are staged in smem
+
+inline uint32_t seed_k0(uint64_t seed) { return (uint32_t)seed; }
+inline uint32_t seed_k1(uint64_t seed) { return (uint32_t)(seed >> 32); }
+}  // namespace
+
+extern "C" wrs_status wrs_alias_sample(const wrs_alias_row* d_table, int64_t n, uint64_t num_samples, uint64_t seed,
+                                       uint64_t counter_base, const wrs_sample_opts* opts, uint32_t* d_out,
+                                       uint64_t* d_section_counts, void* stream_) {
+    if (!d_table || n < 1 || n > kMaxItems || (num_samples > 0 && !d_out)) return WRS_ERR_INVALID_ARGUMENT;
+    if (((uintptr_t)d_table & 7u) != 0 || ((uintptr_t)d_out & 3u) != 0) return WRS_ERR_INVALID_ARGUMENT;
+    const uint32_t mode = opts ? opts->mode : WRS_SAMPLE_PLAIN;
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+    const DeviceInfo dev = device_info();
+    const uint2* table = reinterpret_cast<const uint2*>(d_table);
+    if (mode == WRS_SAMPLE_PLAIN) {
+        if (num_samples == 0) return WRS_SUCCESS;
+        const uint64_t noct = (num_samples + 7) / 8;
+        const uint32_t threads = (opts && opts->threads) ? opts->threads : 256u;
+        if (threads != 256u) return WRS_ERR_INVALID_ARGUMENT;
+        uint64_t grid = (noct + threads - 1) / threads;
+        const uint64_t cap = (uint64_t)dev.sm_count * 16;
+        if (grid > cap) grid = cap;
+        sample_plain_kernel<<<(uint32_t)grid, threads, 0, stream>>>(table, (uint32_t)n, num_samples, seed_k0(seed),
+                                                                   seed_k1(seed), counter_base, d_out);
+    } else if (mode == WRS_SAMPLE_SECTIONED) {
+        const uint32_t S = (opts && opts->section_items) ? opts->section_items : kDefaultSection;
+        if (S < 2 || (S & 1u)) return WRS_ERR_INVALID_ARGUMENT;
+        const uint64_t K = ((uint64_t)n + S - 1) / S;
+        const size_t sec_bytes = (size_t)S * sizeof(uint2);
+        const bool stage = sec_bytes <= kStageMaxBytes && ((uintptr_t)d_table & 15u) == 0;
+        const uint32_t threads = 512;
+        if (stage) {
+            const int per_sm = (int)(200 * 1024 / sec_bytes) < 4 ? (int)(200 * 1024 / sec_bytes) : 4;
+            uint64_t grid = (uint64_t)dev.sm_count * (per_sm > 0 ? per_sm : 1);
+            if (grid > K) grid = K;
+            cudaError_t e = cudaFuncSetAttribute(sample_sectioned_kernel<true>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sec_bytes);
+            if (e != cudaSuccess) return WRS_ERR_CUDA;
+            sample_sectioned_kernel<true><<<(uint32_t)grid, threads, sec_bytes, stream>>>(
+                table, (uint32_t)n, num_samples, S, (uint32_t)K, seed_k0(seed), seed_k1(seed), counter_base, d_out,
+                d_section_counts);
+        } else {
+            // one CTA per SM: the sections in flight (SMs x section bytes) stay L2-resident
+            uint64_t grid = (uint64_t)dev.sm_count;
+            if (grid > K) grid = K;
+            sample_sectioned_kernel<false><<<(uint32_t)grid, threads, 0, stream>>>(
+                table, (uint32_t)n, num_samples, S, (uint32_t)K, seed_k0(seed), seed_k1(seed), counter_base, d_out,
+                d_section_counts);
+        }
+    } else {
+        return WRS_ERR_INVALID_ARGUMENT;
+    }
+    const wrs_status st = launch_status();
+    if (st != WRS_SUCCESS) return st;
+    if (opts && (opts->flags & WRS_FLAG_SYNC)) return cuda_status(cudaStreamSynchronize(stream));
+    return WRS_SUCCESS;
+}
+
+// ---------------------------------------------------------------- rejection
+namespace {
+struct RejLayout {
+    BuildHeader* hdr;
+    double2* partials;
+    uint64_t* tile_words;
+    RejBigEntry* big;
+    uint64_t big_capacity;
+    size_t bytes;
+};
+constexpr int kRejIpt = 8;
+RejLayout carve_rej(void* scratch, uint64_t n) {
+    const uint64_t T = (uint64_t)kBuildThreads * kRejIpt;
+    const uint64_t nt = (n + T - 1) / T;
+    Carver c(scratch);
+    RejLayout L;
+    L.hdr = c.take<BuildHeader>(1);
+    L.partials = c.take<double2>(kWsumMaxGrid);
+    L.tile_words = c.take<uint64_t>(nt);
+    L.big_capacity = (2 * n) / kRejBig + 16;
+    L.big = c.take<RejBigEntry>(L.big_capacity);
+    L.bytes = c.off;
+    return L;
+}
+}  // namespace
+
+extern "C" size_t wrs_rejection_build_scratch_bytes(int64_t n) {
+    if (n < 1) return 0;
+    return carve_rej(nullptr, (uint64_t)n).bytes;
+}
+
+extern "C" wrs_status wrs_rejection_build_f32(const float* d_w, int64_t n, uint32_t* d_A, uint64_t a_capacity,
+                                              float* d_frac, uint64_t* d_A_size, double* d_W, void* d_scratch,
+                                              size_t scratch_bytes, uint32_t flags, void* stream_) {
+    if (!d_w || !d_A || !d_frac || !d_scratch || n < 1 || n > kMaxItems / 2) return WRS_ERR_INVALID_ARGUMENT;
+    if (scratch_bytes < carve_rej(nullptr, (uint64_t)n).bytes) return WRS_ERR_SCRATCH_TOO_SMALL;
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+    const RejLayout L = carve_rej(d_scratch, (uint64_t)n);
+    const uint64_t T = (uint64_t)kBuildThreads * kRejIpt;
+    const uint64_t nt = ((uint64_t)n + T - 1) / T;
+    if (cudaMemsetAsync(L.hdr, 0, sizeof(BuildHeader), stream) != cudaSuccess) return WRS_ERR_CUDA;
+    wsum_kernel<kWsumBlock><<<wsum_grid((uint64_t)n), kWsumBlock, 0, stream>>>(
+        d_w, (uint64_t)n, L.hdr, L.partials, reinterpret_cast<uint32_t*>(L.tile_words), 2 * nt, d_W);
+    rejection_tile_kernel<kRejIpt><<<(uint32_t)nt, kBuildThreads, 0, stream>>>(
+        d_w, (uint64_t)n, L.hdr, L.tile_words, (uint32_t)nt, d_A, a_capacity, d_frac, L.big, L.big_capacity, d_A_size);
+    const DeviceInfo dev = device_info();
+    rejection_big_kernel<<<(uint32_t)dev.sm_count * 4, 256, 0, stream>>>(L.hdr, L.big, L.big_capacity, d_A, a_capacity);
+    const wrs_status st = launch_status();
+    if (st != WRS_SUCCESS) return st;
+    if (flags & WRS_FLAG_SYNC) return read_device_status(&L.hdr->status, stream);
+    return WRS_SUCCESS;
+}
+
+extern "C" wrs_status wrs_rejection_sample(const uint32_t* d_A, const uint64_t* d_A_size, const float* d_frac,
+                                           int64_t n, uint64_t num_samples, uint64_t seed, uint64_t counter_base,
+                                           uint32_t max_tries, uint32_t* d_out, uint32_t* d_status, uint32_t flags,
+                                           void* stream_) {
+    if (!d_A || !d_A_size || !d_frac || n < 1 || (num_samples > 0 && !d_out)) return WRS_ERR_INVALID_ARGUMENT;
+    if (num_samples == 0) return WRS_SUCCESS;
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+    const DeviceInfo dev = device_info();
+    const uint32_t tries = max_tries ? max_tries : 64u;
+    uint64_t grid = (num_samples + 255) / 256;
+    const uint64_t cap = (uint64_t)dev.sm_count * 16;
+    if (grid > cap) grid = cap;
+    rejection_sample_kernel<<<(uint32_t)grid, 256, 0, stream>>>(d_A, d_A_size, d_frac, num_samples, seed_k0(seed),
+                                                               seed_k1(seed), counter_base, tries, d_out, d_status);
+    const wrs_status st = launch_status();
+    if (st != WRS_SUCCESS) return st;
+    if (flags & WRS_FLAG_SYNC) {
+        if (d_status) return read_device_status(d_status, stream);
+        return cuda_status(cudaStreamSynchronize(stream));
+    }
+    return WRS_SUCCESS;
+}

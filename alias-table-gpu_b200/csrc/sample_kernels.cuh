@@ -1,0 +1,165 @@
+// sample_kernels.cuh — alias-table samplers for sm_100a.
+//
+// Replaces SamplerGpuBasic (sampling/aliasTable/SamplerGpuBasic.cu:28-133) and
+// SamplerGpuSectioned[Shared] (SamplerGpuSectioned.cu:19-166, SamplerGpuSectionedShared.cu:19-111).
+// The reference draws an FP64 uniform u from clock-seeded XORWOW, takes row = (int)(u*N) and
+// compares W/N * frac(u*N) with the row weight; it writes no output. Here every sample is
+// a pure function of (seed, counter_base, output position) through Philox4x32-10:
+//   block b = counter_base + s/2 gives words x0..x3; sample s uses (x0, x1) if s is even,
+//   (x2, x3) if odd; row = floor(x_first * len / 2^32) + offset, coin = (x_second >> 8) 2^-24,
+//   result = coin < prob[row] ? row : alias[row]
+// — the reference's decision (SamplerGpuBasic.cu:48-69) with frac := coin and
+// weight := prob * W/N. Each sample is one 8-byte gather of a packed {prob, alias} row.
+#pragma once
+
+#include <cstdint>
+
+#include "binomial.cuh"
+#include "wrs_common.cuh"
+
+namespace wrs {
+
+__device__ __forceinline__ uint32_t alias_pick(const uint2 row, uint32_t r, uint32_t coin_bits) {
+    return coin24(coin_bits) < __uint_as_float(row.x) ? r : row.y;
+}
+
+// Plain sampling: each thread handles octets of consecutive output positions (4 Philox
+// blocks, 8 independent gathers in flight, two 16-byte stores).
+__global__ void __launch_bounds__(256) sample_plain_kernel(const uint2* __restrict__ table, uint32_t n, uint64_t m,
+                                                           uint32_t k0, uint32_t k1, uint64_t cbase,
+                                                           uint32_t* __restrict__ out) {
+    const uint64_t noct = (m + 7) >> 3;
+    const uint64_t gsize = (uint64_t)gridDim.x * blockDim.x;
+    const bool out_aligned = ((uintptr_t)out & 15u) == 0;
+    for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < noct; g += gsize) {
+        const uint64_t b = cbase + 4 * g;
+        uint32_t rows[8], coins[8];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint64_t bj = b + j;
+            const Philox4 r = philox4x32_10((uint32_t)bj, (uint32_t)(bj >> 32), 0u, 0u, k0, k1);
+            rows[2 * j] = scale_u32(r.x[0], n);
+            coins[2 * j] = r.x[1];
+            rows[2 * j + 1] = scale_u32(r.x[2], n);
+            coins[2 * j + 1] = r.x[3];
+        }
+        uint2 v[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] = __ldg(table + rows[j]);
+        uint32_t res[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) res[j] = alias_pick(v[j], rows[j], coins[j]);
+        const uint64_t s0 = 8 * g;
+        if (out_aligned && s0 + 8 <= m) {
+            uint4* o4 = reinterpret_cast<uint4*>(out + s0);
+            __stcs(o4, make_uint4(res[0], res[1], res[2], res[3]));
+            __stcs(o4 + 1, make_uint4(res[4], res[5], res[6], res[7]));
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                if (s0 + j < m) out[s0 + j] = res[j];
+        }
+    }
+}
+
+// Sectioned sampling: rows cut into K sections of S rows; section k receives an exact
+// multinomial share of the m samples (binomial tree, section_count) and writes them at its
+// output offset. A persistent CTA handles one section at a time, so the sections being
+// sampled at any moment (grid size x section bytes) stay inside L2; with STAGE the section
+// is first copied into shared memory and gathered from there.
+template <bool STAGE>
+__global__ void __launch_bounds__(512) sample_sectioned_kernel(const uint2* __restrict__ table, uint32_t n,
+                                                               uint64_t m, uint32_t S, uint32_t K, uint32_t k0,
+                                                               uint32_t k1, uint64_t cbase,
+                                                               uint32_t* __restrict__ out,
+                                                               uint64_t* __restrict__ counts_out) {
+    extern __shared__ __align__(16) uint2 s_rows[];
+    __shared__ uint64_t s_cnt, s_off;
+    for (uint32_t sec = blockIdx.x; sec < K; sec += gridDim.x) {
+        if (threadIdx.x == 0) {
+            uint64_t c, o;
+            section_count(sec, K, S, n, m, k0, k1, cbase, &c, &o);
+            s_cnt = c;
+            s_off = o;
+            if (counts_out) counts_out[sec] = c;
+        }
+        const uint32_t start = sec * S;
+        const uint32_t len = (uint32_t)section_rows(sec, sec + 1, S, n);
+        if (STAGE) {
+            const uint4* src = reinterpret_cast<const uint4*>(table + start);
+            uint4* dst = reinterpret_cast<uint4*>(s_rows);
+            const uint32_t n16 = len >> 1;
+            for (uint32_t i = threadIdx.x; i < n16; i += blockDim.x) dst[i] = __ldg(src + i);
+            if ((len & 1u) && threadIdx.x == 0) s_rows[len - 1] = __ldg(table + start + len - 1);
+        }
+        __syncthreads();
+        const uint64_t cnt = s_cnt, off = s_off;
+        if (cnt > 0) {
+            // Philox blocks covering output positions [off, off + cnt)
+            const uint64_t b_lo = off >> 1, b_hi = (off + cnt - 1) >> 1;
+            const uint64_t nb = b_hi - b_lo + 1;
+            for (uint64_t i = threadIdx.x; i < nb; i += blockDim.x) {
+                const uint64_t blk = b_lo + i;
+                const uint64_t bb = cbase + blk;
+                const Philox4 r = philox4x32_10((uint32_t)bb, (uint32_t)(bb >> 32), 0u, 0u, k0, k1);
+                const uint32_t ra = scale_u32(r.x[0], len), rb = scale_u32(r.x[2], len);
+                uint2 va, vb;
+                if (STAGE) {
+                    va = s_rows[ra];
+                    vb = s_rows[rb];
+                } else {
+                    va = __ldg(table + start + ra);
+                    vb = __ldg(table + start + rb);
+                }
+                const uint32_t oa = alias_pick(va, start + ra, r.x[1]);
+                const uint32_t ob = alias_pick(vb, start + rb, r.x[3]);
+                const uint64_t s = 2 * blk;
+                const bool wa = s >= off, wb = s + 1 < off + cnt;
+                if (wa && wb && ((s & 1) == 0) && (((uintptr_t)(out + s) & 7u) == 0)) {
+                    *reinterpret_cast<uint2*>(out + s) = make_uint2(oa, ob);
+                } else {
+                    if (wa) out[s] = oa;
+                    if (wb) out[s + 1] = ob;
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- rejection sampling
+// Replaces SamplerRejection::sample / SamplerRejectionGiveUp::sample
+// (sampling/rejectionSampling/SamplerRejection.cu:17-35, SamplerRejectionGiveUp.cu:17-37):
+// pick a uniform slot of A; a slot that is not its item's first is accepted, the first
+// slot is accepted with probability frac(n w / W). The first-slot test reads a flag bit in
+// the slot itself instead of comparing with A[index - 1].
+__global__ void __launch_bounds__(256) rejection_sample_kernel(const uint32_t* __restrict__ A,
+                                                               const uint64_t* __restrict__ a_size_ptr,
+                                                               const float* __restrict__ frac, uint64_t m,
+                                                               uint32_t k0, uint32_t k1, uint64_t cbase,
+                                                               uint32_t max_tries, uint32_t* __restrict__ out,
+                                                               uint32_t* status) {
+    const uint32_t asz = (uint32_t)*a_size_ptr;
+    const uint64_t gsize = (uint64_t)gridDim.x * blockDim.x;
+    bool failed = false;
+    for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < m; s += gsize) {
+        const uint64_t b = cbase + s;
+        uint32_t res = 0xffffffffu;
+        Philox4 r;
+        for (uint32_t t = 0; t < max_tries; ++t) {
+            if ((t & 1u) == 0) r = philox4x32_10((uint32_t)b, (uint32_t)(b >> 32), t >> 1, 0x52454a00u, k0, k1);
+            const uint32_t xs = r.x[(t & 1u) * 2], xc = r.x[(t & 1u) * 2 + 1];
+            const uint32_t e = __ldg(A + scale_u32(xs, asz));
+            const uint32_t item = e & 0x7fffffffu;
+            if ((e >> 31) == 0u || coin24(xc) < __ldg(frac + item)) {
+                res = item;
+                break;
+            }
+        }
+        if (res == 0xffffffffu) failed = true;
+        out[s] = res;
+    }
+    if (failed && status) record_status(status, kErrTooManyTries);
+}
+
+}  // namespace wrs

@@ -1,0 +1,362 @@
+"""wrs — Python binding of the B200 weighted-random-sampling library (libwrs.so).
+
+Two layers:
+
+* thin ctypes wrappers over the C ABI declared in include/wrs.h (device pointers, sizes,
+  streams), used with torch CUDA tensors for device memory;
+* classes that keep the reference's build(weights) -> sample(n) surface
+  (construction/SamplingAlgorithm.cuh:30-48, sampling/Sampler.cuh:10-31):
+  ``AliasTableSplitGpu`` / ``RejectionSamplingGpu`` (preBuild, build, postBuild, fullBuild,
+  name, weights, W, N) and ``SamplerGpuBasic`` / ``SamplerGpuSectioned`` / ``SamplerRejection``
+  (name, benchmarkSampling, getSamplingDistribution, sample).
+
+The CUDA path is the only path: importing this module without libwrs.so, or calling it
+without a CUDA device, raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libwrs.so")
+
+WRS_SUCCESS = 0
+WRS_ERR_INVALID_ARGUMENT = 1
+WRS_ERR_INVALID_WEIGHT = 2
+WRS_ERR_ZERO_TOTAL = 3
+WRS_ERR_SCRATCH_TOO_SMALL = 4
+WRS_ERR_CUDA = 5
+WRS_ERR_DEVICE_TIMEOUT = 6
+WRS_ERR_TOO_MANY_TRIES = 7
+WRS_ERR_UNSUPPORTED = 8
+WRS_ERR_CAPACITY = 9
+
+WRS_METHOD_SPLIT = 0
+WRS_METHOD_PSA_PLUS = 1
+WRS_FLAG_SYNC = 1
+WRS_SAMPLE_PLAIN = 0
+WRS_SAMPLE_SECTIONED = 1
+
+
+class BuildOpts(ctypes.Structure):
+    _fields_ = [("method", ctypes.c_uint32), ("tile_items", ctypes.c_uint32),
+                ("flags", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class SampleOpts(ctypes.Structure):
+    _fields_ = [("mode", ctypes.c_uint32), ("section_items", ctypes.c_uint32),
+                ("flags", ctypes.c_uint32), ("threads", ctypes.c_uint32)]
+
+
+class WrsError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        super().__init__(f"{what}: {status_string(status)} ({status})" if what else status_string(status))
+
+
+_lib = None
+_P = ctypes.c_void_p
+_I64 = ctypes.c_int64
+_U64 = ctypes.c_uint64
+_U32 = ctypes.c_uint32
+_SZ = ctypes.c_size_t
+
+_SIGNATURES = {
+    "wrs_sum_scratch_bytes": (_SZ, [_I64]),
+    "wrs_sum_f32": (ctypes.c_int, [_P, _I64, _P, _P, _SZ, _P]),
+    "wrs_alias_build_scratch_bytes": (_SZ, [_I64, _P]),
+    "wrs_alias_build_f32": (ctypes.c_int, [_P, _I64, _P, _P, _P, _P, _SZ, _P]),
+    "wrs_alias_sample": (ctypes.c_int, [_P, _I64, _U64, _U64, _U64, _P, _P, _P, _P]),
+    "wrs_rejection_build_scratch_bytes": (_SZ, [_I64]),
+    "wrs_rejection_build_f32": (ctypes.c_int, [_P, _I64, _P, _U64, _P, _P, _P, _P, _SZ, _U32, _P]),
+    "wrs_rejection_sample": (ctypes.c_int, [_P, _P, _P, _I64, _U64, _U64, _U64, _U32, _P, _P, _U32, _P]),
+    "wrs_batched_build_scratch_bytes": (_SZ, [_P, _I64, _P]),
+    "wrs_batched_build_f32": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P, _SZ, _P]),
+    "wrs_batched_sample": (ctypes.c_int, [_P, _P, _I64, _P, _U64, _U64, _U64, _P, _P]),
+    "wrs_scratch_status": (ctypes.c_int, [_P, _P]),
+    "wrs_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "wrs_check_device": (ctypes.c_int, []),
+    "wrs_version": (ctypes.c_int, []),
+}
+
+
+def lib() -> ctypes.CDLL:
+    """Loads libwrs.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"libwrs.so not built at {LIB_PATH}; run `make -C {_HERE}`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def status_string(status: int) -> str:
+    return lib().wrs_status_string(int(status)).decode()
+
+
+def _check(status: int, what: str):
+    if status != WRS_SUCCESS:
+        raise WrsError(status, what)
+
+
+def _ptr(t) -> Optional[int]:
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    return t.data_ptr()
+
+
+def _stream(stream) -> Optional[int]:
+    import torch
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+# ---------------------------------------------------------------- C ABI wrappers
+
+def build_opts(method: int = WRS_METHOD_SPLIT, tile_items: int = 0, sync: bool = False) -> BuildOpts:
+    return BuildOpts(method, tile_items, WRS_FLAG_SYNC if sync else 0, 0)
+
+
+def alias_build_scratch_bytes(n: int, opts: Optional[BuildOpts] = None) -> int:
+    return int(lib().wrs_alias_build_scratch_bytes(n, ctypes.byref(opts) if opts else None))
+
+
+def alias_build(w, table, scratch, opts: Optional[BuildOpts] = None, W_out=None, stream=None) -> int:
+    """Builds into `table` (torch int64/uint32 tensor of n rows, 8 bytes each) from FP32 `w`."""
+    n = w.numel()
+    st = lib().wrs_alias_build_f32(_ptr(w), n, ctypes.byref(opts) if opts else None, _ptr(table), _ptr(W_out),
+                                   _ptr(scratch), scratch.numel() * scratch.element_size(), _stream(stream))
+    return st
+
+
+def alias_sample(table, n: int, num_samples: int, seed: int, out, counter_base: int = 0,
+                 mode: int = WRS_SAMPLE_PLAIN, section_items: int = 0, section_counts=None,
+                 sync: bool = False, stream=None) -> int:
+    opts = SampleOpts(mode, section_items, WRS_FLAG_SYNC if sync else 0, 0)
+    return lib().wrs_alias_sample(_ptr(table), n, num_samples, seed & (2**64 - 1), counter_base & (2**64 - 1),
+                                  ctypes.byref(opts), _ptr(out), _ptr(section_counts), _stream(stream))
+
+
+def rejection_build_scratch_bytes(n: int) -> int:
+    return int(lib().wrs_rejection_build_scratch_bytes(n))
+
+
+def rejection_build(w, A, frac, a_size, scratch, W_out=None, sync: bool = False, stream=None) -> int:
+    return lib().wrs_rejection_build_f32(_ptr(w), w.numel(), _ptr(A), A.numel(), _ptr(frac), _ptr(a_size),
+                                         _ptr(W_out), _ptr(scratch), scratch.numel() * scratch.element_size(),
+                                         WRS_FLAG_SYNC if sync else 0, _stream(stream))
+
+
+def rejection_sample(A, a_size, frac, n: int, num_samples: int, seed: int, out, counter_base: int = 0,
+                     max_tries: int = 0, status=None, sync: bool = False, stream=None) -> int:
+    return lib().wrs_rejection_sample(_ptr(A), _ptr(a_size), _ptr(frac), n, num_samples, seed & (2**64 - 1),
+                                      counter_base & (2**64 - 1), max_tries, _ptr(out), _ptr(status),
+                                      WRS_FLAG_SYNC if sync else 0, _stream(stream))
+
+
+def scratch_status(scratch, stream=None) -> int:
+    return lib().wrs_scratch_status(_ptr(scratch), _stream(stream))
+
+
+def sum_f32(w, total, scratch, stream=None) -> int:
+    return lib().wrs_sum_f32(_ptr(w), w.numel(), _ptr(total), _ptr(scratch),
+                             scratch.numel() * scratch.element_size(), _stream(stream))
+
+
+# ---------------------------------------------------------------- reference-shaped surface
+
+def _device_bytes(nbytes: int, device):
+    import torch
+    return torch.empty(max(int(nbytes), 16), dtype=torch.uint8, device=device)
+
+
+class SamplingAlgorithm:
+    """build(weights) surface of construction/SamplingAlgorithm.cuh:30-48.
+
+    ``weights`` is a host array of N FP32 weights; ``W`` and ``N`` as in the reference.
+    """
+
+    def __init__(self, weights, device: str = "cuda"):
+        self.weights = np.ascontiguousarray(np.asarray(weights, dtype=np.float32))
+        self.N = int(self.weights.shape[0])
+        self.W = 0.0
+        self.device = device
+
+    def name(self) -> str:
+        raise NotImplementedError
+
+    def preBuild(self):
+        raise NotImplementedError
+
+    def build(self):
+        raise NotImplementedError
+
+    def postBuild(self) -> bool:
+        raise NotImplementedError
+
+    def fullBuild(self) -> bool:
+        self.preBuild()
+        self.build()
+        return self.postBuild()
+
+
+class AliasTableSplitGpu(SamplingAlgorithm):
+    """AliasTableSplitGpu (construction/aliasTable/buildMethod/AliasTableSplitGpu.cu).
+
+    After postBuild(), ``aliasTable`` holds the host table as (prob float32, alias uint32)
+    arrays; ``table`` is the device table (int64 tensor, one packed row per item).
+    """
+
+    def __init__(self, weights, method: int = WRS_METHOD_SPLIT, tile_items: int = 0, device: str = "cuda"):
+        super().__init__(weights, device)
+        self.method = method
+        self.opts = build_opts(method, tile_items)
+        self.table = None
+        self.aliasTable = None
+
+    def name(self) -> str:
+        return "AliasTableSplitGpu" + ("PsaPlus" if self.method == WRS_METHOD_PSA_PLUS else "")
+
+    def preBuild(self):
+        import torch
+        self.weightsGpu = torch.from_numpy(self.weights).to(self.device)
+        self.table = torch.empty(self.N, dtype=torch.int64, device=self.device)
+        self.scratch = _device_bytes(alias_build_scratch_bytes(self.N, self.opts), self.device)
+        self.W_dev = torch.zeros(1, dtype=torch.float64, device=self.device)
+
+    def build(self):
+        _check(alias_build(self.weightsGpu, self.table, self.scratch, self.opts, self.W_dev), "alias build")
+
+    def postBuild(self) -> bool:
+        st = scratch_status(self.scratch)
+        _check(st, "alias build (device)")
+        self.W = float(self.W_dev.item())
+        rows = self.table.cpu().numpy().view(np.uint32).reshape(-1, 2)
+        self.aliasTable = (rows[:, 0].view(np.float32).copy(), rows[:, 1].copy())
+        return True
+
+
+class RejectionSamplingGpu(SamplingAlgorithm):
+    """RejectionSampling (construction/rejectionSampling/RejectionSampling.cu)."""
+
+    def __init__(self, weights, device: str = "cuda"):
+        super().__init__(weights, device)
+
+    def name(self) -> str:
+        return "RejectionSamplingGpu"
+
+    def preBuild(self):
+        import torch
+        self.weightsGpu = torch.from_numpy(self.weights).to(self.device)
+        self.A = torch.empty(2 * self.N + 1, dtype=torch.int32, device=self.device)
+        self.frac = torch.empty(self.N, dtype=torch.float32, device=self.device)
+        self.A_size = torch.zeros(1, dtype=torch.int64, device=self.device)
+        self.scratch = _device_bytes(rejection_build_scratch_bytes(self.N), self.device)
+        self.W_dev = torch.zeros(1, dtype=torch.float64, device=self.device)
+
+    def build(self):
+        _check(rejection_build(self.weightsGpu, self.A, self.frac, self.A_size, self.scratch, self.W_dev),
+               "rejection build")
+
+    def postBuild(self) -> bool:
+        _check(scratch_status(self.scratch), "rejection build (device)")
+        self.W = float(self.W_dev.item())
+        return True
+
+
+class Sampler:
+    """sampling/Sampler.cuh:10-31: name(), benchmarkSampling(n) in Gsamples/s,
+    getSamplingDistribution(n) -> per-item counts; plus sample(n) -> device tensor."""
+
+    def __init__(self, algorithm: SamplingAlgorithm, seed: int = 0x5EED):
+        self.algorithm = algorithm
+        self.seed = seed
+        self.counter = 0
+
+    def name(self) -> str:
+        raise NotImplementedError
+
+    def sample(self, numSamples: int, out=None):
+        raise NotImplementedError
+
+    def benchmarkSampling(self, numSamples: int) -> float:
+        import torch
+        out = torch.empty(numSamples, dtype=torch.int32, device=self.algorithm.device)
+        self.sample(numSamples, out)
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        self.sample(numSamples, out)
+        stop.record()
+        stop.synchronize()
+        return numSamples / (start.elapsed_time(stop) * 1e6)
+
+    def getSamplingDistribution(self, numSamples: int) -> np.ndarray:
+        import torch
+        out = self.sample(numSamples)
+        return torch.bincount(out.long(), minlength=self.algorithm.N).cpu().numpy()
+
+
+class SamplerGpuBasic(Sampler):
+    def name(self) -> str:
+        return "SamplerGpuBasic"
+
+    def sample(self, numSamples: int, out=None):
+        import torch
+        a = self.algorithm
+        if out is None:
+            out = torch.empty(numSamples, dtype=torch.int32, device=a.device)
+        _check(alias_sample(a.table, a.N, numSamples, self.seed, out, self.counter), "plain sample")
+        self.counter += (numSamples + 1) // 2
+        return out
+
+
+class SamplerGpuSectioned(Sampler):
+    def __init__(self, algorithm: SamplingAlgorithm, itemsPerSection: int = 0, seed: int = 0x5EED):
+        super().__init__(algorithm, seed)
+        self.itemsPerSection = itemsPerSection
+
+    def name(self) -> str:
+        return "SamplerGpuSectioned"
+
+    def sample(self, numSamples: int, out=None):
+        import torch
+        a = self.algorithm
+        if out is None:
+            out = torch.empty(numSamples, dtype=torch.int32, device=a.device)
+        _check(alias_sample(a.table, a.N, numSamples, self.seed, out, self.counter, mode=WRS_SAMPLE_SECTIONED,
+                            section_items=self.itemsPerSection), "sectioned sample")
+        self.counter += (numSamples + 1) // 2
+        return out
+
+
+class SamplerRejection(Sampler):
+    def __init__(self, algorithm: RejectionSamplingGpu, seed: int = 0x5EED, max_tries: int = 0):
+        super().__init__(algorithm, seed)
+        self.max_tries = max_tries
+
+    def name(self) -> str:
+        return "SamplerRejection"
+
+    def sample(self, numSamples: int, out=None):
+        import torch
+        a = self.algorithm
+        if out is None:
+            out = torch.empty(numSamples, dtype=torch.int32, device=a.device)
+        _check(rejection_sample(a.A, a.A_size, a.frac, a.N, numSamples, self.seed, out, self.counter,
+                                self.max_tries), "rejection sample")
+        self.counter += numSamples
+        return out

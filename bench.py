@@ -1,0 +1,399 @@
+#!/usr/bin/env python
+"""bench.py — throughput of the weighted-random-sampling hot path on B200.
+
+Workload (the large single-table configuration): n = 2^26 FP32 weights w_i = (i+1)^-1.1
+(computed in FP64, rounded to FP32) under a seeded random permutation; one step = one
+split-method alias build of the whole table followed by 2^30 plain samples (uint32 indices
+written to HBM). `value` = (items built + samples drawn) per second over all GPUs, from CUDA
+events around K steps with every input already resident in HBM (weights 256 MB, output
+4 GB: larger than L2, so no flush is needed between steps). `e2e` measures the same step
+through the public API from pinned host memory: weights copied in and all samples copied
+out inside the timed region.
+
+The JSON line also carries the per-phase numbers of the workload (split build Gitems/s,
+plain and sectioned Gsamples/s), the per-item probability error of the built table, the
+roofline of the dominant kernel (the plain sampler), the SM clocks seen while timing, and
+the reference's CPU path timed on this host (`cpu_baseline`).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun, one replica per GPU (the path does not need a collective:
+"replicas only"); value is the sum over replicas, time the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "alias-table-gpu_b200"))
+
+N_ITEMS = 1 << 26
+N_SAMPLES = 1 << 30
+SECTION_ITEMS = 1 << 16
+SEED_WEIGHTS = 0x5EED + 2
+SEED_SAMPLES = 0xC0FFEE
+METRIC = "build Gitems/s + Gsamples/s, batched vs per-table, %HBM peak, at ≤1e-6 prob err"
+UNIT = "G(items+samples)/s"
+WORKLOAD = "single large table: n=2^26 w=(i+1)^-1.1 permuted; split build + 2^30 plain samples per step"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def make_weights(n: int = N_ITEMS, seed: int = SEED_WEIGHTS) -> np.ndarray:
+    w = (np.arange(1, n + 1, dtype=np.float64) ** -1.1).astype(np.float32)
+    return w[np.random.default_rng(seed).permutation(n)]
+
+
+def measured_peak():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per launch of the plain sampler from the committed ncu summary, if any."""
+    path = os.path.join(REPO, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d.get("sample_plain_kernel_bytes_per_launch")
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_uuid: str | None):
+        self.uuid = gpu_uuid
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100"]
+        if self.uuid:
+            cmd += ["-i", self.uuid]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
+        sm, smax, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "power_w_max": max(power),
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def table_error(w: np.ndarray, rows_u32: np.ndarray) -> dict:
+    """Per-item relative error of the table against w_i / W (W summed in FP64 pairwise)."""
+    n = w.size
+    p = rows_u32[:, 0].view(np.float32).astype(np.float64)
+    a = rows_u32[:, 1].astype(np.int64)
+    got = p + np.bincount(a, weights=1.0 - p, minlength=n)
+    wd = w.astype(np.float64)
+    W = math.fsum(wd.tolist()) if n <= (1 << 20) else float(np.sum(wd))
+    exp = n * wd / W
+    nz = wd > 0
+    rel = np.abs(got[nz] - exp[nz]) / exp[nz]
+    return {"max_rel": float(rel.max()), "p9999_rel": float(np.quantile(rel, 0.9999)),
+            "zero_weight_mass": float(got[~nz].sum()) if (~nz).any() else 0.0}
+
+
+# ---------------------------------------------------------------- our arm
+
+def run_ours(args, rank: int, world: int, local_rank: int):
+    import torch
+    import wrs
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    if wrs.lib().wrs_check_device() != 0:
+        raise RuntimeError("not an sm_100 device")
+    n, m = N_ITEMS, N_SAMPLES
+    w_np = make_weights()
+    w_host = torch.from_numpy(w_np).pin_memory()
+    w = w_host.to(dev)
+    opts = wrs.build_opts(wrs.WRS_METHOD_SPLIT)
+    table = torch.empty(n, dtype=torch.int64, device=dev)
+    scratch = torch.empty(wrs.alias_build_scratch_bytes(n, opts), dtype=torch.uint8, device=dev)
+    out = torch.empty(m, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+
+    def build():
+        st = wrs.alias_build(w, table, scratch, opts, None, sp)
+        if st:
+            raise wrs.WrsError(st, "build")
+
+    def sample(counter_base, mode=wrs.WRS_SAMPLE_PLAIN, section_items=0):
+        st = wrs.alias_sample(table, n, m, SEED_SAMPLES, out, counter_base, mode=mode, section_items=section_items,
+                              stream=sp)
+        if st:
+            raise wrs.WrsError(st, "sample")
+
+    # correctness of this exact table (before timing)
+    build()
+    st = wrs.scratch_status(scratch, sp)
+    if st:
+        raise wrs.WrsError(st, "build (device)")
+    err = table_error(w_np, table.cpu().numpy().view(np.uint32).reshape(-1, 2)) if rank == 0 else None
+
+    for i in range(args.warmup):
+        build()
+        sample(i * (m // 2))
+    torch.cuda.synchronize()
+
+    K = args.steps
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(K)]
+    smi_uuid = None
+    try:
+        smi_uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    clocks = ClockSampler(smi_uuid if rank == 0 else None)
+    if rank == 0:
+        clocks.start()
+        time.sleep(0.3)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    for k in range(K):
+        ev[k][0].record(stream)
+        build()
+        ev[k][1].record(stream)
+        sample((args.warmup + k) * (m // 2))
+        ev[k][2].record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clk = clocks.stop() if rank == 0 else None
+    total_ms = ev[0][0].elapsed_time(ev[K - 1][2])
+    build_ms = statistics.median([e[0].elapsed_time(e[1]) for e in ev])
+    sample_ms = statistics.median([e[1].elapsed_time(e[2]) for e in ev])
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+
+    # sectioned sampling on the same table (reported beside the headline)
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sample(0, wrs.WRS_SAMPLE_SECTIONED, SECTION_ITEMS)
+    torch.cuda.synchronize()
+    reps = 5
+    s0.record(stream)
+    for r in range(reps):
+        sample((r + 1) * (m // 2), wrs.WRS_SAMPLE_SECTIONED, SECTION_ITEMS)
+    s1.record(stream)
+    torch.cuda.synchronize()
+    sect_ms = s0.elapsed_time(s1) / reps
+
+    # end to end through the API with host buffers: H2D weights, build, sample, D2H samples
+    out_host = torch.empty(m, dtype=torch.int32).pin_memory()
+    e2e_steps = max(3, min(K, 10))
+    for i in range(2):
+        w.copy_(w_host, non_blocking=True)
+        build()
+        sample(i)
+        out_host.copy_(out, non_blocking=True)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(e2e_steps):
+        w.copy_(w_host, non_blocking=True)
+        build()
+        sample(i * (m // 2))
+        out_host.copy_(out, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+
+    if rank != 0:
+        return None
+    peak, peak_kind = measured_peak()
+    achieved = 12.0 * m / (sample_ms * 1e-3) / 1e9  # GB/s, 12 B per sample (8 B gather + 4 B write)
+    build_gbs = 12.0 * n / (build_ms * 1e-3) / 1e9  # 12 B per item (4 B read + 8 B write)
+    step_ms = total_ms / K
+    value = world * (n + m) / (step_ms * 1e-3) / 1e9
+    cpu = cpu_baseline(w_np) if not args.no_cpu_baseline else None
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": round(step_ms, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_items": n, "n_samples_per_step": m, "build": "split",
+                   "sampling": "plain", "weights": "w_i=(i+1)^-1.1 FP64->FP32, seeded permutation",
+                   "l2": "inputs larger than L2 (256 MB weights, 4 GB samples); no flush",
+                   "parallelism": f"replicas x{world}"},
+        "phases": {"build_ms": round(build_ms, 4), "build_gitems_s": round(n / build_ms / 1e6, 3),
+                   "build_hbm_gbs": round(build_gbs, 1), "build_hbm_frac": round(build_gbs / peak, 4),
+                   "sample_ms": round(sample_ms, 4), "sample_gsamples_s": round(m / sample_ms / 1e6, 3),
+                   "sectioned_sample_ms": round(sect_ms, 4),
+                   "sectioned_gsamples_s": round(m / sect_ms / 1e6, 3),
+                   "section_items": SECTION_ITEMS},
+        "prob_error": err,
+        "roofline": {"kernel": "sample_plain_kernel", "bound": "hbm", "achieved": round(achieved, 1),
+                     "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "traffic": ncu_traffic(),
+                     "algorithmic_bytes": "12 B/sample x 2^30 samples per launch (8 B row gather + 4 B write)"},
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "e2e": {"value": round(world * (n + m) / (e2e_ms * 1e-3) / 1e9, 4), "unit": UNIT,
+                "ms_per_step": round(e2e_ms, 3), "h2d_bytes_per_step": 4 * n, "d2h_bytes_per_step": 4 * m},
+        "gpu_launches": 4 * K,
+    }
+    return line
+
+
+# ---------------------------------------------------------------- reference CPU
+
+def cpu_baseline(w_np: np.ndarray, n_build: int = N_ITEMS, n_samp: int = 1 << 22) -> dict:
+    """The reference's CPU path on this host's cores, on a bounded sample of the workload:
+    AliasTableSplit::build's split and pack loops over all cores (the reference's own
+    functions, a harness like the reference's build) for the first `n_build` weights, and
+    SamplerCpu::sample (1 core, rand()-bound, as shipped) for `n_samp` samples; the step
+    time of the full workload is n/build_rate + m/sample_rate."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import py_oracle as po  # the CPU-baseline leg is the one place bench.py runs the oracle
+
+    threads = os.cpu_count() or 1
+    w64 = w_np[:n_build].astype(np.float64)
+    p = 64 * threads
+    if po.ref_available():
+        wt, al, W, t_build = po.ref_split_build_parallel(w64, p, threads)
+        t_samp, _ = po.ref_sampler_cpu(wt, al, W, n_samp)
+        kind = "reference"
+        what = (f"reference AliasTableSplit split+pack loops on {threads} threads (p={p}) over the first "
+                f"{n_build} weights; reference SamplerCpu::sample (1 thread, rand()) for {n_samp} samples; "
+                f"step time = 2^26/build_rate + 2^30/sample_rate")
+    else:
+        t0 = time.time()
+        wt, al, W, rc = po.split_build(w64, p, threads)
+        t_build = time.time() - t0
+        rows = np.zeros((w64.size, 2), dtype=np.uint32)
+        rows[:, 0] = (wt / (W / w64.size)).astype(np.float32).view(np.uint32)
+        rows[:, 1] = np.clip(al, 0, w64.size - 1).astype(np.uint32)
+        rate = po.sample_plain_timed(rows, n_samp, SEED_SAMPLES, threads)
+        t_samp = n_samp / rate
+        kind = "port"
+        what = (f"oracle restatement of AliasTableSplit::build on {threads} threads over the first {n_build} "
+                f"weights; restated doSample with Philox on {threads} threads for {n_samp} samples; "
+                f"step time = 2^26/build_rate + 2^30/sample_rate")
+    build_rate = n_build / t_build
+    sample_rate = n_samp / t_samp
+    t_step = N_ITEMS / build_rate + N_SAMPLES / sample_rate
+    return {"value": round((N_ITEMS + N_SAMPLES) / t_step / 1e9, 6), "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": what, "build_gitems_s": round(build_rate / 1e9, 5),
+            "sample_gsamples_s": round(sample_rate / 1e9, 5), "step_s": round(t_step, 2)}
+
+
+def run_reference(args, rank: int):
+    """The reference arm: the reference's CPU implementation of the path (compiled from its
+    sources) on this host's cores; rank 0 only. Each step is a bounded sample of the
+    workload (a 2^24-item build and 2^21 samples) scaled to the full step."""
+    if rank != 0:
+        return None
+    w_np = make_weights()
+    for _ in range(min(args.warmup, 1)):
+        cpu_baseline(w_np, 1 << 24, 1 << 21)
+    vals, last = [], None
+    t0 = time.time()
+    for _ in range(args.steps):
+        last = cpu_baseline(w_np, 1 << 24, 1 << 21)
+        vals.append(last["value"])
+    wall = time.time() - t0
+    value = statistics.median(vals)
+    step_s = (N_ITEMS + N_SAMPLES) / (value * 1e9)
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(step_s * 1e3, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n_items": N_ITEMS, "n_samples_per_step": N_SAMPLES},
+            "impl": "reference", "cpu_baseline": dict(last, value=value, wall_s=round(wall, 1)),
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        line = run_reference(args, rank)
+    else:
+        if world > 1:
+            import datetime
+
+            import torch
+            torch.cuda.set_device(local_rank)
+            torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        line = run_ours(args, rank, world, local_rank)
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

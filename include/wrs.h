@@ -1,0 +1,189 @@
+/*
+ * wrs.h — C ABI of the B200 (sm_100a) weighted-random-sampling library.
+ *
+ * The library builds alias tables and rejection-sampling structures from FP32
+ * weights that already live in device memory, and draws samples from them with
+ * a counter-based Philox4x32-10 stream. Every entry point is stream-ordered,
+ * allocates no device memory itself (the caller passes a scratch buffer sized by
+ * the matching *_scratch_bytes query), never traps, and returns a wrs_status.
+ *
+ * Errors found on the device while a launch runs (an invalid weight, a bounded
+ * device wait that gave up, a rejection sample that ran out of tries) are
+ * written into a status word inside the scratch buffer (or the sampler's
+ * d_status argument) and read back with wrs_scratch_status(); passing
+ * WRS_FLAG_SYNC in the options makes the call itself synchronise and return it.
+ *
+ * Each entry point replaces one interface of ByteHamster/alias-table-gpu:
+ *   wrs_alias_build_f32   <- AliasTableSplitGpu<TableStorage>::build()
+ *                            (construction/aliasTable/buildMethod/AliasTableSplitGpu.cu:388-468),
+ *                            with psaPlus() (:342-386) selected by WRS_METHOD_PSA_PLUS
+ *   wrs_alias_sample      <- SamplerGpuBasic::executeBenchmarkSampling
+ *                            (sampling/aliasTable/SamplerGpuBasic.cu:109-133) and
+ *                            SamplerGpuSectioned[Shared]::executeBenchmarkSampling
+ *                            (sampling/aliasTable/SamplerGpuSectioned.cu:138-166,
+ *                             SamplerGpuSectionedShared.cu:90-111)
+ *   wrs_rejection_build_f32 <- RejectionSampling::build() + fillA()
+ *                            (construction/rejectionSampling/RejectionSampling.cu:35-56,
+ *                             RejectionSamplingBinarySearch.cu:12-37)
+ *   wrs_rejection_sample  <- SamplerRejection / SamplerRejectionGiveUp
+ *                            (sampling/rejectionSampling/SamplerRejection.cu:17-72,
+ *                             SamplerRejectionGiveUp.cu:17-79)
+ *   wrs_batched_*         <- a loop of AliasTableSplitGpu objects (one per table) in the
+ *                            reference's experiment drivers; the reference has no batched form
+ *   wrs_sum_f32           <- Adder::addGpuCub (utils/Adder.cu:144-157)
+ */
+#ifndef WRS_H
+#define WRS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define WRS_API __attribute__((visibility("default")))
+#else
+#define WRS_API
+#endif
+
+#define WRS_VERSION_MAJOR 0
+#define WRS_VERSION_MINOR 1
+
+typedef enum wrs_status {
+    WRS_SUCCESS = 0,
+    WRS_ERR_INVALID_ARGUMENT = 1,  /* null pointer, size out of range, unknown option */
+    WRS_ERR_INVALID_WEIGHT = 2,    /* a weight is NaN, negative or infinite */
+    WRS_ERR_ZERO_TOTAL = 3,        /* all weights are zero: no distribution */
+    WRS_ERR_SCRATCH_TOO_SMALL = 4, /* scratch_bytes below the *_scratch_bytes query */
+    WRS_ERR_CUDA = 5,              /* a CUDA runtime call failed */
+    WRS_ERR_DEVICE_TIMEOUT = 6,    /* a bounded device-side wait gave up */
+    WRS_ERR_TOO_MANY_TRIES = 7,    /* a rejection sample exhausted max_tries */
+    WRS_ERR_UNSUPPORTED = 8,       /* the device is not an sm_100 part */
+    WRS_ERR_CAPACITY = 9           /* an output buffer is too small (rejection array) */
+} wrs_status;
+
+/* One alias-table row: the row keeps itself with probability `prob`, else
+ * yields `alias`. Item i's probability is
+ *   (prob_i + sum_{r : alias_r = i, r != i} (1 - prob_r)) / n.
+ * The reference stores {double weight (absolute, in [0, W/N]); int alias}
+ * (construction/aliasTable/TableStorage.cuh:8-11); prob = weight / (W/N). */
+typedef struct wrs_alias_row {
+    float prob;
+    uint32_t alias;
+} wrs_alias_row;
+
+typedef enum wrs_build_method {
+    WRS_METHOD_SPLIT = 0,     /* split/pack over light/heavy residual prefix sums ("PSA") */
+    WRS_METHOD_PSA_PLUS = 1   /* tile-local greedy pre-pack, leftovers through split/pack */
+} wrs_build_method;
+
+#define WRS_FLAG_SYNC 1u      /* synchronise the stream and return the device status */
+
+typedef struct wrs_build_opts {
+    uint32_t method;          /* wrs_build_method */
+    uint32_t tile_items;      /* 0 = default (2048); a power of two in [512, 4096] */
+    uint32_t flags;           /* WRS_FLAG_* */
+    uint32_t reserved;
+} wrs_build_opts;
+
+typedef enum wrs_sample_mode {
+    WRS_SAMPLE_PLAIN = 0,     /* sample s at output position s, any row */
+    WRS_SAMPLE_SECTIONED = 1  /* rows cut into sections; per-section counts from an exact
+                                 binomial tree; output grouped by section */
+} wrs_sample_mode;
+
+typedef struct wrs_sample_opts {
+    uint32_t mode;            /* wrs_sample_mode */
+    uint32_t section_items;   /* SECTIONED: rows per section (0 = 65536) */
+    uint32_t flags;           /* WRS_FLAG_* */
+    uint32_t threads;         /* 0 = default launch shape */
+} wrs_sample_opts;
+
+/* ---- weight total ------------------------------------------------------- */
+
+/* Compensated (double-double) sum of n FP32 weights. Writes the correctly rounded
+ * total to *d_total (device). Rejects NaN / negative / infinite weights. */
+WRS_API size_t     wrs_sum_scratch_bytes(int64_t n);
+WRS_API wrs_status wrs_sum_f32(const float* d_w, int64_t n, double* d_total,
+                       void* d_scratch, size_t scratch_bytes, void* stream);
+
+/* ---- alias tables ------------------------------------------------------- */
+
+WRS_API size_t     wrs_alias_build_scratch_bytes(int64_t n, const wrs_build_opts* opts);
+/* Builds an n-row table in d_table from n FP32 weights d_w (1 <= n <= 2^31-1).
+ * d_W (optional, device) receives the weight total used. opts may be NULL. */
+WRS_API wrs_status wrs_alias_build_f32(const float* d_w, int64_t n, const wrs_build_opts* opts,
+                               wrs_alias_row* d_table, double* d_W,
+                               void* d_scratch, size_t scratch_bytes, void* stream);
+
+/* Sampling-input contract (bit-exact, see the oracle):
+ *   output position s uses Philox4x32-10 with key (lo32(seed), hi32(seed)) and counter
+ *   (lo32(b), hi32(b), 0, 0), b = counter_base + floor(s / 2); even s reads words (x0, x1),
+ *   odd s reads (x2, x3). row = floor(x_first * len / 2^32) + offset (PLAIN: len = n,
+ *   offset = 0; SECTIONED: the section of s), coin = (x_second >> 8) * 2^-24,
+ *   result = coin < prob[row] ? row : alias[row].
+ * SECTIONED derives the per-section counts from a binomial tree keyed by the same
+ * (seed, counter_base). d_section_counts (optional, device, ceil(n/section_items) u64)
+ * receives them. */
+WRS_API wrs_status wrs_alias_sample(const wrs_alias_row* d_table, int64_t n, uint64_t num_samples,
+                            uint64_t seed, uint64_t counter_base, const wrs_sample_opts* opts,
+                            uint32_t* d_out, uint64_t* d_section_counts, void* stream);
+
+/* ---- rejection sampling ------------------------------------------------- */
+
+WRS_API size_t     wrs_rejection_build_scratch_bytes(int64_t n);
+/* Slot array A: item i owns c_i = floor(n*w_i/W) + 1 consecutive slots (|A| <= 2n);
+ * d_A[s] = item | 0x80000000 on the item's first slot. d_frac[i] = frac(n*w_i/W) as FP32,
+ * the acceptance probability of the first slot. d_A_size (device u64) receives |A|.
+ * a_capacity is the number of u32 entries d_A can hold (2n always suffices). */
+WRS_API wrs_status wrs_rejection_build_f32(const float* d_w, int64_t n, uint32_t* d_A, uint64_t a_capacity,
+                                   float* d_frac, uint64_t* d_A_size, double* d_W,
+                                   void* d_scratch, size_t scratch_bytes, uint32_t flags,
+                                   void* stream);
+/* Sample s, try t uses Philox counter (lo32(b), hi32(b), t >> 1, 0x52454a00) with
+ * b = counter_base + s and words (x0, x1) for even t, (x2, x3) for odd t:
+ * slot = floor(x_first * |A| / 2^32); a first slot is accepted iff
+ * (x_second >> 8) * 2^-24 < frac[item]; other slots always accept.
+ * After max_tries (0 = 64) failed tries the output is 0xFFFFFFFF and *d_status
+ * (optional, device u32) gets WRS_ERR_TOO_MANY_TRIES. */
+WRS_API wrs_status wrs_rejection_sample(const uint32_t* d_A, const uint64_t* d_A_size, const float* d_frac,
+                                int64_t n, uint64_t num_samples, uint64_t seed,
+                                uint64_t counter_base, uint32_t max_tries, uint32_t* d_out,
+                                uint32_t* d_status, uint32_t flags, void* stream);
+
+/* ---- batched (CSR) ------------------------------------------------------ */
+
+/* Tables t = 0..num_tables-1 own weights d_w[d_offsets[t] .. d_offsets[t+1]); their rows are
+ * written at the same positions of d_table. h_offsets is the same offset array in host
+ * memory (used to plan the launch; it is read during the call only). */
+WRS_API size_t     wrs_batched_build_scratch_bytes(const int64_t* h_offsets, int64_t num_tables,
+                                           const wrs_build_opts* opts);
+WRS_API wrs_status wrs_batched_build_f32(const float* d_w, const int64_t* d_offsets,
+                                 const int64_t* h_offsets, int64_t num_tables,
+                                 const wrs_build_opts* opts, wrs_alias_row* d_table,
+                                 double* d_W /* num_tables, optional */,
+                                 void* d_scratch, size_t scratch_bytes, void* stream);
+/* Table t draws d_sample_offsets[t+1] - d_sample_offsets[t] samples, written (as table-local
+ * row indices) at d_out[d_sample_offsets[t] ...]. Output position s of table t uses the
+ * plain contract with b = counter_base + floor(s / 2) over the global position s. */
+WRS_API wrs_status wrs_batched_sample(const wrs_alias_row* d_table, const int64_t* d_offsets,
+                              int64_t num_tables, const int64_t* d_sample_offsets,
+                              uint64_t total_samples, uint64_t seed, uint64_t counter_base,
+                              uint32_t* d_out, void* stream);
+
+/* ---- status / misc ------------------------------------------------------ */
+
+/* Reads (synchronising `stream`) the device status word of a build scratch buffer. */
+WRS_API wrs_status wrs_scratch_status(const void* d_scratch, void* stream);
+WRS_API const char* wrs_status_string(wrs_status status);
+/* Returns WRS_SUCCESS when the current device is an sm_100 part the kernels were built for. */
+WRS_API wrs_status wrs_check_device(void);
+WRS_API int        wrs_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WRS_H */

@@ -1,0 +1,74 @@
+/*
+ * wrs_oracle.h — CPU oracle of the weighted-random-sampling hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY. The library never links, loads or calls anything here; only
+ * tests/, __graft_entry__.smoke() and bench.py's CPU-baseline arm use it, and only as the
+ * checker or the timed CPU reference — never as the thing measured on the GPU.
+ *
+ * Contents (each function cites the reference file:line it restates):
+ *   - or_sweep_build / or_split_build: the reference's sequential CPU alias builds in FP64
+ *     (AliasTableSweep::build, AliasTableSplit::build + PackMethodSweep::pack);
+ *   - or_check_table / or_check_ref_table: per-item probability reconstruction against
+ *     w_i / W with W summed exactly (AliasTable::verifyTableCorrectness, tightened to a
+ *     relative per-item error);
+ *   - or_exact_build: a sequential restatement of the library's exact merge build (bit-exact
+ *     reference for the GPU tables);
+ *   - or_philox4x32_10 / or_sample_plain / or_sample_sectioned: the sampling-input contract
+ *     and the reference's doSample decision (SamplerGpuBasic.cu:28-69);
+ *   - or_rejection_build / or_rejection_sample: RejectionSampling::build + fillA and
+ *     SamplerRejection::sample;
+ *   - or_binomial / or_section_counts: the sectioned sampler's binomial tree.
+ */
+#ifndef WRS_ORACLE_H
+#define WRS_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* exact (correctly rounded) sum of FP32 weights (Shewchuk expansion, as math.fsum) */
+double or_exact_sum_f32(const float* w, int64_t n);
+
+void or_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+
+/* reference-format tables: weight (absolute, FP64) + alias (int32) */
+int or_sweep_build(const double* w, int64_t n, double* weight, int32_t* alias, double* W_out);
+int or_split_build(const double* w, int64_t n, int64_t p, double* weight, int32_t* alias, double* W_out,
+                   int threads);
+
+/* per-item check of a {f32 prob, u32 alias} table (rows interleaved: prob bits, alias).
+ * stats[0] = max relative error over items with w > 0, stats[1] = p99.99 relative error,
+ * stats[2] = index of the worst item, stats[3] = number of zero-weight items that got mass,
+ * stats[4] = number of rows with prob outside [0, 1] or alias >= n. W_used = the sum. */
+int or_check_table(const float* w, int64_t n, const uint32_t* rows, double* stats, double* W_used);
+/* same for a reference-format table, prob = weight / (W/N), alias ignored when weight >= W/N */
+int or_check_ref_table(const double* w, int64_t n, const double* weight, const int32_t* alias, double W,
+                       double* stats);
+
+/* the library's exact merge build, sequentially; W = the weight total the build uses */
+int or_exact_build(const float* w, int64_t n, double W, uint32_t* rows);
+
+/* sampling contract */
+void or_sample_plain(const uint32_t* rows, int64_t n, uint64_t m, uint64_t seed, uint64_t cbase, uint32_t* out);
+uint64_t or_binomial(uint64_t n, double p, uint32_t k0, uint32_t k1, uint64_t cbase, uint32_t node);
+void or_section_counts(int64_t n, uint32_t S, uint64_t m, uint64_t seed, uint64_t cbase, uint64_t* counts);
+void or_sample_sectioned(const uint32_t* rows, int64_t n, uint64_t m, uint32_t S, uint64_t seed, uint64_t cbase,
+                         uint32_t* out, uint64_t* counts);
+
+/* rejection: A holds item | 0x80000000 on first slots; returns |A| (or 0 on capacity error) */
+uint64_t or_rejection_build(const float* w, int64_t n, double W, uint32_t* A, uint64_t a_capacity, float* frac);
+int or_rejection_sample(const uint32_t* A, uint64_t a_size, const float* frac, uint64_t m, uint64_t seed,
+                        uint64_t cbase, uint32_t max_tries, uint32_t* out);
+
+/* reference CPU sampler restatement with the Philox contract, all cores; returns samples/s */
+double or_sample_plain_timed(const uint32_t* rows, int64_t n, uint64_t m, uint64_t seed, int threads,
+                             uint32_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

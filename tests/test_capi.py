@@ -1,0 +1,81 @@
+"""The C ABI library loads and exports every entry point include/wrs.h declares; the
+calls that need no GPU (sizes, status strings, argument checks) behave as documented."""
+import ctypes
+import os
+import re
+
+import pytest
+
+import wrs
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "wrs.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(wrs_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_declares_expected_entry_points():
+    names = declared_functions()
+    for required in ["wrs_alias_build_f32", "wrs_alias_sample", "wrs_rejection_build_f32", "wrs_rejection_sample",
+                     "wrs_batched_build_f32", "wrs_batched_sample", "wrs_sum_f32", "wrs_status_string"]:
+        assert required in names
+
+
+def test_library_exports_every_declared_symbol():
+    L = wrs.lib()
+    missing = [n for n in declared_functions() if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_library_exports_nothing_undeclared():
+    # symbols come from the C ABI only (the library builds with -fvisibility=hidden)
+    import subprocess
+    out = subprocess.run(["nm", "-D", "--defined-only", wrs.LIB_PATH], capture_output=True, text=True).stdout
+    exported = sorted(set(re.findall(r" T (wrs_[a-z0-9_]+)$", out, flags=re.M)))
+    assert exported == declared_functions()
+
+
+def test_status_strings():
+    assert wrs.status_string(wrs.WRS_SUCCESS) == "success"
+    for s in range(1, 10):
+        assert wrs.status_string(s) not in ("", "unknown status")
+    assert wrs.status_string(1234) == "unknown status"
+
+
+def test_version():
+    assert wrs.lib().wrs_version() == 1
+
+
+def test_scratch_sizes_are_host_only_and_monotone():
+    a = wrs.alias_build_scratch_bytes(1000)
+    b = wrs.alias_build_scratch_bytes(1 << 20)
+    c = wrs.alias_build_scratch_bytes(1 << 26)
+    assert 0 < a <= b <= c
+    assert wrs.alias_build_scratch_bytes(0) == 0
+    bad = wrs.build_opts(tile_items=3000)
+    assert wrs.alias_build_scratch_bytes(1000, bad) == 0
+    assert wrs.rejection_build_scratch_bytes(1 << 20) > 0
+    assert wrs.lib().wrs_sum_scratch_bytes(10) > 0
+
+
+def test_argument_checks_before_any_device_work():
+    L = wrs.lib()
+    # null weights / table / scratch, n out of range: rejected without touching the GPU
+    assert L.wrs_alias_build_f32(None, 10, None, None, None, None, 0, None) == wrs.WRS_ERR_INVALID_ARGUMENT
+    assert L.wrs_alias_build_f32(16, 0, None, 16, None, 16, 1 << 20, None) == wrs.WRS_ERR_INVALID_ARGUMENT
+    assert L.wrs_alias_build_f32(16, 1 << 40, None, 16, None, 16, 1 << 20, None) == wrs.WRS_ERR_INVALID_ARGUMENT
+    # scratch too small
+    assert L.wrs_alias_build_f32(16, 1000, None, 16, None, 16, 8, None) == wrs.WRS_ERR_SCRATCH_TOO_SMALL
+    # unknown method / tile size
+    opts = wrs.BuildOpts(7, 0, 0, 0)
+    assert L.wrs_alias_build_f32(16, 1000, ctypes.byref(opts), 16, None, 16, 1 << 30, None) == \
+        wrs.WRS_ERR_INVALID_ARGUMENT
+    assert L.wrs_alias_sample(None, 10, 10, 0, 0, None, 16, None, None) == wrs.WRS_ERR_INVALID_ARGUMENT
+    assert L.wrs_rejection_build_f32(None, 10, None, 0, None, None, None, None, 0, 0, None) == \
+        wrs.WRS_ERR_INVALID_ARGUMENT
+    assert L.wrs_rejection_sample(None, None, None, 10, 10, 0, 0, 0, None, None, 0, None) == \
+        wrs.WRS_ERR_INVALID_ARGUMENT
+    assert L.wrs_scratch_status(None, None) == wrs.WRS_ERR_INVALID_ARGUMENT
