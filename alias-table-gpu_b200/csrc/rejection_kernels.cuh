@@ -173,7 +173,8 @@ __global__ void __launch_bounds__(kBuildThreads) rejection_tile_kernel(
             if (tile == num_tiles - 1) {
                 const uint64_t asz = excl + tile_total;
                 hdr->a_size = asz;
-                if (a_size_out) *a_size_out = asz;
+                // an array that does not fit reports size 0, so that no sampler reads past it
+                if (a_size_out) *a_size_out = (asz > a_capacity) ? 0ull : asz;
                 if (asz > a_capacity) record_status(&hdr->status, kErrCapacity);
             }
         }

@@ -139,9 +139,15 @@ __global__ void __launch_bounds__(256) rejection_sample_kernel(const uint32_t* _
                                                                uint32_t k0, uint32_t k1, uint64_t cbase,
                                                                uint32_t max_tries, uint32_t* __restrict__ out,
                                                                uint32_t* status) {
-    const uint32_t asz = (uint32_t)*a_size_ptr;
+    const uint64_t asz64 = *a_size_ptr;
     const uint64_t gsize = (uint64_t)gridDim.x * blockDim.x;
     bool failed = false;
+    if (asz64 == 0 || asz64 > 0xffffffffull) {  // no (or an unusable) slot array: nothing to sample
+        for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < m; s += gsize) out[s] = 0xffffffffu;
+        if (status && blockIdx.x == 0 && threadIdx.x == 0) record_status(status, kErrCapacity);
+        return;
+    }
+    const uint32_t asz = (uint32_t)asz64;
     for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < m; s += gsize) {
         const uint64_t b = cbase + s;
         uint32_t res = 0xffffffffu;
