@@ -6,7 +6,8 @@
 //
 // Unlike the reference build (>= 5 blocking device-to-host copies and >= 3 cudaMalloc/cudaFree
 // pairs inside build()), the whole build is four stream-ordered operations on caller memory:
-// a 128-byte memset of the scratch header, then the wsum, tile_scan and split_pack kernels.
+// a 128-byte memset of the scratch header, then the wsum, tile_reduce, tile_prefix, tile_link
+// and split_pack kernels.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -80,9 +81,11 @@ int ipt_for(const wrs_build_opts* opts) {
 struct BuildLayout {
     BuildHeader* hdr;
     double2* partials;
-    uint32_t* flags;
+    BlockWord* blocks;
+    uint64_t num_blocks;
     TileVals* agg;
     TileVals* incl;
+    TileLink* links;
     size_t bytes;
 };
 
@@ -92,9 +95,11 @@ BuildLayout carve_build(void* scratch, uint64_t num_tiles, bool psa) {
     BuildLayout L;
     L.hdr = c.take<BuildHeader>(1);
     L.partials = c.take<double2>(kWsumMaxGrid);
-    L.flags = c.take<uint32_t>(num_tiles);
+    L.num_blocks = (num_tiles + kPrefixTiles - 1) / kPrefixTiles;
+    L.blocks = c.take<BlockWord>(L.num_blocks);
     L.agg = c.take<TileVals>(num_tiles);
     L.incl = c.take<TileVals>(num_tiles);
+    L.links = c.take<TileLink>(num_tiles + 1);
     L.bytes = c.off;
     return L;
 }
@@ -107,15 +112,20 @@ wrs_status launch_build(const float* d_w, uint64_t n, uint32_t method, wrs_alias
     cudaError_t e = cudaMemsetAsync(L.hdr, 0, sizeof(BuildHeader), stream);
     if (e != cudaSuccess) return WRS_ERR_CUDA;
     const uint32_t g = wsum_grid(n);
-    const uint64_t zero_words = num_tiles;
-    wsum_kernel<kWsumBlock><<<g, kWsumBlock, 0, stream>>>(d_w, n, L.hdr, L.partials, L.flags, zero_words, d_W);
-    tile_scan_kernel<IPT><<<(uint32_t)num_tiles, kBuildThreads, 0, stream>>>(d_w, n, L.hdr, L.agg, L.incl, L.flags,
-                                                                              (uint32_t)num_tiles);
+    const uint64_t zero_words = L.num_blocks * sizeof(BlockWord) / sizeof(uint32_t);
+    wsum_kernel<kWsumBlock><<<g, kWsumBlock, 0, stream>>>(d_w, n, L.hdr, L.partials,
+                                                          reinterpret_cast<uint32_t*>(L.blocks), zero_words, d_W);
+    tile_reduce_kernel<IPT><<<(uint32_t)num_tiles, kBuildThreads, 0, stream>>>(d_w, n, L.hdr, L.agg,
+                                                                                (uint32_t)num_tiles);
+    tile_prefix_kernel<<<(uint32_t)L.num_blocks, kPrefixThreads, 0, stream>>>(L.hdr, L.agg, L.incl, L.blocks,
+                                                                               (uint32_t)num_tiles);
+    tile_link_kernel<<<(uint32_t)((num_tiles + 1 + 255) / 256), 256, 0, stream>>>(L.hdr, L.agg, L.incl,
+                                                                                  (uint32_t)num_tiles, L.links);
     {
-        const size_t smem = (size_t)T * (2 * sizeof(u128) + 2 * sizeof(uint32_t));
+        const size_t smem = pack_smem_bytes(T);
         e = cudaFuncSetAttribute(split_pack_kernel<IPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return WRS_ERR_CUDA;
-        split_pack_kernel<IPT><<<(uint32_t)num_tiles, kBuildThreads, smem, stream>>>(d_w, n, L.hdr, L.agg, L.incl,
+        split_pack_kernel<IPT><<<(uint32_t)num_tiles, kBuildThreads, smem, stream>>>(d_w, n, L.hdr, L.incl, L.links,
                                                                                      (uint32_t)num_tiles, d_table);
     }
     return launch_status();

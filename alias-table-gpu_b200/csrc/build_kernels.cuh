@@ -32,11 +32,12 @@
 //     N = round(2^64 * D / E_total) (q_scale_excess), so no single heavy absorbs it.
 // Per-item relative error is then below ~2^-23 + |D| / E_total for every input.
 //
-// Passes: (1) wsum: compensated W; (2) tile_scan: per-tile counts and Q64.64 sums of the
-// three streams (small-light deficits S, large-light true deficits L, heavy excess E),
-// decoupled look-back -> inclusive tile prefixes; (3) split_pack: per light tile, locate
-// the heavy tiles whose excess range covers the tile's deficit range (the split), merge
-// (the pack), and write rows. Tile t owns (writes the row of) every heavy whose corrected
+// Passes: (1) wsum: compensated W; (2) tile_reduce: per-tile counts and sums of the three
+// streams (small-light deficits S, large-light true deficits L, heavy excess E);
+// (3) tile_prefix: inclusive Q64.64 tile prefixes (block scans chained by a short
+// decoupled look-back); (4) tile_link: per light tile, the heavy tiles whose excess range
+// covers the tile's deficit range (the split); (5) split_pack: pair the tile's lights with
+// those heavies (the pack) and write rows. Tile t owns (writes the row of) every heavy whose corrected
 // excess end lies in (A_before(t), A_after(t)]; tile 0's interval is open to the left and
 // the last tile's to the right, so every heavy is written exactly once.
 #pragma once
@@ -103,57 +104,93 @@ static_assert(sizeof(BuildHeader) == 128, "header layout");
 
 // ---------------------------------------------------------------- classification
 // The per-item quantities; the same code runs in every pass that needs them, and the
-// CPU oracle restates it operation by operation.
+// CPU oracle restates it operation by operation. Within a tile, deficits are summed as
+// u64 in Q16.48 and excess in Q40.24 (rounded per item); tile aggregates and prefixes are
+// Q64.64. A light's merge key is exact on the 2^-48 grid, so comparisons against the
+// (full-resolution) corrected excess line stay exact; the per-item rounding only moves
+// a heavy's reconstructed probability by at most (number of donees) x 2^-49 rows.
+//
+// Classes, with thresholds computed once per build from W/N (ClassParams):
+//   heavy        w > H1 (H1 = largest float <= W/N, so exactly w > W/N): excess h - 1,
+//                h = w * (N/W) in FP64;
+//   large light  Hh <= w <= H1 (Hh = smallest float >= W/(2N)): true deficit 1 - w*(N/W)
+//                in FP64, stored probability dithered (large_light_prob);
+//   small light  w < Hh: stored probability p = w * fl32(N/W) in FP32 (within 2 ulp of
+//                w/(W/N)), deficit 1 - p.
 enum : int { kAbsent = 0, kSmallLight = 1, kLargeLight = 2, kHeavy = 3 };
 
-struct ItemClass {
-    int kind;
-    float p;  // small light: stored probability
-    u128 q;   // small light: stored deficit; large light: true deficit; heavy: excess
+struct ClassParams {
+    double R;   // N / W
+    float R32;  // fl32(R)
+    float H1;   // largest float <= W/N
+    float Hh;   // smallest float >= W/(2N)
 };
 
-__device__ __forceinline__ ItemClass classify(float wf, double W_N, double R) {
-    ItemClass c;
-    const double w = (double)wf;
-    if (w > W_N) {
-        c.kind = kHeavy;
-        double h = w * R;
-        if (h < 1.0) h = 1.0;
-        c.q = q_from_double(h) - q_one();
-        c.p = 1.0f;
+__device__ __forceinline__ ClassParams class_params(const double W_N, const double R) {
+    ClassParams c;
+    c.R = R;
+    c.R32 = __double2float_rn(R);
+    c.H1 = __double2float_rd(W_N);
+    c.Hh = __double2float_ru(__dmul_rn(0.5, W_N));
+    return c;
+}
+
+// round(p * 2^48) (ties away from zero) for a float p in [0, 1], from its bits (branch-free:
+// t = mantissa * 2^25, sh = 127 - exponent >= 1, result ((t >> (sh - 1)) + 1) >> 1).
+__host__ __device__ __forceinline__ uint64_t fix48f(uint32_t b) {
+    const int e = (int)((b >> 23) & 0xff);
+    const uint64_t t = (uint64_t)((b & 0x7fffffu) | 0x800000u) << 25;
+    const int sh = 127 - e;
+    const uint64_t r = ((t >> ((sh - 1) & 63)) + 1) >> 1;
+    return (e == 0 || sh > 63) ? 0ull : r;
+}
+
+struct ItemQ {
+    int kind;
+    float p;     // small light: stored probability
+    uint64_t q;  // light: deficit in Q16.48 (stored for small, true for large); heavy: excess in Q40.24
+};
+
+// Caller guarantees wf >= 0 (a present item).
+__device__ __forceinline__ ItemQ classify(float wf, const ClassParams& cp) {
+    ItemQ c;
+    if (wf < cp.Hh) {
+        c.kind = kSmallLight;
+        c.p = __fmul_rn(wf, cp.R32);
+        c.q = (1ull << 48) - fix48f(__float_as_uint(c.p));
     } else {
-        double p = w * R;
-        if (p > 1.0) p = 1.0;
-        if (p >= 0.5) {
-            c.kind = kLargeLight;
-            c.q = q_from_double(1.0 - p);  // exact: 1 - p is a multiple of 2^-53 in [0, 1/2]
-            c.p = 1.0f;
-        } else {
-            c.kind = kSmallLight;
-            const float ps = __double2float_rn(p);
-            c.p = ps;
-            c.q = q_one() - q_from_double((double)ps);
-        }
+        const double hd = __dmul_rn((double)wf, cp.R);
+        const bool heavy = wf > cp.H1;
+        const double v = heavy ? __dsub_rn(fmax(hd, 1.0), 1.0) : __dsub_rn(1.0, fmin(hd, 1.0));
+        c.q = fixq(v, heavy ? 24 : 48);
+        c.kind = heavy ? kHeavy : kLargeLight;
+        c.p = 1.0f;
     }
     return c;
 }
 
-// Stored probability of a dithered large light from its prefix L_i and true deficit d.
-__device__ __forceinline__ float large_light_prob(u128 L_i, u128 d) {
-    const u128 dd = q_round24(L_i + d) - q_round24(L_i);  // multiple of 2^-24, <= 2^23 + 1 units
-    const uint32_t units = (uint32_t)(dd >> 40);
-    return (float)(16777216u - units) * 5.9604644775390625e-8f;  // exact
+// Heavy excess only (the caller has checked wf > H1).
+__device__ __forceinline__ uint64_t heavy_excess(float wf, const ClassParams& cp) {
+    return fixq(__dsub_rn(fmax(__dmul_rn((double)wf, cp.R), 1.0), 1.0), 24);
 }
-__device__ __forceinline__ u128 large_light_deficit(u128 L_i, u128 d) {
-    return q_round24(L_i + d) - q_round24(L_i);
+
+// Stored probability of a dithered large light: deficit round24(L_i + d) - round24(L_i),
+// a multiple of 2^-24, so 1 - deficit is exact in FP32.
+__device__ __forceinline__ float large_light_prob(u128 L_i, uint64_t d48) {
+    const u128 dd = q_round24(L_i + ((u128)d48 << 16)) - q_round24(L_i);
+    const uint32_t units = (uint32_t)(dd >> 40);
+    return (float)(16777216u - units) * 5.9604644775390625e-8f;
 }
 
 // A heavy's row probability from r in Q64.64 (clamped to [0, 1]).
 __device__ __forceinline__ float heavy_row_prob(u128 r) {
     if (q_is_negative(r)) return 0.0f;
     if (r >= q_one()) return 1.0f;
-    return __double2float_rn((double)(q_lo(r) >> 11) * 1.1102230246251565404e-16);
+    return __double2float_rn(__dmul_rn((double)(q_lo(r) >> 11), 1.1102230246251565404e-16));
 }
+
+// Start of the deficit line of everything before a tile prefix.
+__device__ __forceinline__ u128 deficit_line(const TileVals& v) { return v.S + q_round24(v.L); }
 
 // ---------------------------------------------------------------- double-double sums
 __device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
@@ -306,8 +343,8 @@ __global__ void __launch_bounds__(BLOCK) wsum_kernel(const float* __restrict__ w
 // ---------------------------------------------------------------- CTA scan helpers
 struct ScanVal {
     uint32_t c;
-    u128 a;
-    u128 b;
+    uint64_t a;
+    uint64_t b;
 };
 __device__ __forceinline__ ScanVal sv_add(const ScanVal& x, const ScanVal& y) {
     ScanVal r;
@@ -334,32 +371,21 @@ __device__ __forceinline__ ScanVal cta_exclusive_scan(ScanVal v, ScanVal* s_warp
     for (int off = 1; off < 32; off <<= 1) {
         ScanVal o;
         o.c = __shfl_up_sync(0xffffffffu, inc.c, off);
-        o.a = shfl_up_u128(inc.a, off);
-        o.b = shfl_up_u128(inc.b, off);
+        o.a = __shfl_up_sync(0xffffffffu, inc.a, off);
+        o.b = __shfl_up_sync(0xffffffffu, inc.b, off);
         if (lane >= off) inc = sv_add(inc, o);
     }
     if (lane == 31) s_warp[warp] = inc;
     __syncthreads();
-    if (warp == 0) {
-        const ScanVal x = (lane < BLOCK / 32) ? s_warp[lane] : sv_zero();
-        ScanVal xi = x;
+    if (threadIdx.x == 0) {
+        ScanVal acc = sv_zero();
 #pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-            ScanVal o;
-            o.c = __shfl_up_sync(0xffffffffu, xi.c, off);
-            o.a = shfl_up_u128(xi.a, off);
-            o.b = shfl_up_u128(xi.b, off);
-            if (lane >= off) xi = sv_add(xi, o);
+        for (int i = 0; i < BLOCK / 32; ++i) {
+            const ScanVal t = s_warp[i];
+            s_warp[i] = acc;
+            acc = sv_add(acc, t);
         }
-        __syncwarp();
-        if (lane < BLOCK / 32) {
-            ScanVal ex;
-            ex.c = xi.c - x.c;
-            ex.a = xi.a - x.a;
-            ex.b = xi.b - x.b;
-            s_warp[lane] = ex;
-        }
-        if (lane == BLOCK / 32 - 1) s_warp[BLOCK / 32] = xi;
+        s_warp[BLOCK / 32] = acc;
     }
     __syncthreads();
     const ScanVal base = s_warp[warp];
@@ -409,231 +435,414 @@ __device__ __forceinline__ TileVals ldcg_tilevals(const TileVals* src) {
     return v;
 }
 
-// ---------------------------------------------------------------- pass 2: tile scan
-// One tile per CTA, tiles taken in ticket order (a CTA only ever waits for tiles whose
-// CTAs are already running). Publishes the tile aggregate (flag 1), looks back warp-wide,
-// publishes the inclusive prefix (flag 2). agg[] keeps first/last heavy of each tile.
+__device__ __forceinline__ u128 ldcg_E(const TileVals* src) {
+    const uint4 w3 = __ldcg(reinterpret_cast<const uint4*>(src) + 3);
+    return q_make(((uint64_t)w3.w << 32) | w3.z, ((uint64_t)w3.y << 32) | w3.x);
+}
+
+// ---------------------------------------------------------------- pass 2: tile reduce
+// One tile per CTA: counts and sums of the three streams, plus the tile's first and last
+// heavy item. No inter-CTA waits.
 template <int IPT>
-__global__ void __launch_bounds__(kBuildThreads) tile_scan_kernel(const float* __restrict__ w, uint64_t n,
-                                                                  BuildHeader* hdr, TileVals* agg,
-                                                                  TileVals* incl, uint32_t* flags,
-                                                                  uint32_t num_tiles) {
+__global__ void __launch_bounds__(kBuildThreads) tile_reduce_kernel(const float* __restrict__ w, uint64_t n,
+                                                                    const BuildHeader* hdr, TileVals* agg,
+                                                                    uint32_t num_tiles) {
     constexpr int T = kBuildThreads * IPT;
-    __shared__ uint32_t s_tile;
-    __shared__ ScanVal s_warp[kBuildThreads / 32 + 1];
-    __shared__ uint32_t s_fh[kBuildThreads / 32];
-    __shared__ uint32_t s_lh[kBuildThreads / 32];
-    __shared__ TileVals s_agg;
-    __shared__ int s_abort;
-
-    if (threadIdx.x == 0) {
-        s_tile = atomicAdd(&hdr->tile_ticket, 1u);
-        s_abort = (load_relaxed(&hdr->status) != 0);
-    }
-    __syncthreads();
-    const uint32_t tile = s_tile;
-    if (tile >= num_tiles) return;
-    if (s_abort) {
-        // publish a placeholder so that successors do not wait for the time limit
-        if (threadIdx.x == 0) {
-            incl[tile] = tv_zero();
-            __threadfence();
-            store_release(&flags[tile], 2u);
-        }
-        return;
-    }
-    const double W_N = hdr->W_N;
-    const double R = hdr->R;
-
+    constexpr int NW = kBuildThreads / 32;
+    __shared__ uint32_t s_nl[NW], s_nh[NW], s_fh[NW], s_lh[NW];
+    __shared__ uint64_t s_s[NW], s_l[NW], s_e[NW];
+    if (load_relaxed(&hdr->status) != 0) return;
+    const uint32_t tile = blockIdx.x;
+    const ClassParams cp = class_params(hdr->W_N, hdr->R);
     float x[IPT];
     load_tile_items<IPT>(w, n, tile, threadIdx.x, x);
-    uint32_t nL = 0, nH = 0, fh = 0xffffffffu, lh = 0;
-    bool anyh = false;
-    u128 S = 0, L = 0, E = 0;
+    uint32_t nL = 0, nH = 0, fh = 0xffffffffu, lh = 0xffffffffu;
+    uint64_t S = 0, L = 0, E = 0;
     const uint32_t item0 = (uint32_t)((uint64_t)tile * T + (uint64_t)threadIdx.x * IPT);
 #pragma unroll
     for (int k = 0; k < IPT; ++k) {
         if (x[k] < 0.0f) continue;
-        const ItemClass c = classify(x[k], W_N, R);
+        const ItemQ c = classify(x[k], cp);
         if (c.kind == kHeavy) {
             ++nH;
             E += c.q;
-            fh = min(fh, item0 + k);
+            if (fh == 0xffffffffu) fh = item0 + k;
             lh = item0 + k;
-            anyh = true;
         } else {
             ++nL;
             if (c.kind == kSmallLight) S += c.q; else L += c.q;
         }
     }
-    ScanVal v;
-    v.c = nL;
-    v.a = S;
-    v.b = L;
-    ScanVal tot;
-    (void)cta_exclusive_scan<kBuildThreads>(v, s_warp, &tot);
-    ScanVal vh;
-    vh.c = nH;
-    vh.a = E;
-    vh.b = 0;
-    ScanVal toth;
-    (void)cta_exclusive_scan<kBuildThreads>(vh, s_warp, &toth);
-    uint32_t f = fh;
-    uint32_t l = anyh ? lh : 0u;
-    uint32_t has = anyh ? 1u : 0u;
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
-        f = min(f, __shfl_xor_sync(0xffffffffu, f, off));
-        l = max(l, __shfl_xor_sync(0xffffffffu, l, off));
-        has |= __shfl_xor_sync(0xffffffffu, has, off);
+        nL += __shfl_xor_sync(0xffffffffu, nL, off);
+        nH += __shfl_xor_sync(0xffffffffu, nH, off);
+        S += __shfl_xor_sync(0xffffffffu, S, off);
+        L += __shfl_xor_sync(0xffffffffu, L, off);
+        E += __shfl_xor_sync(0xffffffffu, E, off);
+        fh = min(fh, __shfl_xor_sync(0xffffffffu, fh, off));
+        const uint32_t o = __shfl_xor_sync(0xffffffffu, lh, off);
+        lh = (lh == 0xffffffffu) ? o : (o == 0xffffffffu ? lh : max(lh, o));
     }
+    const int warp = threadIdx.x >> 5;
     if ((threadIdx.x & 31) == 0) {
-        s_fh[threadIdx.x >> 5] = f;
-        s_lh[threadIdx.x >> 5] = has ? l : 0xffffffffu;
+        s_nl[warp] = nL;
+        s_nh[warp] = nH;
+        s_s[warp] = S;
+        s_l[warp] = L;
+        s_e[warp] = E;
+        s_fh[warp] = fh;
+        s_lh[warp] = lh;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        TileVals a = tv_zero();
-        uint32_t mf = 0xffffffffu, ml = 0xffffffffu;
-        for (int i = 0; i < kBuildThreads / 32; ++i) {
-            mf = min(mf, s_fh[i]);
-            if (s_lh[i] != 0xffffffffu) ml = (ml == 0xffffffffu) ? s_lh[i] : max(ml, s_lh[i]);
-        }
-        a.nL = tot.c;
-        a.S = tot.a;
-        a.L = tot.b;
-        a.nH = toth.c;
-        a.E = toth.a;
-        a.first_heavy = mf;
-        a.last_heavy = ml;
-        s_agg = a;
+    if (threadIdx.x != 0) return;
+    uint32_t tl = 0, th = 0, mf = 0xffffffffu, ml = 0xffffffffu;
+    uint64_t ts = 0, tlv = 0, te = 0;
+#pragma unroll
+    for (int i = 0; i < NW; ++i) {
+        tl += s_nl[i];
+        th += s_nh[i];
+        ts += s_s[i];
+        tlv += s_l[i];
+        te += s_e[i];
+        mf = min(mf, s_fh[i]);
+        if (s_lh[i] != 0xffffffffu) ml = (ml == 0xffffffffu) ? s_lh[i] : max(ml, s_lh[i]);
     }
-    __syncthreads();
+    TileVals a;
+    a.nL = tl;
+    a.nH = th;
+    a.first_heavy = mf;
+    a.last_heavy = ml;
+    a.S = (u128)ts << 16;
+    a.L = (u128)tlv << 16;
+    a.E = (u128)te << 40;
+    agg[tile] = a;
+}
 
-    if (threadIdx.x >= 32) return;
-    const int lane = threadIdx.x;
-    const TileVals a = s_agg;
-    if (tile == 0) {
-        if (lane == 0) {
-            agg[0] = a;
-            incl[0] = tv_add(tv_zero(), a);
-            __threadfence();
-            store_release(&flags[0], 2u);
-        }
+// ---------------------------------------------------------------- pass 3: tile prefix
+// Inclusive prefixes of the tile aggregates: each CTA scans kPrefixTiles consecutive tiles,
+// and CTAs chain their totals with a decoupled look-back (at most num_tiles / kPrefixTiles
+// CTAs, taken in ticket order; every wait is bounded).
+constexpr int kPrefixThreads = 256;
+constexpr int kPrefixPerThread = 4;
+constexpr int kPrefixTiles = kPrefixThreads * kPrefixPerThread;
+
+struct PVals {
+    uint32_t nL, nH;
+    u128 S, L, E;
+};
+__device__ __forceinline__ PVals pv_zero() {
+    PVals v;
+    v.nL = 0;
+    v.nH = 0;
+    v.S = 0;
+    v.L = 0;
+    v.E = 0;
+    return v;
+}
+__device__ __forceinline__ PVals pv_add(const PVals& a, const PVals& b) {
+    PVals r;
+    r.nL = a.nL + b.nL;
+    r.nH = a.nH + b.nH;
+    r.S = a.S + b.S;
+    r.L = a.L + b.L;
+    r.E = a.E + b.E;
+    return r;
+}
+__device__ __forceinline__ PVals pv_of(const TileVals& t) {
+    PVals v;
+    v.nL = t.nL;
+    v.nH = t.nH;
+    v.S = t.S;
+    v.L = t.L;
+    v.E = t.E;
+    return v;
+}
+__device__ __forceinline__ PVals pv_shfl_up(const PVals& v, int d) {
+    PVals o;
+    o.nL = __shfl_up_sync(0xffffffffu, v.nL, d);
+    o.nH = __shfl_up_sync(0xffffffffu, v.nH, d);
+    o.S = shfl_up_u128(v.S, d);
+    o.L = shfl_up_u128(v.L, d);
+    o.E = shfl_up_u128(v.E, d);
+    return o;
+}
+__device__ __forceinline__ PVals pv_shfl_xor(const PVals& v, int d) {
+    PVals o;
+    o.nL = __shfl_xor_sync(0xffffffffu, v.nL, d);
+    o.nH = __shfl_xor_sync(0xffffffffu, v.nH, d);
+    o.S = shfl_xor_u128(v.S, d);
+    o.L = shfl_xor_u128(v.L, d);
+    o.E = shfl_xor_u128(v.E, d);
+    return o;
+}
+
+struct __align__(16) BlockWord {  // look-back record of one prefix CTA
+    uint32_t flag;  // 0 = not ready, 1 = aggregate, 2 = inclusive
+    uint32_t pad[3];
+    PVals agg;
+    PVals incl;
+};
+
+static __global__ void __launch_bounds__(kPrefixThreads) tile_prefix_kernel(BuildHeader* hdr, const TileVals* agg,
+                                                                     TileVals* incl, BlockWord* blocks,
+                                                                     uint32_t num_tiles) {
+    __shared__ uint32_t s_blk;
+    __shared__ PVals s_warp[kPrefixThreads / 32 + 1];
+    __shared__ PVals s_base;
+    __shared__ int s_abort;
+    if (threadIdx.x == 0) {
+        s_blk = atomicAdd(&hdr->aux_ticket, 1u);
+        s_abort = load_relaxed(&hdr->status) != 0;
+    }
+    __syncthreads();
+    const uint32_t blk = s_blk;
+    if (s_abort) {
+        if (threadIdx.x == 0) store_release(&blocks[blk].flag, 2u);
         return;
     }
-    if (lane == 0) {
-        agg[tile] = a;
-        __threadfence();
-        store_release(&flags[tile], 1u);
+    const uint32_t t0 = blk * kPrefixTiles + threadIdx.x * kPrefixPerThread;
+    PVals loc[kPrefixPerThread];
+    PVals run = pv_zero();
+#pragma unroll
+    for (int k = 0; k < kPrefixPerThread; ++k) {
+        const PVals v = (t0 + k < num_tiles) ? pv_of(agg[t0 + k]) : pv_zero();
+        run = pv_add(run, v);
+        loc[k] = run;  // thread-local inclusive
     }
-    TileVals excl = tv_zero();
-    int64_t pred = (int64_t)tile - 1;
-    bool timed_out = false;
-    const uint64_t t_start = global_ns();
-    while (true) {
-        const int64_t p = pred - lane;
-        uint32_t fl = 2u;
-        TileVals pv = tv_zero();
-        if (p >= 0) {
-            uint32_t spins = 0;
-            while ((fl = load_acquire(&flags[p])) == 0u) {
-                __nanosleep(32);
-                if ((++spins & 255u) == 0u) {
-                    if (global_ns() - t_start > kWaitLimitNs || load_relaxed(&hdr->status) != 0) {
-                        timed_out = true;
-                        break;
+    // CTA exclusive scan of the thread totals
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    PVals inc = run;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const PVals o = pv_shfl_up(inc, d);
+        if (lane >= d) inc = pv_add(inc, o);
+    }
+    if (lane == 31) s_warp[warp] = inc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        PVals acc = pv_zero();
+        for (int i = 0; i < kPrefixThreads / 32; ++i) {
+            const PVals t = s_warp[i];
+            s_warp[i] = acc;
+            acc = pv_add(acc, t);
+        }
+        s_warp[kPrefixThreads / 32] = acc;
+    }
+    __syncthreads();
+    PVals texcl = pv_add(s_warp[warp], inc);
+    texcl.nL -= run.nL;
+    texcl.nH -= run.nH;
+    texcl.S -= run.S;
+    texcl.L -= run.L;
+    texcl.E -= run.E;
+    const PVals btot = s_warp[kPrefixThreads / 32];
+    // look-back over the preceding prefix CTAs (warp 0)
+    if (warp == 0) {
+        PVals excl = pv_zero();
+        if (blk == 0) {
+            if (lane == 0) {
+                blocks[0].agg = btot;
+                blocks[0].incl = btot;
+                store_release(&blocks[0].flag, 2u);
+            }
+        } else {
+            if (lane == 0) {
+                blocks[blk].agg = btot;
+                store_release(&blocks[blk].flag, 1u);
+            }
+            int64_t pred = (int64_t)blk - 1;
+            bool timed_out = false;
+            const uint64_t t_start = global_ns();
+            while (true) {
+                const int64_t p = pred - lane;
+                uint32_t fl = 2u;
+                PVals pv = pv_zero();
+                if (p >= 0) {
+                    uint32_t spins = 0;
+                    while ((fl = load_acquire(&blocks[p].flag)) == 0u) {
+                        __nanosleep(20);
+                        if ((++spins & 255u) == 0u) {
+                            if (global_ns() - t_start > kWaitLimitNs || load_relaxed(&hdr->status) != 0) {
+                                timed_out = true;
+                                break;
+                            }
+                        }
+                    }
+                    if (!timed_out) {
+                        const PVals* src = (fl == 2u) ? &blocks[p].incl : &blocks[p].agg;
+                        pv.nL = __ldcg(&src->nL);
+                        pv.nH = __ldcg(&src->nH);
+                        const uint4* q4 = reinterpret_cast<const uint4*>(&src->S);
+                        for (int i = 0; i < 3; ++i) {
+                            const uint4 v = __ldcg(q4 + i);
+                            const u128 x = q_make(((uint64_t)v.w << 32) | v.z, ((uint64_t)v.y << 32) | v.x);
+                            if (i == 0) pv.S = x; else if (i == 1) pv.L = x; else pv.E = x;
+                        }
                     }
                 }
-            }
-            if (!timed_out) pv = ldcg_tilevals((fl == 2u) ? (incl + p) : (agg + p));
-        }
-        if (__any_sync(0xffffffffu, timed_out)) {
-            if (lane == 0) record_status(&hdr->status, kErrTimeout);
-            break;
-        }
-        const uint32_t incl_mask = __ballot_sync(0xffffffffu, fl == 2u);
-        const int stop = incl_mask ? (__ffs(incl_mask) - 1) : 31;
-        if (lane > stop) pv = tv_zero();
+                if (__any_sync(0xffffffffu, timed_out)) {
+                    if (lane == 0) record_status(&hdr->status, kErrTimeout);
+                    break;
+                }
+                const uint32_t incl_mask = __ballot_sync(0xffffffffu, fl == 2u);
+                const int stop = incl_mask ? (__ffs(incl_mask) - 1) : 31;
+                if (lane > stop) pv = pv_zero();
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            TileVals o;
-            o.nL = __shfl_xor_sync(0xffffffffu, pv.nL, off);
-            o.nH = __shfl_xor_sync(0xffffffffu, pv.nH, off);
-            o.S = shfl_xor_u128(pv.S, off);
-            o.L = shfl_xor_u128(pv.L, off);
-            o.E = shfl_xor_u128(pv.E, off);
-            pv = tv_add(pv, o);
+                for (int d = 16; d > 0; d >>= 1) pv = pv_add(pv, pv_shfl_xor(pv, d));
+                excl = pv_add(excl, pv);
+                if (incl_mask) break;
+                pred -= 32;
+            }
+            if (lane == 0) {
+                blocks[blk].incl = pv_add(excl, btot);
+                store_release(&blocks[blk].flag, 2u);
+            }
         }
-        excl = tv_add(excl, pv);
-        if (incl_mask) break;
-        pred -= 32;
+        if (lane == 0) s_base = excl;
     }
-    if (lane == 0) {
-        incl[tile] = tv_add(excl, a);
-        __threadfence();
-        store_release(&flags[tile], 2u);
+    __syncthreads();
+    const PVals base = pv_add(s_base, texcl);
+#pragma unroll
+    for (int k = 0; k < kPrefixPerThread; ++k) {
+        if (t0 + k >= num_tiles) break;
+        const PVals v = pv_add(base, loc[k]);
+        TileVals o;
+        o.nL = v.nL;
+        o.nH = v.nH;
+        o.first_heavy = 0xffffffffu;
+        o.last_heavy = 0xffffffffu;
+        o.S = v.S;
+        o.L = v.L;
+        o.E = v.E;
+        incl[t0 + k] = o;
     }
 }
 
-// ---------------------------------------------------------------- pass 3: split + pack
-// Tile-level prefix access used by the pack kernel.
+// ---------------------------------------------------------------- pass 4: split
+// Per light tile t, the range [u0, u1] of tiles whose heavies' corrected excess ends meet
+// the tile's deficit range (A_before(t), A_after(t)] (the reference's split search, at tile
+// granularity), and the item of the first heavy after tile t. links[num_tiles].next_item
+// is the last heavy item of the whole table.
+struct TileLink {
+    uint32_t u0;
+    uint32_t u1;
+    uint32_t next_item;
+    uint32_t pad;
+};
+
+__device__ __forceinline__ u128 excess_before(const TileVals* incl, uint32_t u) {
+    return u ? ldcg_E(incl + u - 1) : (u128)0;
+}
+
+static __global__ void __launch_bounds__(256) tile_link_kernel(const BuildHeader* hdr, const TileVals* agg,
+                                                               const TileVals* incl, uint32_t num_tiles,
+                                                               TileLink* links) {
+    if (load_relaxed(&hdr->status) != 0) return;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t > num_tiles) return;
+    const TileVals tot = ldcg_tilevals(incl + num_tiles - 1);
+    if (t == num_tiles) {
+        // last heavy of the table: in the last tile whose predecessors hold fewer than nH heavies
+        uint32_t item = 0xffffffffu;
+        if (tot.nH > 0) {
+            uint32_t lo = 0, hi = num_tiles - 1;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi + 1) >> 1;
+                if (ldcg_tilevals(incl + mid - 1).nH < tot.nH) lo = mid; else hi = mid - 1;
+            }
+            item = ldcg_tilevals(agg + lo).last_heavy;
+        }
+        TileLink l;
+        l.u0 = 0;
+        l.u1 = 0;
+        l.next_item = item;
+        l.pad = 0;
+        links[num_tiles] = l;
+        return;
+    }
+    const int64_t nfix = excess_correction(deficit_line(tot), tot.E);
+    const u128 A_b = t ? deficit_line(ldcg_tilevals(incl + t - 1)) : (u128)0;
+    const TileVals me = ldcg_tilevals(incl + t);
+    const u128 A_a = deficit_line(me);
+    TileLink l;
+    l.pad = 0;
+    // largest u with corrected E_before(u) <= x (E_before(0) = 0 <= x)
+    auto last_le = [&](u128 xv) {
+        uint32_t lo = 0, hi = num_tiles - 1;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (q_scale_excess(excess_before(incl, mid), nfix) <= xv) lo = mid; else hi = mid - 1;
+        }
+        return lo;
+    };
+    l.u0 = (t == 0) ? 0u : last_le(A_b);
+    l.u1 = (t == num_tiles - 1) ? num_tiles - 1 : last_le(A_a);
+    // first heavy after tile t: tile v = first tile whose inclusive count exceeds g
+    const uint32_t g = me.nH;
+    l.next_item = 0xffffffffu;
+    if (g < tot.nH) {
+        uint32_t lo = t, hi = num_tiles - 1;  // last v with incl[v].nH <= g
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (ldcg_tilevals(incl + mid).nH <= g) lo = mid; else hi = mid - 1;
+        }
+        l.next_item = ldcg_tilevals(agg + lo + 1).first_heavy;
+    }
+    links[t] = l;
+}
+
+// ---------------------------------------------------------------- pass 5: pack
 __device__ __forceinline__ TileVals incl_before(const TileVals* incl, uint32_t u) {
     return u ? ldcg_tilevals(incl + u - 1) : tv_zero();
 }
 
-// Warp-cooperative search: largest u in [lo, hi] with pred(u) true, given pred(lo) true and
-// pred monotone (true on a prefix). All 32 lanes must call it; every lane gets the answer.
-template <typename Pred>
-__device__ __forceinline__ uint32_t warp_last_true(uint32_t lo, uint32_t hi, Pred pred) {
-    const int lane = threadIdx.x & 31;
-    while (hi > lo) {
-        const uint64_t span = (uint64_t)(hi - lo);
-        const uint32_t pos = lo + (uint32_t)((span * (uint64_t)(lane + 1) + 31) / 32);
-        const bool t = (pos <= hi) && pred(pos);
-        const uint32_t mask = __ballot_sync(0xffffffffu, t);
-        const int c = __popc(mask);
-        const uint32_t pos0 = __shfl_sync(0xffffffffu, pos, 0);
-        if (c == 0) {
-            hi = pos0 - 1;
-        } else {
-            const uint32_t posc1 = __shfl_sync(0xffffffffu, pos, c - 1);
-            const uint32_t posc = __shfl_sync(0xffffffffu, pos, c < 32 ? c : 31);
-            lo = posc1;
-            if (c < 32) hi = posc - 1;
-        }
-    }
-    return lo;
+// Shared memory of the pack kernel for T items per tile: light keys (u64), heavy keys (u64),
+// heavy local excess (u64), heavy items (u32), light aliases (u32).
+__host__ __device__ constexpr size_t pack_smem_bytes(int T) {
+    return (size_t)T * (3 * sizeof(uint64_t) + 2 * sizeof(uint32_t));
 }
 
+// One light tile per CTA. Its lights' deficit-interval starts go to shared memory as keys
+// in the tile's frame (A - A_before(t), Q16.48). The heavies of the partner tiles
+// [u0, u1] arrive one tile at a time (the next one prefetched into registers), as keys in
+// the same frame: key = ceil((E~ - A_before(t)) / 2^-48), clamped, so that key(light) <
+// key(heavy) exactly when A < E~. Each thread then resolves its own (consecutive, sorted)
+// lights' aliases J(i) = #{E~ <= A_i} by a galloping search through the heavy keys that
+// resumes where its previous light stopped, and a contiguous block of the heavies owned by
+// the tile finds the light after each heavy, I(j) = #{A < E~_j}, the same way.
 template <int IPT>
-__global__ void __launch_bounds__(kBuildThreads, 2) split_pack_kernel(const float* __restrict__ w, uint64_t n,
-                                                                     const BuildHeader* hdr,
-                                                                     const TileVals* agg,
-                                                                     const TileVals* incl,
-                                                                     uint32_t num_tiles,
-                                                                     wrs_alias_row* __restrict__ table) {
+__global__ void __launch_bounds__(kBuildThreads, (IPT <= 8 ? 3 : 1)) split_pack_kernel(const float* __restrict__ w,
+                                                                                     uint64_t n,
+                                                                                     const BuildHeader* hdr,
+                                                                                     const TileVals* incl,
+                                                                                     const TileLink* links,
+                                                                                     uint32_t num_tiles,
+                                                                                     wrs_alias_row* __restrict__ table) {
     constexpr int T = kBuildThreads * IPT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    u128* sA = reinterpret_cast<u128*>(smem_raw);          // light deficit-interval starts
-    u128* sE = sA + T;                                     // chunk heavy excess ends (corrected)
-    uint32_t* sLalias = reinterpret_cast<uint32_t*>(sE + T);  // alias of each own light
-    uint32_t* sHitem = sLalias + T;                        // chunk heavy items
+    uint64_t* sLkey = reinterpret_cast<uint64_t*>(smem_raw);
+    uint64_t* sHkey = sLkey + T;
+    uint64_t* sHe = sHkey + T;
+    uint32_t* sHitem = reinterpret_cast<uint32_t*>(sHe + T);
+    uint32_t* sLalias = sHitem + T;
     __shared__ ScanVal s_warp[kBuildThreads / 32 + 1];
-    __shared__ uint32_t s_u0, s_u1, s_next, s_r0, s_last_item, s_nlt;
+    __shared__ uint32_t s_own_lo, s_own_hi;
 
     if (load_relaxed(&hdr->status) != 0) return;
-    const uint32_t tile = num_tiles - 1 - blockIdx.x;  // descending: the last tiles of the
-                                                       // previous pass are still in L2
-    const double W_N = hdr->W_N;
-    const double R = hdr->R;
+    const uint32_t tile = num_tiles - 1 - blockIdx.x;  // descending: the previous passes ended at
+                                                       // the last tiles, still in L2
+    const ClassParams cp = class_params(hdr->W_N, hdr->R);
+    const TileLink link = links[tile];
+    // prefetch the first partner tile while the own tile is processed
+    float y[IPT];
+    load_tile_items<IPT>(w, n, link.u0, threadIdx.x, y);
     const TileVals tot = ldcg_tilevals(incl + num_tiles - 1);
     const TileVals before = incl_before(incl, tile);
     const TileVals after = ldcg_tilevals(incl + tile);
-    const u128 A_before = before.S + q_round24(before.L);
-    const u128 A_after = after.S + q_round24(after.L);
-    const u128 A_tot = tot.S + q_round24(tot.L);
-    const int64_t nfix = excess_correction(A_tot, tot.E);
+    const u128 A_before = deficit_line(before);
+    const u128 A_after = deficit_line(after);
+    const int64_t nfix = excess_correction(deficit_line(tot), tot.E);
     const bool lo_inf = (tile == 0);
     const bool hi_inf = (tile == num_tiles - 1);
     const uint32_t nH_tot = tot.nH;
@@ -642,41 +851,48 @@ __global__ void __launch_bounds__(kBuildThreads, 2) split_pack_kernel(const floa
     float x[IPT];
     load_tile_items<IPT>(w, n, tile, threadIdx.x, x);
     const uint32_t item0 = (uint32_t)((uint64_t)tile * T + (uint64_t)threadIdx.x * IPT);
+    float pk[IPT];
     ScanVal v = sv_zero();
+    uint32_t lmask = 0, bigmask = 0;  // bit k: item k is a light / a large light
 #pragma unroll
     for (int k = 0; k < IPT; ++k) {
+        pk[k] = 0.0f;
         if (x[k] < 0.0f) continue;
-        const ItemClass c = classify(x[k], W_N, R);
+        const ItemQ c = classify(x[k], cp);
         if (c.kind == kHeavy) continue;
+        lmask |= 1u << k;
         v.c += 1;
-        if (c.kind == kSmallLight) v.a += c.q; else v.b += c.q;
+        if (c.kind == kSmallLight) {
+            pk[k] = c.p;
+            v.a += c.q;
+        } else {
+            bigmask |= 1u << k;
+            v.b += c.q;
+        }
     }
     ScanVal tot_l;
     const ScanVal ex = cta_exclusive_scan<kBuildThreads>(v, s_warp, &tot_l);
     const uint32_t nLt = tot_l.c;
-    float pk[IPT];
-    uint32_t lk[IPT];
+    const uint32_t l0 = ex.c;  // this thread's lights are l0 .. l0 + popc(lmask) - 1
     {
-        uint32_t li = ex.c;
-        u128 Sr = before.S + ex.a;
-        u128 Lr = before.L + ex.b;
+        uint32_t li = l0;
+        uint64_t sr = ex.a;
+        u128 Lg = before.L + ((u128)ex.b << 16);
+        const u128 rb = q_round24(before.L);
+        uint64_t dith = (uint64_t)((q_round24(Lg) - rb) >> 16);
 #pragma unroll
         for (int k = 0; k < IPT; ++k) {
-            lk[k] = 0xffffffffu;
-            pk[k] = 0.0f;
-            if (x[k] < 0.0f) continue;
-            const ItemClass c = classify(x[k], W_N, R);
-            if (c.kind == kHeavy) continue;
-            sA[li] = Sr + q_round24(Lr);
-            lk[k] = li;
-            if (c.kind == kSmallLight) {
-                pk[k] = c.p;
-                Sr += c.q;
+            if (!(lmask >> k & 1u)) continue;
+            sLalias[li] = 0xffffffffu;
+            sLkey[li++] = sr + dith;
+            if (bigmask >> k & 1u) {
+                const uint64_t q = classify(x[k], cp).q;
+                pk[k] = large_light_prob(Lg, q);
+                Lg += (u128)q << 16;
+                dith = (uint64_t)((q_round24(Lg) - rb) >> 16);
             } else {
-                pk[k] = large_light_prob(Lr, c.q);
-                Lr += c.q;
+                sr += (1ull << 48) - fix48f(__float_as_uint(pk[k]));
             }
-            ++li;
         }
     }
     __syncthreads();
@@ -685,7 +901,7 @@ __global__ void __launch_bounds__(kBuildThreads, 2) split_pack_kernel(const floa
         // no heavy item anywhere: every row keeps itself
 #pragma unroll
         for (int k = 0; k < IPT; ++k) {
-            if (lk[k] == 0xffffffffu) continue;
+            if (!(lmask >> k & 1u)) continue;
             wrs_alias_row r;
             r.prob = pk[k];
             r.alias = item0 + k;
@@ -695,141 +911,144 @@ __global__ void __launch_bounds__(kBuildThreads, 2) split_pack_kernel(const floa
     }
     if (!lo_inf && !hi_inf && nLt == 0) return;  // empty ownership interval, no lights
 
-    // ---- split: heavy tiles whose corrected excess range meets (A_before, A_after]
-    if (threadIdx.x < 32) {
-        auto key_le = [&](uint32_t u, u128 xv) {
-            const u128 eb = q_scale_excess(incl_before(incl, u).E, nfix);
-            return eb <= xv;
-        };
-        const uint32_t u0 = lo_inf ? 0u : warp_last_true(0u, num_tiles - 1, [&](uint32_t u) { return key_le(u, A_before); });
-        const uint32_t u1 = hi_inf ? num_tiles - 1 : warp_last_true(0u, num_tiles - 1, [&](uint32_t u) { return key_le(u, A_after); });
-        if (threadIdx.x == 0) {
-            s_u0 = u0;
-            s_u1 = u1;
-            s_r0 = 0;
-            s_last_item = 0xffffffffu;
-            s_nlt = nLt;
-        }
-    }
-    __syncthreads();
-    const uint32_t u0 = s_u0, u1 = s_u1;
-
-    for (uint32_t u = u0; u <= u1; ++u) {
-        const TileVals ub = incl_before(incl, u);
-        const TileVals ua = ldcg_tilevals(incl + u);
-        const uint32_t m = ua.nH - ub.nH;
+    const uint32_t nl_mine = __popc(lmask);
+    uint32_t resolved = 0;  // lights of this thread resolved so far (they resolve in order)
+    uint32_t last_item = 0xffffffffu;
+    for (uint32_t u = link.u0; u <= link.u1; ++u) {
+        const u128 E_b = excess_before(incl, u);
+        const uint32_t nh_b = u ? __ldcg(&incl[u - 1].nH) : 0u;
+        const uint32_t m = __ldcg(&incl[u].nH) - nh_b;
+        float yc[IPT];
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) yc[k] = y[k];
+        if (u < link.u1) load_tile_items<IPT>(w, n, u + 1, threadIdx.x, y);  // prefetch the next
         if (m == 0) continue;
-        // heavies of tile u: corrected excess ends + items
-        float y[IPT];
-        load_tile_items<IPT>(w, n, u, threadIdx.x, y);
         const uint32_t uitem0 = (uint32_t)((uint64_t)u * T + (uint64_t)threadIdx.x * IPT);
         ScanVal hv = sv_zero();
 #pragma unroll
         for (int k = 0; k < IPT; ++k) {
-            if (y[k] < 0.0f || !((double)y[k] > W_N)) continue;
-            const ItemClass c = classify(y[k], W_N, R);
+            if (!(yc[k] > cp.H1)) continue;  // absent items read as -1
             hv.c += 1;
-            hv.a += c.q;
+            hv.a += heavy_excess(yc[k], cp);
+        }
+        if (threadIdx.x == 0) {
+            s_own_lo = 0xffffffffu;
+            s_own_hi = 0;
         }
         ScanVal tot_h;
         const ScanVal hex = cta_exclusive_scan<kBuildThreads>(hv, s_warp, &tot_h);
         {
             uint32_t hj = hex.c;
-            u128 Er = ub.E + hex.a;
+            uint64_t er = hex.a;
+            uint32_t own_lo = 0xffffffffu, own_hi = 0;
 #pragma unroll
             for (int k = 0; k < IPT; ++k) {
-                if (y[k] < 0.0f || !((double)y[k] > W_N)) continue;
-                const ItemClass c = classify(y[k], W_N, R);
-                Er += c.q;
-                sE[hj] = q_scale_excess(Er, nfix);
+                if (!(yc[k] > cp.H1)) continue;
+                er += heavy_excess(yc[k], cp);
+                const u128 Et = q_scale_excess(E_b + ((u128)er << 40), nfix);
+                uint64_t key;
+                if (Et <= A_before) {
+                    key = 0;
+                } else {
+                    const u128 d = Et - A_before + 0xffff;
+                    key = (q_hi(d) >> 16) ? ~0ull : (uint64_t)(d >> 16);
+                }
+                if ((lo_inf || Et > A_before) && (hi_inf || Et <= A_after)) {
+                    own_lo = min(own_lo, hj);
+                    own_hi = hj + 1;
+                }
+                sHkey[hj] = key;
+                sHe[hj] = er;
                 sHitem[hj] = uitem0 + k;
                 ++hj;
             }
-        }
-        // the heavy after this tile's last heavy (alias of that heavy when owned here)
-        if (threadIdx.x < 32) {
-            const uint32_t g = ua.nH;  // heavies through tile u
-            uint32_t nxt = 0xffffffffu;
-            if (g < nH_tot) {
-                // first tile v > u with incl[v].nH > g  <=>  last tile v' with incl[v'].nH <= g, plus one
-                const uint32_t vp = warp_last_true(u, num_tiles - 1, [&](uint32_t vv) { return ldcg_tilevals(incl + vv).nH <= g; });
-                nxt = ldcg_tilevals(agg + vp + 1).first_heavy;
+            if (own_hi > 0) {
+                atomicMin(&s_own_lo, own_lo);
+                atomicMax(&s_own_hi, own_hi);
             }
-            if (threadIdx.x == 0) s_next = nxt;
         }
         __syncthreads();
-        const uint32_t r0 = s_r0;
-        const uint32_t nl = nLt - r0;
-        const uint32_t total = nl + m;
-        const uint32_t next_after = s_next;
-        // merge path: lights [r0, nLt) (keys sA) against heavies [0, m) (keys sE);
-        // a light precedes a heavy iff A < E.
-        const uint32_t d0 = (uint32_t)(((uint64_t)total * threadIdx.x) / kBuildThreads);
-        const uint32_t d1 = (uint32_t)(((uint64_t)total * (threadIdx.x + 1)) / kBuildThreads);
-        uint32_t lo = d0 > m ? d0 - m : 0u;
-        uint32_t hi = d0 < nl ? d0 : nl;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi + 1) >> 1;
-            if (sA[r0 + mid - 1] < sE[d0 - mid]) lo = mid; else hi = mid - 1;
-        }
-        uint32_t a = lo, b = d0 - lo;
-        for (uint32_t d = d0; d < d1; ++d) {
-            if (a < nl && (b >= m || sA[r0 + a] < sE[b])) {
-                if (b < m) sLalias[r0 + a] = sHitem[b];
-                ++a;
-            } else {
-                const u128 Ev = sE[b];
-                const bool owned = (lo_inf || Ev > A_before) && (hi_inf || Ev <= A_after);
-                if (owned) {
-                    const u128 A_next = (r0 + a < nLt) ? sA[r0 + a] : A_after;
-                    const u128 r = q_one() + Ev - A_next;
-                    uint32_t al = (b + 1 < m) ? sHitem[b + 1] : next_after;
-                    if (al == 0xffffffffu) al = sHitem[b];
-                    wrs_alias_row row;
-                    row.prob = heavy_row_prob(r);
-                    row.alias = al;
-                    table[sHitem[b]] = row;
+        // lights: alias = first chunk heavy whose key exceeds the light's (galloping search)
+        if (resolved < nl_mine) {
+            uint32_t pos = 0;
+            for (uint32_t r = resolved; r < nl_mine; ++r) {
+                const uint64_t ak = sLkey[l0 + r];
+                uint32_t lo = pos;  // invariant: sHkey[< lo] <= ak
+                if (lo < m && sHkey[lo] > ak) {
+                    pos = lo;
+                } else {
+                    uint32_t step = 1, hi = lo + 1;
+                    while (hi < m && sHkey[hi] <= ak) {
+                        lo = hi;
+                        step <<= 1;
+                        hi = lo + step;
+                    }
+                    if (hi > m) hi = m;
+                    // sHkey[lo] <= ak; first index in (lo, hi] with key > ak (hi == m: none)
+                    uint32_t a = lo + 1, b = hi;
+                    while (a < b) {
+                        const uint32_t mid = (a + b) >> 1;
+                        if (sHkey[mid] <= ak) a = mid + 1; else b = mid;
+                    }
+                    pos = a;
                 }
-                ++b;
+                if (pos >= m) break;  // this and later lights lie past the chunk
+                sLalias[l0 + r] = sHitem[pos];
+                resolved = r + 1;
             }
         }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            // lights placed before the chunk's last heavy are resolved
-            const u128 elast = sE[m - 1];
-            uint32_t l2 = r0, h2 = nLt;  // first x in [r0, nLt) with A[x] >= elast
-            while (l2 < h2) {
-                const uint32_t mid = (l2 + h2) >> 1;
-                if (sA[mid] < elast) l2 = mid + 1; else h2 = mid;
+        // owned heavies [own_lo, own_hi): the light after heavy j is the first light whose key
+        // reaches the heavy's; each thread takes a contiguous block
+        const uint32_t olo = s_own_lo, ohi = s_own_hi;
+        if (olo < ohi) {
+            const uint32_t cnt = ohi - olo;
+            const uint32_t per = (cnt + kBuildThreads - 1) / kBuildThreads;
+            const uint32_t j0 = olo + threadIdx.x * per;
+            const uint32_t j1 = min(ohi, j0 + per);
+            const uint32_t next_after = links[u].next_item;
+            uint32_t pos = 0;
+            for (uint32_t j = j0; j < j1; ++j) {
+                const uint64_t hk = sHkey[j];
+                uint32_t lo = pos;  // invariant: sLkey[< lo] < hk
+                if (lo < nLt && sLkey[lo] < hk) {
+                    uint32_t step = 1, hi = lo + 1;
+                    while (hi < nLt && sLkey[hi] < hk) {
+                        lo = hi;
+                        step <<= 1;
+                        hi = lo + step;
+                    }
+                    if (hi > nLt) hi = nLt;
+                    uint32_t a = lo + 1, b = hi;  // first index in [lo + 1, hi) with key >= hk, else hi
+                    while (a < b) {
+                        const uint32_t mid = (a + b) >> 1;
+                        if (sLkey[mid] < hk) a = mid + 1; else b = mid;
+                    }
+                    lo = a;
+                }
+                pos = lo;
+                const u128 Et = q_scale_excess(E_b + ((u128)sHe[j] << 40), nfix);
+                const u128 A_next = (pos < nLt) ? A_before + ((u128)sLkey[pos] << 16) : A_after;
+                uint32_t al = (j + 1 < m) ? sHitem[j + 1] : next_after;
+                if (al == 0xffffffffu) al = sHitem[j];
+                wrs_alias_row row;
+                row.prob = heavy_row_prob(q_one() + Et - A_next);
+                row.alias = al;
+                table[sHitem[j]] = row;
             }
-            s_r0 = l2;
-            s_last_item = sHitem[m - 1];
         }
+        last_item = sHitem[m - 1];
         __syncthreads();
     }
-    // lights past every heavy's excess (rounding residue only): alias the last heavy
-    uint32_t r0 = s_r0;
-    if (r0 < nLt) {
-        if (threadIdx.x < 32) {
-            uint32_t last_item = s_last_item;
-            if (last_item == 0xffffffffu) {
-                const uint32_t vp = warp_last_true(0u, num_tiles - 1, [&](uint32_t vv) { return incl_before(incl, vv).nH < nH_tot; });
-                last_item = ldcg_tilevals(agg + vp).last_heavy;
-            }
-            if (threadIdx.x == 0) s_last_item = last_item;
-        }
-        __syncthreads();
-        const uint32_t last_item = s_last_item;
-        for (uint32_t xx = r0 + threadIdx.x; xx < nLt; xx += kBuildThreads) sLalias[xx] = last_item;
-    }
-    __syncthreads();
-    // own light rows, in item order
+    // lights past every heavy's excess (rounding residue only) alias the last heavy
+    if (last_item == 0xffffffffu) last_item = links[num_tiles].next_item;
+    uint32_t li = l0;
 #pragma unroll
     for (int k = 0; k < IPT; ++k) {
-        if (lk[k] == 0xffffffffu) continue;
+        if (!(lmask >> k & 1u)) continue;
+        const uint32_t al = sLalias[li++];
         wrs_alias_row r;
         r.prob = pk[k];
-        r.alias = sLalias[lk[k]];
+        r.alias = al != 0xffffffffu ? al : last_item;
         table[item0 + k] = r;
     }
 }

@@ -87,11 +87,17 @@ __host__ __device__ __forceinline__ u128 q_from_double(double x) {
     return m >> (-sh);
 }
 
-// Q64.64 value in [0, 2^53) to double: round toward zero to 53 bits then exact.
-__host__ __device__ __forceinline__ double q_to_double(u128 x) {
-    if (q_hi(x) == 0) return (double)(q_lo(x) >> 11) * 1.1102230246251565404e-16;  // 2^-53
-    // large values: drop fractional bits below 2^-(64-11)
-    return (double)q_hi(x) + (double)(q_lo(x) >> 11) * 1.1102230246251565404e-16;
+// round(x * 2^fb) (ties away from zero) for a finite double x >= 0, from its bits; the
+// caller keeps the result below 2^62. Subnormal inputs give 0. Branch-free: with
+// t = mantissa * 2^10 and sh = 1085 - fb - exponent (>= 1), the result is
+// ((t >> (sh - 1)) + 1) >> 1, or 0 when sh > 63.
+__host__ __device__ __forceinline__ uint64_t fixq(double x, int fb) {
+    const uint64_t b = double_bits(x);
+    const int e = (int)((b >> 52) & 0x7ff);
+    const uint64_t t = ((b & 0xfffffffffffffull) | 0x10000000000000ull) << 10;
+    const int sh = 1085 - fb - e;
+    const uint64_t r = ((t >> ((sh - 1) & 63)) + 1) >> 1;
+    return (e == 0 || sh > 63) ? 0ull : r;
 }
 
 // Q64.64 (interpreted as signed) to double. Separate multiply and add (never fused), so

@@ -458,53 +458,98 @@ static inline float heavy_row_prob(u128 r) {
     if (r >= q_one()) return 1.0f;
     return (float)((double)((uint64_t)r >> 11) * 1.1102230246251565404e-16);
 }
-static inline float large_light_prob(u128 Li, u128 d) {
-    u128 dd = q_round24(Li + d) - q_round24(Li);
+static inline float large_light_prob(u128 Li, uint64_t d48) {
+    u128 dd = q_round24(Li + ((u128)d48 << 16)) - q_round24(Li);
     uint32_t units = (uint32_t)(dd >> 40);
     return (float)(16777216u - units) * 5.9604644775390625e-8f;
 }
 
+/* round(x * 2^fb), ties away from zero, from the bits of x >= 0 (subnormals give 0). */
+static inline uint64_t fixq(double x, int fb) {
+    uint64_t b = dbits(x);
+    int e = (int)((b >> 52) & 0x7ff);
+    if (e == 0) return 0;
+    uint64_t m = (b & 0xfffffffffffffull) | 0x10000000000000ull;
+    int s = e - 1075 + fb;
+    if (s >= 0) return m << s;
+    if (s < -54) return 0;
+    return (m + (1ull << (-s - 1))) >> (-s);
+}
+
 enum { K_SMALL = 1, K_LARGE = 2, K_HEAVY = 3 };
 
-/* classify(): the per-item quantities of the build (build_kernels.cuh, restated). */
-static inline int classify(float wf, double W_N, double R, float* p_out, u128* q_out) {
-    double w = (double)wf;
-    if (w > W_N) {
-        double h = w * R;
+/* round(p * 2^48), ties away from zero, from the bits of a float p >= 0. */
+static inline uint64_t fix48f(float p) {
+    uint32_t b = f_bits(p);
+    int e = (int)((b >> 23) & 0xff);
+    if (e == 0) return 0;
+    uint64_t m = (b & 0x7fffffu) | 0x800000u;
+    int s = e - 102;
+    if (s >= 0) return m << s;
+    if (s < -25) return 0;
+    return (m + (1ull << (-s - 1))) >> (-s);
+}
+
+typedef struct {
+    double R;
+    float R32, H1, Hh;
+} ClassParams;
+
+/* The build's class thresholds: H1 = largest float <= W/N, Hh = smallest float >= W/(2N). */
+static ClassParams class_params(double W_N, double R) {
+    ClassParams c;
+    c.R = R;
+    c.R32 = (float)R;
+    float h1 = (float)W_N;
+    if ((double)h1 > W_N) h1 = nextafterf(h1, -INFINITY);
+    c.H1 = h1;
+    double half = 0.5 * W_N;
+    float hh = (float)half;
+    if ((double)hh < half) hh = nextafterf(hh, INFINITY);
+    c.Hh = hh;
+    return c;
+}
+
+/* classify(): the per-item quantities of the build, restated: light deficits in Q16.48
+ * (stored for small lights, true for large ones), heavy excess in Q40.24. */
+static inline int classify(float wf, const ClassParams* cp, float* p_out, uint64_t* q_out) {
+    if (wf > cp->H1) {
+        double h = (double)wf * cp->R;
         if (h < 1.0) h = 1.0;
-        *q_out = q_from_double(h) - q_one();
+        *q_out = fixq(h - 1.0, 24);
         *p_out = 1.0f;
         return K_HEAVY;
     }
-    double p = w * R;
-    if (p > 1.0) p = 1.0;
-    if (p >= 0.5) {
-        *q_out = q_from_double(1.0 - p);
+    if (wf >= cp->Hh) {
+        double p = (double)wf * cp->R;
+        if (p > 1.0) p = 1.0;
+        *q_out = fixq(1.0 - p, 48);
         *p_out = 1.0f;
         return K_LARGE;
     }
-    float ps = (float)p;
+    float ps = wf * cp->R32;
     *p_out = ps;
-    *q_out = q_one() - q_from_double((double)ps);
+    *q_out = (1ull << 48) - fix48f(ps);
     return K_SMALL;
 }
 
 int or_exact_build(const float* w, int64_t n, double W, uint32_t* rows) {
     const double W_N = W / (double)n;
     const double R = 1.0 / W_N;
+    const ClassParams cp = class_params(W_N, R);
     int64_t nL = 0, nH = 0;
     u128 S = 0, L = 0, E = 0;
     for (int64_t i = 0; i < n; ++i) {
         float p;
-        u128 q;
-        int k = classify(w[i], W_N, R, &p, &q);
+        uint64_t q;
+        int k = classify(w[i], &cp, &p, &q);
         if (k == K_HEAVY) {
             ++nH;
-            E += q;
+            E += (u128)q << 40;
         } else {
             ++nL;
-            if (k == K_SMALL) S += q;
-            else L += q;
+            if (k == K_SMALL) S += (u128)q << 16;
+            else L += (u128)q << 16;
         }
     }
     const u128 A_tot = S + q_round24(L);
@@ -518,10 +563,10 @@ int or_exact_build(const float* w, int64_t n, double W, uint32_t* rows) {
     u128 Sr = 0, Lr = 0, Er = 0;
     for (int64_t i = 0; i < n; ++i) {
         float p;
-        u128 q;
-        int k = classify(w[i], W_N, R, &p, &q);
+        uint64_t q;
+        int k = classify(w[i], &cp, &p, &q);
         if (k == K_HEAVY) {
-            Er += q;
+            Er += (u128)q << 40;
             Eh[hj] = q_scale_excess(Er, nfix);
             hitem[hj] = (uint32_t)i;
             ++hj;
@@ -530,10 +575,10 @@ int or_exact_build(const float* w, int64_t n, double W, uint32_t* rows) {
             litem[li] = (uint32_t)i;
             if (k == K_SMALL) {
                 lp[li] = p;
-                Sr += q;
+                Sr += (u128)q << 16;
             } else {
                 lp[li] = large_light_prob(Lr, q);
-                Lr += q;
+                Lr += (u128)q << 16;
             }
             ++li;
         }
