@@ -70,6 +70,7 @@ _SIGNATURES = {
     "wrs_sum_f32": (ctypes.c_int, [_P, _I64, _P, _P, _SZ, _P]),
     "wrs_alias_build_scratch_bytes": (_SZ, [_I64, _P]),
     "wrs_alias_build_f32": (ctypes.c_int, [_P, _I64, _P, _P, _P, _P, _SZ, _P]),
+    "wrs_alias_build_f32_static_scratch": (ctypes.c_int, [_P, _I64, _P, _P, _P, _P]),
     "wrs_alias_sample": (ctypes.c_int, [_P, _I64, _U64, _U64, _U64, _P, _P, _P, _P]),
     "wrs_rejection_build_scratch_bytes": (_SZ, [_I64]),
     "wrs_rejection_build_f32": (ctypes.c_int, [_P, _I64, _P, _U64, _P, _P, _P, _P, _SZ, _U32, _P]),
@@ -141,6 +142,13 @@ def alias_build(w, table, scratch, opts: Optional[BuildOpts] = None, W_out=None,
     st = lib().wrs_alias_build_f32(_ptr(w), n, ctypes.byref(opts) if opts else None, _ptr(table), _ptr(W_out),
                                    _ptr(scratch), scratch.numel() * scratch.element_size(), _stream(stream))
     return st
+
+
+def alias_build_static_scratch(w, table, opts: Optional[BuildOpts] = None, W_out=None, stream=None) -> int:
+    """Builds without any caller scratch (n <= 2^22): for callers that cannot allocate device
+    memory; the scratch is a fixed array inside the library, shared by all calls on a device."""
+    return lib().wrs_alias_build_f32_static_scratch(_ptr(w), w.numel(), ctypes.byref(opts) if opts else None,
+                                                    _ptr(table), _ptr(W_out), _stream(stream))
 
 
 def alias_sample(table, n: int, num_samples: int, seed: int, out, counter_base: int = 0,

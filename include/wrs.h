@@ -118,6 +118,18 @@ WRS_API wrs_status wrs_alias_build_f32(const float* d_w, int64_t n, const wrs_bu
                                wrs_alias_row* d_table, double* d_W,
                                void* d_scratch, size_t scratch_bytes, void* stream);
 
+/* The same build for callers that cannot allocate device memory (code under an allocator
+ * that forbids cudaMalloc, plugins that must not touch the host process's memory pools,
+ * paths that may not block on an allocation). No counterpart in the reference. Its scratch
+ * is a fixed 1 MiB device array inside this library (held on every GPU that loads it until
+ * the process exits), so it takes n <= 4,194,304 (2^22) items and rejects larger n with
+ * WRS_ERR_INVALID_ARGUMENT. It calls no allocating routine. The first call on each device
+ * looks up the array's device address (make it before any stream capture). All calls on a
+ * device share the array, so calls that overlap on the GPU race: serialise them. Device-side
+ * errors are returned when opts->flags has WRS_FLAG_SYNC. */
+WRS_API wrs_status wrs_alias_build_f32_static_scratch(const float* d_w, int64_t n, const wrs_build_opts* opts,
+                                                      wrs_alias_row* d_table, double* d_W, void* stream);
+
 /* Sampling-input contract (bit-exact, see the oracle):
  *   output position s uses Philox4x32-10 with key (lo32(seed), hi32(seed)) and counter
  *   (lo32(b), hi32(b), 0, 0), b = counter_base + floor(s / 2); even s reads words (x0, x1),
