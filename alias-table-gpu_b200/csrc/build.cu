@@ -86,10 +86,11 @@ struct BuildLayout {
     TileVals* agg;
     TileVals* incl;
     TileLink* links;
+    uint32_t* hmask;
     size_t bytes;
 };
 
-BuildLayout carve_build(void* scratch, uint64_t num_tiles, bool psa) {
+BuildLayout carve_build(void* scratch, uint64_t num_tiles, uint64_t tile_items, bool psa) {
     (void)psa;
     Carver c(scratch);
     BuildLayout L;
@@ -100,6 +101,7 @@ BuildLayout carve_build(void* scratch, uint64_t num_tiles, bool psa) {
     L.agg = c.take<TileVals>(num_tiles);
     L.incl = c.take<TileVals>(num_tiles);
     L.links = c.take<TileLink>(num_tiles + 1);
+    L.hmask = c.take<uint32_t>(num_tiles * (tile_items / 32));
     L.bytes = c.off;
     return L;
 }
@@ -115,7 +117,7 @@ wrs_status launch_build(const float* d_w, uint64_t n, uint32_t method, wrs_alias
     const uint64_t zero_words = L.num_blocks * sizeof(BlockWord) / sizeof(uint32_t);
     wsum_kernel<kWsumBlock><<<g, kWsumBlock, 0, stream>>>(d_w, n, L.hdr, L.partials,
                                                           reinterpret_cast<uint32_t*>(L.blocks), zero_words, d_W);
-    tile_reduce_kernel<IPT><<<(uint32_t)num_tiles, kBuildThreads, 0, stream>>>(d_w, n, L.hdr, L.agg,
+    tile_reduce_kernel<IPT><<<(uint32_t)num_tiles, kBuildThreads, 0, stream>>>(d_w, n, L.hdr, L.agg, L.hmask,
                                                                                 (uint32_t)num_tiles);
     tile_prefix_kernel<<<(uint32_t)L.num_blocks, kPrefixThreads, 0, stream>>>(L.hdr, L.agg, L.incl, L.blocks,
                                                                                (uint32_t)num_tiles);
@@ -125,8 +127,8 @@ wrs_status launch_build(const float* d_w, uint64_t n, uint32_t method, wrs_alias
         const size_t smem = pack_smem_bytes(T);
         e = cudaFuncSetAttribute(split_pack_kernel<IPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return WRS_ERR_CUDA;
-        split_pack_kernel<IPT><<<(uint32_t)num_tiles, kBuildThreads, smem, stream>>>(d_w, n, L.hdr, L.incl, L.links,
-                                                                                     (uint32_t)num_tiles, d_table);
+        split_pack_kernel<IPT><<<(uint32_t)num_tiles, kBuildThreads, smem, stream>>>(
+            d_w, n, L.hdr, L.incl, L.links, L.hmask, (uint32_t)num_tiles, d_table);
     }
     return launch_status();
 }
@@ -164,7 +166,7 @@ extern "C" size_t wrs_alias_build_scratch_bytes(int64_t n, const wrs_build_opts*
     const uint64_t T = (uint64_t)kBuildThreads * ipt;
     const uint64_t nt = ((uint64_t)n + T - 1) / T;
     const bool psa = opts && opts->method == WRS_METHOD_PSA_PLUS;
-    return carve_build(nullptr, nt, psa).bytes;
+    return carve_build(nullptr, nt, T, psa).bytes;
 }
 
 extern "C" wrs_status wrs_alias_build_f32(const float* d_w, int64_t n, const wrs_build_opts* opts,
@@ -178,9 +180,9 @@ extern "C" wrs_status wrs_alias_build_f32(const float* d_w, int64_t n, const wrs
     const uint64_t T = (uint64_t)kBuildThreads * ipt;
     const uint64_t nt = ((uint64_t)n + T - 1) / T;
     const bool psa = method == WRS_METHOD_PSA_PLUS;
-    if (scratch_bytes < carve_build(nullptr, nt, psa).bytes) return WRS_ERR_SCRATCH_TOO_SMALL;
+    if (scratch_bytes < carve_build(nullptr, nt, T, psa).bytes) return WRS_ERR_SCRATCH_TOO_SMALL;
     cudaStream_t stream = static_cast<cudaStream_t>(stream_);
-    const BuildLayout L = carve_build(d_scratch, nt, psa);
+    const BuildLayout L = carve_build(d_scratch, nt, T, psa);
     wrs_status st;
     switch (ipt) {
         case 4: st = launch_build<4>(d_w, (uint64_t)n, method, d_table, d_W, L, nt, stream); break;

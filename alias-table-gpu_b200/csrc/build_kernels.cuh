@@ -446,6 +446,7 @@ __device__ __forceinline__ u128 ldcg_E(const TileVals* src) {
 template <int IPT>
 __global__ void __launch_bounds__(kBuildThreads) tile_reduce_kernel(const float* __restrict__ w, uint64_t n,
                                                                     const BuildHeader* hdr, TileVals* agg,
+                                                                    uint32_t* __restrict__ hmask,
                                                                     uint32_t num_tiles) {
     constexpr int T = kBuildThreads * IPT;
     constexpr int NW = kBuildThreads / 32;
@@ -456,7 +457,7 @@ __global__ void __launch_bounds__(kBuildThreads) tile_reduce_kernel(const float*
     const ClassParams cp = class_params(hdr->W_N, hdr->R);
     float x[IPT];
     load_tile_items<IPT>(w, n, tile, threadIdx.x, x);
-    uint32_t nL = 0, nH = 0, fh = 0xffffffffu, lh = 0xffffffffu;
+    uint32_t nL = 0, nH = 0, fh = 0xffffffffu, lh = 0xffffffffu, hbits = 0;
     uint64_t S = 0, L = 0, E = 0;
     const uint32_t item0 = (uint32_t)((uint64_t)tile * T + (uint64_t)threadIdx.x * IPT);
 #pragma unroll
@@ -466,12 +467,21 @@ __global__ void __launch_bounds__(kBuildThreads) tile_reduce_kernel(const float*
         if (c.kind == kHeavy) {
             ++nH;
             E += c.q;
+            hbits |= 1u << k;
             if (fh == 0xffffffffu) fh = item0 + k;
             lh = item0 + k;
         } else {
             ++nL;
             if (c.kind == kSmallLight) S += c.q; else L += c.q;
         }
+    }
+    // heavy mask: bit i of word i/32 <=> tile item i is heavy (32 / IPT lanes per word)
+    {
+        constexpr int LPW = 32 / IPT;
+        uint32_t word = hbits << ((threadIdx.x % LPW) * IPT);
+#pragma unroll
+        for (int d = 1; d < LPW; d <<= 1) word |= __shfl_xor_sync(0xffffffffu, word, d);
+        if (threadIdx.x % LPW == 0) hmask[(uint64_t)tile * (T / 32) + threadIdx.x / LPW] = word;
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
@@ -798,34 +808,41 @@ __device__ __forceinline__ TileVals incl_before(const TileVals* incl, uint32_t u
 }
 
 // Shared memory of the pack kernel for T items per tile: light keys (u64), heavy keys (u64),
-// heavy local excess (u64), heavy items (u32), light aliases (u32).
+// heavy local excess (u64), heavy items (u32), light aliases (u32), heavy ranks (u32).
 __host__ __device__ constexpr size_t pack_smem_bytes(int T) {
-    return (size_t)T * (3 * sizeof(uint64_t) + 2 * sizeof(uint32_t));
+    return (size_t)T * (3 * sizeof(uint64_t) + 3 * sizeof(uint32_t));
 }
 
 // One light tile per CTA. Its lights' deficit-interval starts go to shared memory as keys
 // in the tile's frame (A - A_before(t), Q16.48). The heavies of the partner tiles
-// [u0, u1] arrive one tile at a time (the next one prefetched into registers), as keys in
-// the same frame: key = ceil((E~ - A_before(t)) / 2^-48), clamped, so that key(light) <
-// key(heavy) exactly when A < E~. Each thread then resolves its own (consecutive, sorted)
-// lights' aliases J(i) = #{E~ <= A_i} by a galloping search through the heavy keys that
-// resumes where its previous light stopped, and a contiguous block of the heavies owned by
-// the tile finds the light after each heavy, I(j) = #{A < E~_j}, the same way.
+// [u0, u1] are taken one tile at a time from the tile's heavy mask (written by the reduce
+// pass): only the heavies' weights are gathered (from L2), so a partner costs work in
+// proportion to its heavies. Their corrected excess ends become keys in the same frame:
+// key = ceil((E~ - A_before(t)) / 2^-48), clamped, so that key(light) < key(heavy) exactly
+// when A < E~. A merge path over the still unresolved lights and the chunk's heavies gives
+// every thread an equal slice of the merged order; the slice only records ranks: a light's
+// alias is the heavy at its rank (J(i) = #{E~ <= A_i}), a heavy's rank is the light after
+// it (I(j) = #{A < E~_j}). Owned heavies then write their rows from those ranks, and the
+// last heavy's rank is the number of lights resolved so far.
 template <int IPT>
 __global__ void __launch_bounds__(kBuildThreads, (IPT <= 8 ? 3 : 1)) split_pack_kernel(const float* __restrict__ w,
                                                                                      uint64_t n,
                                                                                      const BuildHeader* hdr,
                                                                                      const TileVals* incl,
                                                                                      const TileLink* links,
+                                                                                     const uint32_t* __restrict__ hmask,
                                                                                      uint32_t num_tiles,
                                                                                      wrs_alias_row* __restrict__ table) {
     constexpr int T = kBuildThreads * IPT;
+    constexpr int WPT = T / 32;  // heavy-mask words per tile
+    static_assert(WPT <= kBuildThreads, "one mask word per thread");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint64_t* sLkey = reinterpret_cast<uint64_t*>(smem_raw);
     uint64_t* sHkey = sLkey + T;
     uint64_t* sHe = sHkey + T;
     uint32_t* sHitem = reinterpret_cast<uint32_t*>(sHe + T);
     uint32_t* sLalias = sHitem + T;
+    uint32_t* sHrank = sLalias + T;
     __shared__ ScanVal s_warp[kBuildThreads / 32 + 1];
     __shared__ uint32_t s_own_lo, s_own_hi;
 
@@ -834,9 +851,6 @@ __global__ void __launch_bounds__(kBuildThreads, (IPT <= 8 ? 3 : 1)) split_pack_
                                                        // the last tiles, still in L2
     const ClassParams cp = class_params(hdr->W_N, hdr->R);
     const TileLink link = links[tile];
-    // prefetch the first partner tile while the own tile is processed
-    float y[IPT];
-    load_tile_items<IPT>(w, n, link.u0, threadIdx.x, y);
     const TileVals tot = ldcg_tilevals(incl + num_tiles - 1);
     const TileVals before = incl_before(incl, tile);
     const TileVals after = ldcg_tilevals(incl + tile);
@@ -911,40 +925,41 @@ __global__ void __launch_bounds__(kBuildThreads, (IPT <= 8 ? 3 : 1)) split_pack_
     }
     if (!lo_inf && !hi_inf && nLt == 0) return;  // empty ownership interval, no lights
 
-    const uint32_t nl_mine = __popc(lmask);
-    uint32_t resolved = 0;  // lights of this thread resolved so far (they resolve in order)
+    uint32_t r0 = 0;  // lights [0, r0) are resolved
     uint32_t last_item = 0xffffffffu;
     for (uint32_t u = link.u0; u <= link.u1; ++u) {
-        const u128 E_b = excess_before(incl, u);
         const uint32_t nh_b = u ? __ldcg(&incl[u - 1].nH) : 0u;
         const uint32_t m = __ldcg(&incl[u].nH) - nh_b;
-        float yc[IPT];
-#pragma unroll
-        for (int k = 0; k < IPT; ++k) yc[k] = y[k];
-        if (u < link.u1) load_tile_items<IPT>(w, n, u + 1, threadIdx.x, y);  // prefetch the next
         if (m == 0) continue;
-        const uint32_t uitem0 = (uint32_t)((uint64_t)u * T + (uint64_t)threadIdx.x * IPT);
-        ScanVal hv = sv_zero();
-#pragma unroll
-        for (int k = 0; k < IPT; ++k) {
-            if (!(yc[k] > cp.H1)) continue;  // absent items read as -1
-            hv.c += 1;
-            hv.a += heavy_excess(yc[k], cp);
+        const u128 E_b = excess_before(incl, u);
+        // expand the heavy mask of tile u into the heavies' items, in order
+        {
+            const uint32_t word = threadIdx.x < WPT ? __ldg(hmask + (uint64_t)u * WPT + threadIdx.x) : 0u;
+            ScanVal wv = sv_zero();
+            wv.c = __popc(word);
+            ScanVal wt;
+            const ScanVal wex = cta_exclusive_scan<kBuildThreads>(wv, s_warp, &wt);
+            uint32_t o = wex.c;
+            const uint32_t base = u * (uint32_t)T + threadIdx.x * 32u;
+            for (uint32_t bits = word; bits; bits &= bits - 1) sHitem[o++] = base + (uint32_t)(__ffs(bits) - 1);
         }
         if (threadIdx.x == 0) {
             s_own_lo = 0xffffffffu;
             s_own_hi = 0;
         }
+        __syncthreads();
+        // excess of each heavy (weights gathered from L2), contiguous blocks per thread
+        const uint32_t per = (m + kBuildThreads - 1) / kBuildThreads;
+        const uint32_t j0 = min(m, threadIdx.x * per), j1 = min(m, j0 + per);
+        ScanVal hv = sv_zero();
+        for (uint32_t j = j0; j < j1; ++j) hv.a += heavy_excess(__ldg(w + sHitem[j]), cp);
         ScanVal tot_h;
         const ScanVal hex = cta_exclusive_scan<kBuildThreads>(hv, s_warp, &tot_h);
         {
-            uint32_t hj = hex.c;
             uint64_t er = hex.a;
             uint32_t own_lo = 0xffffffffu, own_hi = 0;
-#pragma unroll
-            for (int k = 0; k < IPT; ++k) {
-                if (!(yc[k] > cp.H1)) continue;
-                er += heavy_excess(yc[k], cp);
+            for (uint32_t j = j0; j < j1; ++j) {
+                er += heavy_excess(__ldg(w + sHitem[j]), cp);
                 const u128 Et = q_scale_excess(E_b + ((u128)er << 40), nfix);
                 uint64_t key;
                 if (Et <= A_before) {
@@ -954,13 +969,11 @@ __global__ void __launch_bounds__(kBuildThreads, (IPT <= 8 ? 3 : 1)) split_pack_
                     key = (q_hi(d) >> 16) ? ~0ull : (uint64_t)(d >> 16);
                 }
                 if ((lo_inf || Et > A_before) && (hi_inf || Et <= A_after)) {
-                    own_lo = min(own_lo, hj);
-                    own_hi = hj + 1;
+                    own_lo = min(own_lo, j);
+                    own_hi = j + 1;
                 }
-                sHkey[hj] = key;
-                sHe[hj] = er;
-                sHitem[hj] = uitem0 + k;
-                ++hj;
+                sHkey[j] = key;
+                sHe[j] = er;
             }
             if (own_hi > 0) {
                 atomicMin(&s_own_lo, own_lo);
@@ -968,74 +981,48 @@ __global__ void __launch_bounds__(kBuildThreads, (IPT <= 8 ? 3 : 1)) split_pack_
             }
         }
         __syncthreads();
-        // lights: alias = first chunk heavy whose key exceeds the light's (galloping search)
-        if (resolved < nl_mine) {
-            uint32_t pos = 0;
-            for (uint32_t r = resolved; r < nl_mine; ++r) {
-                const uint64_t ak = sLkey[l0 + r];
-                uint32_t lo = pos;  // invariant: sHkey[< lo] <= ak
-                if (lo < m && sHkey[lo] > ak) {
-                    pos = lo;
+        // merge path over lights [r0, nLt) and heavies [0, m); a light precedes a heavy iff
+        // its key is below the heavy's. Each thread records ranks for an equal slice.
+        {
+            const uint32_t nl = nLt - r0;
+            const uint32_t total = nl + m;
+            const uint32_t d0 = (uint32_t)(((uint64_t)total * threadIdx.x) / kBuildThreads);
+            const uint32_t d1 = (uint32_t)(((uint64_t)total * (threadIdx.x + 1)) / kBuildThreads);
+            uint32_t lo = d0 > m ? d0 - m : 0u;
+            uint32_t hi = d0 < nl ? d0 : nl;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi + 1) >> 1;
+                if (sLkey[r0 + mid - 1] < sHkey[d0 - mid]) lo = mid; else hi = mid - 1;
+            }
+            uint32_t a = lo, b = d0 - lo;
+            for (uint32_t d = d0; d < d1; ++d) {
+                const bool take_light = a < nl && (b >= m || sLkey[r0 + a] < sHkey[b]);
+                if (take_light) {
+                    if (b < m) sLalias[r0 + a] = sHitem[b];
+                    ++a;
                 } else {
-                    uint32_t step = 1, hi = lo + 1;
-                    while (hi < m && sHkey[hi] <= ak) {
-                        lo = hi;
-                        step <<= 1;
-                        hi = lo + step;
-                    }
-                    if (hi > m) hi = m;
-                    // sHkey[lo] <= ak; first index in (lo, hi] with key > ak (hi == m: none)
-                    uint32_t a = lo + 1, b = hi;
-                    while (a < b) {
-                        const uint32_t mid = (a + b) >> 1;
-                        if (sHkey[mid] <= ak) a = mid + 1; else b = mid;
-                    }
-                    pos = a;
+                    sHrank[b] = r0 + a;
+                    ++b;
                 }
-                if (pos >= m) break;  // this and later lights lie past the chunk
-                sLalias[l0 + r] = sHitem[pos];
-                resolved = r + 1;
             }
         }
-        // owned heavies [own_lo, own_hi): the light after heavy j is the first light whose key
-        // reaches the heavy's; each thread takes a contiguous block
+        __syncthreads();
+        // owned heavies [own_lo, own_hi): rows from the ranks
         const uint32_t olo = s_own_lo, ohi = s_own_hi;
-        if (olo < ohi) {
-            const uint32_t cnt = ohi - olo;
-            const uint32_t per = (cnt + kBuildThreads - 1) / kBuildThreads;
-            const uint32_t j0 = olo + threadIdx.x * per;
-            const uint32_t j1 = min(ohi, j0 + per);
-            const uint32_t next_after = links[u].next_item;
-            uint32_t pos = 0;
-            for (uint32_t j = j0; j < j1; ++j) {
-                const uint64_t hk = sHkey[j];
-                uint32_t lo = pos;  // invariant: sLkey[< lo] < hk
-                if (lo < nLt && sLkey[lo] < hk) {
-                    uint32_t step = 1, hi = lo + 1;
-                    while (hi < nLt && sLkey[hi] < hk) {
-                        lo = hi;
-                        step <<= 1;
-                        hi = lo + step;
-                    }
-                    if (hi > nLt) hi = nLt;
-                    uint32_t a = lo + 1, b = hi;  // first index in [lo + 1, hi) with key >= hk, else hi
-                    while (a < b) {
-                        const uint32_t mid = (a + b) >> 1;
-                        if (sLkey[mid] < hk) a = mid + 1; else b = mid;
-                    }
-                    lo = a;
-                }
-                pos = lo;
-                const u128 Et = q_scale_excess(E_b + ((u128)sHe[j] << 40), nfix);
-                const u128 A_next = (pos < nLt) ? A_before + ((u128)sLkey[pos] << 16) : A_after;
-                uint32_t al = (j + 1 < m) ? sHitem[j + 1] : next_after;
-                if (al == 0xffffffffu) al = sHitem[j];
-                wrs_alias_row row;
-                row.prob = heavy_row_prob(q_one() + Et - A_next);
-                row.alias = al;
-                table[sHitem[j]] = row;
-            }
+        const uint32_t next_after = links[u].next_item;
+        for (uint32_t j = olo + threadIdx.x; j < ohi; j += kBuildThreads) {
+            const uint32_t rk = sHrank[j];
+            const u128 Et = q_scale_excess(E_b + ((u128)sHe[j] << 40), nfix);
+            const u128 A_next = (rk < nLt) ? A_before + ((u128)sLkey[rk] << 16) : A_after;
+            uint32_t al = (j + 1 < m) ? sHitem[j + 1] : next_after;
+            if (al == 0xffffffffu) al = sHitem[j];
+            wrs_alias_row row;
+            row.prob = heavy_row_prob(q_one() + Et - A_next);
+            row.alias = al;
+            table[sHitem[j]] = row;
         }
+        // lights before the chunk's last heavy are resolved
+        r0 = sHrank[m - 1];
         last_item = sHitem[m - 1];
         __syncthreads();
     }
