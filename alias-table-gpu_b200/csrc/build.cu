@@ -5,9 +5,9 @@
 //                         (construction/aliasTable/buildMethod/AliasTableSplitGpu.cu:388-468)
 //
 // Unlike the reference build (>= 5 blocking device-to-host copies and >= 3 cudaMalloc/cudaFree
-// pairs inside build()), the whole build is four stream-ordered operations on caller memory:
-// a 128-byte memset of the scratch header, then the wsum, tile_reduce, tile_prefix, tile_link
-// and split_pack kernels.
+// pairs inside build()), the whole build is stream-ordered work on caller memory: a 128-byte
+// memset of the scratch header, then the wsum, tile_reduce, tile_prefix, heavy_list,
+// tile_link and split_pack kernels.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -67,16 +67,33 @@ namespace {
 
 constexpr int64_t kMaxItems = (int64_t)0x7fffffff - 8192;
 
-int ipt_for(const wrs_build_opts* opts) {
+// Items per tile of the reduce and pack passes (0 = the default 2048).
+int64_t tile_items_for(const wrs_build_opts* opts) {
     const uint32_t t = opts ? opts->tile_items : 0u;
     switch (t) {
         case 0:
-        case 2048: return 8;
-        case 1024: return 4;
-        case 4096: return 16;
+        case 2048: return 2048;
+        case 1024: return 1024;
+        case 4096: return 4096;
         default: return -1;
     }
 }
+
+// Pack CTA shape per tile size: threads x items per thread.
+template <int T>
+struct PackShape;
+template <>
+struct PackShape<1024> {
+    static constexpr int NT = 128, IPT = 8;
+};
+template <>
+struct PackShape<2048> {
+    static constexpr int NT = 128, IPT = 16;
+};
+template <>
+struct PackShape<4096> {
+    static constexpr int NT = 256, IPT = 16;
+};
 
 struct BuildLayout {
     BuildHeader* hdr;
@@ -85,13 +102,14 @@ struct BuildLayout {
     uint64_t num_blocks;
     TileVals* agg;
     TileVals* incl;
-    TileLink* links;
+    uint32_t* bound;
     uint32_t* hmask;
+    uint32_t* heavy_item;
+    uint4* heavy_E;
     size_t bytes;
 };
 
-BuildLayout carve_build(void* scratch, uint64_t num_tiles, uint64_t tile_items, bool psa) {
-    (void)psa;
+BuildLayout carve_build(void* scratch, uint64_t n, uint64_t num_tiles, uint64_t tile_items) {
     Carver c(scratch);
     BuildLayout L;
     L.hdr = c.take<BuildHeader>(1);
@@ -100,16 +118,18 @@ BuildLayout carve_build(void* scratch, uint64_t num_tiles, uint64_t tile_items, 
     L.blocks = c.take<BlockWord>(L.num_blocks);
     L.agg = c.take<TileVals>(num_tiles);
     L.incl = c.take<TileVals>(num_tiles);
-    L.links = c.take<TileLink>(num_tiles + 1);
+    L.bound = c.take<uint32_t>(num_tiles + 1);
     L.hmask = c.take<uint32_t>(num_tiles * (tile_items / 32));
+    L.heavy_item = c.take<uint32_t>(n);
+    L.heavy_E = c.take<uint4>(n);
     L.bytes = c.off;
     return L;
 }
 
-template <int IPT>
+template <int T>
 wrs_status launch_build(const float* d_w, uint64_t n, uint32_t method, wrs_alias_row* d_table, double* d_W,
                         const BuildLayout& L, uint64_t num_tiles, cudaStream_t stream) {
-    constexpr int T = kBuildThreads * IPT;
+    constexpr int NT = PackShape<T>::NT, IPT = PackShape<T>::IPT;
     (void)method;
     cudaError_t e = cudaMemsetAsync(L.hdr, 0, sizeof(BuildHeader), stream);
     if (e != cudaSuccess) return WRS_ERR_CUDA;
@@ -117,18 +137,21 @@ wrs_status launch_build(const float* d_w, uint64_t n, uint32_t method, wrs_alias
     const uint64_t zero_words = L.num_blocks * sizeof(BlockWord) / sizeof(uint32_t);
     wsum_kernel<kWsumBlock><<<g, kWsumBlock, 0, stream>>>(d_w, n, L.hdr, L.partials,
                                                           reinterpret_cast<uint32_t*>(L.blocks), zero_words, d_W);
-    tile_reduce_kernel<IPT><<<(uint32_t)num_tiles, kBuildThreads, 0, stream>>>(d_w, n, L.hdr, L.agg, L.hmask,
-                                                                                (uint32_t)num_tiles);
+    tile_reduce_kernel<T><<<(uint32_t)num_tiles, kReduceThreads, 0, stream>>>(d_w, n, L.hdr, L.agg, L.hmask,
+                                                                              (uint32_t)num_tiles);
     tile_prefix_kernel<<<(uint32_t)L.num_blocks, kPrefixThreads, 0, stream>>>(L.hdr, L.agg, L.incl, L.blocks,
                                                                                (uint32_t)num_tiles);
-    tile_link_kernel<<<(uint32_t)((num_tiles + 1 + 255) / 256), 256, 0, stream>>>(L.hdr, L.agg, L.incl,
-                                                                                  (uint32_t)num_tiles, L.links);
+    heavy_list_kernel<T><<<(uint32_t)num_tiles, kReduceThreads, 0, stream>>>(d_w, L.hdr, L.agg, L.incl, L.hmask,
+                                                                             (uint32_t)num_tiles, L.heavy_item,
+                                                                             L.heavy_E);
+    tile_link_kernel<<<(uint32_t)((num_tiles + 1 + 255) / 256), 256, 0, stream>>>(L.hdr, L.incl, (uint32_t)num_tiles,
+                                                                                  L.heavy_E, L.bound);
     {
         const size_t smem = pack_smem_bytes(T);
-        e = cudaFuncSetAttribute(split_pack_kernel<IPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = cudaFuncSetAttribute(split_pack_kernel<NT, IPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return WRS_ERR_CUDA;
-        split_pack_kernel<IPT><<<(uint32_t)num_tiles, kBuildThreads, smem, stream>>>(
-            d_w, n, L.hdr, L.incl, L.links, L.hmask, (uint32_t)num_tiles, d_table);
+        split_pack_kernel<NT, IPT><<<(uint32_t)num_tiles, NT, smem, stream>>>(
+            d_w, n, L.hdr, L.incl, L.bound, L.heavy_item, L.heavy_E, (uint32_t)num_tiles, d_table);
     }
     return launch_status();
 }
@@ -161,33 +184,29 @@ extern "C" wrs_status wrs_sum_f32(const float* d_w, int64_t n, double* d_total, 
 }
 
 extern "C" size_t wrs_alias_build_scratch_bytes(int64_t n, const wrs_build_opts* opts) {
-    const int ipt = ipt_for(opts);
-    if (n < 1 || ipt < 0) return 0;
-    const uint64_t T = (uint64_t)kBuildThreads * ipt;
+    const int64_t T = tile_items_for(opts);
+    if (n < 1 || T < 0) return 0;
     const uint64_t nt = ((uint64_t)n + T - 1) / T;
-    const bool psa = opts && opts->method == WRS_METHOD_PSA_PLUS;
-    return carve_build(nullptr, nt, T, psa).bytes;
+    return carve_build(nullptr, (uint64_t)n, nt, T).bytes;
 }
 
 extern "C" wrs_status wrs_alias_build_f32(const float* d_w, int64_t n, const wrs_build_opts* opts,
                                           wrs_alias_row* d_table, double* d_W, void* d_scratch,
                                           size_t scratch_bytes, void* stream_) {
     if (!d_w || !d_table || !d_scratch || n < 1 || n > kMaxItems) return WRS_ERR_INVALID_ARGUMENT;
-    const int ipt = ipt_for(opts);
+    const int64_t T = tile_items_for(opts);
     const uint32_t method = opts ? opts->method : WRS_METHOD_SPLIT;
-    if (ipt < 0 || method > WRS_METHOD_PSA_PLUS) return WRS_ERR_INVALID_ARGUMENT;
+    if (T < 0 || method > WRS_METHOD_PSA_PLUS) return WRS_ERR_INVALID_ARGUMENT;
     if (method == WRS_METHOD_PSA_PLUS) return WRS_ERR_UNSUPPORTED;
-    const uint64_t T = (uint64_t)kBuildThreads * ipt;
     const uint64_t nt = ((uint64_t)n + T - 1) / T;
-    const bool psa = method == WRS_METHOD_PSA_PLUS;
-    if (scratch_bytes < carve_build(nullptr, nt, T, psa).bytes) return WRS_ERR_SCRATCH_TOO_SMALL;
+    if (scratch_bytes < carve_build(nullptr, (uint64_t)n, nt, T).bytes) return WRS_ERR_SCRATCH_TOO_SMALL;
     cudaStream_t stream = static_cast<cudaStream_t>(stream_);
-    const BuildLayout L = carve_build(d_scratch, nt, T, psa);
+    const BuildLayout L = carve_build(d_scratch, (uint64_t)n, nt, T);
     wrs_status st;
-    switch (ipt) {
-        case 4: st = launch_build<4>(d_w, (uint64_t)n, method, d_table, d_W, L, nt, stream); break;
-        case 16: st = launch_build<16>(d_w, (uint64_t)n, method, d_table, d_W, L, nt, stream); break;
-        default: st = launch_build<8>(d_w, (uint64_t)n, method, d_table, d_W, L, nt, stream); break;
+    switch (T) {
+        case 1024: st = launch_build<1024>(d_w, (uint64_t)n, method, d_table, d_W, L, nt, stream); break;
+        case 4096: st = launch_build<4096>(d_w, (uint64_t)n, method, d_table, d_W, L, nt, stream); break;
+        default: st = launch_build<2048>(d_w, (uint64_t)n, method, d_table, d_W, L, nt, stream); break;
     }
     if (st != WRS_SUCCESS) return st;
     if (opts && (opts->flags & WRS_FLAG_SYNC)) return read_device_status(&L.hdr->status, stream);

@@ -103,22 +103,23 @@ struct __align__(16) BuildHeader {
 static_assert(sizeof(BuildHeader) == 128, "header layout");
 
 // ---------------------------------------------------------------- classification
-// The per-item quantities; the same code runs in every pass that needs them, and the
-// CPU oracle restates it operation by operation. Within a tile, deficits are summed as
-// u64 in Q16.48 and excess in Q40.24 (rounded per item); tile aggregates and prefixes are
-// Q64.64. A light's merge key is exact on the 2^-48 grid, so comparisons against the
-// (full-resolution) corrected excess line stay exact; the per-item rounding only moves
-// a heavy's reconstructed probability by at most (number of donees) x 2^-49 rows.
+// The per-item quantities; every pass that needs them computes them the same way, and the
+// CPU oracle restates them operation by operation. Within a tile, light deficits are
+// summed as u64 in Q16.48 and heavy excess in Q40.24 (each rounded to nearest, ties to
+// even, by one hardware conversion of an exactly scaled value); tile aggregates and
+// prefixes are Q64.64. A light's merge key is exact on the 2^-48 grid, so comparisons
+// against the (full-resolution) corrected excess line stay exact; the per-item rounding
+// only moves a heavy's reconstructed probability by at most (number of donees) x 2^-49 rows.
 //
 // Classes, with thresholds computed once per build from W/N (ClassParams):
 //   heavy        w > H1 (H1 = largest float <= W/N, so exactly w > W/N): excess h - 1,
 //                h = w * (N/W) in FP64;
 //   large light  Hh <= w <= H1 (Hh = smallest float >= W/(2N)): true deficit 1 - w*(N/W)
-//                in FP64, stored probability dithered (large_light_prob);
+//                in FP64, stored probability dithered (see the pack pass);
 //   small light  w < Hh: stored probability p = w * fl32(N/W) in FP32 (within 2 ulp of
 //                w/(W/N)), deficit 1 - p.
-enum : int { kAbsent = 0, kSmallLight = 1, kLargeLight = 2, kHeavy = 3 };
-
+// Large lights and heavies are the "rare" classes: the passes handle them in a second,
+// per-thread loop over their bits, so the FP64 path costs work only where it is needed.
 struct ClassParams {
     double R;   // N / W
     float R32;  // fl32(R)
@@ -135,50 +136,43 @@ __device__ __forceinline__ ClassParams class_params(const double W_N, const doub
     return c;
 }
 
-// round(p * 2^48) (ties away from zero) for a float p in [0, 1], from its bits (branch-free:
-// t = mantissa * 2^25, sh = 127 - exponent >= 1, result ((t >> (sh - 1)) + 1) >> 1).
-__host__ __device__ __forceinline__ uint64_t fix48f(uint32_t b) {
-    const int e = (int)((b >> 23) & 0xff);
-    const uint64_t t = (uint64_t)((b & 0x7fffffu) | 0x800000u) << 25;
-    const int sh = 127 - e;
-    const uint64_t r = ((t >> ((sh - 1) & 63)) + 1) >> 1;
-    return (e == 0 || sh > 63) ? 0ull : r;
+constexpr uint64_t kOneQ48 = 1ull << 48;
+
+// Q16.48 deficit of a small light with stored probability p: 2^48 - rne(p * 2^48)
+// (p * 2^48 is exact in FP32).
+__device__ __forceinline__ uint64_t small_deficit(float p) {
+    return kOneQ48 - __float2ull_rn(__fmul_rn(p, 281474976710656.0f));
 }
 
-struct ItemQ {
-    int kind;
-    float p;     // small light: stored probability
-    uint64_t q;  // light: deficit in Q16.48 (stored for small, true for large); heavy: excess in Q40.24
+// A rare item's quantity: heavy excess max(h, 1) - 1 in Q40.24, or a large light's true
+// deficit 1 - min(h, 1) in Q16.48, with h = w * (N/W) in FP64.
+__device__ __forceinline__ uint64_t rare_q(float wf, bool heavy, const ClassParams& cp) {
+    const double hd = __dmul_rn((double)wf, cp.R);
+    const double v = heavy ? __dsub_rn(fmax(hd, 1.0), 1.0) : __dsub_rn(1.0, fmin(hd, 1.0));
+    return __double2ull_rn(__dmul_rn(v, heavy ? 16777216.0 : 281474976710656.0));
+}
+
+// Dithering of large lights, in the tile frame. Globally, A_i = S_i + round24(L_i) with S_i,
+// L_i the Q64.64 prefixes of small-light deficits and large-light true deficits; a large
+// light stores the deficit round24(L_i + d) - round24(L_i), a multiple of 2^-24 (exact in
+// FP32). Inside a tile with L_i = L_before + x (x in Q16.48), only the low 40 bits of
+// L_before matter: with c0 = ((L_before mod 2^40) >> 16) + 2^23,
+//   round24(L_before + x) - round24(L_before) = (((c0 + x) >> 24) - (c0 >> 24)) << 24
+// in Q16.48 units, which needs only 64-bit arithmetic.
+struct Dither {
+    uint64_t c0;
+    uint64_t c0h;
 };
-
-// Caller guarantees wf >= 0 (a present item).
-__device__ __forceinline__ ItemQ classify(float wf, const ClassParams& cp) {
-    ItemQ c;
-    if (wf < cp.Hh) {
-        c.kind = kSmallLight;
-        c.p = __fmul_rn(wf, cp.R32);
-        c.q = (1ull << 48) - fix48f(__float_as_uint(c.p));
-    } else {
-        const double hd = __dmul_rn((double)wf, cp.R);
-        const bool heavy = wf > cp.H1;
-        const double v = heavy ? __dsub_rn(fmax(hd, 1.0), 1.0) : __dsub_rn(1.0, fmin(hd, 1.0));
-        c.q = fixq(v, heavy ? 24 : 48);
-        c.kind = heavy ? kHeavy : kLargeLight;
-        c.p = 1.0f;
-    }
-    return c;
+__device__ __forceinline__ Dither make_dither(u128 L_before) {
+    Dither d;
+    d.c0 = ((q_lo(L_before) & ((1ull << 40) - 1)) >> 16) + (1ull << 23);
+    d.c0h = d.c0 >> 24;
+    return d;
 }
-
-// Heavy excess only (the caller has checked wf > H1).
-__device__ __forceinline__ uint64_t heavy_excess(float wf, const ClassParams& cp) {
-    return fixq(__dsub_rn(fmax(__dmul_rn((double)wf, cp.R), 1.0), 1.0), 24);
-}
-
-// Stored probability of a dithered large light: deficit round24(L_i + d) - round24(L_i),
-// a multiple of 2^-24, so 1 - deficit is exact in FP32.
-__device__ __forceinline__ float large_light_prob(u128 L_i, uint64_t d48) {
-    const u128 dd = q_round24(L_i + ((u128)d48 << 16)) - q_round24(L_i);
-    const uint32_t units = (uint32_t)(dd >> 40);
+__device__ __forceinline__ uint64_t dither_at(const Dither& d, uint64_t x) { return (((d.c0 + x) >> 24) - d.c0h) << 24; }
+// Stored probability of a large light from the dithered deficit (a multiple of 2^-24).
+__device__ __forceinline__ float dithered_prob(uint64_t dd48) {
+    const uint32_t units = (uint32_t)(dd48 >> 24);
     return (float)(16777216u - units) * 5.9604644775390625e-8f;
 }
 
@@ -341,61 +335,110 @@ __global__ void __launch_bounds__(BLOCK) wsum_kernel(const float* __restrict__ w
 }
 
 // ---------------------------------------------------------------- CTA scan helpers
-struct ScanVal {
+// Exclusive CTA-wide scans. Each warp scans with shuffles, the last lane of every warp
+// publishes its total in s[warp], and after one barrier every warp scans the NT/32 totals
+// itself (no serial step). The caller must not rewrite s before a barrier that follows all
+// reads of it (each scan below gets its own slots).
+struct Scan3 {  // a count and two u64 sums
     uint32_t c;
     uint64_t a;
     uint64_t b;
 };
-__device__ __forceinline__ ScanVal sv_add(const ScanVal& x, const ScanVal& y) {
-    ScanVal r;
+__device__ __forceinline__ Scan3 s3_add(const Scan3& x, const Scan3& y) {
+    Scan3 r;
     r.c = x.c + y.c;
     r.a = x.a + y.a;
     r.b = x.b + y.b;
     return r;
 }
-__device__ __forceinline__ ScanVal sv_zero() {
-    ScanVal r;
-    r.c = 0;
-    r.a = 0;
-    r.b = 0;
-    return r;
+__device__ __forceinline__ Scan3 s3_shfl_up(const Scan3& v, int d) {
+    Scan3 o;
+    o.c = __shfl_up_sync(0xffffffffu, v.c, d);
+    o.a = __shfl_up_sync(0xffffffffu, v.a, d);
+    o.b = __shfl_up_sync(0xffffffffu, v.b, d);
+    return o;
+}
+__device__ __forceinline__ Scan3 s3_shfl(const Scan3& v, int src) {
+    Scan3 o;
+    o.c = __shfl_sync(0xffffffffu, v.c, src);
+    o.a = __shfl_sync(0xffffffffu, v.a, src);
+    o.b = __shfl_sync(0xffffffffu, v.b, src);
+    return o;
 }
 
-// Exclusive CTA-wide scan of (count, a, b); the CTA total goes to *total.
-// s_warp needs BLOCK/32 + 1 entries. Ends with a barrier (s_warp reusable).
-template <int BLOCK>
-__device__ __forceinline__ ScanVal cta_exclusive_scan(ScanVal v, ScanVal* s_warp, ScanVal* total) {
+template <int NT>
+__device__ __forceinline__ Scan3 block_scan3(const Scan3 v, Scan3* s, Scan3& total) {
+    constexpr int NW = NT / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    ScanVal inc = v;
+    Scan3 inc = v;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
-        ScanVal o;
-        o.c = __shfl_up_sync(0xffffffffu, inc.c, off);
-        o.a = __shfl_up_sync(0xffffffffu, inc.a, off);
-        o.b = __shfl_up_sync(0xffffffffu, inc.b, off);
-        if (lane >= off) inc = sv_add(inc, o);
+        const Scan3 o = s3_shfl_up(inc, off);
+        if (lane >= off) inc = s3_add(inc, o);
     }
-    if (lane == 31) s_warp[warp] = inc;
+    if (lane == 31) s[warp] = inc;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        ScanVal acc = sv_zero();
+    Scan3 t = {0u, 0ull, 0ull};
+    if (lane < NW) t = s[lane];
 #pragma unroll
-        for (int i = 0; i < BLOCK / 32; ++i) {
-            const ScanVal t = s_warp[i];
-            s_warp[i] = acc;
-            acc = sv_add(acc, t);
-        }
-        s_warp[BLOCK / 32] = acc;
+    for (int off = 1; off < NW; off <<= 1) {
+        const Scan3 o = s3_shfl_up(t, off);
+        if (lane >= off) t = s3_add(t, o);
     }
-    __syncthreads();
-    const ScanVal base = s_warp[warp];
-    *total = s_warp[BLOCK / 32];
-    ScanVal ex;
-    ex.c = base.c + inc.c - v.c;
-    ex.a = base.a + inc.a - v.a;
-    ex.b = base.b + inc.b - v.b;
-    __syncthreads();
+    total = s3_shfl(t, NW - 1);
+    const Scan3 base = s3_shfl(t, warp > 0 ? warp - 1 : 0);
+    Scan3 ex;
+    ex.c = (warp ? base.c : 0u) + inc.c - v.c;
+    ex.a = (warp ? base.a : 0ull) + inc.a - v.a;
+    ex.b = (warp ? base.b : 0ull) + inc.b - v.b;
     return ex;
+}
+
+template <int NT, typename U>
+__device__ __forceinline__ U block_scan1(const U v, U* s, U& total) {
+    constexpr int NW = NT / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    U inc = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const U o = __shfl_up_sync(0xffffffffu, inc, off);
+        if (lane >= off) inc += o;
+    }
+    if (lane == 31) s[warp] = inc;
+    __syncthreads();
+    U t = (lane < NW) ? s[lane] : (U)0;
+#pragma unroll
+    for (int off = 1; off < NW; off <<= 1) {
+        const U o = __shfl_up_sync(0xffffffffu, t, off);
+        if (lane >= off) t += o;
+    }
+    total = __shfl_sync(0xffffffffu, t, NW - 1);
+    const U base = __shfl_sync(0xffffffffu, t, warp > 0 ? warp - 1 : 0);
+    return (warp ? base : (U)0) + inc - v;
+}
+
+// The IPT consecutive weights of thread `tid` of an NT-thread CTA in tile `tile`
+// (T = NT * IPT items); items past n read as -1.
+template <int NT, int IPT>
+__device__ __forceinline__ void load_items(const float* __restrict__ w, uint64_t n, uint64_t tile, int tid,
+                                           float (&x)[IPT]) {
+    constexpr uint64_t T = (uint64_t)NT * IPT;
+    const uint64_t base = tile * T + (uint64_t)tid * IPT;
+    const bool aligned = ((uintptr_t)w & 15u) == 0;
+    if (aligned && base + IPT <= n) {
+        const float4* p = reinterpret_cast<const float4*>(w + base);
+#pragma unroll
+        for (int k = 0; k < IPT / 4; ++k) {
+            const float4 v = __ldg(p + k);
+            x[4 * k + 0] = v.x;
+            x[4 * k + 1] = v.y;
+            x[4 * k + 2] = v.z;
+            x[4 * k + 3] = v.w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) x[k] = (base + k < n) ? __ldg(w + base + k) : -1.0f;
+    }
 }
 
 // The IPT weights of thread `tid` in tile `tile`; items past n read as -1.
@@ -441,88 +484,100 @@ __device__ __forceinline__ u128 ldcg_E(const TileVals* src) {
 }
 
 // ---------------------------------------------------------------- pass 2: tile reduce
-// One tile per CTA: counts and sums of the three streams, plus the tile's first and last
-// heavy item. No inter-CTA waits.
-template <int IPT>
-__global__ void __launch_bounds__(kBuildThreads) tile_reduce_kernel(const float* __restrict__ w, uint64_t n,
-                                                                    const BuildHeader* hdr, TileVals* agg,
-                                                                    uint32_t* __restrict__ hmask,
-                                                                    uint32_t num_tiles) {
-    constexpr int T = kBuildThreads * IPT;
-    constexpr int NW = kBuildThreads / 32;
+// One tile per CTA: counts and sums of the three streams, the tile's first and last heavy
+// item, and its heavy mask (bit i of word i/32 <=> tile item i is heavy). No inter-CTA waits.
+constexpr int kReduceThreads = 128;
+
+__device__ __forceinline__ uint64_t warp_sum_u64(uint64_t v) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    return v;
+}
+
+template <int T>
+__global__ void __launch_bounds__(kReduceThreads) tile_reduce_kernel(const float* __restrict__ w, uint64_t n,
+                                                                     const BuildHeader* hdr, TileVals* agg,
+                                                                     uint32_t* __restrict__ hmask,
+                                                                     uint32_t num_tiles) {
+    constexpr int IPT = T / kReduceThreads;
+    constexpr int NW = kReduceThreads / 32;
+    static_assert(IPT >= 4 && IPT <= 32 && (IPT & (IPT - 1)) == 0, "items per thread");
     __shared__ uint32_t s_nl[NW], s_nh[NW], s_fh[NW], s_lh[NW];
     __shared__ uint64_t s_s[NW], s_l[NW], s_e[NW];
+    (void)num_tiles;
     if (load_relaxed(&hdr->status) != 0) return;
     const uint32_t tile = blockIdx.x;
     const ClassParams cp = class_params(hdr->W_N, hdr->R);
     float x[IPT];
-    load_tile_items<IPT>(w, n, tile, threadIdx.x, x);
-    uint32_t nL = 0, nH = 0, fh = 0xffffffffu, lh = 0xffffffffu, hbits = 0;
-    uint64_t S = 0, L = 0, E = 0;
-    const uint32_t item0 = (uint32_t)((uint64_t)tile * T + (uint64_t)threadIdx.x * IPT);
+    load_items<kReduceThreads, IPT>(w, n, tile, threadIdx.x, x);
+    const uint64_t item0 = (uint64_t)tile * T + (uint64_t)threadIdx.x * IPT;
+    uint32_t lbits = 0, sbits = 0, hbits = 0;
+    uint64_t S = 0;
 #pragma unroll
     for (int k = 0; k < IPT; ++k) {
-        if (x[k] < 0.0f) continue;
-        const ItemQ c = classify(x[k], cp);
-        if (c.kind == kHeavy) {
-            ++nH;
-            E += c.q;
-            hbits |= 1u << k;
-            if (fh == 0xffffffffu) fh = item0 + k;
-            lh = item0 + k;
-        } else {
-            ++nL;
-            if (c.kind == kSmallLight) S += c.q; else L += c.q;
-        }
+        const float wk = x[k];
+        const bool heavy = wk > cp.H1;
+        const bool light = wk >= 0.0f && !heavy;
+        const bool small = wk >= 0.0f && wk < cp.Hh;
+        const uint64_t d = small_deficit(__fmul_rn(wk, cp.R32));
+        S += small ? d : 0ull;
+        lbits |= (uint32_t)light << k;
+        sbits |= (uint32_t)small << k;
+        hbits |= (uint32_t)heavy << k;
     }
-    // heavy mask: bit i of word i/32 <=> tile item i is heavy (32 / IPT lanes per word)
+    // rare items (large lights and heavies), weights re-read from L1
+    uint64_t L = 0, E = 0;
+    for (uint32_t bits = (lbits & ~sbits) | hbits; bits; bits &= bits - 1) {
+        const int k = __ffs(bits) - 1;
+        const bool heavy = (hbits >> k) & 1u;
+        const uint64_t q = rare_q(__ldg(w + item0 + k), heavy, cp);
+        E += heavy ? q : 0ull;
+        L += heavy ? 0ull : q;
+    }
+    // heavy mask words (32 / IPT lanes per word)
     {
         constexpr int LPW = 32 / IPT;
-        uint32_t word = hbits << ((threadIdx.x % LPW) * IPT);
+        uint32_t word = (IPT == 32) ? hbits : (hbits << ((threadIdx.x % LPW) * IPT));
 #pragma unroll
         for (int d = 1; d < LPW; d <<= 1) word |= __shfl_xor_sync(0xffffffffu, word, d);
         if (threadIdx.x % LPW == 0) hmask[(uint64_t)tile * (T / 32) + threadIdx.x / LPW] = word;
     }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        nL += __shfl_xor_sync(0xffffffffu, nL, off);
-        nH += __shfl_xor_sync(0xffffffffu, nH, off);
-        S += __shfl_xor_sync(0xffffffffu, S, off);
-        L += __shfl_xor_sync(0xffffffffu, L, off);
-        E += __shfl_xor_sync(0xffffffffu, E, off);
-        fh = min(fh, __shfl_xor_sync(0xffffffffu, fh, off));
-        const uint32_t o = __shfl_xor_sync(0xffffffffu, lh, off);
-        lh = (lh == 0xffffffffu) ? o : (o == 0xffffffffu ? lh : max(lh, o));
-    }
+    const uint32_t nL = __reduce_add_sync(0xffffffffu, (uint32_t)__popc(lbits));
+    const uint32_t nH = __reduce_add_sync(0xffffffffu, (uint32_t)__popc(hbits));
+    const uint32_t fh = __reduce_min_sync(0xffffffffu, hbits ? (uint32_t)item0 + (uint32_t)(__ffs(hbits) - 1) : 0xffffffffu);
+    const uint32_t lh = __reduce_max_sync(0xffffffffu, hbits ? (uint32_t)item0 + 31u - (uint32_t)__clz(hbits) : 0u);
+    S = warp_sum_u64(S);
+    L = warp_sum_u64(L);
+    E = warp_sum_u64(E);
     const int warp = threadIdx.x >> 5;
     if ((threadIdx.x & 31) == 0) {
         s_nl[warp] = nL;
         s_nh[warp] = nH;
+        s_fh[warp] = fh;
+        s_lh[warp] = lh;
         s_s[warp] = S;
         s_l[warp] = L;
         s_e[warp] = E;
-        s_fh[warp] = fh;
-        s_lh[warp] = lh;
     }
     __syncthreads();
     if (threadIdx.x != 0) return;
-    uint32_t tl = 0, th = 0, mf = 0xffffffffu, ml = 0xffffffffu;
+    TileVals a;
+    uint32_t tl = 0, th = 0, mf = 0xffffffffu, ml = 0;
     uint64_t ts = 0, tlv = 0, te = 0;
 #pragma unroll
     for (int i = 0; i < NW; ++i) {
         tl += s_nl[i];
         th += s_nh[i];
+        mf = min(mf, s_fh[i]);
+        ml = max(ml, s_lh[i]);
         ts += s_s[i];
         tlv += s_l[i];
         te += s_e[i];
-        mf = min(mf, s_fh[i]);
-        if (s_lh[i] != 0xffffffffu) ml = (ml == 0xffffffffu) ? s_lh[i] : max(ml, s_lh[i]);
     }
-    TileVals a;
     a.nL = tl;
     a.nH = th;
     a.first_heavy = mf;
-    a.last_heavy = ml;
+    a.last_heavy = th ? ml : 0xffffffffu;
     a.S = (u128)ts << 16;
     a.L = (u128)tlv << 16;
     a.E = (u128)te << 40;
@@ -729,238 +784,242 @@ static __global__ void __launch_bounds__(kPrefixThreads) tile_prefix_kernel(Buil
     }
 }
 
-// ---------------------------------------------------------------- pass 4: split
-// Per light tile t, the range [u0, u1] of tiles whose heavies' corrected excess ends meet
-// the tile's deficit range (A_before(t), A_after(t)] (the reference's split search, at tile
-// granularity), and the item of the first heavy after tile t. links[num_tiles].next_item
-// is the last heavy item of the whole table.
-struct TileLink {
-    uint32_t u0;
-    uint32_t u1;
-    uint32_t next_item;
-    uint32_t pad;
-};
-
-__device__ __forceinline__ u128 excess_before(const TileVals* incl, uint32_t u) {
-    return u ? ldcg_E(incl + u - 1) : (u128)0;
+// ---------------------------------------------------------------- pass 4: heavy list
+// One tile per CTA: the tile's heavies in item order (expanded from its heavy mask), their
+// excess (weights gathered again), and their corrected excess ends E~ (Q64.64), written at
+// their global heavy index g: heavy_item[g], heavy_E[g]. The list is sorted by E~.
+__device__ __forceinline__ void store_u128(uint4* p, u128 v) {
+    const uint64_t lo = q_lo(v), hi = q_hi(v);
+    *p = make_uint4((uint32_t)lo, (uint32_t)(lo >> 32), (uint32_t)hi, (uint32_t)(hi >> 32));
+}
+__device__ __forceinline__ u128 load_u128(const uint4* p) {
+    const uint4 v = __ldcg(p);
+    return q_make(((uint64_t)v.w << 32) | v.z, ((uint64_t)v.y << 32) | v.x);
 }
 
-static __global__ void __launch_bounds__(256) tile_link_kernel(const BuildHeader* hdr, const TileVals* agg,
-                                                               const TileVals* incl, uint32_t num_tiles,
-                                                               TileLink* links) {
+template <int T>
+__global__ void __launch_bounds__(kReduceThreads) heavy_list_kernel(const float* __restrict__ w,
+                                                                    const BuildHeader* hdr, const TileVals* agg,
+                                                                    const TileVals* incl,
+                                                                    const uint32_t* __restrict__ hmask,
+                                                                    uint32_t num_tiles, uint32_t* heavy_item,
+                                                                    uint4* heavy_E) {
+    constexpr int NT = kReduceThreads;
+    constexpr int WPT = T / 32;
+    static_assert(WPT <= NT, "one mask word per thread");
+    __shared__ uint32_t sItem[T];
+    __shared__ uint32_t s_scan32[NT / 32];
+    __shared__ uint64_t s_scan64[NT / 32];
     if (load_relaxed(&hdr->status) != 0) return;
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t > num_tiles) return;
+    const uint32_t u = blockIdx.x;
+    const uint32_t m = __ldcg(&agg[u].nH);
+    if (m == 0) return;
+    const int tid = threadIdx.x;
+    const ClassParams cp = class_params(hdr->W_N, hdr->R);
     const TileVals tot = ldcg_tilevals(incl + num_tiles - 1);
-    if (t == num_tiles) {
-        // last heavy of the table: in the last tile whose predecessors hold fewer than nH heavies
-        uint32_t item = 0xffffffffu;
-        if (tot.nH > 0) {
-            uint32_t lo = 0, hi = num_tiles - 1;
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi + 1) >> 1;
-                if (ldcg_tilevals(incl + mid - 1).nH < tot.nH) lo = mid; else hi = mid - 1;
-            }
-            item = ldcg_tilevals(agg + lo).last_heavy;
-        }
-        TileLink l;
-        l.u0 = 0;
-        l.u1 = 0;
-        l.next_item = item;
-        l.pad = 0;
-        links[num_tiles] = l;
-        return;
-    }
     const int64_t nfix = excess_correction(deficit_line(tot), tot.E);
-    const u128 A_b = t ? deficit_line(ldcg_tilevals(incl + t - 1)) : (u128)0;
-    const TileVals me = ldcg_tilevals(incl + t);
-    const u128 A_a = deficit_line(me);
-    TileLink l;
-    l.pad = 0;
-    // largest u with corrected E_before(u) <= x (E_before(0) = 0 <= x)
-    auto last_le = [&](u128 xv) {
-        uint32_t lo = 0, hi = num_tiles - 1;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi + 1) >> 1;
-            if (q_scale_excess(excess_before(incl, mid), nfix) <= xv) lo = mid; else hi = mid - 1;
-        }
-        return lo;
-    };
-    l.u0 = (t == 0) ? 0u : last_le(A_b);
-    l.u1 = (t == num_tiles - 1) ? num_tiles - 1 : last_le(A_a);
-    // first heavy after tile t: tile v = first tile whose inclusive count exceeds g
-    const uint32_t g = me.nH;
-    l.next_item = 0xffffffffu;
-    if (g < tot.nH) {
-        uint32_t lo = t, hi = num_tiles - 1;  // last v with incl[v].nH <= g
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi + 1) >> 1;
-            if (ldcg_tilevals(incl + mid).nH <= g) lo = mid; else hi = mid - 1;
-        }
-        l.next_item = ldcg_tilevals(agg + lo + 1).first_heavy;
+    const uint32_t g0 = u ? __ldcg(&incl[u - 1].nH) : 0u;
+    const u128 Eb = u ? ldcg_E(incl + u - 1) : (u128)0;
+    {
+        const uint32_t word = tid < WPT ? __ldg(hmask + (uint64_t)u * WPT + tid) : 0u;
+        uint32_t ctot;
+        uint32_t o = block_scan1<NT, uint32_t>((uint32_t)__popc(word), s_scan32, ctot);
+        const uint32_t ibase = u * (uint32_t)T + (uint32_t)tid * 32u;
+        for (uint32_t b = word; b; b &= b - 1) sItem[o++] = ibase + (uint32_t)(__ffs(b) - 1);
     }
-    links[t] = l;
+    __syncthreads();
+    const uint32_t per = (m + NT - 1) / NT;
+    const uint32_t j0 = min(m, (uint32_t)tid * per), j1 = min(m, j0 + per);
+    uint64_t hs = 0;
+    for (uint32_t j = j0; j < j1; ++j) hs += rare_q(__ldg(w + sItem[j]), true, cp);
+    uint64_t htot;
+    uint64_t er = block_scan1<NT, uint64_t>(hs, s_scan64, htot);
+    for (uint32_t j = j0; j < j1; ++j) {
+        er += rare_q(__ldg(w + sItem[j]), true, cp);  // the weight again, from L1
+        heavy_item[g0 + j] = sItem[j];
+        store_u128(heavy_E + g0 + j, q_scale_excess(Eb + ((u128)er << 40), nfix));
+    }
 }
 
-// ---------------------------------------------------------------- pass 5: pack
-__device__ __forceinline__ TileVals incl_before(const TileVals* incl, uint32_t u) {
-    return u ? ldcg_tilevals(incl + u - 1) : tv_zero();
+// ---------------------------------------------------------------- pass 5: split
+// Per tile boundary b (0..num_tiles), bound[b] = #{heavies with E~ <= A_before(b)}, by a
+// binary search of the heavy list (the reference's split search, at tile granularity);
+// bound[0] = 0 and bound[num_tiles] = nH, so light tile t owns heavies [bound[t], bound[t+1]).
+static __global__ void __launch_bounds__(256) tile_link_kernel(const BuildHeader* hdr, const TileVals* incl,
+                                                               uint32_t num_tiles, const uint4* heavy_E,
+                                                               uint32_t* bound) {
+    if (load_relaxed(&hdr->status) != 0) return;
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b > num_tiles) return;
+    const uint32_t nH = __ldcg(&incl[num_tiles - 1].nH);
+    uint32_t g;
+    if (b == 0) {
+        g = 0;
+    } else if (b == num_tiles) {
+        g = nH;
+    } else {
+        const u128 X = deficit_line(ldcg_tilevals(incl + b - 1));
+        uint32_t lo = 0, hi = nH;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (load_u128(heavy_E + mid) <= X) lo = mid + 1; else hi = mid;
+        }
+        g = lo;
+    }
+    bound[b] = g;
 }
 
-// Shared memory of the pack kernel for T items per tile: light keys (u64), heavy keys (u64),
-// heavy local excess (u64), heavy items (u32), light aliases (u32), heavy ranks (u32).
+// ---------------------------------------------------------------- pass 6: pack
+// Heavies per chunk for T items per tile (the own-tile phase keeps a u64 per tile item in
+// the chunk arrays, so 12 * C >= 8 * T).
+__host__ __device__ constexpr int pack_chunk(int T) { return (2 * T) / 3 + 64 > 1024 ? (2 * T) / 3 + 64 : 1024; }
+
+// Shared memory of the pack kernel, in this order: light keys (u64 x T; the staged rows at
+// the end), light rank counts (u32 x T), heavy keys (u64 x C), heavy items (u32 x C).
 __host__ __device__ constexpr size_t pack_smem_bytes(int T) {
-    return (size_t)T * (3 * sizeof(uint64_t) + 3 * sizeof(uint32_t));
+    return (size_t)T * (sizeof(uint64_t) + sizeof(uint32_t)) + (size_t)pack_chunk(T) * (sizeof(uint64_t) + sizeof(uint32_t));
 }
 
-// One light tile per CTA. Its lights' deficit-interval starts go to shared memory as keys
-// in the tile's frame (A - A_before(t), Q16.48). The heavies of the partner tiles
-// [u0, u1] are taken one tile at a time from the tile's heavy mask (written by the reduce
-// pass): only the heavies' weights are gathered (from L2), so a partner costs work in
-// proportion to its heavies. Their corrected excess ends become keys in the same frame:
-// key = ceil((E~ - A_before(t)) / 2^-48), clamped, so that key(light) < key(heavy) exactly
-// when A < E~. A merge path over the still unresolved lights and the chunk's heavies gives
-// every thread an equal slice of the merged order; the slice only records ranks: a light's
-// alias is the heavy at its rank (J(i) = #{E~ <= A_i}), a heavy's rank is the light after
-// it (I(j) = #{A < E~_j}). Owned heavies then write their rows from those ranks, and the
-// last heavy's rank is the number of lights resolved so far.
+// Staged row position of tile item i (XOR swizzle of the IPT items of a thread, so that
+// neither the per-thread writes nor the per-warp reads of the stage conflict on banks).
 template <int IPT>
-__global__ void __launch_bounds__(kBuildThreads, (IPT <= 8 ? 3 : 1)) split_pack_kernel(const float* __restrict__ w,
-                                                                                     uint64_t n,
-                                                                                     const BuildHeader* hdr,
-                                                                                     const TileVals* incl,
-                                                                                     const TileLink* links,
-                                                                                     const uint32_t* __restrict__ hmask,
-                                                                                     uint32_t num_tiles,
-                                                                                     wrs_alias_row* __restrict__ table) {
-    constexpr int T = kBuildThreads * IPT;
-    constexpr int WPT = T / 32;  // heavy-mask words per tile
-    static_assert(WPT <= kBuildThreads, "one mask word per thread");
+__device__ __forceinline__ uint32_t stage_pos(uint32_t i) {
+    return (i & ~(uint32_t)(IPT - 1)) | ((i ^ (i / IPT)) & (uint32_t)(IPT - 1));
+}
+
+// One light tile per CTA of NT threads, IPT consecutive items per thread.
+//  (1) Own tile: every light's deficit-interval start goes to shared memory as a key in
+//      the tile's frame, key = (A - A_before(t)) / 2^-48 (exact), with large lights dithered.
+//  (2) Heavies [bound[t], bound[t+1]] of the heavy list (the owned ones and the next one),
+//      in chunks of at most C. A heavy's key in the same frame is ceil((E~ - A_before) /
+//      2^-48) clamped to [0, 2^64 - 1], so key(light) < key(heavy) exactly when A < E~. Its
+//      rank r = #{lights with key < its key} (I(j) = #{A < E~_j}) gives an owned heavy's row,
+//      r = 1 + E~ - A_r, aliasing the next heavy. A light's alias is the first heavy whose key
+//      exceeds its own (J(i) = #{E~ <= A_i}): the number of the chunk's heavies of rank <= i,
+//      an inclusive prefix sum over a histogram of the ranks, valid for the lights from the
+//      previous chunk's last rank on whose count stays inside the chunk.
+//  (3) Light rows, staged in shared memory and written out coalesced (the heavies' rows of
+//      this tile belong to the tiles that own them).
+template <int NT, int IPT>
+__global__ void __launch_bounds__(NT) split_pack_kernel(const float* __restrict__ w, uint64_t n,
+                                                        const BuildHeader* hdr, const TileVals* incl,
+                                                        const uint32_t* __restrict__ bound,
+                                                        const uint32_t* __restrict__ heavy_item,
+                                                        const uint4* __restrict__ heavy_E, uint32_t num_tiles,
+                                                        wrs_alias_row* __restrict__ table) {
+    constexpr int T = NT * IPT;
+    constexpr int C = pack_chunk(T);
+    static_assert(12 * C >= 8 * T, "own-tile slots live in the chunk arrays");
+    static_assert(IPT >= 4 && IPT <= 32 && (IPT & (IPT - 1)) == 0, "items per thread");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint64_t* sLkey = reinterpret_cast<uint64_t*>(smem_raw);
-    uint64_t* sHkey = sLkey + T;
-    uint64_t* sHe = sHkey + T;
-    uint32_t* sHitem = reinterpret_cast<uint32_t*>(sHe + T);
-    uint32_t* sLalias = sHitem + T;
-    uint32_t* sHrank = sLalias + T;
-    __shared__ ScanVal s_warp[kBuildThreads / 32 + 1];
-    __shared__ uint32_t s_own_lo, s_own_hi;
+    uint32_t* sCnt = reinterpret_cast<uint32_t*>(sLkey + T);
+    uint64_t* sHkey = reinterpret_cast<uint64_t*>(sCnt + T);  // 16-byte aligned: T % 4 == 0
+    uint32_t* sHitem = reinterpret_cast<uint32_t*>(sHkey + C);
+    uint64_t* sSlotQ = sHkey;  // own-tile phase: per item slot, over sHkey and sHitem (8T <= 12C bytes)
+    float* sSlotP = reinterpret_cast<float*>(sCnt);  // own-tile phase: per item slot
+    uint64_t* sStage = sLkey;                        // row phase: staged rows
+    __shared__ Scan3 s_scan3[NT / 32];
+    __shared__ uint32_t s_scan32[NT / 32];
+    __shared__ uint32_t s_r0, s_pend_item;
+    __shared__ float s_pend_prob;
 
     if (load_relaxed(&hdr->status) != 0) return;
+    const int tid = threadIdx.x;
     const uint32_t tile = num_tiles - 1 - blockIdx.x;  // descending: the previous passes ended at
                                                        // the last tiles, still in L2
     const ClassParams cp = class_params(hdr->W_N, hdr->R);
-    const TileLink link = links[tile];
-    const TileVals tot = ldcg_tilevals(incl + num_tiles - 1);
-    const TileVals before = incl_before(incl, tile);
-    const TileVals after = ldcg_tilevals(incl + tile);
+    const uint32_t nH = __ldcg(&incl[num_tiles - 1].nH);
+    const TileVals before = tile ? ldcg_tilevals(incl + tile - 1) : tv_zero();
     const u128 A_before = deficit_line(before);
-    const u128 A_after = deficit_line(after);
-    const int64_t nfix = excess_correction(deficit_line(tot), tot.E);
-    const bool lo_inf = (tile == 0);
-    const bool hi_inf = (tile == num_tiles - 1);
-    const uint32_t nH_tot = tot.nH;
+    const u128 A_after = deficit_line(ldcg_tilevals(incl + tile));
 
-    // ---- own tile: light deficit intervals
+    // ---- (1) own tile
     float x[IPT];
-    load_tile_items<IPT>(w, n, tile, threadIdx.x, x);
-    const uint32_t item0 = (uint32_t)((uint64_t)tile * T + (uint64_t)threadIdx.x * IPT);
+    load_items<NT, IPT>(w, n, tile, tid, x);
+    const uint32_t item0 = (uint32_t)((uint64_t)tile * T + (uint64_t)tid * IPT);
     float pk[IPT];
-    ScanVal v = sv_zero();
-    uint32_t lmask = 0, bigmask = 0;  // bit k: item k is a light / a large light
+    uint32_t lbits = 0, gbits = 0;  // bit k: item k is a light / a large light
+    uint64_t asum = 0;
 #pragma unroll
     for (int k = 0; k < IPT; ++k) {
-        pk[k] = 0.0f;
-        if (x[k] < 0.0f) continue;
-        const ItemQ c = classify(x[k], cp);
-        if (c.kind == kHeavy) continue;
-        lmask |= 1u << k;
-        v.c += 1;
-        if (c.kind == kSmallLight) {
-            pk[k] = c.p;
-            v.a += c.q;
-        } else {
-            bigmask |= 1u << k;
-            v.b += c.q;
+        const float wk = x[k];
+        const bool small = wk >= 0.0f && wk < cp.Hh;
+        const float p = __fmul_rn(wk, cp.R32);
+        pk[k] = p;
+        asum += small ? small_deficit(p) : 0ull;
+        lbits |= (uint32_t)(wk >= 0.0f && !(wk > cp.H1)) << k;
+        gbits |= (uint32_t)(wk >= cp.Hh && !(wk > cp.H1)) << k;
+    }
+    uint64_t lsum = 0;
+    for (uint32_t bits = gbits; bits; bits &= bits - 1) {
+        const int k = __ffs(bits) - 1;
+        const uint64_t q = rare_q(__ldg(w + item0 + k), false, cp);
+        sSlotQ[tid * IPT + k] = q;
+        lsum += q;
+    }
+    const uint32_t nl = (uint32_t)__popc(lbits);
+    Scan3 tot_l;
+    const Scan3 ex = block_scan3<NT>(Scan3{nl, asum, lsum}, s_scan3, tot_l);
+    const uint32_t nLt = tot_l.c;
+    const uint32_t l0 = ex.c;  // this thread's lights are l0 .. lend - 1 in tile light order
+    const uint32_t lend = l0 + nl;
+    const Dither dth = make_dither(before.L);
+    const uint64_t D0 = dither_at(dth, ex.b);
+    {
+        uint64_t lr = ex.b, dprev = D0;
+        for (uint32_t bits = gbits; bits; bits &= bits - 1) {
+            const int slot = tid * IPT + __ffs(bits) - 1;
+            lr += sSlotQ[slot];
+            const uint64_t d1 = dither_at(dth, lr);
+            sSlotP[slot] = dithered_prob(d1 - dprev);
+            sSlotQ[slot] = d1;
+            dprev = d1;
         }
     }
-    ScanVal tot_l;
-    const ScanVal ex = cta_exclusive_scan<kBuildThreads>(v, s_warp, &tot_l);
-    const uint32_t nLt = tot_l.c;
-    const uint32_t l0 = ex.c;  // this thread's lights are l0 .. l0 + popc(lmask) - 1
     {
+        uint64_t sr = ex.a, D = D0;
         uint32_t li = l0;
-        uint64_t sr = ex.a;
-        u128 Lg = before.L + ((u128)ex.b << 16);
-        const u128 rb = q_round24(before.L);
-        uint64_t dith = (uint64_t)((q_round24(Lg) - rb) >> 16);
 #pragma unroll
         for (int k = 0; k < IPT; ++k) {
-            if (!(lmask >> k & 1u)) continue;
-            sLalias[li] = 0xffffffffu;
-            sLkey[li++] = sr + dith;
-            if (bigmask >> k & 1u) {
-                const uint64_t q = classify(x[k], cp).q;
-                pk[k] = large_light_prob(Lg, q);
-                Lg += (u128)q << 16;
-                dith = (uint64_t)((q_round24(Lg) - rb) >> 16);
-            } else {
-                sr += (1ull << 48) - fix48f(__float_as_uint(pk[k]));
+            const bool light = (lbits >> k) & 1u;
+            if (light) sLkey[li] = sr + D;
+            li += light ? 1u : 0u;
+            sr += (light && !((gbits >> k) & 1u)) ? small_deficit(pk[k]) : 0ull;
+            if ((gbits >> k) & 1u) {
+                D = sSlotQ[tid * IPT + k];
+                pk[k] = sSlotP[tid * IPT + k];
             }
         }
     }
-    __syncthreads();
+    if (tid == 0) {
+        s_r0 = 0;
+        s_pend_item = 0xffffffffu;
+    }
+    __syncthreads();  // keys complete; the slot arrays are free again
 
-    if (nH_tot == 0) {
+    uint32_t al[IPT];
+    if (nH == 0) {
         // no heavy item anywhere: every row keeps itself
 #pragma unroll
-        for (int k = 0; k < IPT; ++k) {
-            if (!(lmask >> k & 1u)) continue;
-            wrs_alias_row r;
-            r.prob = pk[k];
-            r.alias = item0 + k;
-            table[item0 + k] = r;
-        }
-        return;
-    }
-    if (!lo_inf && !hi_inf && nLt == 0) return;  // empty ownership interval, no lights
-
-    uint32_t r0 = 0;  // lights [0, r0) are resolved
-    uint32_t last_item = 0xffffffffu;
-    for (uint32_t u = link.u0; u <= link.u1; ++u) {
-        const uint32_t nh_b = u ? __ldcg(&incl[u - 1].nH) : 0u;
-        const uint32_t m = __ldcg(&incl[u].nH) - nh_b;
-        if (m == 0) continue;
-        const u128 E_b = excess_before(incl, u);
-        // expand the heavy mask of tile u into the heavies' items, in order
-        {
-            const uint32_t word = threadIdx.x < WPT ? __ldg(hmask + (uint64_t)u * WPT + threadIdx.x) : 0u;
-            ScanVal wv = sv_zero();
-            wv.c = __popc(word);
-            ScanVal wt;
-            const ScanVal wex = cta_exclusive_scan<kBuildThreads>(wv, s_warp, &wt);
-            uint32_t o = wex.c;
-            const uint32_t base = u * (uint32_t)T + threadIdx.x * 32u;
-            for (uint32_t bits = word; bits; bits &= bits - 1) sHitem[o++] = base + (uint32_t)(__ffs(bits) - 1);
-        }
-        if (threadIdx.x == 0) {
-            s_own_lo = 0xffffffffu;
-            s_own_hi = 0;
-        }
-        __syncthreads();
-        // excess of each heavy (weights gathered from L2), contiguous blocks per thread
-        const uint32_t per = (m + kBuildThreads - 1) / kBuildThreads;
-        const uint32_t j0 = min(m, threadIdx.x * per), j1 = min(m, j0 + per);
-        ScanVal hv = sv_zero();
-        for (uint32_t j = j0; j < j1; ++j) hv.a += heavy_excess(__ldg(w + sHitem[j]), cp);
-        ScanVal tot_h;
-        const ScanVal hex = cta_exclusive_scan<kBuildThreads>(hv, s_warp, &tot_h);
-        {
-            uint64_t er = hex.a;
-            uint32_t own_lo = 0xffffffffu, own_hi = 0;
-            for (uint32_t j = j0; j < j1; ++j) {
-                er += heavy_excess(__ldg(w + sHitem[j]), cp);
-                const u128 Et = q_scale_excess(E_b + ((u128)er << 40), nfix);
+        for (int k = 0; k < IPT; ++k) al[k] = item0 + k;
+    } else {
+        // ---- (2) owned heavies and the next one, chunk by chunk
+        const uint32_t last_heavy = __ldg(heavy_item + nH - 1);
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) al[k] = last_heavy;  // lights past every heavy's excess
+                                                            // (rounding residue only)
+        for (uint32_t li = l0; li < lend; ++li) sCnt[li] = 0u;
+        const uint32_t g_lo = bound[tile], g_hi = bound[tile + 1];
+        const uint32_t g_end = min(g_hi + 1u, nH);
+        for (uint32_t cs = g_lo; cs < g_end; cs += (uint32_t)C) {
+            const uint32_t m = min((uint32_t)C, g_end - cs);
+            // state left by the previous chunk (rewritten below only after the next barrier)
+            const uint32_t r0 = s_r0;  // lights below r0 already have their alias
+            const uint32_t pend = s_pend_item;
+            const float pend_prob = s_pend_prob;
+            for (uint32_t j = tid; j < m; j += NT) {
+                const u128 Et = load_u128(heavy_E + cs + j);
                 uint64_t key;
                 if (Et <= A_before) {
                     key = 0;
@@ -968,75 +1027,87 @@ __global__ void __launch_bounds__(kBuildThreads, (IPT <= 8 ? 3 : 1)) split_pack_
                     const u128 d = Et - A_before + 0xffff;
                     key = (q_hi(d) >> 16) ? ~0ull : (uint64_t)(d >> 16);
                 }
-                if ((lo_inf || Et > A_before) && (hi_inf || Et <= A_after)) {
-                    own_lo = min(own_lo, j);
-                    own_hi = j + 1;
-                }
                 sHkey[j] = key;
-                sHe[j] = er;
+                sHitem[j] = __ldg(heavy_item + cs + j);
             }
-            if (own_hi > 0) {
-                atomicMin(&s_own_lo, own_lo);
-                atomicMax(&s_own_hi, own_hi);
+            __syncthreads();
+            // the previous chunk's last owned heavy aliases this chunk's first
+            if (tid == 0 && pend != 0xffffffffu) {
+                wrs_alias_row r;
+                r.prob = pend_prob;
+                r.alias = sHitem[0];
+                table[pend] = r;
             }
-        }
-        __syncthreads();
-        // merge path over lights [r0, nLt) and heavies [0, m); a light precedes a heavy iff
-        // its key is below the heavy's. Each thread records ranks for an equal slice.
-        {
-            const uint32_t nl = nLt - r0;
-            const uint32_t total = nl + m;
-            const uint32_t d0 = (uint32_t)(((uint64_t)total * threadIdx.x) / kBuildThreads);
-            const uint32_t d1 = (uint32_t)(((uint64_t)total * (threadIdx.x + 1)) / kBuildThreads);
-            uint32_t lo = d0 > m ? d0 - m : 0u;
-            uint32_t hi = d0 < nl ? d0 : nl;
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi + 1) >> 1;
-                if (sLkey[r0 + mid - 1] < sHkey[d0 - mid]) lo = mid; else hi = mid - 1;
-            }
-            uint32_t a = lo, b = d0 - lo;
-            for (uint32_t d = d0; d < d1; ++d) {
-                const bool take_light = a < nl && (b >= m || sLkey[r0 + a] < sHkey[b]);
-                if (take_light) {
-                    if (b < m) sLalias[r0 + a] = sHitem[b];
-                    ++a;
-                } else {
-                    sHrank[b] = r0 + a;
-                    ++b;
+            // ranks: histogram, and the rows of the owned heavies
+            for (uint32_t j = tid; j < m; j += NT) {
+                const uint64_t kh = sHkey[j];
+                uint32_t lo = r0, hi = nLt;  // first light whose key is not below kh
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (sLkey[mid] < kh) lo = mid + 1; else hi = mid;
+                }
+                if (lo < nLt) atomicAdd(&sCnt[lo], 1u);
+                const uint32_t g = cs + j;
+                if (j + 1 == m) {
+                    s_r0 = lo;
+                    s_pend_item = 0xffffffffu;
+                }
+                if (g < g_hi) {
+                    const u128 Et = load_u128(heavy_E + g);
+                    const u128 A_next = (lo < nLt) ? A_before + ((u128)sLkey[lo] << 16) : A_after;
+                    const float prob = heavy_row_prob(q_one() + Et - A_next);
+                    if (j + 1 < m) {
+                        wrs_alias_row r;
+                        r.prob = prob;
+                        r.alias = sHitem[j + 1];
+                        table[sHitem[j]] = r;
+                    } else if (g + 1 < nH) {
+                        s_pend_item = sHitem[j];  // its alias opens the next chunk
+                        s_pend_prob = prob;
+                    } else {
+                        wrs_alias_row r;  // the last heavy of the table keeps itself
+                        r.prob = prob;
+                        r.alias = sHitem[j];
+                        table[sHitem[j]] = r;
+                    }
                 }
             }
+            __syncthreads();
+            // lights: alias index = number of the chunk's heavies with rank <= light index
+            uint32_t csum = 0;
+            for (uint32_t li = max(l0, r0); li < lend; ++li) csum += sCnt[li];
+            uint32_t ctot;
+            uint32_t run = block_scan1<NT, uint32_t>(csum, s_scan32, ctot);
+            if (lend > r0) {
+                uint32_t li = l0;
+#pragma unroll
+                for (int k = 0; k < IPT; ++k) {
+                    const bool light = (lbits >> k) & 1u;
+                    if (light && li >= r0) {
+                        run += sCnt[li];
+                        sCnt[li] = 0u;
+                        if (run < m) al[k] = sHitem[run];
+                    }
+                    li += light ? 1u : 0u;
+                }
+            }
+            __syncthreads();  // the next chunk overwrites the chunk arrays
         }
-        __syncthreads();
-        // owned heavies [own_lo, own_hi): rows from the ranks
-        const uint32_t olo = s_own_lo, ohi = s_own_hi;
-        const uint32_t next_after = links[u].next_item;
-        for (uint32_t j = olo + threadIdx.x; j < ohi; j += kBuildThreads) {
-            const uint32_t rk = sHrank[j];
-            const u128 Et = q_scale_excess(E_b + ((u128)sHe[j] << 40), nfix);
-            const u128 A_next = (rk < nLt) ? A_before + ((u128)sLkey[rk] << 16) : A_after;
-            uint32_t al = (j + 1 < m) ? sHitem[j + 1] : next_after;
-            if (al == 0xffffffffu) al = sHitem[j];
-            wrs_alias_row row;
-            row.prob = heavy_row_prob(q_one() + Et - A_next);
-            row.alias = al;
-            table[sHitem[j]] = row;
-        }
-        // lights before the chunk's last heavy are resolved
-        r0 = sHrank[m - 1];
-        last_item = sHitem[m - 1];
-        __syncthreads();
     }
-    // lights past every heavy's excess (rounding residue only) alias the last heavy
-    if (last_item == 0xffffffffu) last_item = links[num_tiles].next_item;
-    uint32_t li = l0;
+
+    // ---- (3) light rows: staged, then coalesced stores (heavy positions are skipped)
 #pragma unroll
     for (int k = 0; k < IPT; ++k) {
-        if (!(lmask >> k & 1u)) continue;
-        const uint32_t al = sLalias[li++];
-        wrs_alias_row r;
-        r.prob = pk[k];
-        r.alias = al != 0xffffffffu ? al : last_item;
-        table[item0 + k] = r;
+        const bool light = (lbits >> k) & 1u;
+        const uint64_t row = light ? (((uint64_t)al[k] << 32) | __float_as_uint(pk[k])) : ~0ull;
+        sStage[stage_pos<IPT>((uint32_t)(tid * IPT + k))] = row;
+    }
+    __syncthreads();
+    uint64_t* out = reinterpret_cast<uint64_t*>(table) + (uint64_t)tile * T;
+    const uint32_t cnt = (uint32_t)min((uint64_t)T, n - (uint64_t)tile * T);
+    for (uint32_t i = tid; i < cnt; i += NT) {
+        const uint64_t row = sStage[stage_pos<IPT>(i)];
+        if (row != ~0ull) out[i] = row;
     }
 }
 

@@ -4,7 +4,7 @@
 // need a table: code running under an allocator that forbids it, plugins that must not
 // touch the host process's memory pools, or paths that may not block on an allocation.
 // wrs_alias_build_f32_static_scratch builds tables of up to kStaticMaxItems items with
-// its scratch in a fixed device array of kStaticScratchBytes (2 MiB) that lives in this
+// its scratch in a fixed device array of kStaticScratchBytes (8 MiB) that lives in this
 // library: every GPU that loads the library holds that array until the process exits.
 // The caller still passes the weights, the table and the optional W output.
 //
@@ -23,8 +23,8 @@
 
 namespace {
 
-constexpr int64_t kStaticMaxItems = (int64_t)1 << 22;  // 4,194,304 items
-constexpr size_t kStaticScratchBytes = (size_t)2 << 20;  // 2 MiB (>= the build's need at the limit, any tile size)
+constexpr int64_t kStaticMaxItems = (int64_t)1 << 18;  // 262,144 items
+constexpr size_t kStaticScratchBytes = (size_t)8 << 20;  // 8 MiB (>= the build's need at the limit, any tile size)
 
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 

@@ -145,7 +145,7 @@ def alias_build(w, table, scratch, opts: Optional[BuildOpts] = None, W_out=None,
 
 
 def alias_build_static_scratch(w, table, opts: Optional[BuildOpts] = None, W_out=None, stream=None) -> int:
-    """Builds without any caller scratch (n <= 2^22): for callers that cannot allocate device
+    """Builds without any caller scratch (n <= 2^18): for callers that cannot allocate device
     memory; the scratch is a fixed array inside the library, shared by all calls on a device."""
     return lib().wrs_alias_build_f32_static_scratch(_ptr(w), w.numel(), ctypes.byref(opts) if opts else None,
                                                     _ptr(table), _ptr(W_out), _stream(stream))

@@ -121,8 +121,8 @@ WRS_API wrs_status wrs_alias_build_f32(const float* d_w, int64_t n, const wrs_bu
 /* The same build for callers that cannot allocate device memory (code under an allocator
  * that forbids cudaMalloc, plugins that must not touch the host process's memory pools,
  * paths that may not block on an allocation). No counterpart in the reference. Its scratch
- * is a fixed 2 MiB device array inside this library (held on every GPU that loads it until
- * the process exits), so it takes n <= 4,194,304 (2^22) items and rejects larger n with
+ * is a fixed 8 MiB device array inside this library (held on every GPU that loads it until
+ * the process exits), so it takes n <= 262,144 (2^18) items and rejects larger n with
  * WRS_ERR_INVALID_ARGUMENT. It calls no allocating routine. The first call on each device
  * looks up the array's device address (make it before any stream capture). All calls on a
  * device share the array, so calls that overlap on the GPU race: serialise them. Device-side

@@ -464,31 +464,14 @@ static inline float large_light_prob(u128 Li, uint64_t d48) {
     return (float)(16777216u - units) * 5.9604644775390625e-8f;
 }
 
-/* round(x * 2^fb), ties away from zero, from the bits of x >= 0 (subnormals give 0). */
-static inline uint64_t fixq(double x, int fb) {
-    uint64_t b = dbits(x);
-    int e = (int)((b >> 52) & 0x7ff);
-    if (e == 0) return 0;
-    uint64_t m = (b & 0xfffffffffffffull) | 0x10000000000000ull;
-    int s = e - 1075 + fb;
-    if (s >= 0) return m << s;
-    if (s < -54) return 0;
-    return (m + (1ull << (-s - 1))) >> (-s);
-}
+/* round(x * 2^fb) for x >= 0, to nearest with ties to even: x * 2^fb is exact in FP64
+ * and llrint rounds in the default (nearest-even) mode. */
+static inline uint64_t fixq(double x, int fb) { return (uint64_t)llrint(ldexp(x, fb)); }
 
 enum { K_SMALL = 1, K_LARGE = 2, K_HEAVY = 3 };
 
-/* round(p * 2^48), ties away from zero, from the bits of a float p >= 0. */
-static inline uint64_t fix48f(float p) {
-    uint32_t b = f_bits(p);
-    int e = (int)((b >> 23) & 0xff);
-    if (e == 0) return 0;
-    uint64_t m = (b & 0x7fffffu) | 0x800000u;
-    int s = e - 102;
-    if (s >= 0) return m << s;
-    if (s < -25) return 0;
-    return (m + (1ull << (-s - 1))) >> (-s);
-}
+/* round(p * 2^48) for a float p in [0, 1/2), ties to even (p * 2^48 is exact). */
+static inline uint64_t fix48f(float p) { return (uint64_t)llrint(ldexp((double)p, 48)); }
 
 typedef struct {
     double R;

@@ -14,7 +14,7 @@ import wrs
 
 pytestmark = pytest.mark.gpu
 
-MAX_ITEMS = 1 << 22
+MAX_ITEMS = 1 << 18
 
 
 def weights(kind, n, seed):
