@@ -102,7 +102,7 @@ struct BuildLayout {
     uint64_t num_blocks;
     TileVals* agg;
     TileVals* incl;
-    uint32_t* bound;
+    TileStart* starts;
     uint32_t* hmask;
     uint32_t* heavy_item;
     uint4* heavy_E;
@@ -118,7 +118,7 @@ BuildLayout carve_build(void* scratch, uint64_t n, uint64_t num_tiles, uint64_t 
     L.blocks = c.take<BlockWord>(L.num_blocks);
     L.agg = c.take<TileVals>(num_tiles);
     L.incl = c.take<TileVals>(num_tiles);
-    L.bound = c.take<uint32_t>(num_tiles + 1);
+    L.starts = c.take<TileStart>(num_tiles + 1);
     L.hmask = c.take<uint32_t>(num_tiles * (tile_items / 32));
     L.heavy_item = c.take<uint32_t>(n);
     L.heavy_E = c.take<uint4>(n);
@@ -141,17 +141,17 @@ wrs_status launch_build(const float* d_w, uint64_t n, uint32_t method, wrs_alias
                                                                               (uint32_t)num_tiles);
     tile_prefix_kernel<<<(uint32_t)L.num_blocks, kPrefixThreads, 0, stream>>>(L.hdr, L.agg, L.incl, L.blocks,
                                                                                (uint32_t)num_tiles);
-    heavy_list_kernel<T><<<(uint32_t)num_tiles, kReduceThreads, 0, stream>>>(d_w, L.hdr, L.agg, L.incl, L.hmask,
+    heavy_list_kernel<T><<<(uint32_t)((num_tiles + heavy_warps(T) - 1) / heavy_warps(T)), 32 * heavy_warps(T), 0, stream>>>(d_w, L.hdr, L.agg, L.incl, L.hmask,
                                                                              (uint32_t)num_tiles, L.heavy_item,
                                                                              L.heavy_E);
     tile_link_kernel<<<(uint32_t)((num_tiles + 1 + 255) / 256), 256, 0, stream>>>(L.hdr, L.incl, (uint32_t)num_tiles,
-                                                                                  L.heavy_E, L.bound);
+                                                                                  L.heavy_E, L.starts);
     {
         const size_t smem = pack_smem_bytes(T);
         e = cudaFuncSetAttribute(split_pack_kernel<NT, IPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return WRS_ERR_CUDA;
         split_pack_kernel<NT, IPT><<<(uint32_t)num_tiles, NT, smem, stream>>>(
-            d_w, n, L.hdr, L.incl, L.bound, L.heavy_item, L.heavy_E, (uint32_t)num_tiles, d_table);
+            d_w, n, L.hdr, L.incl, L.starts, L.heavy_item, L.heavy_E, (uint32_t)num_tiles, d_table);
     }
     return launch_status();
 }

@@ -98,7 +98,12 @@ struct __align__(16) BuildHeader {
     double R;           // 1 / W_N
     uint64_t a_size;    // rejection: |A|
     uint64_t big_count; // rejection: number of deferred large items
-    uint64_t pad[8];
+    float R32;          // class thresholds (ClassParams), set with W
+    float H1;
+    float Hh;
+    uint32_t pad0;
+    int64_t nfix;       // excess correction, set with the tile prefixes
+    uint64_t pad[5];
 };
 static_assert(sizeof(BuildHeader) == 128, "header layout");
 
@@ -135,6 +140,20 @@ __device__ __forceinline__ ClassParams class_params(const double W_N, const doub
     c.Hh = __double2float_ru(__dmul_rn(0.5, W_N));
     return c;
 }
+
+// The class thresholds of this build, as the weight-total pass stored them in the header.
+// Passes after that one read header fields through the read-only (L1) path: every warp of
+// every CTA reads them, and an L2-only load would send all of those reads to one L2 line.
+__device__ __forceinline__ ClassParams load_class_params(const BuildHeader* hdr) {
+    ClassParams c;
+    c.R = __ldg(&hdr->R);
+    c.R32 = __ldg(&hdr->R32);
+    c.H1 = __ldg(&hdr->H1);
+    c.Hh = __ldg(&hdr->Hh);
+    return c;
+}
+// Status left by the earlier passes of this build (set only before this kernel started).
+__device__ __forceinline__ uint32_t earlier_status(const BuildHeader* hdr) { return __ldg(&hdr->status); }
 
 constexpr uint64_t kOneQ48 = 1ull << 48;
 
@@ -328,6 +347,10 @@ __global__ void __launch_bounds__(BLOCK) wsum_kernel(const float* __restrict__ w
         const double W_N = r.hi / (double)n;
         hdr->W_N = W_N;
         hdr->R = 1.0 / W_N;
+        const ClassParams cp = class_params(W_N, 1.0 / W_N);
+        hdr->R32 = cp.R32;
+        hdr->H1 = cp.H1;
+        hdr->Hh = cp.Hh;
         if (W_out) *W_out = r.hi;
         if (!(r.hi > 0.0) || isinf(r.hi)) record_status(&hdr->status, isinf(r.hi) ? kErrInvalidWeight : kErrZeroTotal);
         hdr->wsum_ticket = 0u;
@@ -505,11 +528,11 @@ __global__ void __launch_bounds__(kReduceThreads) tile_reduce_kernel(const float
     __shared__ uint32_t s_nl[NW], s_nh[NW], s_fh[NW], s_lh[NW];
     __shared__ uint64_t s_s[NW], s_l[NW], s_e[NW];
     (void)num_tiles;
-    if (load_relaxed(&hdr->status) != 0) return;
     const uint32_t tile = blockIdx.x;
-    const ClassParams cp = class_params(hdr->W_N, hdr->R);
     float x[IPT];
-    load_items<kReduceThreads, IPT>(w, n, tile, threadIdx.x, x);
+    load_items<kReduceThreads, IPT>(w, n, tile, threadIdx.x, x);  // first: independent of the header
+    if (earlier_status(hdr) != 0) return;
+    const ClassParams cp = load_class_params(hdr);
     const uint64_t item0 = (uint64_t)tile * T + (uint64_t)threadIdx.x * IPT;
     uint32_t lbits = 0, sbits = 0, hbits = 0;
     uint64_t S = 0;
@@ -781,11 +804,12 @@ static __global__ void __launch_bounds__(kPrefixThreads) tile_prefix_kernel(Buil
         o.L = v.L;
         o.E = v.E;
         incl[t0 + k] = o;
+        if (t0 + k == num_tiles - 1) hdr->nfix = excess_correction(v.S + q_round24(v.L), v.E);
     }
 }
 
 // ---------------------------------------------------------------- pass 4: heavy list
-// One tile per CTA: the tile's heavies in item order (expanded from its heavy mask), their
+// One tile per warp: the tile's heavies in item order (expanded from its heavy mask), their
 // excess (weights gathered again), and their corrected excess ends E~ (Q64.64), written at
 // their global heavy index g: heavy_item[g], heavy_E[g]. The list is sorted by E~.
 __device__ __forceinline__ void store_u128(uint4* p, u128 v) {
@@ -797,68 +821,117 @@ __device__ __forceinline__ u128 load_u128(const uint4* p) {
     return q_make(((uint64_t)v.w << 32) | v.z, ((uint64_t)v.y << 32) | v.x);
 }
 
+// Tiles (warps) per CTA of the heavy-list pass: each warp keeps its tile's heavy items in
+// shared memory.
+__host__ __device__ constexpr int heavy_warps(int T) { return T >= 4096 ? 2 : 4; }
+
+__device__ __forceinline__ uint32_t warp_excl_scan_u32(uint32_t v, uint32_t& total) {
+    const int lane = threadIdx.x & 31;
+    uint32_t inc = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xffffffffu, inc, off);
+        if (lane >= off) inc += o;
+    }
+    total = __shfl_sync(0xffffffffu, inc, 31);
+    return inc - v;
+}
+__device__ __forceinline__ uint64_t warp_excl_scan_u64(uint64_t v, uint64_t& total) {
+    const int lane = threadIdx.x & 31;
+    uint64_t inc = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint64_t o = __shfl_up_sync(0xffffffffu, inc, off);
+        if (lane >= off) inc += o;
+    }
+    total = __shfl_sync(0xffffffffu, inc, 31);
+    return inc - v;
+}
+
 template <int T>
-__global__ void __launch_bounds__(kReduceThreads) heavy_list_kernel(const float* __restrict__ w,
-                                                                    const BuildHeader* hdr, const TileVals* agg,
-                                                                    const TileVals* incl,
-                                                                    const uint32_t* __restrict__ hmask,
-                                                                    uint32_t num_tiles, uint32_t* heavy_item,
-                                                                    uint4* heavy_E) {
-    constexpr int NT = kReduceThreads;
-    constexpr int WPT = T / 32;
-    static_assert(WPT <= NT, "one mask word per thread");
-    __shared__ uint32_t sItem[T];
-    __shared__ uint32_t s_scan32[NT / 32];
-    __shared__ uint64_t s_scan64[NT / 32];
-    if (load_relaxed(&hdr->status) != 0) return;
-    const uint32_t u = blockIdx.x;
+__global__ void __launch_bounds__(32 * heavy_warps(T)) heavy_list_kernel(const float* __restrict__ w,
+                                                                      const BuildHeader* hdr, const TileVals* agg,
+                                                                      const TileVals* incl,
+                                                                      const uint32_t* __restrict__ hmask,
+                                                                      uint32_t num_tiles, uint32_t* heavy_item,
+                                                                      uint4* heavy_E) {
+    constexpr int WPT = T / 32;  // mask words per tile
+    constexpr int WPL = WPT / 32;  // mask words per lane
+    static_assert(WPL >= 1 && WPL <= 4, "mask words per lane");
+    constexpr int NWARP = heavy_warps(T);
+    __shared__ uint32_t sItem[NWARP][T];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t u = blockIdx.x * NWARP + warp;
+    if (u >= num_tiles) return;
+    if (earlier_status(hdr) != 0) return;
     const uint32_t m = __ldcg(&agg[u].nH);
     if (m == 0) return;
-    const int tid = threadIdx.x;
-    const ClassParams cp = class_params(hdr->W_N, hdr->R);
-    const TileVals tot = ldcg_tilevals(incl + num_tiles - 1);
-    const int64_t nfix = excess_correction(deficit_line(tot), tot.E);
+    const ClassParams cp = load_class_params(hdr);
+    const int64_t nfix = __ldg(&hdr->nfix);
     const uint32_t g0 = u ? __ldcg(&incl[u - 1].nH) : 0u;
     const u128 Eb = u ? ldcg_E(incl + u - 1) : (u128)0;
+    uint32_t* items = sItem[warp];
     {
-        const uint32_t word = tid < WPT ? __ldg(hmask + (uint64_t)u * WPT + tid) : 0u;
+        // lane l holds mask words l*WPL .. l*WPL + WPL - 1 (consecutive tile items)
+        uint32_t wd[WPL];
+        uint32_t c = 0;
+#pragma unroll
+        for (int i = 0; i < WPL; ++i) {
+            wd[i] = __ldg(hmask + (uint64_t)u * WPT + lane * WPL + i);
+            c += (uint32_t)__popc(wd[i]);
+        }
         uint32_t ctot;
-        uint32_t o = block_scan1<NT, uint32_t>((uint32_t)__popc(word), s_scan32, ctot);
-        const uint32_t ibase = u * (uint32_t)T + (uint32_t)tid * 32u;
-        for (uint32_t b = word; b; b &= b - 1) sItem[o++] = ibase + (uint32_t)(__ffs(b) - 1);
+        uint32_t o = warp_excl_scan_u32(c, ctot);
+#pragma unroll
+        for (int i = 0; i < WPL; ++i) {
+            const uint32_t ibase = u * (uint32_t)T + (uint32_t)(lane * WPL + i) * 32u;
+            for (uint32_t b = wd[i]; b; b &= b - 1) items[o++] = ibase + (uint32_t)(__ffs(b) - 1);
+        }
     }
-    __syncthreads();
-    const uint32_t per = (m + NT - 1) / NT;
-    const uint32_t j0 = min(m, (uint32_t)tid * per), j1 = min(m, j0 + per);
+    __syncwarp();
+    const uint32_t per = (m + 31) / 32;
+    const uint32_t j0 = min(m, (uint32_t)lane * per), j1 = min(m, j0 + per);
     uint64_t hs = 0;
-    for (uint32_t j = j0; j < j1; ++j) hs += rare_q(__ldg(w + sItem[j]), true, cp);
+    for (uint32_t j = j0; j < j1; ++j) hs += rare_q(__ldg(w + items[j]), true, cp);
     uint64_t htot;
-    uint64_t er = block_scan1<NT, uint64_t>(hs, s_scan64, htot);
+    uint64_t er = warp_excl_scan_u64(hs, htot);
     for (uint32_t j = j0; j < j1; ++j) {
-        er += rare_q(__ldg(w + sItem[j]), true, cp);  // the weight again, from L1
-        heavy_item[g0 + j] = sItem[j];
+        er += rare_q(__ldg(w + items[j]), true, cp);  // the weight again, from L1
+        heavy_item[g0 + j] = items[j];
         store_u128(heavy_E + g0 + j, q_scale_excess(Eb + ((u128)er << 40), nfix));
     }
 }
 
 // ---------------------------------------------------------------- pass 5: split
-// Per tile boundary b (0..num_tiles), bound[b] = #{heavies with E~ <= A_before(b)}, by a
-// binary search of the heavy list (the reference's split search, at tile granularity);
-// bound[0] = 0 and bound[num_tiles] = nH, so light tile t owns heavies [bound[t], bound[t+1]).
+// Per tile boundary b (0..num_tiles): the start of the deficit line A_before(b), the base of
+// its dithering (Dither::c0), and bound = #{heavies with E~ <= A_before(b)} by a binary
+// search of the heavy list (the reference's split search, at tile granularity), with
+// bound = 0 at b = 0 and nH at b = num_tiles, so light tile t owns heavies
+// [start[t].bound, start[t+1].bound).
+struct __align__(16) TileStart {
+    uint64_t A_lo;
+    uint64_t A_hi;
+    uint64_t c0;
+    uint32_t bound;
+    uint32_t pad;
+};
+static_assert(sizeof(TileStart) == 32, "TileStart layout");
+
 static __global__ void __launch_bounds__(256) tile_link_kernel(const BuildHeader* hdr, const TileVals* incl,
                                                                uint32_t num_tiles, const uint4* heavy_E,
-                                                               uint32_t* bound) {
-    if (load_relaxed(&hdr->status) != 0) return;
+                                                               TileStart* starts) {
+    if (earlier_status(hdr) != 0) return;
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b > num_tiles) return;
-    const uint32_t nH = __ldcg(&incl[num_tiles - 1].nH);
+    const uint32_t nH = __ldg(&incl[num_tiles - 1].nH);
+    const TileVals pv = b ? ldcg_tilevals(incl + b - 1) : tv_zero();
+    const u128 X = deficit_line(pv);
     uint32_t g;
     if (b == 0) {
         g = 0;
     } else if (b == num_tiles) {
         g = nH;
     } else {
-        const u128 X = deficit_line(ldcg_tilevals(incl + b - 1));
         uint32_t lo = 0, hi = nH;
         while (lo < hi) {
             const uint32_t mid = (lo + hi) >> 1;
@@ -866,18 +939,24 @@ static __global__ void __launch_bounds__(256) tile_link_kernel(const BuildHeader
         }
         g = lo;
     }
-    bound[b] = g;
+    TileStart ts;
+    ts.A_lo = q_lo(X);
+    ts.A_hi = q_hi(X);
+    ts.c0 = make_dither(pv.L).c0;
+    ts.bound = g;
+    ts.pad = 0;
+    starts[b] = ts;
 }
 
 // ---------------------------------------------------------------- pass 6: pack
-// Heavies per chunk for T items per tile (the own-tile phase keeps a u64 per tile item in
-// the chunk arrays, so 12 * C >= 8 * T).
-__host__ __device__ constexpr int pack_chunk(int T) { return (2 * T) / 3 + 64 > 1024 ? (2 * T) / 3 + 64 : 1024; }
+// Heavies per chunk for T items per tile: the own-tile phase keeps a u64 and a float per
+// tile item in the chunk arrays (16 * C >= 12 * T bytes).
+__host__ __device__ constexpr int pack_chunk(int T) { return (3 * T) / 4 > 1024 ? (3 * T) / 4 : 1024; }
 
 // Shared memory of the pack kernel, in this order: light keys (u64 x T; the staged rows at
-// the end), light rank counts (u32 x T), heavy keys (u64 x C), heavy items (u32 x C).
+// the end), heavy keys (u64 x C), heavy items (u32 x C), heavy ranks (u32 x C).
 __host__ __device__ constexpr size_t pack_smem_bytes(int T) {
-    return (size_t)T * (sizeof(uint64_t) + sizeof(uint32_t)) + (size_t)pack_chunk(T) * (sizeof(uint64_t) + sizeof(uint32_t));
+    return (size_t)T * sizeof(uint64_t) + (size_t)pack_chunk(T) * (sizeof(uint64_t) + 2 * sizeof(uint32_t));
 }
 
 // Staged row position of tile item i (XOR swizzle of the IPT items of a thread, so that
@@ -890,53 +969,52 @@ __device__ __forceinline__ uint32_t stage_pos(uint32_t i) {
 // One light tile per CTA of NT threads, IPT consecutive items per thread.
 //  (1) Own tile: every light's deficit-interval start goes to shared memory as a key in
 //      the tile's frame, key = (A - A_before(t)) / 2^-48 (exact), with large lights dithered.
-//  (2) Heavies [bound[t], bound[t+1]] of the heavy list (the owned ones and the next one),
-//      in chunks of at most C. A heavy's key in the same frame is ceil((E~ - A_before) /
-//      2^-48) clamped to [0, 2^64 - 1], so key(light) < key(heavy) exactly when A < E~. Its
-//      rank r = #{lights with key < its key} (I(j) = #{A < E~_j}) gives an owned heavy's row,
-//      r = 1 + E~ - A_r, aliasing the next heavy. A light's alias is the first heavy whose key
-//      exceeds its own (J(i) = #{E~ <= A_i}): the number of the chunk's heavies of rank <= i,
-//      an inclusive prefix sum over a histogram of the ranks, valid for the lights from the
-//      previous chunk's last rank on whose count stays inside the chunk.
+//  (2) Heavies [start[t].bound, start[t+1].bound] of the heavy list (the owned ones and the
+//      next one), in chunks of at most C. A heavy's key in the same frame is
+//      ceil((E~ - A_before) / 2^-48) clamped to [0, 2^64 - 1], so key(light) < key(heavy)
+//      exactly when A < E~. A heavy's rank is the index of the first light whose key is not
+//      below its own (I(j) = #{A < E~_j}, a binary search of the light keys); an owned heavy's
+//      row keeps r = 1 + E~ - A_rank and aliases the next heavy. A light's alias is the first
+//      heavy whose key exceeds its own (J(i) = #{E~ <= A_i}), i.e. the first heavy whose rank
+//      exceeds the light's index: each thread finds it for its first light and then only
+//      compares indices with ranks.
 //  (3) Light rows, staged in shared memory and written out coalesced (the heavies' rows of
 //      this tile belong to the tiles that own them).
 template <int NT, int IPT>
 __global__ void __launch_bounds__(NT) split_pack_kernel(const float* __restrict__ w, uint64_t n,
                                                         const BuildHeader* hdr, const TileVals* incl,
-                                                        const uint32_t* __restrict__ bound,
+                                                        const TileStart* __restrict__ starts,
                                                         const uint32_t* __restrict__ heavy_item,
                                                         const uint4* __restrict__ heavy_E, uint32_t num_tiles,
                                                         wrs_alias_row* __restrict__ table) {
     constexpr int T = NT * IPT;
     constexpr int C = pack_chunk(T);
-    static_assert(12 * C >= 8 * T, "own-tile slots live in the chunk arrays");
+    static_assert(16 * C >= 12 * T, "own-tile slots live in the chunk arrays");
     static_assert(IPT >= 4 && IPT <= 32 && (IPT & (IPT - 1)) == 0, "items per thread");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint64_t* sLkey = reinterpret_cast<uint64_t*>(smem_raw);
-    uint32_t* sCnt = reinterpret_cast<uint32_t*>(sLkey + T);
-    uint64_t* sHkey = reinterpret_cast<uint64_t*>(sCnt + T);  // 16-byte aligned: T % 4 == 0
+    uint64_t* sHkey = sLkey + T;
     uint32_t* sHitem = reinterpret_cast<uint32_t*>(sHkey + C);
-    uint64_t* sSlotQ = sHkey;  // own-tile phase: per item slot, over sHkey and sHitem (8T <= 12C bytes)
-    float* sSlotP = reinterpret_cast<float*>(sCnt);  // own-tile phase: per item slot
-    uint64_t* sStage = sLkey;                        // row phase: staged rows
+    uint32_t* sHrank = sHitem + C;
+    uint64_t* sSlotQ = sHkey;                                // own-tile phase: per item slot
+    float* sSlotP = reinterpret_cast<float*>(sSlotQ + T);   // own-tile phase: per item slot
+    uint64_t* sStage = sLkey;                                // row phase: staged rows
     __shared__ Scan3 s_scan3[NT / 32];
-    __shared__ uint32_t s_scan32[NT / 32];
     __shared__ uint32_t s_r0, s_pend_item;
     __shared__ float s_pend_prob;
 
-    if (load_relaxed(&hdr->status) != 0) return;
     const int tid = threadIdx.x;
     const uint32_t tile = num_tiles - 1 - blockIdx.x;  // descending: the previous passes ended at
                                                        // the last tiles, still in L2
-    const ClassParams cp = class_params(hdr->W_N, hdr->R);
-    const uint32_t nH = __ldcg(&incl[num_tiles - 1].nH);
-    const TileVals before = tile ? ldcg_tilevals(incl + tile - 1) : tv_zero();
-    const u128 A_before = deficit_line(before);
-    const u128 A_after = deficit_line(ldcg_tilevals(incl + tile));
-
-    // ---- (1) own tile
+    // ---- (1) own tile (the weights' loads go out first: they do not depend on the header)
     float x[IPT];
     load_items<NT, IPT>(w, n, tile, tid, x);
+    if (earlier_status(hdr) != 0) return;
+    const ClassParams cp = load_class_params(hdr);
+    const uint32_t nH = __ldg(&incl[num_tiles - 1].nH);
+    const TileStart st0 = starts[tile], st1 = starts[tile + 1];
+    const u128 A_before = q_make(st0.A_hi, st0.A_lo);
+    const u128 A_after = q_make(st1.A_hi, st1.A_lo);
     const uint32_t item0 = (uint32_t)((uint64_t)tile * T + (uint64_t)tid * IPT);
     float pk[IPT];
     uint32_t lbits = 0, gbits = 0;  // bit k: item k is a light / a large light
@@ -962,9 +1040,10 @@ __global__ void __launch_bounds__(NT) split_pack_kernel(const float* __restrict_
     Scan3 tot_l;
     const Scan3 ex = block_scan3<NT>(Scan3{nl, asum, lsum}, s_scan3, tot_l);
     const uint32_t nLt = tot_l.c;
-    const uint32_t l0 = ex.c;  // this thread's lights are l0 .. lend - 1 in tile light order
-    const uint32_t lend = l0 + nl;
-    const Dither dth = make_dither(before.L);
+    const uint32_t l0 = ex.c;  // this thread's lights are l0 .. l0 + nl - 1 in tile light order
+    Dither dth;
+    dth.c0 = st0.c0;
+    dth.c0h = st0.c0 >> 24;
     const uint64_t D0 = dither_at(dth, ex.b);
     {
         uint64_t lr = ex.b, dprev = D0;
@@ -1009,8 +1088,7 @@ __global__ void __launch_bounds__(NT) split_pack_kernel(const float* __restrict_
 #pragma unroll
         for (int k = 0; k < IPT; ++k) al[k] = last_heavy;  // lights past every heavy's excess
                                                             // (rounding residue only)
-        for (uint32_t li = l0; li < lend; ++li) sCnt[li] = 0u;
-        const uint32_t g_lo = bound[tile], g_hi = bound[tile + 1];
+        const uint32_t g_lo = st0.bound, g_hi = st1.bound;
         const uint32_t g_end = min(g_hi + 1u, nH);
         for (uint32_t cs = g_lo; cs < g_end; cs += (uint32_t)C) {
             const uint32_t m = min((uint32_t)C, g_end - cs);
@@ -1038,23 +1116,55 @@ __global__ void __launch_bounds__(NT) split_pack_kernel(const float* __restrict_
                 r.alias = sHitem[0];
                 table[pend] = r;
             }
-            // ranks: histogram, and the rows of the owned heavies
+            // ranks: the index of the first light whose key is not below the heavy's
+            // (all heavies of this chunk rank at r0 or later)
             for (uint32_t j = tid; j < m; j += NT) {
                 const uint64_t kh = sHkey[j];
-                uint32_t lo = r0, hi = nLt;  // first light whose key is not below kh
+                uint32_t lo = r0, hi = nLt;
                 while (lo < hi) {
                     const uint32_t mid = (lo + hi) >> 1;
                     if (sLkey[mid] < kh) lo = mid + 1; else hi = mid;
                 }
-                if (lo < nLt) atomicAdd(&sCnt[lo], 1u);
+                sHrank[j] = lo;
+            }
+            __syncthreads();
+            // this thread's lights: alias = the first heavy whose rank exceeds the light's index
+            if (l0 + nl > r0) {
+                const uint32_t ls = max(l0, r0);
+                uint32_t a = 0, hi = m;  // first heavy with rank > ls
+                while (a < hi) {
+                    const uint32_t mid = (a + hi) >> 1;
+                    if (sHrank[mid] <= ls) a = mid + 1; else hi = mid;
+                }
+                uint32_t ra = a < m ? sHrank[a] : 0xffffffffu;
+                uint32_t ia = a < m ? sHitem[a] : 0u;
+                uint32_t li = l0;
+#pragma unroll
+                for (int k = 0; k < IPT; ++k) {
+                    if ((lbits >> k) & 1u) {
+                        if (li >= r0) {
+                            while (ra <= li) {
+                                ++a;
+                                ra = a < m ? sHrank[a] : 0xffffffffu;
+                                ia = a < m ? sHitem[a] : 0u;
+                            }
+                            if (a < m) al[k] = ia;
+                        }
+                        ++li;
+                    }
+                }
+            }
+            // rows of the owned heavies
+            for (uint32_t j = tid; j < m; j += NT) {
                 const uint32_t g = cs + j;
+                const uint32_t rk = sHrank[j];
                 if (j + 1 == m) {
-                    s_r0 = lo;
+                    s_r0 = rk;
                     s_pend_item = 0xffffffffu;
                 }
                 if (g < g_hi) {
                     const u128 Et = load_u128(heavy_E + g);
-                    const u128 A_next = (lo < nLt) ? A_before + ((u128)sLkey[lo] << 16) : A_after;
+                    const u128 A_next = (rk < nLt) ? A_before + ((u128)sLkey[rk] << 16) : A_after;
                     const float prob = heavy_row_prob(q_one() + Et - A_next);
                     if (j + 1 < m) {
                         wrs_alias_row r;
@@ -1072,25 +1182,6 @@ __global__ void __launch_bounds__(NT) split_pack_kernel(const float* __restrict_
                     }
                 }
             }
-            __syncthreads();
-            // lights: alias index = number of the chunk's heavies with rank <= light index
-            uint32_t csum = 0;
-            for (uint32_t li = max(l0, r0); li < lend; ++li) csum += sCnt[li];
-            uint32_t ctot;
-            uint32_t run = block_scan1<NT, uint32_t>(csum, s_scan32, ctot);
-            if (lend > r0) {
-                uint32_t li = l0;
-#pragma unroll
-                for (int k = 0; k < IPT; ++k) {
-                    const bool light = (lbits >> k) & 1u;
-                    if (light && li >= r0) {
-                        run += sCnt[li];
-                        sCnt[li] = 0u;
-                        if (run < m) al[k] = sHitem[run];
-                    }
-                    li += light ? 1u : 0u;
-                }
-            }
             __syncthreads();  // the next chunk overwrites the chunk arrays
         }
     }
@@ -1105,9 +1196,18 @@ __global__ void __launch_bounds__(NT) split_pack_kernel(const float* __restrict_
     __syncthreads();
     uint64_t* out = reinterpret_cast<uint64_t*>(table) + (uint64_t)tile * T;
     const uint32_t cnt = (uint32_t)min((uint64_t)T, n - (uint64_t)tile * T);
-    for (uint32_t i = tid; i < cnt; i += NT) {
-        const uint64_t row = sStage[stage_pos<IPT>(i)];
-        if (row != ~0ull) out[i] = row;
+    if (cnt == (uint32_t)T) {
+#pragma unroll
+        for (int it = 0; it < IPT; ++it) {
+            const uint32_t i = (uint32_t)(it * NT + tid);
+            const uint64_t row = sStage[stage_pos<IPT>(i)];
+            if (row != ~0ull) out[i] = row;
+        }
+    } else {
+        for (uint32_t i = tid; i < cnt; i += NT) {
+            const uint64_t row = sStage[stage_pos<IPT>(i)];
+            if (row != ~0ull) out[i] = row;
+        }
     }
 }
 
