@@ -949,9 +949,9 @@ static __global__ void __launch_bounds__(256) tile_link_kernel(const BuildHeader
 }
 
 // ---------------------------------------------------------------- pass 6: pack
-// Heavies per chunk for T items per tile: the own-tile phase keeps a u64 and a float per
-// tile item in the chunk arrays (16 * C >= 12 * T bytes).
-__host__ __device__ constexpr int pack_chunk(int T) { return (3 * T) / 4 > 1024 ? (3 * T) / 4 : 1024; }
+// Heavies per chunk for T items per tile: the own-tile phase keeps a u64 per tile item in
+// the chunk arrays (16 * C >= 8 * T bytes).
+__host__ __device__ constexpr int pack_chunk(int T) { return T / 2 > 1024 ? T / 2 : 1024; }
 
 // Shared memory of the pack kernel, in this order: light keys (u64 x T; the staged rows at
 // the end), heavy keys (u64 x C), heavy items (u32 x C), heavy ranks (u32 x C).
@@ -981,7 +981,7 @@ __device__ __forceinline__ uint32_t stage_pos(uint32_t i) {
 //  (3) Light rows, staged in shared memory and written out coalesced (the heavies' rows of
 //      this tile belong to the tiles that own them).
 template <int NT, int IPT>
-__global__ void __launch_bounds__(NT) split_pack_kernel(const float* __restrict__ w, uint64_t n,
+__global__ void __launch_bounds__(NT, (NT == 128 && IPT == 16) ? 6 : 1) split_pack_kernel(const float* __restrict__ w, uint64_t n,
                                                         const BuildHeader* hdr, const TileVals* incl,
                                                         const TileStart* __restrict__ starts,
                                                         const uint32_t* __restrict__ heavy_item,
@@ -989,15 +989,14 @@ __global__ void __launch_bounds__(NT) split_pack_kernel(const float* __restrict_
                                                         wrs_alias_row* __restrict__ table) {
     constexpr int T = NT * IPT;
     constexpr int C = pack_chunk(T);
-    static_assert(16 * C >= 12 * T, "own-tile slots live in the chunk arrays");
+    static_assert(16 * C >= 8 * T, "own-tile slots live in the chunk arrays");
     static_assert(IPT >= 4 && IPT <= 32 && (IPT & (IPT - 1)) == 0, "items per thread");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint64_t* sLkey = reinterpret_cast<uint64_t*>(smem_raw);
     uint64_t* sHkey = sLkey + T;
     uint32_t* sHitem = reinterpret_cast<uint32_t*>(sHkey + C);
     uint32_t* sHrank = sHitem + C;
-    uint64_t* sSlotQ = sHkey;                                // own-tile phase: per item slot
-    float* sSlotP = reinterpret_cast<float*>(sSlotQ + T);   // own-tile phase: per item slot
+    uint64_t* sSlotQ = sHkey;  // own-tile phase: per item slot
     uint64_t* sStage = sLkey;                                // row phase: staged rows
     __shared__ Scan3 s_scan3[NT / 32];
     __shared__ uint32_t s_r0, s_pend_item;
@@ -1046,14 +1045,12 @@ __global__ void __launch_bounds__(NT) split_pack_kernel(const float* __restrict_
     dth.c0h = st0.c0 >> 24;
     const uint64_t D0 = dither_at(dth, ex.b);
     {
-        uint64_t lr = ex.b, dprev = D0;
+        // a large light's slot now holds the dithering after it
+        uint64_t lr = ex.b;
         for (uint32_t bits = gbits; bits; bits &= bits - 1) {
             const int slot = tid * IPT + __ffs(bits) - 1;
             lr += sSlotQ[slot];
-            const uint64_t d1 = dither_at(dth, lr);
-            sSlotP[slot] = dithered_prob(d1 - dprev);
-            sSlotQ[slot] = d1;
-            dprev = d1;
+            sSlotQ[slot] = dither_at(dth, lr);
         }
     }
     {
@@ -1066,8 +1063,9 @@ __global__ void __launch_bounds__(NT) split_pack_kernel(const float* __restrict_
             li += light ? 1u : 0u;
             sr += (light && !((gbits >> k) & 1u)) ? small_deficit(pk[k]) : 0ull;
             if ((gbits >> k) & 1u) {
-                D = sSlotQ[tid * IPT + k];
-                pk[k] = sSlotP[tid * IPT + k];
+                const uint64_t D1 = sSlotQ[tid * IPT + k];
+                pk[k] = dithered_prob(D1 - D);
+                D = D1;
             }
         }
     }
