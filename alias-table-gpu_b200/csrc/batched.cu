@@ -1,28 +1,307 @@
-// batched.cu — C ABI of the batched (CSR) alias build and sampler.
+// batched.cu — C ABI of the batched (CSR) alias build, its sampler and its autotuner.
+//
+// wrs_batched_build_f32 / wrs_batched_sample replace a loop of AliasTableSplitGpu objects
+// (construction/aliasTable/buildMethod/AliasTableSplitGpu.cu:388-468) and of
+// SamplerGpuBasic::executeBenchmarkSampling (sampling/aliasTable/SamplerGpuBasic.cu:109-133),
+// one per table, with a fixed launch sequence for the whole batch; wrs_batched_autotune
+// replaces the reference's compile-time launch constants (AliasTableSplitGpu.cuh:60-94).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
+#include "batched_kernels.cuh"
 #include "host_util.h"
+
+namespace wrs {
+namespace {
+
+constexpr uint32_t kDefaultSmall = 128;
+const uint32_t kSmallChoices[] = {32, 64, 128, 256, 512};
+const uint32_t kTileChoices[] = {1024, 2048, 4096};
+
+bool valid_small(uint32_t s) {
+    for (uint32_t c : kSmallChoices)
+        if (c == s) return true;
+    return false;
+}
+bool valid_tile(uint32_t t) {
+    for (uint32_t c : kTileChoices)
+        if (c == t) return true;
+    return false;
+}
+
+struct Shape {
+    uint32_t small_max;
+    uint32_t tile;
+};
+
+bool shape_of(const wrs_build_opts* opts, Shape* sh) {
+    sh->small_max = (opts && opts->small_table_items) ? opts->small_table_items : kDefaultSmall;
+    sh->tile = (opts && opts->tile_items) ? opts->tile_items : 2048u;
+    return valid_small(sh->small_max) && valid_tile(sh->tile);
+}
+
+// The host's view of the batch for one shape (from h_offsets).
+struct HostPlan {
+    uint32_t small_tables;  // tables with 1 <= n <= small_max
+    uint32_t big_tables;    // tables with n > small_max
+    uint32_t tiles;         // tiles of the big tables
+    uint64_t big_items;
+    bool valid;
+};
+
+HostPlan host_plan(const int64_t* h_offsets, int64_t num_tables, const Shape& sh) {
+    HostPlan p{0, 0, 0, 0, true};
+    if (!h_offsets || num_tables < 1 || h_offsets[0] != 0) {
+        p.valid = false;
+        return p;
+    }
+    uint64_t tiles = 0, tables = 0, small = 0;
+    for (int64_t t = 0; t < num_tables; ++t) {
+        const int64_t n = h_offsets[t + 1] - h_offsets[t];
+        if (n < 0 || n > (int64_t)0x7fffffff - 8192) {
+            p.valid = false;
+            return p;
+        }
+        if (n == 0) continue;
+        if (n <= (int64_t)sh.small_max) {
+            ++small;
+        } else {
+            ++tables;
+            tiles += (uint64_t)((n + sh.tile - 1) / sh.tile);
+            p.big_items += (uint64_t)n;
+        }
+    }
+    if (tables > 0x7fffffffull || tiles > 0x7fffffffull || small > 0xffffffffull) p.valid = false;
+    p.small_tables = (uint32_t)small;
+    p.big_tables = (uint32_t)tables;
+    p.tiles = (uint32_t)tiles;
+    return p;
+}
+
+struct BatchLayout {
+    BuildHeader* hdr0;  // batch status word
+    uint32_t* plan_status;
+    BuildHeader* hdrs;  // one per big table
+    PlanCounts* blk;
+    TableDesc* desc;
+    uint32_t* tile_table;
+    double2* partials;
+    TileVals* agg;
+    TileVals* incl;
+    TileStart* starts;
+    uint32_t* hmask;
+    uint32_t* heavy_item;
+    uint4* heavy_E;
+    size_t bytes;
+};
+
+BatchLayout carve_batch(void* scratch, int64_t num_tables, const HostPlan& p, uint32_t tile) {
+    Carver c(scratch);
+    BatchLayout L;
+    // the batch header, the plan header and the per-table headers are contiguous: one memset
+    // clears them all; the batch header comes first, so wrs_scratch_status reads its status
+    L.hdr0 = c.take<BuildHeader>(2 + (size_t)p.big_tables);
+    L.plan_status = &(L.hdr0 + 1)->status;
+    L.hdrs = L.hdr0 + 2;
+    L.blk = c.take<PlanCounts>((size_t)((num_tables + kPlanBlock - 1) / kPlanBlock));
+    L.desc = c.take<TableDesc>(p.big_tables);
+    L.tile_table = c.take<uint32_t>(p.tiles);
+    L.partials = c.take<double2>(p.tiles);
+    L.agg = c.take<TileVals>(p.tiles);
+    L.incl = c.take<TileVals>(p.tiles);
+    L.starts = c.take<TileStart>((size_t)p.tiles + p.big_tables);
+    L.hmask = c.take<uint32_t>((size_t)p.tiles * (tile / 32));
+    L.heavy_item = c.take<uint32_t>(p.big_items);
+    L.heavy_E = c.take<uint4>(p.big_items);
+    L.bytes = c.off;
+    return L;
+}
+
+template <int SPL>
+wrs_status launch_small(const float* d_w, const int64_t* d_offsets, int64_t num_tables, wrs_alias_row* d_table,
+                        double* d_W, uint32_t* status, uint32_t small_tables, cudaStream_t stream) {
+    const size_t smem = sizeof(SmallSmem<SPL>) * kSmallWarps;
+    cudaError_t e = cudaFuncSetAttribute(small_tables_kernel<SPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return WRS_ERR_CUDA;
+    // persistent warps over all tables (each warp skips the large and empty ones)
+    const DeviceInfo d = device_info();
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, small_tables_kernel<SPL>, 32 * kSmallWarps, smem);
+    if (e != cudaSuccess || per_sm < 1) per_sm = 1;
+    const uint64_t want = ((uint64_t)small_tables + kSmallWarps - 1) / kSmallWarps;
+    const uint64_t cap = (uint64_t)d.sm_count * per_sm;
+    const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min(want, cap));
+    small_tables_kernel<SPL><<<grid, 32 * kSmallWarps, smem, stream>>>(d_w, d_offsets, num_tables, 32u * SPL,
+                                                                        d_table, d_W, status);
+    return launch_status();
+}
+
+template <int T>
+wrs_status launch_big(const float* d_w, const int64_t* d_offsets, int64_t num_tables, uint32_t small_max,
+                      wrs_alias_row* d_table, double* d_W, const BatchLayout& L, const HostPlan& p,
+                      cudaStream_t stream) {
+    constexpr int NT = PackShape<T>::NT, IPT = PackShape<T>::IPT;
+    const uint32_t nblk = (uint32_t)((num_tables + kPlanBlock - 1) / kPlanBlock);
+    const PlanCounts cap{p.big_tables, p.tiles, p.big_items};
+    plan_count_kernel<<<nblk, kPlanBlock, 0, stream>>>(d_offsets, num_tables, small_max, T, L.blk);
+    plan_scan_kernel<<<1, kPlanBlock, 0, stream>>>(L.blk, nblk, cap, L.plan_status);
+    plan_fill_kernel<<<nblk, kPlanBlock, 0, stream>>>(d_offsets, num_tables, small_max, T, L.blk, cap, L.desc,
+                                                      L.tile_table);
+    const TileMap map{L.tile_table, L.desc, L.plan_status, 0, 0};
+    const uint32_t nt = p.tiles;
+    batch_wsum_kernel<T><<<nt, kBatchWsumThreads, 0, stream>>>(d_w, L.hdrs, L.partials, map, d_W);
+    tile_reduce_kernel<T, true><<<nt, kReduceThreads, 0, stream>>>(d_w, L.hdrs, L.agg, L.hmask, map);
+    batch_prefix_kernel<<<p.big_tables, kPrefixThreads, 0, stream>>>(L.hdrs, L.agg, L.incl, L.desc, L.plan_status);
+    heavy_list_kernel<T, true><<<(nt + heavy_warps(T) - 1) / heavy_warps(T), 32 * heavy_warps(T), 0, stream>>>(
+        d_w, L.hdrs, L.agg, L.incl, L.hmask, nt, L.heavy_item, L.heavy_E, map);
+    tile_link_kernel<true><<<(nt + p.big_tables + 255) / 256, 256, 0, stream>>>(L.hdrs, L.incl, nt, p.big_tables,
+                                                                               L.heavy_E, L.starts, map);
+    const size_t smem = pack_smem_bytes(T);
+    const cudaError_t e = cudaFuncSetAttribute(split_pack_kernel<NT, IPT, true>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return WRS_ERR_CUDA;
+    split_pack_kernel<NT, IPT, true><<<nt, NT, smem, stream>>>(d_w, L.hdrs, L.incl, L.starts, L.heavy_item,
+                                                                L.heavy_E, nt, d_table, map);
+    batch_status_kernel<<<(p.big_tables + 1 + 255) / 256, 256, 0, stream>>>(L.hdr0 + 1, p.big_tables + 1,
+                                                                           &L.hdr0->status);
+    return launch_status();
+}
+
+wrs_status batched_build(const float* d_w, const int64_t* d_offsets, const int64_t* h_offsets, int64_t num_tables,
+                         const Shape& sh, wrs_alias_row* d_table, double* d_W, void* d_scratch, size_t scratch_bytes,
+                         cudaStream_t stream, BatchLayout* out_layout) {
+    const HostPlan p = host_plan(h_offsets, num_tables, sh);
+    if (!p.valid) return WRS_ERR_INVALID_ARGUMENT;
+    const BatchLayout L = carve_batch(d_scratch, num_tables, p, sh.tile);
+    if (scratch_bytes < L.bytes) return WRS_ERR_SCRATCH_TOO_SMALL;
+    if (out_layout) *out_layout = L;
+    if (cudaMemsetAsync(L.hdr0, 0, sizeof(BuildHeader) * (2 + (size_t)p.big_tables), stream) != cudaSuccess)
+        return WRS_ERR_CUDA;
+    wrs_status st = WRS_SUCCESS;
+    if (p.small_tables > 0) {
+        uint32_t* status = &L.hdr0->status;
+        switch (sh.small_max) {
+            case 32: st = launch_small<1>(d_w, d_offsets, num_tables, d_table, d_W, status, p.small_tables, stream); break;
+            case 64: st = launch_small<2>(d_w, d_offsets, num_tables, d_table, d_W, status, p.small_tables, stream); break;
+            case 128: st = launch_small<4>(d_w, d_offsets, num_tables, d_table, d_W, status, p.small_tables, stream); break;
+            case 256: st = launch_small<8>(d_w, d_offsets, num_tables, d_table, d_W, status, p.small_tables, stream); break;
+            default: st = launch_small<16>(d_w, d_offsets, num_tables, d_table, d_W, status, p.small_tables, stream); break;
+        }
+        if (st != WRS_SUCCESS) return st;
+    }
+    if (p.big_tables > 0) {
+        switch (sh.tile) {
+            case 1024: st = launch_big<1024>(d_w, d_offsets, num_tables, sh.small_max, d_table, d_W, L, p, stream); break;
+            case 4096: st = launch_big<4096>(d_w, d_offsets, num_tables, sh.small_max, d_table, d_W, L, p, stream); break;
+            default: st = launch_big<2048>(d_w, d_offsets, num_tables, sh.small_max, d_table, d_W, L, p, stream); break;
+        }
+    }
+    return st;
+}
+
+}  // namespace
+}  // namespace wrs
+
+using namespace wrs;
 
 extern "C" size_t wrs_batched_build_scratch_bytes(const int64_t* h_offsets, int64_t num_tables,
                                                   const wrs_build_opts* opts) {
-    (void)h_offsets;
-    (void)num_tables;
-    (void)opts;
-    return 0;
+    if (opts) {
+        Shape sh;
+        if (!shape_of(opts, &sh)) return 0;
+        const HostPlan p = host_plan(h_offsets, num_tables, sh);
+        return p.valid ? carve_batch(nullptr, num_tables, p, sh.tile).bytes : 0;
+    }
+    size_t best = 0;
+    for (uint32_t s : kSmallChoices)
+        for (uint32_t t : kTileChoices) {
+            const Shape sh{s, t};
+            const HostPlan p = host_plan(h_offsets, num_tables, sh);
+            if (!p.valid) return 0;
+            best = std::max(best, carve_batch(nullptr, num_tables, p, t).bytes);
+        }
+    return best;
 }
 
 extern "C" wrs_status wrs_batched_build_f32(const float* d_w, const int64_t* d_offsets, const int64_t* h_offsets,
                                             int64_t num_tables, const wrs_build_opts* opts, wrs_alias_row* d_table,
-                                            double* d_W, void* d_scratch, size_t scratch_bytes, void* stream) {
-    (void)d_w; (void)d_offsets; (void)h_offsets; (void)num_tables; (void)opts; (void)d_table; (void)d_W;
-    (void)d_scratch; (void)scratch_bytes; (void)stream;
-    return WRS_ERR_UNSUPPORTED;
+                                            double* d_W, void* d_scratch, size_t scratch_bytes, void* stream_) {
+    if (!d_w || !d_offsets || !h_offsets || !d_table || !d_scratch || num_tables < 1) return WRS_ERR_INVALID_ARGUMENT;
+    Shape sh;
+    if (!shape_of(opts, &sh)) return WRS_ERR_INVALID_ARGUMENT;
+    if (opts && opts->method != WRS_METHOD_SPLIT) return WRS_ERR_UNSUPPORTED;
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+    BatchLayout L;
+    const wrs_status st = batched_build(d_w, d_offsets, h_offsets, num_tables, sh, d_table, d_W, d_scratch,
+                                        scratch_bytes, stream, &L);
+    if (st != WRS_SUCCESS) return st;
+    if (opts && (opts->flags & WRS_FLAG_SYNC)) return read_device_status(&L.hdr0->status, stream);
+    return WRS_SUCCESS;
 }
 
 extern "C" wrs_status wrs_batched_sample(const wrs_alias_row* d_table, const int64_t* d_offsets, int64_t num_tables,
                                          const int64_t* d_sample_offsets, uint64_t total_samples, uint64_t seed,
-                                         uint64_t counter_base, uint32_t* d_out, void* stream) {
-    (void)d_table; (void)d_offsets; (void)num_tables; (void)d_sample_offsets; (void)total_samples; (void)seed;
-    (void)counter_base; (void)d_out; (void)stream;
-    return WRS_ERR_UNSUPPORTED;
+                                         uint64_t counter_base, uint32_t* d_out, void* stream_) {
+    if (!d_table || !d_offsets || !d_sample_offsets || !d_out || num_tables < 1) return WRS_ERR_INVALID_ARGUMENT;
+    if (total_samples == 0) return WRS_SUCCESS;
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+    const uint64_t per_cta = (uint64_t)kBatchSampleThreads * kBatchSamplePer;
+    const uint64_t grid = (total_samples + per_cta - 1) / per_cta;
+    if (grid > 0x7fffffffull) return WRS_ERR_INVALID_ARGUMENT;
+    batch_sample_kernel<<<(uint32_t)grid, kBatchSampleThreads, 0, stream>>>(
+        d_table, d_offsets, num_tables, d_sample_offsets, total_samples, seed, counter_base, d_out, nullptr);
+    return launch_status();
+}
+
+extern "C" wrs_status wrs_batched_autotune(const float* d_w, const int64_t* d_offsets, const int64_t* h_offsets,
+                                           int64_t num_tables, wrs_alias_row* d_table, void* d_scratch,
+                                           size_t scratch_bytes, wrs_build_opts* opts, void* stream_) {
+    if (!opts || !d_w || !d_offsets || !h_offsets || !d_table || !d_scratch) return WRS_ERR_INVALID_ARGUMENT;
+    if (scratch_bytes < wrs_batched_build_scratch_bytes(h_offsets, num_tables, nullptr))
+        return WRS_ERR_SCRATCH_TOO_SMALL;
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess) return WRS_ERR_CUDA;
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return WRS_ERR_CUDA;
+    }
+    float best_ms = 1e30f;
+    Shape best{kDefaultSmall, 2048};
+    wrs_status result = WRS_SUCCESS;
+    for (uint32_t s : kSmallChoices) {
+        for (uint32_t t : kTileChoices) {
+            const Shape sh{s, t};
+            float ms_min = 1e30f;
+            for (int rep = 0; rep < 3; ++rep) {  // the first run warms up
+                BatchLayout L;
+                cudaEventRecord(e0, stream);
+                wrs_status st = batched_build(d_w, d_offsets, h_offsets, num_tables, sh, d_table, nullptr, d_scratch,
+                                              scratch_bytes, stream, &L);
+                cudaEventRecord(e1, stream);
+                if (st == WRS_SUCCESS) st = read_device_status(&L.hdr0->status, stream);
+                if (st != WRS_SUCCESS) {
+                    result = st;
+                    break;
+                }
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (rep > 0) ms_min = std::min(ms_min, ms);
+            }
+            if (result != WRS_SUCCESS) break;
+            if (ms_min < best_ms) {
+                best_ms = ms_min;
+                best = sh;
+            }
+        }
+        if (result != WRS_SUCCESS) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (result != WRS_SUCCESS) return result;
+    opts->small_table_items = best.small_max;
+    opts->tile_items = best.tile;
+    return WRS_SUCCESS;
 }

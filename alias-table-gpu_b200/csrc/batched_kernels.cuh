@@ -1,0 +1,524 @@
+// batched_kernels.cuh — the batched (CSR) alias build and sampler for sm_100a.
+//
+// The reference has no batched form: its experiment drivers build many tables by looping
+// over AliasTableSplitGpu objects, one build() (several launches, device-to-host copies and
+// allocations) per table (construction/aliasTable/buildMethod/AliasTableSplitGpu.cu:388-468).
+// Here a whole CSR batch is built by a fixed sequence of launches that depends only on the
+// batch's shape, so it can be captured in a CUDA graph:
+//   * small tables (n <= small_max, at most 32 * SPL items) are built one per warp by a
+//     persistent kernel, everything in registers and shared memory;
+//   * larger tables go through the tiled passes of the single-table build, run once over
+//     the tiles of all of them (tile_reduce, heavy_list, tile_link, split_pack with
+//     BATCH = true), with per-table weight totals and tile prefixes from the kernels below.
+// Both produce, for every table, exactly the rows a single-table build of its weights gives.
+// The plan (which tables are large, their tiles) is computed on the device from the CSR
+// offsets by three small kernels.
+#pragma once
+
+#include "build_kernels.cuh"
+
+namespace wrs {
+
+// ---------------------------------------------------------------- planning
+// A table is "large" when small_max < n. Planning block pb covers tables
+// [pb * kPlanBlock, (pb + 1) * kPlanBlock): plan_count counts its large tables, their tiles
+// and their items, plan_scan turns the counts into offsets, plan_fill writes the TableDesc
+// of every large table and the table of every global tile. Totals that differ from the
+// host's plan (made from its copy of the offsets) are reported as WRS_ERR_INVALID_ARGUMENT
+// in the plan status, and the batched passes then do nothing.
+constexpr int kPlanBlock = 1024;
+
+struct PlanCounts {
+    uint32_t tables;
+    uint32_t tiles;
+    uint64_t items;
+};
+__device__ __forceinline__ PlanCounts pc_add(const PlanCounts& a, const PlanCounts& b) {
+    return PlanCounts{a.tables + b.tables, a.tiles + b.tiles, a.items + b.items};
+}
+__device__ __forceinline__ PlanCounts pc_sub(const PlanCounts& a, const PlanCounts& b) {
+    return PlanCounts{a.tables - b.tables, a.tiles - b.tiles, a.items - b.items};
+}
+__device__ __forceinline__ PlanCounts pc_shfl_up(const PlanCounts& v, int d) {
+    return PlanCounts{__shfl_up_sync(0xffffffffu, v.tables, d), __shfl_up_sync(0xffffffffu, v.tiles, d),
+                      __shfl_up_sync(0xffffffffu, v.items, d)};
+}
+__device__ __forceinline__ PlanCounts pc_shfl(const PlanCounts& v, int src) {
+    return PlanCounts{__shfl_sync(0xffffffffu, v.tables, src), __shfl_sync(0xffffffffu, v.tiles, src),
+                      __shfl_sync(0xffffffffu, v.items, src)};
+}
+static_assert(kPlanBlock == 32 * 32, "one scan slot per lane");
+// Exclusive scan over a kPlanBlock-thread CTA; *total gets the CTA total. Ends with a barrier.
+__device__ __forceinline__ PlanCounts pc_block_scan(const PlanCounts v, PlanCounts* s, PlanCounts* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    PlanCounts inc = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const PlanCounts o = pc_shfl_up(inc, off);
+        if (lane >= off) inc = pc_add(inc, o);
+    }
+    if (lane == 31) s[warp] = inc;
+    __syncthreads();
+    PlanCounts t = s[lane];
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const PlanCounts o = pc_shfl_up(t, off);
+        if (lane >= off) t = pc_add(t, o);
+    }
+    *total = pc_shfl(t, 31);
+    const PlanCounts zero{0u, 0u, 0ull};
+    const PlanCounts base = pc_shfl(t, warp > 0 ? warp - 1 : 0);
+    __syncthreads();
+    return pc_sub(pc_add(warp ? base : zero, inc), v);
+}
+
+__device__ __forceinline__ PlanCounts plan_of(const int64_t* offsets, int64_t num_tables, int64_t t,
+                                             uint32_t small_max, uint32_t tile_items, int64_t* n_out) {
+    PlanCounts c{0u, 0u, 0ull};
+    int64_t n = 0;
+    if (t < num_tables) {
+        n = offsets[t + 1] - offsets[t];
+        if (n > (int64_t)small_max) c = PlanCounts{1u, (uint32_t)((n + tile_items - 1) / tile_items), (uint64_t)n};
+    }
+    *n_out = n;
+    return c;
+}
+
+__global__ void __launch_bounds__(kPlanBlock) plan_count_kernel(const int64_t* __restrict__ offsets,
+                                                               int64_t num_tables, uint32_t small_max,
+                                                               uint32_t tile_items, PlanCounts* blk) {
+    __shared__ PlanCounts s[32];
+    int64_t n;
+    const PlanCounts c =
+        plan_of(offsets, num_tables, (int64_t)blockIdx.x * kPlanBlock + threadIdx.x, small_max, tile_items, &n);
+    PlanCounts tot;
+    pc_block_scan(c, s, &tot);
+    if (threadIdx.x == 0) blk[blockIdx.x] = tot;
+}
+
+// One CTA: exclusive scan of the block counts (in place), in chunks of kPlanBlock; checks
+// the totals against the host's plan.
+__global__ void __launch_bounds__(kPlanBlock) plan_scan_kernel(PlanCounts* blk, uint32_t num_blk, PlanCounts cap,
+                                                              uint32_t* plan_status) {
+    __shared__ PlanCounts s[32];
+    PlanCounts carry{0u, 0u, 0ull};
+    for (uint32_t c = 0; c < num_blk; c += kPlanBlock) {
+        const uint32_t i = c + threadIdx.x;
+        const PlanCounts v = i < num_blk ? blk[i] : PlanCounts{0u, 0u, 0ull};
+        PlanCounts tot;
+        const PlanCounts ex = pc_block_scan(v, s, &tot);
+        if (i < num_blk) blk[i] = pc_add(carry, ex);
+        carry = pc_add(carry, tot);
+    }
+    if (threadIdx.x == 0 && (carry.tables != cap.tables || carry.tiles != cap.tiles || carry.items != cap.items))
+        record_status(plan_status, WRS_ERR_INVALID_ARGUMENT);
+}
+
+__global__ void __launch_bounds__(kPlanBlock) plan_fill_kernel(const int64_t* __restrict__ offsets,
+                                                              int64_t num_tables, uint32_t small_max,
+                                                              uint32_t tile_items, const PlanCounts* blk,
+                                                              PlanCounts cap, TableDesc* desc, uint32_t* tile_table) {
+    __shared__ PlanCounts s[32];
+    const int64_t t = (int64_t)blockIdx.x * kPlanBlock + threadIdx.x;
+    int64_t n;
+    const PlanCounts c = plan_of(offsets, num_tables, t, small_max, tile_items, &n);
+    PlanCounts tot;
+    const PlanCounts ex = pc_add(blk[blockIdx.x], pc_block_scan(c, s, &tot));
+    if (c.tables == 0) return;
+    // a plan that does not fit the host's capacities is reported by plan_scan_kernel
+    if (ex.tables >= cap.tables || ex.tiles + c.tiles > cap.tiles || ex.items + c.items > cap.items) return;
+    TableDesc d;
+    d.item_off = (uint64_t)offsets[t];
+    d.n = (uint64_t)n;
+    d.heavy_off = ex.items;
+    d.tile0 = ex.tiles;
+    d.ntiles = c.tiles;
+    d.id = (uint32_t)t;
+    d.pad = 0;
+    desc[ex.tables] = d;
+    for (uint32_t k = 0; k < c.tiles; ++k) tile_table[ex.tiles + k] = ex.tables;
+}
+
+// ---------------------------------------------------------------- large tables: W
+// One CTA per global tile sums its items (double-double, the partial goes to partials[g]);
+// the last CTA of each table (ticket in the table's header) combines the table's partials
+// in tile order and fills the header as wsum_kernel does for a single table.
+constexpr int kBatchWsumThreads = 256;
+
+template <int T>
+__global__ void __launch_bounds__(kBatchWsumThreads) batch_wsum_kernel(const float* __restrict__ w,
+                                                                       BuildHeader* hdrs, double2* partials,
+                                                                       TileMap map, double* W_out) {
+    constexpr int NT = kBatchWsumThreads;
+    const uint32_t g = blockIdx.x;
+    if (plan_failed<true>(map)) return;
+    const TileRef tr = tile_ref<true>(map, g);
+    BuildHeader* hdr = hdrs + tr.table;
+    const float* wt = w + tr.item_off;
+    const uint64_t i0 = (uint64_t)tr.local * T, i1 = min(tr.n, i0 + T);
+    DD acc = {0.0, 0.0};
+    bool bad = false;
+    for (uint64_t i = i0 + threadIdx.x; i < i1; i += NT) {
+        const float x = __ldg(wt + i);
+        bad |= weight_invalid(x);
+        acc = dd_add_d(acc, (double)x);
+    }
+    if (bad) record_status(&hdr->status, kErrInvalidWeight);
+    __shared__ DD s_part[NT / 32];
+    __shared__ bool s_last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    acc = dd_norm(acc);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        DD o;
+        o.hi = __shfl_down_sync(0xffffffffu, acc.hi, off);
+        o.lo = __shfl_down_sync(0xffffffffu, acc.lo, off);
+        acc = dd_add(acc, o);
+    }
+    if (lane == 0) s_part[warp] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        DD t = s_part[0];
+        for (int i = 1; i < NT / 32; ++i) t = dd_add(t, s_part[i]);
+        partials[g] = make_double2(t.hi, t.lo);
+        __threadfence();
+        const uint32_t ticket = atomicAdd(&hdr->wsum_ticket, 1u);
+        s_last = (ticket == tr.ntiles - 1);
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    DD t = {0.0, 0.0};
+    for (uint32_t i = threadIdx.x; i < tr.ntiles; i += NT) {
+        const double2 p = __ldcg(partials + tr.tile0 + i);
+        const DD pd = {p.x, p.y};
+        t = dd_add(t, pd);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        DD o;
+        o.hi = __shfl_down_sync(0xffffffffu, t.hi, off);
+        o.lo = __shfl_down_sync(0xffffffffu, t.lo, off);
+        t = dd_add(t, o);
+    }
+    __syncthreads();
+    if (lane == 0) s_part[warp] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        DD r = s_part[0];
+        for (int i = 1; i < NT / 32; ++i) r = dd_add(r, s_part[i]);
+        r = dd_norm(r);
+        hdr->W_hi = r.hi;
+        hdr->W_lo = r.lo;
+        const double W_N = r.hi / (double)tr.n;
+        hdr->W_N = W_N;
+        hdr->R = 1.0 / W_N;
+        const ClassParams cp = class_params(W_N, 1.0 / W_N);
+        hdr->R32 = cp.R32;
+        hdr->H1 = cp.H1;
+        hdr->Hh = cp.Hh;
+        if (W_out) W_out[map.desc[tr.table].id] = r.hi;
+        if (!(r.hi > 0.0) || isinf(r.hi)) record_status(&hdr->status, isinf(r.hi) ? kErrInvalidWeight : kErrZeroTotal);
+    }
+}
+
+// ---------------------------------------------------------------- large tables: tile prefixes
+// One CTA per large table: inclusive prefixes of its tiles' aggregates (chunks of
+// kPrefixTiles tiles with a carry), and the table's excess correction.
+__global__ void __launch_bounds__(kPrefixThreads) batch_prefix_kernel(BuildHeader* hdrs, const TileVals* agg,
+                                                                     TileVals* incl, const TableDesc* desc,
+                                                                     const uint32_t* plan_status) {
+    __shared__ PVals s_warp[kPrefixThreads / 32];
+    if (__ldg(plan_status) != 0) return;
+    const TableDesc d = desc[blockIdx.x];
+    BuildHeader* hdr = hdrs + blockIdx.x;
+    if (load_relaxed(&hdr->status) != 0) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    PVals carry = pv_zero();
+    for (uint32_t c = 0; c < d.ntiles; c += kPrefixTiles) {
+        const uint32_t t0 = c + threadIdx.x * kPrefixPerThread;
+        PVals loc[kPrefixPerThread];
+        PVals run = pv_zero();
+#pragma unroll
+        for (int k = 0; k < kPrefixPerThread; ++k) {
+            const PVals v = (t0 + k < d.ntiles) ? pv_of(agg[d.tile0 + t0 + k]) : pv_zero();
+            run = pv_add(run, v);
+            loc[k] = run;
+        }
+        PVals inc = run;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const PVals o = pv_shfl_up(inc, off);
+            if (lane >= off) inc = pv_add(inc, o);
+        }
+        if (lane == 31) s_warp[warp] = inc;
+        __syncthreads();
+        PVals base = carry, tot = carry;
+        for (int i = 0; i < kPrefixThreads / 32; ++i) {
+            const PVals t = s_warp[i];
+            if (i < warp) base = pv_add(base, t);
+            tot = pv_add(tot, t);
+        }
+        base = pv_add(base, inc);
+        base.nL -= run.nL;
+        base.nH -= run.nH;
+        base.S -= run.S;
+        base.L -= run.L;
+        base.E -= run.E;
+#pragma unroll
+        for (int k = 0; k < kPrefixPerThread; ++k) {
+            if (t0 + k >= d.ntiles) break;
+            const PVals v = pv_add(base, loc[k]);
+            TileVals o;
+            o.nL = v.nL;
+            o.nH = v.nH;
+            o.first_heavy = 0xffffffffu;
+            o.last_heavy = 0xffffffffu;
+            o.S = v.S;
+            o.L = v.L;
+            o.E = v.E;
+            incl[d.tile0 + t0 + k] = o;
+            if (t0 + k == d.ntiles - 1) hdr->nfix = excess_correction(v.S + q_round24(v.L), v.E);
+        }
+        carry = tot;
+        __syncthreads();
+    }
+}
+
+// The first error of any large table's build (or of the plan) goes to the batch status word.
+__global__ void batch_status_kernel(const BuildHeader* hdrs, uint32_t num_tables, uint32_t* status) {
+    for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < num_tables; b += gridDim.x * blockDim.x) {
+        const uint32_t st = hdrs[b].status;
+        if (st != 0) record_status(status, st);
+    }
+}
+
+// ---------------------------------------------------------------- small tables: one warp each
+// The whole build of a table of n <= 32 * SPL items in one warp. Lane l holds the
+// ipl = ceil(n / 32) consecutive items l * ipl ..; the quantities are those of the tiled
+// passes for a one-tile table (A_before = 0, no dithering offset), so the rows equal a
+// single-table build's. Shared memory per warp: light keys from the front and heavy keys
+// from the back of one u64 array, and the heavies' corrected excess ends and items.
+constexpr int kSmallWarps = 4;
+
+template <int SPL>
+struct SmallSmem {
+    static constexpr int CAP = 32 * SPL;
+    uint64_t key[CAP];
+    uint64_t elo[CAP];
+    uint32_t ehi[CAP];
+    uint32_t item[CAP];
+};
+
+template <int SPL>
+__global__ void __launch_bounds__(32 * kSmallWarps) small_tables_kernel(const float* __restrict__ w,
+                                                                       const int64_t* __restrict__ offsets,
+                                                                       int64_t num_tables, uint32_t small_max,
+                                                                       wrs_alias_row* __restrict__ table,
+                                                                       double* W_out, uint32_t* status) {
+    constexpr int CAP = 32 * SPL;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    SmallSmem<SPL>& sm = reinterpret_cast<SmallSmem<SPL>*>(smem_raw)[warp];
+    const int64_t nwarps = (int64_t)gridDim.x * kSmallWarps;
+    for (int64_t t = (int64_t)blockIdx.x * kSmallWarps + warp; t < num_tables; t += nwarps) {
+        const int64_t off = offsets[t];
+        const int64_t nn = offsets[t + 1] - off;
+        if (nn < 1 || nn > (int64_t)small_max || nn > CAP) continue;
+        const uint32_t n = (uint32_t)nn;
+        const uint32_t ipl = (n + 31) / 32;
+        const float* wt = w + off;
+        wrs_alias_row* rows = table + off;
+        const uint32_t i0 = (uint32_t)lane * ipl;
+        float x[SPL];
+        DD acc = {0.0, 0.0};
+        bool bad = false;
+#pragma unroll
+        for (int k = 0; k < SPL; ++k) {
+            const uint32_t i = i0 + k;
+            const bool in = (uint32_t)k < ipl && i < n;
+            x[k] = in ? __ldg(wt + i) : -1.0f;
+            if (in) {
+                bad |= weight_invalid(x[k]);
+                acc = dd_add_d(acc, (double)x[k]);
+            }
+        }
+        acc = dd_norm(acc);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            DD v;
+            v.hi = __shfl_down_sync(0xffffffffu, acc.hi, o);
+            v.lo = __shfl_down_sync(0xffffffffu, acc.lo, o);
+            acc = dd_add(acc, v);
+        }
+        acc = dd_norm(acc);
+        const double W = __shfl_sync(0xffffffffu, acc.hi, 0);
+        const bool any_bad = __any_sync(0xffffffffu, bad);
+        if (any_bad || !(W > 0.0) || isinf(W)) {
+            if (lane == 0) record_status(status, (any_bad || isinf(W)) ? kErrInvalidWeight : kErrZeroTotal);
+            continue;
+        }
+        if (lane == 0 && W_out) W_out[t] = W;
+        const double W_N = W / (double)n;
+        const ClassParams cp = class_params(W_N, 1.0 / W_N);
+        // classification and per-lane sums
+        float pk[SPL];
+        uint32_t lbits = 0, hbits = 0, gbits = 0;
+        uint64_t S = 0, L = 0, E = 0;
+#pragma unroll
+        for (int k = 0; k < SPL; ++k) {
+            const float wk = x[k];
+            const bool heavy = wk > cp.H1;
+            const bool small = wk >= 0.0f && wk < cp.Hh;
+            const bool large = wk >= cp.Hh && !heavy;
+            const float p = __fmul_rn(wk, cp.R32);
+            pk[k] = p;
+            lbits |= (uint32_t)(small || large) << k;
+            hbits |= (uint32_t)heavy << k;
+            gbits |= (uint32_t)large << k;
+            if (small) S += small_deficit(p);
+            if (large) L += rare_q(wk, false, cp);
+            if (heavy) E += rare_q(wk, true, cp);
+        }
+        uint32_t nl_tot, nh_tot;
+        const uint32_t l0 = warp_excl_scan_u32((uint32_t)__popc(lbits), nl_tot);
+        const uint32_t h0 = warp_excl_scan_u32((uint32_t)__popc(hbits), nh_tot);
+        uint64_t S_tot, L_tot, E_tot;
+        const uint64_t s0 = warp_excl_scan_u64(S, S_tot);
+        const uint64_t lq0 = warp_excl_scan_u64(L, L_tot);
+        const uint64_t e0 = warp_excl_scan_u64(E, E_tot);
+        const u128 A_tot = ((u128)S_tot << 16) + q_round24((u128)L_tot << 16);
+        const int64_t nfix = excess_correction(A_tot, (u128)E_tot << 40);
+        Dither dth;
+        dth.c0 = 1ull << 23;
+        dth.c0h = 0;
+        // keys: lights from the front, heavies from the back (CAP - nh_tot + j)
+        {
+            uint64_t sr = s0, lr = lq0, er = e0;
+            uint64_t D = dither_at(dth, lr);
+            uint32_t li = l0, hj = h0;
+#pragma unroll
+            for (int k = 0; k < SPL; ++k) {
+                const float wk = x[k];
+                if ((lbits >> k) & 1u) {
+                    sm.key[li++] = sr + D;
+                    if ((gbits >> k) & 1u) {
+                        lr += rare_q(wk, false, cp);
+                        const uint64_t D1 = dither_at(dth, lr);
+                        pk[k] = dithered_prob(D1 - D);
+                        D = D1;
+                    } else {
+                        sr += small_deficit(pk[k]);
+                    }
+                } else if ((hbits >> k) & 1u) {
+                    er += rare_q(wk, true, cp);
+                    const u128 Et = q_scale_excess((u128)er << 40, nfix);
+                    const u128 d = Et + 0xffff;
+                    sm.key[CAP - nh_tot + hj] = (q_hi(d) >> 16) ? ~0ull : (uint64_t)(d >> 16);
+                    sm.elo[hj] = q_lo(Et);
+                    sm.ehi[hj] = (uint32_t)q_hi(Et);
+                    sm.item[hj] = i0 + k;
+                    ++hj;
+                }
+            }
+        }
+        __syncwarp();
+        const uint64_t* hkey = sm.key + (CAP - nh_tot);
+        // heavy rows
+        for (uint32_t j = lane; j < nh_tot; j += 32) {
+            const uint64_t kh = hkey[j];
+            uint32_t lo = 0, hi = nl_tot;  // rank: the first light whose key is not below kh
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (sm.key[mid] < kh) lo = mid + 1; else hi = mid;
+            }
+            const u128 Et = q_make(sm.ehi[j], sm.elo[j]);
+            const u128 A_next = (lo < nl_tot) ? ((u128)sm.key[lo] << 16) : A_tot;
+            wrs_alias_row r;
+            r.prob = heavy_row_prob(q_one() + Et - A_next);
+            r.alias = (j + 1 < nh_tot) ? sm.item[j + 1] : sm.item[j];
+            rows[sm.item[j]] = r;
+        }
+        // light rows: alias = the first heavy whose key exceeds the light's (else the last heavy)
+        {
+            uint32_t li = l0;
+#pragma unroll
+            for (int k = 0; k < SPL; ++k) {
+                if (!((lbits >> k) & 1u)) continue;
+                uint32_t al;
+                if (nh_tot == 0) {
+                    al = i0 + k;
+                } else {
+                    const uint64_t kl = sm.key[li];
+                    uint32_t lo = 0, hi = nh_tot;
+                    while (lo < hi) {
+                        const uint32_t mid = (lo + hi) >> 1;
+                        if (hkey[mid] > kl) hi = mid; else lo = mid + 1;
+                    }
+                    al = sm.item[lo < nh_tot ? lo : nh_tot - 1];
+                }
+                wrs_alias_row r;
+                r.prob = pk[k];
+                r.alias = al;
+                rows[i0 + k] = r;
+                ++li;
+            }
+        }
+        __syncwarp();  // the next table reuses this warp's shared memory
+    }
+}
+
+// ---------------------------------------------------------------- batched plain sampling
+// Output position s of the batch belongs to table t with sample_offsets[t] <= s <
+// sample_offsets[t + 1] and follows the plain contract over the global position s:
+// Philox counter counter_base + floor(s / 2), row = floor(x_first * n_t / 2^32) (table-local),
+// coin = (x_second >> 8) * 2^-24, result = coin < prob[row] ? row : alias[row]. Every thread
+// takes kBatchSamplePer consecutive positions: it finds the table of its first one by a
+// binary search of the sample offsets and walks forward from there.
+constexpr int kBatchSampleThreads = 256;
+constexpr int kBatchSamplePer = 8;
+
+__global__ void __launch_bounds__(kBatchSampleThreads) batch_sample_kernel(
+    const wrs_alias_row* __restrict__ table, const int64_t* __restrict__ offsets, int64_t num_tables,
+    const int64_t* __restrict__ sample_offsets, uint64_t total, uint64_t seed, uint64_t counter_base,
+    uint32_t* __restrict__ out, uint32_t* status) {
+    const uint64_t s0 = ((uint64_t)blockIdx.x * kBatchSampleThreads + threadIdx.x) * kBatchSamplePer;
+    if (s0 >= total) return;
+    // the last table whose sample range starts at or before s0
+    int64_t lo = 0, hi = num_tables - 1;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi + 1) >> 1;
+        if ((uint64_t)__ldg(sample_offsets + mid) <= s0) lo = mid; else hi = mid - 1;
+    }
+    int64_t t = lo;
+    uint64_t s_end_t = (uint64_t)__ldg(sample_offsets + t + 1);
+    const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+    const uint64_t s1 = min(total, s0 + kBatchSamplePer);
+    Philox4 x{};
+    uint64_t have = ~0ull;
+    for (uint64_t s = s0; s < s1; ++s) {
+        while (s >= s_end_t && t + 1 < num_tables) {
+            ++t;
+            s_end_t = (uint64_t)__ldg(sample_offsets + t + 1);
+        }
+        const uint64_t b = counter_base + (s >> 1);
+        if (b != have) {
+            x = philox4x32_10((uint32_t)b, (uint32_t)(b >> 32), 0u, 0u, k0, k1);
+            have = b;
+        }
+        const uint32_t xr = (s & 1) ? x.x[2] : x.x[0];
+        const uint32_t xc = (s & 1) ? x.x[3] : x.x[1];
+        const int64_t off = __ldg(offsets + t);
+        const uint64_t n = (uint64_t)(__ldg(offsets + t + 1) - off);
+        if (n == 0 || n > 0xffffffffull || s >= s_end_t) {
+            out[s] = 0xffffffffu;
+            if (status) record_status(status, WRS_ERR_INVALID_ARGUMENT);
+            continue;
+        }
+        const uint32_t row = scale_u32(xr, (uint32_t)n);
+        const uint2 e = __ldg(reinterpret_cast<const uint2*>(table + off) + row);
+        out[s] = coin24(xc) < __uint_as_float(e.x) ? row : e.y;
+    }
+}
+
+}  // namespace wrs

@@ -79,22 +79,6 @@ int64_t tile_items_for(const wrs_build_opts* opts) {
     }
 }
 
-// Pack CTA shape per tile size: threads x items per thread.
-template <int T>
-struct PackShape;
-template <>
-struct PackShape<1024> {
-    static constexpr int NT = 128, IPT = 8;
-};
-template <>
-struct PackShape<2048> {
-    static constexpr int NT = 128, IPT = 16;
-};
-template <>
-struct PackShape<4096> {
-    static constexpr int NT = 256, IPT = 16;
-};
-
 struct BuildLayout {
     BuildHeader* hdr;
     double2* partials;
@@ -137,21 +121,22 @@ wrs_status launch_build(const float* d_w, uint64_t n, uint32_t method, wrs_alias
     const uint64_t zero_words = L.num_blocks * sizeof(BlockWord) / sizeof(uint32_t);
     wsum_kernel<kWsumBlock><<<g, kWsumBlock, 0, stream>>>(d_w, n, L.hdr, L.partials,
                                                           reinterpret_cast<uint32_t*>(L.blocks), zero_words, d_W);
-    tile_reduce_kernel<T><<<(uint32_t)num_tiles, kReduceThreads, 0, stream>>>(d_w, n, L.hdr, L.agg, L.hmask,
-                                                                              (uint32_t)num_tiles);
+    const TileMap map{nullptr, nullptr, nullptr, n, (uint32_t)num_tiles};
+    tile_reduce_kernel<T, false><<<(uint32_t)num_tiles, kReduceThreads, 0, stream>>>(d_w, L.hdr, L.agg, L.hmask, map);
     tile_prefix_kernel<<<(uint32_t)L.num_blocks, kPrefixThreads, 0, stream>>>(L.hdr, L.agg, L.incl, L.blocks,
                                                                                (uint32_t)num_tiles);
-    heavy_list_kernel<T><<<(uint32_t)((num_tiles + heavy_warps(T) - 1) / heavy_warps(T)), 32 * heavy_warps(T), 0, stream>>>(d_w, L.hdr, L.agg, L.incl, L.hmask,
-                                                                             (uint32_t)num_tiles, L.heavy_item,
-                                                                             L.heavy_E);
-    tile_link_kernel<<<(uint32_t)((num_tiles + 1 + 255) / 256), 256, 0, stream>>>(L.hdr, L.incl, (uint32_t)num_tiles,
-                                                                                  L.heavy_E, L.starts);
+    heavy_list_kernel<T, false><<<(uint32_t)((num_tiles + heavy_warps(T) - 1) / heavy_warps(T)), 32 * heavy_warps(T),
+                                  0, stream>>>(d_w, L.hdr, L.agg, L.incl, L.hmask, (uint32_t)num_tiles, L.heavy_item,
+                                               L.heavy_E, map);
+    tile_link_kernel<false><<<(uint32_t)((num_tiles + 1 + 255) / 256), 256, 0, stream>>>(
+        L.hdr, L.incl, (uint32_t)num_tiles, 1u, L.heavy_E, L.starts, map);
     {
         const size_t smem = pack_smem_bytes(T);
-        e = cudaFuncSetAttribute(split_pack_kernel<NT, IPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = cudaFuncSetAttribute(split_pack_kernel<NT, IPT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
         if (e != cudaSuccess) return WRS_ERR_CUDA;
-        split_pack_kernel<NT, IPT><<<(uint32_t)num_tiles, NT, smem, stream>>>(
-            d_w, n, L.hdr, L.incl, L.starts, L.heavy_item, L.heavy_E, (uint32_t)num_tiles, d_table);
+        split_pack_kernel<NT, IPT, false><<<(uint32_t)num_tiles, NT, smem, stream>>>(
+            d_w, L.hdr, L.incl, L.starts, L.heavy_item, L.heavy_E, (uint32_t)num_tiles, d_table, map);
     }
     return launch_status();
 }

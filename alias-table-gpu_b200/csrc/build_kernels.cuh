@@ -506,6 +506,75 @@ __device__ __forceinline__ u128 ldcg_E(const TileVals* src) {
     return q_make(((uint64_t)w3.w << 32) | w3.z, ((uint64_t)w3.y << 32) | w3.x);
 }
 
+// ---------------------------------------------------------------- tile spaces
+// The passes work on tiles of T items. A single-table build numbers the tiles of its table
+// 0..num_tiles-1. A batched build (many CSR tables) lays the tiles of its multi-tile tables
+// end to end: tile_table[g] names the table (its index in the batch's list of such tables)
+// of global tile g, and TableDesc places that table in the CSR arrays. Rows, heavy items and
+// aliases are table-local; per-table arrays (weights, rows, heavy list) are addressed from
+// the table's offsets, per-tile arrays (aggregates, prefixes, masks) by global tile, and the
+// tile starts of table b from tile0 + b (a table of k tiles has k + 1 starts).
+struct TableDesc {
+    uint64_t item_off;   // first item of the table in the CSR arrays
+    uint64_t n;          // items
+    uint64_t heavy_off;  // first entry of the table's heavy list (the listed tables' items, packed)
+    uint32_t tile0;      // first global tile
+    uint32_t ntiles;
+    uint32_t id;         // the table's index in the CSR offsets
+    uint32_t pad;
+};
+static_assert(sizeof(TableDesc) == 40, "TableDesc layout");
+struct TileMap {
+    const uint32_t* tile_table;   // batched: list index of every global tile's table
+    const TableDesc* desc;        // batched: per listed table
+    const uint32_t* plan_status;  // batched: nonzero if the plan does not match the launch
+    uint64_t n;                   // single table: items
+    uint32_t ntiles;              // single table: tiles
+};
+struct TileRef {
+    uint32_t table;  // list index (0 for a single table)
+    uint32_t local;  // tile index within the table
+    uint32_t tile0;
+    uint32_t ntiles;
+    uint64_t item_off;
+    uint64_t n;
+    uint64_t heavy_off;
+};
+__device__ __forceinline__ TileRef table_ref(const TableDesc& d, uint32_t table, uint32_t local) {
+    TileRef r;
+    r.table = table;
+    r.local = local;
+    r.tile0 = d.tile0;
+    r.ntiles = d.ntiles;
+    r.item_off = d.item_off;
+    r.n = d.n;
+    r.heavy_off = d.heavy_off;
+    return r;
+}
+// Batched kernels return at once when the plan is unusable (then tile_table and desc may be
+// incomplete); a single table has no plan.
+template <bool BATCH>
+__device__ __forceinline__ bool plan_failed(const TileMap& map) {
+    return BATCH && __ldg(map.plan_status) != 0;
+}
+template <bool BATCH>
+__device__ __forceinline__ TileRef tile_ref(const TileMap& map, uint32_t g) {
+    if (BATCH) {
+        const uint32_t t = __ldg(map.tile_table + g);
+        const TableDesc d = map.desc[t];
+        return table_ref(d, t, g - d.tile0);
+    }
+    TileRef r;
+    r.table = 0;
+    r.local = g;
+    r.tile0 = 0;
+    r.ntiles = map.ntiles;
+    r.item_off = 0;
+    r.n = map.n;
+    r.heavy_off = 0;
+    return r;
+}
+
 // ---------------------------------------------------------------- pass 2: tile reduce
 // One tile per CTA: counts and sums of the three streams, the tile's first and last heavy
 // item, and its heavy mask (bit i of word i/32 <=> tile item i is heavy). No inter-CTA waits.
@@ -517,23 +586,25 @@ __device__ __forceinline__ uint64_t warp_sum_u64(uint64_t v) {
     return v;
 }
 
-template <int T>
-__global__ void __launch_bounds__(kReduceThreads) tile_reduce_kernel(const float* __restrict__ w, uint64_t n,
+template <int T, bool BATCH>
+__global__ void __launch_bounds__(kReduceThreads) tile_reduce_kernel(const float* __restrict__ w,
                                                                      const BuildHeader* hdr, TileVals* agg,
-                                                                     uint32_t* __restrict__ hmask,
-                                                                     uint32_t num_tiles) {
+                                                                     uint32_t* __restrict__ hmask, TileMap map) {
     constexpr int IPT = T / kReduceThreads;
     constexpr int NW = kReduceThreads / 32;
     static_assert(IPT >= 4 && IPT <= 32 && (IPT & (IPT - 1)) == 0, "items per thread");
     __shared__ uint32_t s_nl[NW], s_nh[NW], s_fh[NW], s_lh[NW];
     __shared__ uint64_t s_s[NW], s_l[NW], s_e[NW];
-    (void)num_tiles;
-    const uint32_t tile = blockIdx.x;
+    const uint32_t tile = blockIdx.x;  // global tile
+    if (plan_failed<BATCH>(map)) return;
+    const TileRef tr = tile_ref<BATCH>(map, tile);
+    const float* wt = w + tr.item_off;
     float x[IPT];
-    load_items<kReduceThreads, IPT>(w, n, tile, threadIdx.x, x);  // first: independent of the header
+    load_items<kReduceThreads, IPT>(wt, tr.n, tr.local, threadIdx.x, x);  // first: independent of the header
+    hdr += tr.table;
     if (earlier_status(hdr) != 0) return;
     const ClassParams cp = load_class_params(hdr);
-    const uint64_t item0 = (uint64_t)tile * T + (uint64_t)threadIdx.x * IPT;
+    const uint64_t item0 = (uint64_t)tr.local * T + (uint64_t)threadIdx.x * IPT;  // table-local
     uint32_t lbits = 0, sbits = 0, hbits = 0;
     uint64_t S = 0;
 #pragma unroll
@@ -553,7 +624,7 @@ __global__ void __launch_bounds__(kReduceThreads) tile_reduce_kernel(const float
     for (uint32_t bits = (lbits & ~sbits) | hbits; bits; bits &= bits - 1) {
         const int k = __ffs(bits) - 1;
         const bool heavy = (hbits >> k) & 1u;
-        const uint64_t q = rare_q(__ldg(w + item0 + k), heavy, cp);
+        const uint64_t q = rare_q(__ldg(wt + item0 + k), heavy, cp);
         E += heavy ? q : 0ull;
         L += heavy ? 0ull : q;
     }
@@ -848,28 +919,33 @@ __device__ __forceinline__ uint64_t warp_excl_scan_u64(uint64_t v, uint64_t& tot
     return inc - v;
 }
 
-template <int T>
+template <int T, bool BATCH>
 __global__ void __launch_bounds__(32 * heavy_warps(T)) heavy_list_kernel(const float* __restrict__ w,
                                                                       const BuildHeader* hdr, const TileVals* agg,
                                                                       const TileVals* incl,
                                                                       const uint32_t* __restrict__ hmask,
                                                                       uint32_t num_tiles, uint32_t* heavy_item,
-                                                                      uint4* heavy_E) {
+                                                                      uint4* heavy_E, TileMap map) {
     constexpr int WPT = T / 32;  // mask words per tile
     constexpr int WPL = WPT / 32;  // mask words per lane
     static_assert(WPL >= 1 && WPL <= 4, "mask words per lane");
     constexpr int NWARP = heavy_warps(T);
     __shared__ uint32_t sItem[NWARP][T];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t u = blockIdx.x * NWARP + warp;
-    if (u >= num_tiles) return;
+    const uint32_t u = blockIdx.x * NWARP + warp;  // global tile
+    if (u >= num_tiles || plan_failed<BATCH>(map)) return;
+    const TileRef tr = tile_ref<BATCH>(map, u);
+    hdr += tr.table;
     if (earlier_status(hdr) != 0) return;
     const uint32_t m = __ldcg(&agg[u].nH);
     if (m == 0) return;
+    const float* wt = w + tr.item_off;
+    heavy_item += tr.heavy_off;
+    heavy_E += tr.heavy_off;
     const ClassParams cp = load_class_params(hdr);
     const int64_t nfix = __ldg(&hdr->nfix);
-    const uint32_t g0 = u ? __ldcg(&incl[u - 1].nH) : 0u;
-    const u128 Eb = u ? ldcg_E(incl + u - 1) : (u128)0;
+    const uint32_t g0 = tr.local ? __ldcg(&incl[u - 1].nH) : 0u;
+    const u128 Eb = tr.local ? ldcg_E(incl + u - 1) : (u128)0;
     uint32_t* items = sItem[warp];
     {
         // lane l holds mask words l*WPL .. l*WPL + WPL - 1 (consecutive tile items)
@@ -884,7 +960,7 @@ __global__ void __launch_bounds__(32 * heavy_warps(T)) heavy_list_kernel(const f
         uint32_t o = warp_excl_scan_u32(c, ctot);
 #pragma unroll
         for (int i = 0; i < WPL; ++i) {
-            const uint32_t ibase = u * (uint32_t)T + (uint32_t)(lane * WPL + i) * 32u;
+            const uint32_t ibase = tr.local * (uint32_t)T + (uint32_t)(lane * WPL + i) * 32u;
             for (uint32_t b = wd[i]; b; b &= b - 1) items[o++] = ibase + (uint32_t)(__ffs(b) - 1);
         }
     }
@@ -892,11 +968,11 @@ __global__ void __launch_bounds__(32 * heavy_warps(T)) heavy_list_kernel(const f
     const uint32_t per = (m + 31) / 32;
     const uint32_t j0 = min(m, (uint32_t)lane * per), j1 = min(m, j0 + per);
     uint64_t hs = 0;
-    for (uint32_t j = j0; j < j1; ++j) hs += rare_q(__ldg(w + items[j]), true, cp);
+    for (uint32_t j = j0; j < j1; ++j) hs += rare_q(__ldg(wt + items[j]), true, cp);
     uint64_t htot;
     uint64_t er = warp_excl_scan_u64(hs, htot);
     for (uint32_t j = j0; j < j1; ++j) {
-        er += rare_q(__ldg(w + items[j]), true, cp);  // the weight again, from L1
+        er += rare_q(__ldg(wt + items[j]), true, cp);  // the weight again, from L1
         heavy_item[g0 + j] = items[j];
         store_u128(heavy_E + g0 + j, q_scale_excess(Eb + ((u128)er << 40), nfix));
     }
@@ -917,19 +993,36 @@ struct __align__(16) TileStart {
 };
 static_assert(sizeof(TileStart) == 32, "TileStart layout");
 
-static __global__ void __launch_bounds__(256) tile_link_kernel(const BuildHeader* hdr, const TileVals* incl,
-                                                               uint32_t num_tiles, const uint4* heavy_E,
-                                                               TileStart* starts) {
+// One thread per start: the starts of the global tiles, then (batched) the end of each table.
+template <bool BATCH>
+__global__ void __launch_bounds__(256) tile_link_kernel(const BuildHeader* hdr, const TileVals* incl,
+                                                        uint32_t num_tiles, uint32_t num_tables,
+                                                        const uint4* heavy_E, TileStart* starts, TileMap map) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (plan_failed<BATCH>(map)) return;
+    TileRef tr;
+    if (!BATCH) {
+        if (i > num_tiles) return;
+        tr = tile_ref<false>(map, 0);
+        tr.local = i;  // the boundary: i == num_tiles is the table's end
+    } else if (i < num_tiles) {
+        tr = tile_ref<true>(map, i);
+    } else {
+        if (i >= num_tiles + num_tables) return;
+        const uint32_t t = i - num_tiles;
+        tr = table_ref(map.desc[t], t, map.desc[t].ntiles);
+    }
+    hdr += tr.table;
     if (earlier_status(hdr) != 0) return;
-    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b > num_tiles) return;
-    const uint32_t nH = __ldg(&incl[num_tiles - 1].nH);
-    const TileVals pv = b ? ldcg_tilevals(incl + b - 1) : tv_zero();
+    heavy_E += tr.heavy_off;
+    const uint32_t b = tr.local;
+    const uint32_t nH = __ldg(&incl[tr.tile0 + tr.ntiles - 1].nH);
+    const TileVals pv = b ? ldcg_tilevals(incl + tr.tile0 + b - 1) : tv_zero();
     const u128 X = deficit_line(pv);
     uint32_t g;
     if (b == 0) {
         g = 0;
-    } else if (b == num_tiles) {
+    } else if (b == tr.ntiles) {
         g = nH;
     } else {
         uint32_t lo = 0, hi = nH;
@@ -945,10 +1038,26 @@ static __global__ void __launch_bounds__(256) tile_link_kernel(const BuildHeader
     ts.c0 = make_dither(pv.L).c0;
     ts.bound = g;
     ts.pad = 0;
-    starts[b] = ts;
+    starts[tr.tile0 + tr.table + b] = ts;
 }
 
 // ---------------------------------------------------------------- pass 6: pack
+// Pack CTA shape per tile size: threads x items per thread.
+template <int T>
+struct PackShape;
+template <>
+struct PackShape<1024> {
+    static constexpr int NT = 128, IPT = 8;
+};
+template <>
+struct PackShape<2048> {
+    static constexpr int NT = 128, IPT = 16;
+};
+template <>
+struct PackShape<4096> {
+    static constexpr int NT = 256, IPT = 16;
+};
+
 // Heavies per chunk for T items per tile: the own-tile phase keeps a u64 per tile item in
 // the chunk arrays (16 * C >= 8 * T bytes).
 __host__ __device__ constexpr int pack_chunk(int T) { return T / 2 > 1024 ? T / 2 : 1024; }
@@ -980,13 +1089,13 @@ __device__ __forceinline__ uint32_t stage_pos(uint32_t i) {
 //      compares indices with ranks.
 //  (3) Light rows, staged in shared memory and written out coalesced (the heavies' rows of
 //      this tile belong to the tiles that own them).
-template <int NT, int IPT>
-__global__ void __launch_bounds__(NT, (NT == 128 && IPT == 16) ? 6 : 1) split_pack_kernel(const float* __restrict__ w, uint64_t n,
+template <int NT, int IPT, bool BATCH>
+__global__ void __launch_bounds__(NT, (NT == 128 && IPT == 16) ? 6 : 1) split_pack_kernel(const float* __restrict__ w,
                                                         const BuildHeader* hdr, const TileVals* incl,
                                                         const TileStart* __restrict__ starts,
                                                         const uint32_t* __restrict__ heavy_item,
                                                         const uint4* __restrict__ heavy_E, uint32_t num_tiles,
-                                                        wrs_alias_row* __restrict__ table) {
+                                                        wrs_alias_row* __restrict__ table, TileMap map) {
     constexpr int T = NT * IPT;
     constexpr int C = pack_chunk(T);
     static_assert(16 * C >= 8 * T, "own-tile slots live in the chunk arrays");
@@ -1003,15 +1112,24 @@ __global__ void __launch_bounds__(NT, (NT == 128 && IPT == 16) ? 6 : 1) split_pa
     __shared__ float s_pend_prob;
 
     const int tid = threadIdx.x;
-    const uint32_t tile = num_tiles - 1 - blockIdx.x;  // descending: the previous passes ended at
-                                                       // the last tiles, still in L2
+    const uint32_t gtile = num_tiles - 1 - blockIdx.x;  // descending: the previous passes ended at
+                                                        // the last tiles, still in L2
+    if (plan_failed<BATCH>(map)) return;
+    const TileRef tr = tile_ref<BATCH>(map, gtile);
+    const uint32_t tile = tr.local;
+    const uint64_t n = tr.n;
+    w += tr.item_off;
+    table += tr.item_off;
+    heavy_item += tr.heavy_off;
+    heavy_E += tr.heavy_off;
     // ---- (1) own tile (the weights' loads go out first: they do not depend on the header)
     float x[IPT];
     load_items<NT, IPT>(w, n, tile, tid, x);
+    hdr += tr.table;
     if (earlier_status(hdr) != 0) return;
     const ClassParams cp = load_class_params(hdr);
-    const uint32_t nH = __ldg(&incl[num_tiles - 1].nH);
-    const TileStart st0 = starts[tile], st1 = starts[tile + 1];
+    const uint32_t nH = __ldg(&incl[tr.tile0 + tr.ntiles - 1].nH);
+    const TileStart st0 = starts[tr.tile0 + tr.table + tile], st1 = starts[tr.tile0 + tr.table + tile + 1];
     const u128 A_before = q_make(st0.A_hi, st0.A_lo);
     const u128 A_after = q_make(st1.A_hi, st1.A_lo);
     const uint32_t item0 = (uint32_t)((uint64_t)tile * T + (uint64_t)tid * IPT);

@@ -44,7 +44,7 @@ WRS_SAMPLE_SECTIONED = 1
 
 class BuildOpts(ctypes.Structure):
     _fields_ = [("method", ctypes.c_uint32), ("tile_items", ctypes.c_uint32),
-                ("flags", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("flags", ctypes.c_uint32), ("small_table_items", ctypes.c_uint32)]
 
 
 class SampleOpts(ctypes.Structure):
@@ -78,6 +78,7 @@ _SIGNATURES = {
     "wrs_batched_build_scratch_bytes": (_SZ, [_P, _I64, _P]),
     "wrs_batched_build_f32": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P, _SZ, _P]),
     "wrs_batched_sample": (ctypes.c_int, [_P, _P, _I64, _P, _U64, _U64, _U64, _P, _P]),
+    "wrs_batched_autotune": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _SZ, _P, _P]),
     "wrs_scratch_status": (ctypes.c_int, [_P, _P]),
     "wrs_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "wrs_check_device": (ctypes.c_int, []),
@@ -128,8 +129,9 @@ def _stream(stream) -> Optional[int]:
 
 # ---------------------------------------------------------------- C ABI wrappers
 
-def build_opts(method: int = WRS_METHOD_SPLIT, tile_items: int = 0, sync: bool = False) -> BuildOpts:
-    return BuildOpts(method, tile_items, WRS_FLAG_SYNC if sync else 0, 0)
+def build_opts(method: int = WRS_METHOD_SPLIT, tile_items: int = 0, sync: bool = False,
+               small_table_items: int = 0) -> BuildOpts:
+    return BuildOpts(method, tile_items, WRS_FLAG_SYNC if sync else 0, small_table_items)
 
 
 def alias_build_scratch_bytes(n: int, opts: Optional[BuildOpts] = None) -> int:
@@ -178,6 +180,39 @@ def rejection_sample(A, a_size, frac, n: int, num_samples: int, seed: int, out, 
 
 def scratch_status(scratch, stream=None) -> int:
     return lib().wrs_scratch_status(_ptr(scratch), _stream(stream))
+
+
+def _host_i64(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int64))
+
+
+def batched_build_scratch_bytes(h_offsets, opts: Optional[BuildOpts] = None) -> int:
+    """Scratch of a batched build (opts None: enough for every launch shape)."""
+    h = _host_i64(h_offsets)
+    return lib().wrs_batched_build_scratch_bytes(h.ctypes.data, h.shape[0] - 1, ctypes.byref(opts) if opts else None)
+
+
+def batched_build(w, d_offsets, h_offsets, table, scratch, opts: Optional[BuildOpts] = None, W_out=None,
+                  stream=None) -> int:
+    """Builds every CSR table of `w` (table t owns w[off[t]:off[t+1]]) into `table` (same rows)."""
+    h = _host_i64(h_offsets)
+    return lib().wrs_batched_build_f32(_ptr(w), _ptr(d_offsets), h.ctypes.data, h.shape[0] - 1,
+                                       ctypes.byref(opts) if opts else None, _ptr(table), _ptr(W_out),
+                                       _ptr(scratch), scratch.numel() * scratch.element_size(), _stream(stream))
+
+
+def batched_sample(table, d_offsets, num_tables: int, d_sample_offsets, total: int, seed: int, out,
+                   counter_base: int = 0, stream=None) -> int:
+    return lib().wrs_batched_sample(_ptr(table), _ptr(d_offsets), num_tables, _ptr(d_sample_offsets), total,
+                                    seed & (2**64 - 1), counter_base & (2**64 - 1), _ptr(out), _stream(stream))
+
+
+def batched_autotune(w, d_offsets, h_offsets, table, scratch, opts: BuildOpts, stream=None) -> int:
+    """Times every batched launch shape on this batch and stores the fastest in `opts`."""
+    h = _host_i64(h_offsets)
+    return lib().wrs_batched_autotune(_ptr(w), _ptr(d_offsets), h.ctypes.data, h.shape[0] - 1, _ptr(table),
+                                      _ptr(scratch), scratch.numel() * scratch.element_size(), ctypes.byref(opts),
+                                      _stream(stream))
 
 
 def sum_f32(w, total, scratch, stream=None) -> int:
@@ -368,3 +403,78 @@ class SamplerRejection(Sampler):
                                 self.max_tries), "rejection sample")
         self.counter += numSamples
         return out
+
+
+class BatchedAliasTablesGpu:
+    """Many alias tables built at once from CSR weights (the batched form of
+    AliasTableSplitGpu; the reference builds such batches one object per table).
+
+    ``offsets`` (int64, num_tables + 1) delimits the tables in ``weights``; after
+    fullBuild() ``table`` holds every table's rows at its items' positions (table-local
+    aliases) and ``W`` the per-table weight totals.
+    """
+
+    def __init__(self, weights, offsets, device: str = "cuda", opts: Optional[BuildOpts] = None):
+        self.weights = np.ascontiguousarray(np.asarray(weights, dtype=np.float32))
+        self.offsets = _host_i64(offsets)
+        self.num_tables = int(self.offsets.shape[0] - 1)
+        self.device = device
+        self.opts = opts if opts is not None else build_opts()
+        self.table = None
+
+    def name(self) -> str:
+        return "BatchedAliasTablesGpu"
+
+    def preBuild(self):
+        import torch
+        self.weightsGpu = torch.from_numpy(self.weights).to(self.device)
+        self.offsetsGpu = torch.from_numpy(self.offsets).to(self.device)
+        self.table = torch.empty(max(1, self.weights.shape[0]), dtype=torch.int64, device=self.device)
+        self.scratch = _device_bytes(batched_build_scratch_bytes(self.offsets), self.device)
+        self.W_dev = torch.zeros(self.num_tables, dtype=torch.float64, device=self.device)
+
+    def autotune(self):
+        _check(batched_autotune(self.weightsGpu, self.offsetsGpu, self.offsets, self.table, self.scratch, self.opts),
+               "batched autotune")
+
+    def build(self):
+        _check(batched_build(self.weightsGpu, self.offsetsGpu, self.offsets, self.table, self.scratch, self.opts,
+                             self.W_dev), "batched build")
+
+    def postBuild(self) -> bool:
+        _check(scratch_status(self.scratch), "batched build (device)")
+        self.W = self.W_dev.cpu().numpy()
+        return True
+
+    def fullBuild(self) -> bool:
+        self.preBuild()
+        self.build()
+        return self.postBuild()
+
+
+class SamplerBatched:
+    """Per-table sample counts over a BatchedAliasTablesGpu: sample(counts) returns the
+    table-local indices (table t's at [sample_offsets[t], sample_offsets[t+1])) and the
+    sample offsets."""
+
+    def __init__(self, tables: BatchedAliasTablesGpu, seed: int = 0x5EED):
+        self.tables = tables
+        self.seed = seed
+        self.counter = 0
+
+    def name(self) -> str:
+        return "SamplerBatched"
+
+    def sample(self, counts, out=None):
+        import torch
+        t = self.tables
+        soff = np.zeros(t.num_tables + 1, dtype=np.int64)
+        np.cumsum(np.asarray(counts, dtype=np.int64), out=soff[1:])
+        total = int(soff[-1])
+        d_soff = torch.from_numpy(soff).to(t.device)
+        if out is None:
+            out = torch.empty(max(1, total), dtype=torch.int32, device=t.device)
+        _check(batched_sample(t.table, t.offsetsGpu, t.num_tables, d_soff, total, self.seed, out, self.counter),
+               "batched sample")
+        self.counter += (total + 1) // 2
+        return out[:total], soff

@@ -30,6 +30,8 @@
  *                             SamplerRejectionGiveUp.cu:17-79)
  *   wrs_batched_*         <- a loop of AliasTableSplitGpu objects (one per table) in the
  *                            reference's experiment drivers; the reference has no batched form
+ *                            (and no autotuner: its launch shapes are compile-time constants,
+ *                            AliasTableSplitGpu.cuh:60-94)
  *   wrs_sum_f32           <- Adder::addGpuCub (utils/Adder.cu:144-157)
  */
 #ifndef WRS_H
@@ -82,10 +84,11 @@ typedef enum wrs_build_method {
 #define WRS_FLAG_SYNC 1u      /* synchronise the stream and return the device status */
 
 typedef struct wrs_build_opts {
-    uint32_t method;          /* wrs_build_method */
-    uint32_t tile_items;      /* 0 = default (2048); a power of two in [512, 4096] */
-    uint32_t flags;           /* WRS_FLAG_* */
-    uint32_t reserved;
+    uint32_t method;            /* wrs_build_method */
+    uint32_t tile_items;        /* 0 = default (2048); 1024, 2048 or 4096 */
+    uint32_t flags;             /* WRS_FLAG_* */
+    uint32_t small_table_items; /* batched builds: tables of at most this many items are built
+                                   one per warp (0 = default 128; 32, 64, 128, 256 or 512) */
 } wrs_build_opts;
 
 typedef enum wrs_sample_mode {
@@ -168,8 +171,16 @@ WRS_API wrs_status wrs_rejection_sample(const uint32_t* d_A, const uint64_t* d_A
 /* ---- batched (CSR) ------------------------------------------------------ */
 
 /* Tables t = 0..num_tables-1 own weights d_w[d_offsets[t] .. d_offsets[t+1]); their rows are
- * written at the same positions of d_table. h_offsets is the same offset array in host
- * memory (used to plan the launch; it is read during the call only). */
+ * written at the same positions of d_table, with table-local aliases: every table's rows are
+ * exactly those wrs_alias_build_f32 gives for its weights. Empty tables get no rows. The
+ * offsets are int64, non-decreasing, with d_offsets[0] = 0 and tables of at most 2^31 - 8193
+ * items. h_offsets is the same array in host memory: the call reads it to size the launches
+ * (and only during the call); the plan itself is made on the device from d_offsets, so the
+ * call issues kernels and one memset only and can be captured in a CUDA graph. If the two
+ * arrays disagree, the large tables are not built and the status is WRS_ERR_INVALID_ARGUMENT.
+ * d_W (optional, device, num_tables doubles) receives the per-table weight totals.
+ * opts->small_table_items and opts->tile_items pick the launch shape (see
+ * wrs_batched_autotune). The scratch query with opts == NULL covers every shape. */
 WRS_API size_t     wrs_batched_build_scratch_bytes(const int64_t* h_offsets, int64_t num_tables,
                                            const wrs_build_opts* opts);
 WRS_API wrs_status wrs_batched_build_f32(const float* d_w, const int64_t* d_offsets,
@@ -184,6 +195,13 @@ WRS_API wrs_status wrs_batched_sample(const wrs_alias_row* d_table, const int64_
                               int64_t num_tables, const int64_t* d_sample_offsets,
                               uint64_t total_samples, uint64_t seed, uint64_t counter_base,
                               uint32_t* d_out, void* stream);
+/* Times the batched build of this batch for every launch shape (small_table_items in
+ * {32, 64, 128, 256, 512} x tile_items in {1024, 2048, 4096}) and writes the fastest into
+ * *opts (method and flags are kept). Synchronous; it builds into d_table (the same rows every
+ * time). d_scratch must hold the opts == NULL scratch query. */
+WRS_API wrs_status wrs_batched_autotune(const float* d_w, const int64_t* d_offsets, const int64_t* h_offsets,
+                                int64_t num_tables, wrs_alias_row* d_table, void* d_scratch,
+                                size_t scratch_bytes, wrs_build_opts* opts, void* stream);
 
 /* ---- status / misc ------------------------------------------------------ */
 

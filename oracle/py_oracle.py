@@ -53,6 +53,8 @@ def oracle() -> ctypes.CDLL:
             "or_rejection_build": (_U64, [_P, _I64, _D, _P, _U64, _P]),
             "or_rejection_sample": (_I, [_P, _U64, _P, _U64, _U64, _U64, _U32, _P]),
             "or_sample_plain_timed": (_D, [_P, _I64, _U64, _U64, _I, _P]),
+            "or_batched_build": (_I, [_P, _P, _I64, _P, _P]),
+            "or_batched_sample": (None, [_P, _P, _I64, _P, _U64, _U64, _P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -162,6 +164,26 @@ def sample_plain(rows: np.ndarray, m: int, seed: int, cbase: int = 0) -> np.ndar
     out = np.zeros(m, dtype=np.uint32)
     oracle().or_sample_plain(_p(rows), rows.shape[0], m, seed, cbase, _p(out))
     return out
+
+
+def batched_build(w: np.ndarray, off: np.ndarray):
+    """Rows of every CSR table (or_exact_build per table), the per-table totals, and the
+    number of tables left unbuilt (zero or invalid total)."""
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    off = np.ascontiguousarray(off, dtype=np.int64)
+    rows = np.zeros((max(1, w.size), 2), dtype=np.uint32)
+    W = np.zeros(off.size - 1, dtype=np.float64)
+    bad = oracle().or_batched_build(_p(w), _p(off), off.size - 1, _p(rows), _p(W))
+    return rows[:w.size], W, bad
+
+
+def batched_sample(rows: np.ndarray, off: np.ndarray, soff: np.ndarray, seed: int, cbase: int = 0) -> np.ndarray:
+    rows = np.ascontiguousarray(rows, dtype=np.uint32)
+    off = np.ascontiguousarray(off, dtype=np.int64)
+    soff = np.ascontiguousarray(soff, dtype=np.int64)
+    out = np.zeros(max(1, int(soff[-1])), dtype=np.uint32)
+    oracle().or_batched_sample(_p(rows), _p(off), off.size - 1, _p(soff), seed & (2**64 - 1), cbase, _p(out))
+    return out[:int(soff[-1])]
 
 
 def binomial(n: int, p: float, seed: int, cbase: int, node: int) -> int:

@@ -590,6 +590,25 @@ int or_exact_build(const float* w, int64_t n, double W, uint32_t* rows) {
     return 0;
 }
 
+/* ------------------------------------------------------------------ batched (CSR) */
+/* The batched build gives every table the rows of a single-table build of its weights, so
+ * its restatement is a loop of or_exact_build (the reference's batches are such loops). */
+int or_batched_build(const float* w, const int64_t* off, int64_t num_tables, uint32_t* rows, double* W_out) {
+    int bad = 0;
+    for (int64_t t = 0; t < num_tables; ++t) {
+        const int64_t n = off[t + 1] - off[t];
+        if (n <= 0) continue;
+        const double W = or_exact_sum_f32(w + off[t], n);
+        if (W_out) W_out[t] = W;
+        if (!(W > 0.0) || isinf(W)) {
+            ++bad;
+            continue;
+        }
+        or_exact_build(w + off[t], n, W, rows + 2 * off[t]);
+    }
+    return bad;
+}
+
 /* ------------------------------------------------------------------ sampling */
 /* doSample (sampling/aliasTable/SamplerGpuBasic.cu:28-69) with frac := coin and
  * weight := prob * W/N: result = coin < prob ? row : alias (a full row keeps itself). */
@@ -603,6 +622,23 @@ void or_sample_plain(const uint32_t* rows, int64_t n, uint64_t m, uint64_t seed,
         philox_block(cbase + (s >> 1), 0, 0, seed, x);
         out[s] = do_sample(rows, scale_u32(x[0], (uint32_t)n), x[1]);
         if (s + 1 < m) out[s + 1] = do_sample(rows, scale_u32(x[2], (uint32_t)n), x[3]);
+    }
+}
+
+void or_batched_sample(const uint32_t* rows, const int64_t* off, int64_t num_tables, const int64_t* soff,
+                       uint64_t seed, uint64_t cbase, uint32_t* out) {
+    for (int64_t t = 0; t < num_tables; ++t) {
+        const uint64_t n = (uint64_t)(off[t + 1] - off[t]);
+        for (int64_t s = soff[t]; s < soff[t + 1]; ++s) {
+            uint32_t x[4];
+            philox_block(cbase + ((uint64_t)s >> 1), 0, 0, seed, x);
+            const uint32_t xr = (s & 1) ? x[2] : x[0], xc = (s & 1) ? x[3] : x[1];
+            if (n == 0) {
+                out[s] = 0xffffffffu;
+                continue;
+            }
+            out[s] = do_sample(rows + 2 * off[t], scale_u32(xr, (uint32_t)n), xc);
+        }
     }
 }
 

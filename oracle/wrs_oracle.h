@@ -58,6 +58,16 @@ void or_section_counts(int64_t n, uint32_t S, uint64_t m, uint64_t seed, uint64_
 void or_sample_sectioned(const uint32_t* rows, int64_t n, uint64_t m, uint32_t S, uint64_t seed, uint64_t cbase,
                          uint32_t* out, uint64_t* counts);
 
+/* batched (CSR): table t owns items [off[t], off[t+1]); its rows (table-local aliases) are
+ * or_exact_build of its weights with W = their exact sum (empty tables: no rows). W_out
+ * (optional) gets the totals. Returns the number of tables with a zero or invalid total
+ * (left unwritten). */
+int or_batched_build(const float* w, const int64_t* off, int64_t num_tables, uint32_t* rows, double* W_out);
+/* output position s of the batch belongs to table t with soff[t] <= s < soff[t+1] and follows
+ * the plain contract over the global position s (table-local rows) */
+void or_batched_sample(const uint32_t* rows, const int64_t* off, int64_t num_tables, const int64_t* soff,
+                       uint64_t seed, uint64_t cbase, uint32_t* out);
+
 /* rejection: A holds item | 0x80000000 on first slots; returns |A| (or 0 on capacity error) */
 uint64_t or_rejection_build(const float* w, int64_t n, double W, uint32_t* A, uint64_t a_capacity, float* frac);
 int or_rejection_sample(const uint32_t* A, uint64_t a_size, const float* frac, uint64_t m, uint64_t seed,

@@ -163,3 +163,39 @@ def test_philox_matches_curand_golden():
             b = off // 4 + i
             ctr = [b & 0xFFFFFFFF, (b >> 32) & 0xFFFFFFFF, sub & 0xFFFFFFFF, sub >> 32]
             np.testing.assert_array_equal(po.philox(ctr, key), np.array(expect, dtype=np.uint32))
+
+
+def test_batched_oracle_matches_per_table_oracle():
+    """or_batched_build / or_batched_sample restate the per-table build and the plain
+    contract over global output positions."""
+    rng = np.random.default_rng(9)
+    sizes = np.array([3, 0, 40, 1, 700, 5], dtype=np.int64)
+    off = np.zeros(sizes.size + 1, dtype=np.int64)
+    np.cumsum(sizes, out=off[1:])
+    w = rng.random(int(off[-1]), dtype=np.float32)
+    rows, W, bad = po.batched_build(w, off)
+    assert bad == 0
+    for t in range(sizes.size):
+        a, b = off[t], off[t + 1]
+        if b > a:
+            assert W[t] == po.exact_sum(w[a:b])
+            assert np.array_equal(rows[a:b], po.exact_build(w[a:b], W[t]))
+    # one table alone: the batched sampler is the plain sampler
+    r = rows[off[4]:off[5]]
+    assert np.array_equal(po.batched_sample(r, np.array([0, 700]), np.array([0, 1001]), 99, 5),
+                          po.sample_plain(r, 1001, 99, 5))
+    # odd split points keep the global Philox pairing
+    counts = np.array([7, 0, 9, 1, 33, 2], dtype=np.int64)
+    soff = np.zeros(sizes.size + 1, dtype=np.int64)
+    np.cumsum(counts, out=soff[1:])
+    out = po.batched_sample(rows, off, soff, 5, 0)
+    for t in range(sizes.size):
+        n = int(sizes[t])
+        for s in range(soff[t], soff[t + 1]):
+            b = s >> 1
+            x = po.philox([b & 0xffffffff, b >> 32, 0, 0], [5, 0])
+            xr, xc = (x[2], x[3]) if s & 1 else (x[0], x[1])
+            row = (int(xr) * n) >> 32
+            p = rows[off[t] + row, 0].view(np.float32)
+            coin = np.float32((int(xc) >> 8) * 2.0 ** -24)
+            assert out[s] == (row if coin < p else rows[off[t] + row, 1])
