@@ -46,6 +46,12 @@ METRIC = "build Gitems/s + Gsamples/s, batched vs per-table, %HBM peak, at ≤1e
 UNIT = "G(items+samples)/s"
 WORKLOAD = "single large table: n=2^26 w=(i+1)^-1.1 permuted; split build + 2^30 plain samples per step"
 FALLBACK_HBM_GBS = 6650.0
+# kernels one step launches: wsum, tile_reduce, tile_prefix, heavy_list, tile_link, split_pack
+# (the build) and sample_plain
+KERNELS_PER_STEP = 7
+BATCH_TABLES = 1 << 17
+BATCH_SAMPLES_PER_TABLE = 64
+BATCH_PER_TABLE_SAMPLE = 4096  # tables timed one call at a time (the per-table baseline)
 
 
 def make_weights(n: int = N_ITEMS, seed: int = SEED_WEIGHTS) -> np.ndarray:
@@ -294,9 +300,125 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "clocks": clk,
         "e2e": {"value": round(world * (n + m) / (e2e_ms * 1e-3) / 1e9, 4), "unit": UNIT,
                 "ms_per_step": round(e2e_ms, 3), "h2d_bytes_per_step": 4 * n, "d2h_bytes_per_step": 4 * m},
-        "gpu_launches": 4 * K,
+        "gpu_launches": KERNELS_PER_STEP * K,
     }
+    if not args.no_batched:
+        line["batched"] = batched_phase(dev)
     return line
+
+
+def zipf_sizes(num: int, s: float, lo: int, hi: int, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    k = np.arange(lo, hi + 1, dtype=np.float64)
+    p = k ** -s
+    p /= p.sum()
+    return rng.choice(np.arange(lo, hi + 1), size=num, p=p).astype(np.int64)
+
+
+def batched_phase(dev) -> dict:
+    """The batched-tables configuration: 2^17 tables with sizes Zipf(2) on [2, 2^16], FP32
+    weights U(0,1), CSR int64 offsets, 64 samples per table. The batched build and sample
+    (autotuned launch shape, captured in one CUDA graph) against the plain single-table
+    entry points called once per table, timed on the first BATCH_PER_TABLE_SAMPLE tables and
+    scaled to all tables by count (each call pays the same launch sequence)."""
+    import torch
+    import wrs
+
+    sizes = zipf_sizes(BATCH_TABLES, 2.0, 2, 1 << 16, 0x5EED + 4)
+    off = np.zeros(BATCH_TABLES + 1, dtype=np.int64)
+    np.cumsum(sizes, out=off[1:])
+    items = int(off[-1])
+    w_np = np.random.default_rng(0x5EED + 4).random(items, dtype=np.float32)
+    w = torch.from_numpy(w_np).to(dev)
+    d_off = torch.from_numpy(off).to(dev)
+    table = torch.empty(items, dtype=torch.int64, device=dev)
+    scratch = torch.empty(wrs.batched_build_scratch_bytes(off), dtype=torch.uint8, device=dev)
+    soff = np.arange(BATCH_TABLES + 1, dtype=np.int64) * BATCH_SAMPLES_PER_TABLE
+    total = int(soff[-1])
+    d_soff = torch.from_numpy(soff).to(dev)
+    out = torch.empty(total, dtype=torch.int32, device=dev)
+    opts = wrs.build_opts()
+    st = wrs.batched_autotune(w, d_off, off, table, scratch, opts)
+    if st:
+        raise wrs.WrsError(st, "batched autotune")
+    # the batch's rows equal single-table builds of the same weights (a sample of tables,
+    # the largest ones included; the tests check every table against the oracle)
+    st = wrs.batched_build(w, d_off, off, table, scratch, wrs.build_opts(0, opts.tile_items, True,
+                                                                        opts.small_table_items))
+    if st:
+        raise wrs.WrsError(st, "batched build")
+    rows = table.cpu().numpy().view(np.uint32).reshape(-1, 2)
+    check = np.r_[0:64, np.argsort(sizes)[-8:]]
+    exact = True
+    for t in check:
+        n_t = int(sizes[t])
+        t1 = torch.empty(n_t, dtype=torch.int64, device=dev)
+        sc1 = torch.empty(wrs.alias_build_scratch_bytes(n_t), dtype=torch.uint8, device=dev)
+        if wrs.alias_build(w[int(off[t]):int(off[t + 1])], t1, sc1, wrs.build_opts(sync=True)):
+            raise RuntimeError("single-table build failed")
+        exact &= bool(np.array_equal(rows[off[t]:off[t + 1]], t1.cpu().numpy().view(np.uint32).reshape(-1, 2)))
+
+    s = torch.cuda.Stream(dev)
+    s.wait_stream(torch.cuda.current_stream(dev))
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        g.capture_begin()
+        wrs.batched_build(w, d_off, off, table, scratch, opts, stream=s)
+        wrs.batched_sample(table, d_off, BATCH_TABLES, d_soff, total, SEED_SAMPLES, out, 0, stream=s)
+        g.capture_end()
+    torch.cuda.current_stream(dev).wait_stream(s)
+    for _ in range(3):
+        g.replay()
+    torch.cuda.synchronize()
+    reps = 20
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record()
+    for _ in range(reps):
+        g.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    batched_ms = e0.elapsed_time(e1) / reps
+    batched_wall_ms = (time.perf_counter() - t0) * 1e3 / reps
+
+    # per-table launches: build + 64 samples for each of the first tables, one call each
+    k = BATCH_PER_TABLE_SAMPLE
+    big = int(sizes[:k].max())
+    tbl1 = torch.empty(big, dtype=torch.int64, device=dev)
+    scr1 = torch.empty(wrs.alias_build_scratch_bytes(big), dtype=torch.uint8, device=dev)
+    out1 = torch.empty(BATCH_SAMPLES_PER_TABLE, dtype=torch.int32, device=dev)
+    L = wrs.lib()
+    sp = torch.cuda.current_stream(dev).cuda_stream
+    wp, tp, sc, op = w.data_ptr(), tbl1.data_ptr(), scr1.data_ptr(), out1.data_ptr()
+    nbytes = scr1.numel()
+
+    def per_table(lo, hi):
+        for t in range(lo, hi):
+            n = int(sizes[t])
+            L.wrs_alias_build_f32(wp + 4 * int(off[t]), n, None, tp, None, sc, nbytes, sp)
+            L.wrs_alias_sample(tp, n, BATCH_SAMPLES_PER_TABLE, SEED_SAMPLES, 0, None, op, None, sp)
+
+    per_table(0, 64)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0.record()
+    per_table(0, k)
+    e1.record()
+    torch.cuda.synchronize()
+    per_ms = e0.elapsed_time(e1) * BATCH_TABLES / k
+    per_wall_ms = (time.perf_counter() - t0) * 1e3 * BATCH_TABLES / k
+    return {
+        "workload": f"2^17 tables, sizes Zipf(2) on [2, 2^16] ({items} items), w~U(0,1) FP32, int64 CSR offsets; "
+                    f"build + {BATCH_SAMPLES_PER_TABLE} samples per table",
+        "items": items, "samples": total,
+        "autotuned": {"small_table_items": int(opts.small_table_items), "tile_items": int(opts.tile_items)},
+        "batched_ms": round(batched_ms, 4), "batched_wall_ms": round(batched_wall_ms, 4),
+        "batched_g_items_plus_samples_s": round((items + total) / (batched_ms * 1e-3) / 1e9, 3),
+        "per_table_ms": round(per_ms, 2), "per_table_wall_ms": round(per_wall_ms, 2),
+        "per_table_sample": f"first {k} tables timed, scaled by table count",
+        "speedup": round(per_ms / batched_ms, 1),
+        "tables_equal_to_single_builds": f"{int(check.size) if exact else 0} of {int(check.size)} checked",
+    }
 
 
 # ---------------------------------------------------------------- reference CPU
@@ -373,6 +495,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-tables measurement")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
