@@ -165,7 +165,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     dev = torch.device("cuda", local_rank)
     if wrs.lib().wrs_check_device() != 0:
         raise RuntimeError("not an sm_100 device")
-    n, m = N_ITEMS, N_SAMPLES
+    n, m = N_ITEMS, 1 << args.log2_samples
     w_np = make_weights()
     w_host = torch.from_numpy(w_np).pin_memory()
     w = w_host.to(dev)
@@ -496,6 +496,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-tables measurement")
+    ap.add_argument("--log2-samples", type=int, default=30,
+                    help="samples per step (2^k); smaller values are for profiler captures only")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
