@@ -64,66 +64,90 @@ __global__ void __launch_bounds__(256) sample_plain_kernel(const uint2* __restri
 
 // Sectioned sampling: rows cut into K sections of S rows; section k receives an exact
 // multinomial share of the m samples (binomial tree, section_count) and writes them at its
-// output offset. A persistent CTA handles one section at a time, so the sections being
-// sampled at any moment (grid size x section bytes) stay inside L2; with STAGE the section
-// is first copied into shared memory and gathered from there.
+// output offset. CTA c handles sections c, c + gridDim.x, ... in that order, so the sections
+// being sampled at any moment (grid size x section bytes) stay inside L2; with STAGE each
+// section is first copied into shared memory and gathered from there. The counts and offsets
+// of a CTA's sections are computed up front, one thread per section (each a walk down the
+// binomial tree), so no thread waits for them between sections. Each thread draws four
+// consecutive Philox blocks at a time (eight gathers in flight).
+constexpr int kSectThreads = 512;
+
 template <bool STAGE>
-__global__ void __launch_bounds__(512) sample_sectioned_kernel(const uint2* __restrict__ table, uint32_t n,
-                                                               uint64_t m, uint32_t S, uint32_t K, uint32_t k0,
-                                                               uint32_t k1, uint64_t cbase,
-                                                               uint32_t* __restrict__ out,
-                                                               uint64_t* __restrict__ counts_out) {
+__global__ void __launch_bounds__(kSectThreads) sample_sectioned_kernel(const uint2* __restrict__ table, uint32_t n,
+                                                                        uint64_t m, uint32_t S, uint32_t K,
+                                                                        uint32_t k0, uint32_t k1, uint64_t cbase,
+                                                                        uint32_t* __restrict__ out,
+                                                                        uint64_t* __restrict__ counts_out) {
     extern __shared__ __align__(16) uint2 s_rows[];
-    __shared__ uint64_t s_cnt, s_off;
-    for (uint32_t sec = blockIdx.x; sec < K; sec += gridDim.x) {
-        if (threadIdx.x == 0) {
-            uint64_t c, o;
-            section_count(sec, K, S, n, m, k0, k1, cbase, &c, &o);
-            s_cnt = c;
-            s_off = o;
-            if (counts_out) counts_out[sec] = c;
-        }
-        const uint32_t start = sec * S;
-        const uint32_t len = (uint32_t)section_rows(sec, sec + 1, S, n);
-        if (STAGE) {
-            const uint4* src = reinterpret_cast<const uint4*>(table + start);
-            uint4* dst = reinterpret_cast<uint4*>(s_rows);
-            const uint32_t n16 = len >> 1;
-            for (uint32_t i = threadIdx.x; i < n16; i += blockDim.x) dst[i] = __ldg(src + i);
-            if ((len & 1u) && threadIdx.x == 0) s_rows[len - 1] = __ldg(table + start + len - 1);
-        }
-        __syncthreads();
-        const uint64_t cnt = s_cnt, off = s_off;
-        if (cnt > 0) {
-            // Philox blocks covering output positions [off, off + cnt)
-            const uint64_t b_lo = off >> 1, b_hi = (off + cnt - 1) >> 1;
-            const uint64_t nb = b_hi - b_lo + 1;
-            for (uint64_t i = threadIdx.x; i < nb; i += blockDim.x) {
-                const uint64_t blk = b_lo + i;
-                const uint64_t bb = cbase + blk;
-                const Philox4 r = philox4x32_10((uint32_t)bb, (uint32_t)(bb >> 32), 0u, 0u, k0, k1);
-                const uint32_t ra = scale_u32(r.x[0], len), rb = scale_u32(r.x[2], len);
-                uint2 va, vb;
-                if (STAGE) {
-                    va = s_rows[ra];
-                    vb = s_rows[rb];
-                } else {
-                    va = __ldg(table + start + ra);
-                    vb = __ldg(table + start + rb);
-                }
-                const uint32_t oa = alias_pick(va, start + ra, r.x[1]);
-                const uint32_t ob = alias_pick(vb, start + rb, r.x[3]);
-                const uint64_t s = 2 * blk;
-                const bool wa = s >= off, wb = s + 1 < off + cnt;
-                if (wa && wb && ((s & 1) == 0) && (((uintptr_t)(out + s) & 7u) == 0)) {
-                    *reinterpret_cast<uint2*>(out + s) = make_uint2(oa, ob);
-                } else {
-                    if (wa) out[s] = oa;
-                    if (wb) out[s + 1] = ob;
-                }
+    __shared__ uint64_t s_cnt[kSectThreads], s_off[kSectThreads];
+    const uint32_t nsec = K > blockIdx.x ? (K - blockIdx.x + gridDim.x - 1) / gridDim.x : 0u;
+    const bool out16 = ((uintptr_t)out & 15u) == 0;
+    for (uint32_t i0 = 0; i0 < nsec; i0 += kSectThreads) {
+        {
+            const uint32_t i = i0 + threadIdx.x;
+            if (i < nsec) {
+                const uint32_t sec = blockIdx.x + i * gridDim.x;
+                uint64_t c, o;
+                section_count(sec, K, S, n, m, k0, k1, cbase, &c, &o);
+                s_cnt[threadIdx.x] = c;
+                s_off[threadIdx.x] = o;
+                if (counts_out) counts_out[sec] = c;
             }
         }
         __syncthreads();
+        const uint32_t ni = min(nsec - i0, (uint32_t)kSectThreads);
+        for (uint32_t ii = 0; ii < ni; ++ii) {
+            const uint32_t sec = blockIdx.x + (i0 + ii) * gridDim.x;
+            const uint32_t start = sec * S;
+            const uint32_t len = (uint32_t)section_rows(sec, sec + 1, S, n);
+            if (STAGE) {
+                const uint4* src = reinterpret_cast<const uint4*>(table + start);
+                uint4* dst = reinterpret_cast<uint4*>(s_rows);
+                const uint32_t n16 = len >> 1;
+                for (uint32_t i = threadIdx.x; i < n16; i += blockDim.x) dst[i] = __ldg(src + i);
+                if ((len & 1u) && threadIdx.x == 0) s_rows[len - 1] = __ldg(table + start + len - 1);
+                __syncthreads();
+            }
+            const uint64_t cnt = s_cnt[ii], off = s_off[ii];
+            if (cnt > 0) {
+                // Philox blocks covering output positions [off, off + cnt), in groups of four
+                // aligned to the global block index
+                const uint64_t b_lo = off >> 1, b_hi = (off + cnt - 1) >> 1;
+                const uint64_t g_lo = b_lo & ~3ull;
+                const uint64_t ng = ((b_hi - g_lo) >> 2) + 1;
+                for (uint64_t gi = threadIdx.x; gi < ng; gi += blockDim.x) {
+                    const uint64_t blk0 = g_lo + 4 * gi;
+                    uint32_t rows[8], coins[8];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const uint64_t bb = cbase + blk0 + j;
+                        const Philox4 r = philox4x32_10((uint32_t)bb, (uint32_t)(bb >> 32), 0u, 0u, k0, k1);
+                        rows[2 * j] = scale_u32(r.x[0], len);
+                        coins[2 * j] = r.x[1];
+                        rows[2 * j + 1] = scale_u32(r.x[2], len);
+                        coins[2 * j + 1] = r.x[3];
+                    }
+                    uint2 v[8];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) v[j] = STAGE ? s_rows[rows[j]] : __ldg(table + start + rows[j]);
+                    uint32_t res[8];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) res[j] = alias_pick(v[j], start + rows[j], coins[j]);
+                    const uint64_t s0 = 2 * blk0;  // output position of res[0]
+                    if (s0 >= off && s0 + 8 <= off + cnt && out16) {
+                        uint4* o4 = reinterpret_cast<uint4*>(out + s0);
+                        __stcs(o4, make_uint4(res[0], res[1], res[2], res[3]));
+                        __stcs(o4 + 1, make_uint4(res[4], res[5], res[6], res[7]));
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 8; ++j)
+                            if (s0 + j >= off && s0 + j < off + cnt) out[s0 + j] = res[j];
+                    }
+                }
+            }
+            if (STAGE) __syncthreads();  // before the next section overwrites s_rows
+        }
+        __syncthreads();  // s_cnt / s_off are rewritten
     }
 }
 
