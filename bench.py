@@ -59,6 +59,28 @@ def make_weights(n: int = N_ITEMS, seed: int = SEED_WEIGHTS) -> np.ndarray:
     return w[np.random.default_rng(seed).permutation(n)]
 
 
+def uniform_weights(n: int, seed: int) -> np.ndarray:
+    return np.random.default_rng(seed).random(n, dtype=np.float32)
+
+
+def loguniform_weights(n: int, seed: int) -> np.ndarray:
+    return (10.0 ** np.random.default_rng(seed).uniform(-8.0, 8.0, n)).astype(np.float32)
+
+
+# Single-table configurations (--config); "2" is the default and the headline. Each is seeded
+# synthetic data of the configuration's shape and distribution.
+CONFIGS = {
+    "1": dict(log2n=20, log2m=24, make=lambda n: uniform_weights(n, 0x5EED + 1),
+              workload="plain single table: n=2^20 w~U(0,1) FP32; split build + 2^24 plain samples per step "
+                       "(L2-resident)", weights="U(0,1) FP32 (numpy PCG64, seed 0x5EED+1)"),
+    "2": dict(log2n=26, log2m=30, make=lambda n: make_weights(n),
+              workload=WORKLOAD, weights="w_i=(i+1)^-1.1 FP64->FP32, seeded permutation"),
+    "3": dict(log2n=28, log2m=28, make=lambda n: loguniform_weights(n, 0x5EED + 3),
+              workload="precision stress: n=2^28 w=10^U(-8,8) log-uniform FP32; split build + 2^28 plain samples "
+                       "per step", weights="10^U(-8,8) FP32 (numpy PCG64, seed 0x5EED+3)"),
+}
+
+
 def measured_peak():
     path = os.path.join(REPO, "MEASURED_PEAKS.json")
     try:
@@ -140,6 +162,28 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
+def table_error_gpu(w, table) -> dict:
+    """Per-item relative error of a device table against w_i / W, on the device in FP64:
+    P_i = prob_i + sum over rows r aliasing i of (1 - prob_r), against n w_i / W."""
+    import torch
+    n = w.numel()
+    rows = table.view(torch.int32).view(-1, 2)
+    p = rows[:, 0].contiguous().view(torch.float32).double()
+    a = rows[:, 1].long()
+    got = p.clone()
+    got.scatter_add_(0, a, 1.0 - p)
+    del a
+    wd = w.double()
+    W = wd.sum()
+    nz = wd > 0
+    exp = wd[nz] * (n / W)
+    rel = (got[nz] - exp).abs_() / exp
+    k = max(1, int(math.ceil(rel.numel() * 1e-4)))
+    top = torch.topk(rel, k).values
+    zm = float(got[~nz].sum().item()) if bool((~nz).any()) else 0.0
+    return {"max_rel": float(top[0].item()), "p9999_rel": float(top[-1].item()), "zero_weight_mass": zm}
+
+
 def table_error(w: np.ndarray, rows_u32: np.ndarray) -> dict:
     """Per-item relative error of the table against w_i / W (W summed in FP64 pairwise)."""
     n = w.size
@@ -165,8 +209,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     dev = torch.device("cuda", local_rank)
     if wrs.lib().wrs_check_device() != 0:
         raise RuntimeError("not an sm_100 device")
-    n, m = N_ITEMS, 1 << args.log2_samples
-    w_np = make_weights()
+    cfg = CONFIGS[args.config]
+    n, m = 1 << cfg["log2n"], 1 << (args.log2_samples if args.log2_samples else cfg["log2m"])
+    w_np = cfg["make"](n)
     w_host = torch.from_numpy(w_np).pin_memory()
     w = w_host.to(dev)
     opts = wrs.build_opts(wrs.WRS_METHOD_SPLIT)
@@ -192,7 +237,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     st = wrs.scratch_status(scratch, sp)
     if st:
         raise wrs.WrsError(st, "build (device)")
-    err = table_error(w_np, table.cpu().numpy().view(np.uint32).reshape(-1, 2)) if rank == 0 else None
+    err = table_error_gpu(w, table) if rank == 0 else None
 
     for i in range(args.warmup):
         build()
@@ -276,14 +321,15 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     build_gbs = 12.0 * n / (build_ms * 1e-3) / 1e9  # 12 B per item (4 B read + 8 B write)
     step_ms = total_ms / K
     value = world * (n + m) / (step_ms * 1e-3) / 1e9
-    cpu = cpu_baseline(w_np) if not args.no_cpu_baseline else None
+    cpu = cpu_baseline(w_np, min(n, N_ITEMS), 1 << 22, n, m) if not args.no_cpu_baseline else None
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": round(step_ms, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n_items": n, "n_samples_per_step": m, "build": "split",
-                   "sampling": "plain", "weights": "w_i=(i+1)^-1.1 FP64->FP32, seeded permutation",
-                   "l2": "inputs larger than L2 (256 MB weights, 4 GB samples); no flush",
+        "config": {"workload": cfg["workload"], "n_items": n, "n_samples_per_step": m, "build": "split",
+                   "sampling": "plain", "weights": cfg["weights"],
+                   "l2": ("inputs larger than L2; no flush" if 12 * n + 4 * m > (256 << 20)
+                          else "L2-resident table and samples (126 MB L2)"),
                    "parallelism": f"replicas x{world}"},
         "phases": {"build_ms": round(build_ms, 4), "build_gitems_s": round(n / build_ms / 1e6, 3),
                    "build_hbm_gbs": round(build_gbs, 1), "build_hbm_frac": round(build_gbs / peak, 4),
@@ -294,7 +340,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "prob_error": err,
         "roofline": {"kernel": "sample_plain_kernel", "bound": "hbm", "achieved": round(achieved, 1),
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                     "traffic": ncu_traffic(),
+                     "traffic": ncu_traffic() if args.config == "2" else None,
                      "algorithmic_bytes": "12 B/sample x 2^30 samples per launch (8 B row gather + 4 B write)"},
         "cpu_baseline": cpu,
         "clocks": clk,
@@ -302,7 +348,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                 "ms_per_step": round(e2e_ms, 3), "h2d_bytes_per_step": 4 * n, "d2h_bytes_per_step": 4 * m},
         "gpu_launches": KERNELS_PER_STEP * K,
     }
-    if not args.no_batched:
+    if not args.no_batched and args.config == "2":
         line["batched"] = batched_phase(dev)
     return line
 
@@ -315,25 +361,52 @@ def zipf_sizes(num: int, s: float, lo: int, hi: int, seed: int) -> np.ndarray:
     return rng.choice(np.arange(lo, hi + 1), size=num, p=p).astype(np.int64)
 
 
-def batched_phase(dev) -> dict:
-    """The batched-tables configuration: 2^17 tables with sizes Zipf(2) on [2, 2^16], FP32
-    weights U(0,1), CSR int64 offsets, 64 samples per table. The batched build and sample
-    (autotuned launch shape, captured in one CUDA graph) against the plain single-table
-    entry points called once per table, timed on the first BATCH_PER_TABLE_SAMPLE tables and
-    scaled to all tables by count (each call pays the same launch sequence)."""
+def batch_config4():
+    """2^17 tables, sizes Zipf(2) on [2, 2^16], w~U(0,1), 64 samples per table."""
+    sizes = zipf_sizes(BATCH_TABLES, 2.0, 2, 1 << 16, 0x5EED + 4)
+    w = np.random.default_rng(0x5EED + 4).random(int(sizes.sum()), dtype=np.float32)
+    counts = np.full(sizes.size, BATCH_SAMPLES_PER_TABLE, dtype=np.int64)
+    what = (f"2^17 tables, sizes Zipf(2) on [2, 2^16] ({int(sizes.sum())} items), w~U(0,1) FP32, int64 CSR "
+            f"offsets; build + {BATCH_SAMPLES_PER_TABLE} samples per table")
+    return sizes, w, counts, what, [(np.arange(BATCH_PER_TABLE_SAMPLE), np.ones(sizes.size, bool))]
+
+
+def batch_config5():
+    """10^6 tables of U{1..64} items with Exp(1) weights, then 100 tables of 2^20 items with
+    Pareto(1.5) weights; 4 x size samples per table."""
+    rng = np.random.default_rng(0x5EED + 5)
+    small = rng.integers(1, 65, 1_000_000)
+    sizes = np.concatenate([small, np.full(100, 1 << 20)]).astype(np.int64)
+    w_small = rng.exponential(1.0, int(small.sum())).astype(np.float32)
+    w_large = (rng.pareto(1.5, 100 << 20) + 1.0).astype(np.float32)
+    w = np.concatenate([w_small, w_large])
+    counts = 4 * sizes
+    what = (f"10^6 tables of U{{1..64}} items, w~Exp(1), and 100 tables of 2^20 items, w~Pareto(1.5) "
+            f"({int(sizes.sum())} items); build + 4 x size samples per table; alias tables for every size "
+            f"class (the alias-vs-rejection choice per class is not built)")
+    return sizes, w, counts, what, [(np.arange(BATCH_PER_TABLE_SAMPLE), sizes <= 64),
+                                    (np.arange(1_000_000, 1_000_004), sizes > 64)]
+
+
+def batched_phase(dev, make=batch_config4) -> dict:
+    """A batched-tables configuration: the batched build and sample (autotuned launch shape,
+    captured in one CUDA graph) against the plain single-table entry points called once per
+    table, timed on samples of each size class and scaled to all tables of the class by count
+    (each call pays the same launch sequence)."""
     import torch
     import wrs
 
-    sizes = zipf_sizes(BATCH_TABLES, 2.0, 2, 1 << 16, 0x5EED + 4)
-    off = np.zeros(BATCH_TABLES + 1, dtype=np.int64)
+    sizes, w_np, counts, what, per_table_groups = make()
+    nt = sizes.size
+    off = np.zeros(nt + 1, dtype=np.int64)
     np.cumsum(sizes, out=off[1:])
     items = int(off[-1])
-    w_np = np.random.default_rng(0x5EED + 4).random(items, dtype=np.float32)
     w = torch.from_numpy(w_np).to(dev)
     d_off = torch.from_numpy(off).to(dev)
     table = torch.empty(items, dtype=torch.int64, device=dev)
     scratch = torch.empty(wrs.batched_build_scratch_bytes(off), dtype=torch.uint8, device=dev)
-    soff = np.arange(BATCH_TABLES + 1, dtype=np.int64) * BATCH_SAMPLES_PER_TABLE
+    soff = np.zeros(nt + 1, dtype=np.int64)
+    np.cumsum(counts, out=soff[1:])
     total = int(soff[-1])
     d_soff = torch.from_numpy(soff).to(dev)
     out = torch.empty(total, dtype=torch.int32, device=dev)
@@ -348,7 +421,7 @@ def batched_phase(dev) -> dict:
     if st:
         raise wrs.WrsError(st, "batched build")
     rows = table.cpu().numpy().view(np.uint32).reshape(-1, 2)
-    check = np.r_[0:64, np.argsort(sizes)[-8:]]
+    check = np.r_[0:64, np.argsort(sizes, kind="stable")[-8:]]
     exact = True
     for t in check:
         n_t = int(sizes[t])
@@ -364,7 +437,7 @@ def batched_phase(dev) -> dict:
     with torch.cuda.stream(s):
         g.capture_begin()
         wrs.batched_build(w, d_off, off, table, scratch, opts, stream=s)
-        wrs.batched_sample(table, d_off, BATCH_TABLES, d_soff, total, SEED_SAMPLES, out, 0, stream=s)
+        wrs.batched_sample(table, d_off, nt, d_soff, total, SEED_SAMPLES, out, 0, stream=s)
         g.capture_end()
     torch.cuda.current_stream(dev).wait_stream(s)
     for _ in range(3):
@@ -381,49 +454,68 @@ def batched_phase(dev) -> dict:
     batched_ms = e0.elapsed_time(e1) / reps
     batched_wall_ms = (time.perf_counter() - t0) * 1e3 / reps
 
-    # per-table launches: build + 64 samples for each of the first tables, one call each
-    k = BATCH_PER_TABLE_SAMPLE
-    big = int(sizes[:k].max())
-    tbl1 = torch.empty(big, dtype=torch.int64, device=dev)
-    scr1 = torch.empty(wrs.alias_build_scratch_bytes(big), dtype=torch.uint8, device=dev)
-    out1 = torch.empty(BATCH_SAMPLES_PER_TABLE, dtype=torch.int32, device=dev)
+    # per-table launches: build + the table's samples, one call each, per size class
     L = wrs.lib()
     sp = torch.cuda.current_stream(dev).cuda_stream
-    wp, tp, sc, op = w.data_ptr(), tbl1.data_ptr(), scr1.data_ptr(), out1.data_ptr()
-    nbytes = scr1.numel()
+    per_ms = per_wall_ms = 0.0
+    timed = []
+    for grp, cls in per_table_groups:
+        big = int(sizes[grp].max())
+        cmax = int(counts[grp].max())
+        tbl1 = torch.empty(big, dtype=torch.int64, device=dev)
+        scr1 = torch.empty(wrs.alias_build_scratch_bytes(big), dtype=torch.uint8, device=dev)
+        out1 = torch.empty(max(1, cmax), dtype=torch.int32, device=dev)
+        wp, tp, sc, op = w.data_ptr(), tbl1.data_ptr(), scr1.data_ptr(), out1.data_ptr()
+        nbytes = scr1.numel()
 
-    def per_table(lo, hi):
-        for t in range(lo, hi):
-            n = int(sizes[t])
-            L.wrs_alias_build_f32(wp + 4 * int(off[t]), n, None, tp, None, sc, nbytes, sp)
-            L.wrs_alias_sample(tp, n, BATCH_SAMPLES_PER_TABLE, SEED_SAMPLES, 0, None, op, None, sp)
+        def per_table(ts):
+            for t in ts:
+                n_t = int(sizes[t])
+                L.wrs_alias_build_f32(wp + 4 * int(off[t]), n_t, None, tp, None, sc, nbytes, sp)
+                L.wrs_alias_sample(tp, n_t, int(counts[t]), SEED_SAMPLES, 0, None, op, None, sp)
 
-    per_table(0, 64)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    e0.record()
-    per_table(0, k)
-    e1.record()
-    torch.cuda.synchronize()
-    per_ms = e0.elapsed_time(e1) * BATCH_TABLES / k
-    per_wall_ms = (time.perf_counter() - t0) * 1e3 * BATCH_TABLES / k
+        per_table(grp[:8])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0.record()
+        per_table(grp)
+        e1.record()
+        torch.cuda.synchronize()
+        scale = int(cls.sum()) / grp.size
+        per_ms += e0.elapsed_time(e1) * scale
+        per_wall_ms += (time.perf_counter() - t0) * 1e3 * scale
+        timed.append(f"{grp.size} tables of {int(cls.sum())}")
     return {
-        "workload": f"2^17 tables, sizes Zipf(2) on [2, 2^16] ({items} items), w~U(0,1) FP32, int64 CSR offsets; "
-                    f"build + {BATCH_SAMPLES_PER_TABLE} samples per table",
-        "items": items, "samples": total,
+        "workload": what, "items": items, "samples": total,
         "autotuned": {"small_table_items": int(opts.small_table_items), "tile_items": int(opts.tile_items)},
         "batched_ms": round(batched_ms, 4), "batched_wall_ms": round(batched_wall_ms, 4),
         "batched_g_items_plus_samples_s": round((items + total) / (batched_ms * 1e-3) / 1e9, 3),
         "per_table_ms": round(per_ms, 2), "per_table_wall_ms": round(per_wall_ms, 2),
-        "per_table_sample": f"first {k} tables timed, scaled by table count",
+        "per_table_sample": "timed on " + ", ".join(timed) + " per size class, scaled by table count",
         "speedup": round(per_ms / batched_ms, 1),
         "tables_equal_to_single_builds": f"{int(check.size) if exact else 0} of {int(check.size)} checked",
     }
 
 
+def run_batched_only(args, rank: int, local_rank: int):
+    import torch
+    if rank != 0:
+        return None
+    torch.cuda.set_device(local_rank)
+    b = batched_phase(torch.device("cuda", local_rank), batch_config5 if args.config == "5" else batch_config4)
+    items_samples = b["items"] + b["samples"]
+    return {"metric": METRIC, "value": b["batched_g_items_plus_samples_s"], "unit": UNIT, "n_gpus": 1,
+            "steps": 20, "warmup": 3, "ms_per_step": b["batched_ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": b["workload"], "items": b["items"], "samples": b["samples"]},
+            "batched": b, "gpu_launches": None,
+            "e2e": None, "note": f"{items_samples} items+samples per graph replay"}
+
+
 # ---------------------------------------------------------------- reference CPU
 
-def cpu_baseline(w_np: np.ndarray, n_build: int = N_ITEMS, n_samp: int = 1 << 22) -> dict:
+def cpu_baseline(w_np: np.ndarray, n_build: int = N_ITEMS, n_samp: int = 1 << 22, n_total: int = N_ITEMS,
+                 m_total: int = N_SAMPLES) -> dict:
     """The reference's CPU path on this host's cores, on a bounded sample of the workload:
     AliasTableSplit::build's split and pack loops over all cores (the reference's own
     functions, a harness like the reference's build) for the first `n_build` weights, and
@@ -441,7 +533,7 @@ def cpu_baseline(w_np: np.ndarray, n_build: int = N_ITEMS, n_samp: int = 1 << 22
         kind = "reference"
         what = (f"reference AliasTableSplit split+pack loops on {threads} threads (p={p}) over the first "
                 f"{n_build} weights; reference SamplerCpu::sample (1 thread, rand()) for {n_samp} samples; "
-                f"step time = 2^26/build_rate + 2^30/sample_rate")
+                f"step time = n/build_rate + m/sample_rate (n={n_total}, m={m_total})")
     else:
         t0 = time.time()
         wt, al, W, rc = po.split_build(w64, p, threads)
@@ -454,11 +546,11 @@ def cpu_baseline(w_np: np.ndarray, n_build: int = N_ITEMS, n_samp: int = 1 << 22
         kind = "port"
         what = (f"oracle restatement of AliasTableSplit::build on {threads} threads over the first {n_build} "
                 f"weights; restated doSample with Philox on {threads} threads for {n_samp} samples; "
-                f"step time = 2^26/build_rate + 2^30/sample_rate")
+                f"step time = n/build_rate + m/sample_rate (n={n_total}, m={m_total})")
     build_rate = n_build / t_build
     sample_rate = n_samp / t_samp
-    t_step = N_ITEMS / build_rate + N_SAMPLES / sample_rate
-    return {"value": round((N_ITEMS + N_SAMPLES) / t_step / 1e9, 6), "unit": UNIT, "cores": threads, "kind": kind,
+    t_step = n_total / build_rate + m_total / sample_rate
+    return {"value": round((n_total + m_total) / t_step / 1e9, 6), "unit": UNIT, "cores": threads, "kind": kind,
             "sample": what, "build_gitems_s": round(build_rate / 1e9, 5),
             "sample_gsamples_s": round(sample_rate / 1e9, 5), "step_s": round(t_step, 2)}
 
@@ -496,8 +588,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-tables measurement")
-    ap.add_argument("--log2-samples", type=int, default=30,
-                    help="samples per step (2^k); smaller values are for profiler captures only")
+    ap.add_argument("--log2-samples", type=int, default=0,
+                    help="samples per step (2^k, 0 = the configuration's); for profiler captures only")
+    ap.add_argument("--config", default="2", choices=sorted(CONFIGS) + ["4", "5"],
+                    help="BASELINE configuration: 2 (default, headline; includes the batched phase), 1, 3, "
+                         "or 4 / 5 (batched tables only)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
@@ -505,6 +600,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         line = run_reference(args, rank)
+    elif args.config in ("4", "5"):
+        line = run_batched_only(args, rank, local_rank)
     else:
         if world > 1:
             import datetime
