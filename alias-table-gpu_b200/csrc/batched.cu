@@ -159,11 +159,11 @@ wrs_status launch_big(const float* d_w, const int64_t* d_offsets, int64_t num_ta
     tile_link_kernel<true><<<(nt + p.big_tables + 255) / 256, 256, 0, stream>>>(L.hdrs, L.incl, nt, p.big_tables,
                                                                                L.heavy_E, L.starts, map);
     const size_t smem = pack_smem_bytes(T);
-    const cudaError_t e = cudaFuncSetAttribute(split_pack_kernel<NT, IPT, true>,
+    const cudaError_t e = cudaFuncSetAttribute(split_pack_kernel<NT, IPT, true, false>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return WRS_ERR_CUDA;
-    split_pack_kernel<NT, IPT, true><<<nt, NT, smem, stream>>>(d_w, L.hdrs, L.incl, L.starts, L.heavy_item,
-                                                                L.heavy_E, nt, d_table, map);
+    split_pack_kernel<NT, IPT, true, false><<<nt, NT, smem, stream>>>(d_w, L.hdrs, L.incl, L.starts, L.heavy_item,
+                                                                L.heavy_E, nt, d_table, map, nullptr);
     batch_status_kernel<<<(p.big_tables + 1 + 255) / 256, 256, 0, stream>>>(L.hdr0 + 1, p.big_tables + 1,
                                                                            &L.hdr0->status);
     return launch_status();

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "build_kernels.cuh"
+#include "psa_kernels.cuh"
 #include "host_util.h"
 
 namespace wrs {
@@ -132,12 +133,94 @@ wrs_status launch_build(const float* d_w, uint64_t n, uint32_t method, wrs_alias
         L.hdr, L.incl, (uint32_t)num_tiles, 1u, L.heavy_E, L.starts, map);
     {
         const size_t smem = pack_smem_bytes(T);
-        e = cudaFuncSetAttribute(split_pack_kernel<NT, IPT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(split_pack_kernel<NT, IPT, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem);
         if (e != cudaSuccess) return WRS_ERR_CUDA;
-        split_pack_kernel<NT, IPT, false><<<(uint32_t)num_tiles, NT, smem, stream>>>(
-            d_w, L.hdr, L.incl, L.starts, L.heavy_item, L.heavy_E, (uint32_t)num_tiles, d_table, map);
+        split_pack_kernel<NT, IPT, false, false><<<(uint32_t)num_tiles, NT, smem, stream>>>(
+            d_w, L.hdr, L.incl, L.starts, L.heavy_item, L.heavy_E, (uint32_t)num_tiles, d_table, map, nullptr);
     }
+    return launch_status();
+}
+
+// PSA+: the split passes up to the tile prefixes, the local pass, and the split passes again
+// over the leftovers (second header, prefix records, tile starts and heavy list).
+struct PsaLayout {
+    BuildHeader* hdr;  // hdr[0]: the build; hdr[1]: the leftover passes (one memset clears both)
+    BuildHeader* hdr2;
+    double2* partials;
+    BlockWord* blocks;
+    BlockWord* blocks2;
+    uint64_t num_blocks;
+    TileVals* agg;
+    TileVals* incl;
+    TileVals* agg2;
+    TileVals* incl2;
+    TileStart* starts2;
+    uint32_t* hmask;
+    LeftSlot* slots;
+    uint32_t* heavy_item2;
+    uint4* heavy_E2;
+    size_t bytes;
+};
+
+PsaLayout carve_psa(void* scratch, uint64_t n, uint64_t num_tiles, uint64_t tile_items) {
+    Carver c(scratch);
+    PsaLayout L;
+    L.hdr = c.take<BuildHeader>(2);
+    L.hdr2 = L.hdr + 1;
+    L.partials = c.take<double2>(kWsumMaxGrid);
+    L.num_blocks = (num_tiles + kPrefixTiles - 1) / kPrefixTiles;
+    L.blocks = c.take<BlockWord>(L.num_blocks);
+    L.blocks2 = c.take<BlockWord>(L.num_blocks);
+    L.agg = c.take<TileVals>(num_tiles);
+    L.incl = c.take<TileVals>(num_tiles);
+    L.agg2 = c.take<TileVals>(num_tiles);
+    L.incl2 = c.take<TileVals>(num_tiles);
+    L.starts2 = c.take<TileStart>(num_tiles + 1);
+    L.hmask = c.take<uint32_t>(num_tiles * (tile_items / 32));
+    L.slots = c.take<LeftSlot>(num_tiles * tile_items);
+    L.heavy_item2 = c.take<uint32_t>(n);
+    L.heavy_E2 = c.take<uint4>(n);
+    L.bytes = c.off;
+    return L;
+}
+
+template <int T>
+wrs_status launch_psa(const float* d_w, uint64_t n, wrs_alias_row* d_table, double* d_W, const PsaLayout& L,
+                      uint64_t num_tiles, cudaStream_t stream) {
+    constexpr int NT = PackShape<T>::NT, IPT = PackShape<T>::IPT;
+    const uint32_t nt = (uint32_t)num_tiles;
+    if (cudaMemsetAsync(L.hdr, 0, 2 * sizeof(BuildHeader), stream) != cudaSuccess) return WRS_ERR_CUDA;
+    if (cudaMemsetAsync(L.blocks2, 0, L.num_blocks * sizeof(BlockWord), stream) != cudaSuccess) return WRS_ERR_CUDA;
+    const uint64_t zero_words = L.num_blocks * sizeof(BlockWord) / sizeof(uint32_t);
+    wsum_kernel<kWsumBlock><<<wsum_grid(n), kWsumBlock, 0, stream>>>(d_w, n, L.hdr, L.partials,
+                                                                     reinterpret_cast<uint32_t*>(L.blocks), zero_words,
+                                                                     d_W);
+    const TileMap map{nullptr, nullptr, nullptr, n, nt};
+    tile_reduce_kernel<T, false><<<nt, kReduceThreads, 0, stream>>>(d_w, L.hdr, L.agg, L.hmask, map);
+    tile_prefix_kernel<<<(uint32_t)L.num_blocks, kPrefixThreads, 0, stream>>>(L.hdr, L.agg, L.incl, L.blocks, nt);
+    {
+        const size_t smem = psa_local_smem_bytes(T);
+        if (cudaFuncSetAttribute(psa_local_kernel<NT, IPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+            return WRS_ERR_CUDA;
+        psa_local_kernel<NT, IPT><<<nt, NT, smem, stream>>>(d_w, n, L.hdr, L.incl, d_table, L.slots, L.agg2, L.hdr2);
+    }
+    tile_prefix_kernel<<<(uint32_t)L.num_blocks, kPrefixThreads, 0, stream>>>(L.hdr2, L.agg2, L.incl2, L.blocks2, nt);
+    psa_heavy_list_kernel<T><<<(nt + 3) / 4, 128, 0, stream>>>(L.hdr2, L.agg2, L.incl2, L.slots, nt, L.heavy_item2,
+                                                               L.heavy_E2);
+    tile_link_kernel<false><<<(nt + 1 + 255) / 256, 256, 0, stream>>>(L.hdr2, L.incl2, nt, 1u, L.heavy_E2, L.starts2,
+                                                                     map);
+    {
+        const size_t smem = pack_smem_bytes(T);
+        if (cudaFuncSetAttribute(split_pack_kernel<NT, IPT, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem) != cudaSuccess)
+            return WRS_ERR_CUDA;
+        split_pack_kernel<NT, IPT, false, true><<<nt, NT, smem, stream>>>(d_w, L.hdr2, L.incl2, L.starts2,
+                                                                          L.heavy_item2, L.heavy_E2, nt, d_table, map,
+                                                                          L.slots);
+    }
+    copy_status_kernel<<<1, 1, 0, stream>>>(L.hdr2, L.hdr);
     return launch_status();
 }
 
@@ -172,6 +255,7 @@ extern "C" size_t wrs_alias_build_scratch_bytes(int64_t n, const wrs_build_opts*
     const int64_t T = tile_items_for(opts);
     if (n < 1 || T < 0) return 0;
     const uint64_t nt = ((uint64_t)n + T - 1) / T;
+    if (opts && opts->method == WRS_METHOD_PSA_PLUS) return carve_psa(nullptr, (uint64_t)n, nt, T).bytes;
     return carve_build(nullptr, (uint64_t)n, nt, T).bytes;
 }
 
@@ -182,8 +266,21 @@ extern "C" wrs_status wrs_alias_build_f32(const float* d_w, int64_t n, const wrs
     const int64_t T = tile_items_for(opts);
     const uint32_t method = opts ? opts->method : WRS_METHOD_SPLIT;
     if (T < 0 || method > WRS_METHOD_PSA_PLUS) return WRS_ERR_INVALID_ARGUMENT;
-    if (method == WRS_METHOD_PSA_PLUS) return WRS_ERR_UNSUPPORTED;
     const uint64_t nt = ((uint64_t)n + T - 1) / T;
+    if (method == WRS_METHOD_PSA_PLUS) {
+        if (scratch_bytes < carve_psa(nullptr, (uint64_t)n, nt, T).bytes) return WRS_ERR_SCRATCH_TOO_SMALL;
+        cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+        const PsaLayout L = carve_psa(d_scratch, (uint64_t)n, nt, T);
+        wrs_status st;
+        switch (T) {
+            case 1024: st = launch_psa<1024>(d_w, (uint64_t)n, d_table, d_W, L, nt, stream); break;
+            case 4096: st = launch_psa<4096>(d_w, (uint64_t)n, d_table, d_W, L, nt, stream); break;
+            default: st = launch_psa<2048>(d_w, (uint64_t)n, d_table, d_W, L, nt, stream); break;
+        }
+        if (st != WRS_SUCCESS) return st;
+        if (opts->flags & WRS_FLAG_SYNC) return read_device_status(&L.hdr->status, stream);
+        return WRS_SUCCESS;
+    }
     if (scratch_bytes < carve_build(nullptr, (uint64_t)n, nt, T).bytes) return WRS_ERR_SCRATCH_TOO_SMALL;
     cudaStream_t stream = static_cast<cudaStream_t>(stream_);
     const BuildLayout L = carve_build(d_scratch, (uint64_t)n, nt, T);

@@ -1042,6 +1042,17 @@ __global__ void __launch_bounds__(256) tile_link_kernel(const BuildHeader* hdr, 
 }
 
 // ---------------------------------------------------------------- pass 6: pack
+// A leftover of the PSA+ local pass (psa_kernels.cuh), which split_pack reads in its leftover
+// mode. Light: deficit in Q16.48 in `lo`, its row probability in prob_bits. Heavy: excess in
+// Q64.64 in (hi, lo).
+struct __align__(8) LeftSlot {
+    uint32_t item;
+    uint32_t prob_bits;
+    uint64_t lo;
+    uint64_t hi;
+};
+static_assert(sizeof(LeftSlot) == 24, "LeftSlot layout");
+
 // Pack CTA shape per tile size: threads x items per thread.
 template <int T>
 struct PackShape;
@@ -1089,13 +1100,17 @@ __device__ __forceinline__ uint32_t stage_pos(uint32_t i) {
 //      compares indices with ranks.
 //  (3) Light rows, staged in shared memory and written out coalesced (the heavies' rows of
 //      this tile belong to the tiles that own them).
-template <int NT, int IPT, bool BATCH>
+// In the leftover mode (LEFT, the PSA+ build's second pass) a tile's lights are its leftover
+// lights from the slots (deficits and row probabilities given), and their rows are written
+// at their items.
+template <int NT, int IPT, bool BATCH, bool LEFT>
 __global__ void __launch_bounds__(NT, (NT == 128 && IPT == 16) ? 6 : 1) split_pack_kernel(const float* __restrict__ w,
                                                         const BuildHeader* hdr, const TileVals* incl,
                                                         const TileStart* __restrict__ starts,
                                                         const uint32_t* __restrict__ heavy_item,
                                                         const uint4* __restrict__ heavy_E, uint32_t num_tiles,
-                                                        wrs_alias_row* __restrict__ table, TileMap map) {
+                                                        wrs_alias_row* __restrict__ table, TileMap map,
+                                                        const LeftSlot* __restrict__ left) {
     constexpr int T = NT * IPT;
     constexpr int C = pack_chunk(T);
     static_assert(16 * C >= 8 * T, "own-tile slots live in the chunk arrays");
@@ -1124,9 +1139,11 @@ __global__ void __launch_bounds__(NT, (NT == 128 && IPT == 16) ? 6 : 1) split_pa
     heavy_E += tr.heavy_off;
     // ---- (1) own tile (the weights' loads go out first: they do not depend on the header)
     float x[IPT];
-    load_items<NT, IPT>(w, n, tile, tid, x);
+    if (!LEFT) load_items<NT, IPT>(w, n, tile, tid, x);
     hdr += tr.table;
     if (earlier_status(hdr) != 0) return;
+    const LeftSlot* ls = LEFT ? left + (uint64_t)tile * T : nullptr;
+    const uint32_t nvalid = LEFT ? __ldcg(&incl[tile].nL) - (tile ? __ldcg(&incl[tile - 1].nL) : 0u) : 0u;
     const ClassParams cp = load_class_params(hdr);
     const uint32_t nH = __ldg(&incl[tr.tile0 + tr.ntiles - 1].nH);
     const TileStart st0 = starts[tr.tile0 + tr.table + tile], st1 = starts[tr.tile0 + tr.table + tile + 1];
@@ -1138,6 +1155,14 @@ __global__ void __launch_bounds__(NT, (NT == 128 && IPT == 16) ? 6 : 1) split_pa
     uint64_t asum = 0;
 #pragma unroll
     for (int k = 0; k < IPT; ++k) {
+        if constexpr (LEFT) {
+            const uint32_t slot = (uint32_t)(tid * IPT + k);
+            const bool valid = slot < nvalid;
+            pk[k] = valid ? __uint_as_float(ls[slot].prob_bits) : 0.0f;
+            asum += valid ? ls[slot].lo : 0ull;
+            lbits |= (uint32_t)valid << k;
+            continue;
+        }
         const float wk = x[k];
         const bool small = wk >= 0.0f && wk < cp.Hh;
         const float p = __fmul_rn(wk, cp.R32);
@@ -1179,6 +1204,10 @@ __global__ void __launch_bounds__(NT, (NT == 128 && IPT == 16) ? 6 : 1) split_pa
             const bool light = (lbits >> k) & 1u;
             if (light) sLkey[li] = sr + D;
             li += light ? 1u : 0u;
+            if (LEFT) {
+                sr += light ? ls[tid * IPT + k].lo : 0ull;
+                continue;
+            }
             sr += (light && !((gbits >> k) & 1u)) ? small_deficit(pk[k]) : 0ull;
             if ((gbits >> k) & 1u) {
                 const uint64_t D1 = sSlotQ[tid * IPT + k];
@@ -1197,7 +1226,7 @@ __global__ void __launch_bounds__(NT, (NT == 128 && IPT == 16) ? 6 : 1) split_pa
     if (nH == 0) {
         // no heavy item anywhere: every row keeps itself
 #pragma unroll
-        for (int k = 0; k < IPT; ++k) al[k] = item0 + k;
+        for (int k = 0; k < IPT; ++k) al[k] = LEFT ? (((lbits >> k) & 1u) ? ls[tid * IPT + k].item : 0u) : item0 + k;
     } else {
         // ---- (2) owned heavies and the next one, chunk by chunk
         const uint32_t last_heavy = __ldg(heavy_item + nH - 1);
@@ -1303,26 +1332,37 @@ __global__ void __launch_bounds__(NT, (NT == 128 && IPT == 16) ? 6 : 1) split_pa
     }
 
     // ---- (3) light rows: staged, then coalesced stores (heavy positions are skipped)
+    if constexpr (LEFT) {
 #pragma unroll
-    for (int k = 0; k < IPT; ++k) {
-        const bool light = (lbits >> k) & 1u;
-        const uint64_t row = light ? (((uint64_t)al[k] << 32) | __float_as_uint(pk[k])) : ~0ull;
-        sStage[stage_pos<IPT>((uint32_t)(tid * IPT + k))] = row;
-    }
-    __syncthreads();
-    uint64_t* out = reinterpret_cast<uint64_t*>(table) + (uint64_t)tile * T;
-    const uint32_t cnt = (uint32_t)min((uint64_t)T, n - (uint64_t)tile * T);
-    if (cnt == (uint32_t)T) {
-#pragma unroll
-        for (int it = 0; it < IPT; ++it) {
-            const uint32_t i = (uint32_t)(it * NT + tid);
-            const uint64_t row = sStage[stage_pos<IPT>(i)];
-            if (row != ~0ull) out[i] = row;
+        for (int k = 0; k < IPT; ++k) {
+            if (!((lbits >> k) & 1u)) continue;
+            wrs_alias_row r;
+            r.prob = pk[k];
+            r.alias = al[k];
+            table[ls[tid * IPT + k].item] = r;
         }
     } else {
-        for (uint32_t i = tid; i < cnt; i += NT) {
-            const uint64_t row = sStage[stage_pos<IPT>(i)];
-            if (row != ~0ull) out[i] = row;
+    #pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+            const bool light = (lbits >> k) & 1u;
+            const uint64_t row = light ? (((uint64_t)al[k] << 32) | __float_as_uint(pk[k])) : ~0ull;
+            sStage[stage_pos<IPT>((uint32_t)(tid * IPT + k))] = row;
+        }
+        __syncthreads();
+        uint64_t* out = reinterpret_cast<uint64_t*>(table) + (uint64_t)tile * T;
+        const uint32_t cnt = (uint32_t)min((uint64_t)T, n - (uint64_t)tile * T);
+        if (cnt == (uint32_t)T) {
+    #pragma unroll
+            for (int it = 0; it < IPT; ++it) {
+                const uint32_t i = (uint32_t)(it * NT + tid);
+                const uint64_t row = sStage[stage_pos<IPT>(i)];
+                if (row != ~0ull) out[i] = row;
+            }
+        } else {
+            for (uint32_t i = tid; i < cnt; i += NT) {
+                const uint64_t row = sStage[stage_pos<IPT>(i)];
+                if (row != ~0ull) out[i] = row;
+            }
         }
     }
 }

@@ -54,6 +54,7 @@ def oracle() -> ctypes.CDLL:
             "or_rejection_sample": (_I, [_P, _U64, _P, _U64, _U64, _U64, _U32, _P]),
             "or_sample_plain_timed": (_D, [_P, _I64, _U64, _U64, _I, _P]),
             "or_batched_build": (_I, [_P, _P, _I64, _P, _P]),
+            "or_psa_plus_build": (_I, [_P, _I64, _D, _I64, _P]),
             "or_batched_sample": (None, [_P, _P, _I64, _P, _U64, _U64, _P]),
         }
         for name, (res, args) in sig.items():
@@ -164,6 +165,16 @@ def sample_plain(rows: np.ndarray, m: int, seed: int, cbase: int = 0) -> np.ndar
     out = np.zeros(m, dtype=np.uint32)
     oracle().or_sample_plain(_p(rows), rows.shape[0], m, seed, cbase, _p(out))
     return out
+
+
+def psa_plus_build(w: np.ndarray, W: float | None = None, tile: int = 2048) -> np.ndarray:
+    """Rows of the PSA+ build (tile-local pre-pack, then the exact merge of the leftovers)."""
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    if W is None:
+        W = exact_sum(w)
+    rows = np.zeros((w.size, 2), dtype=np.uint32)
+    oracle().or_psa_plus_build(_p(w), w.size, W, tile, _p(rows))
+    return rows
 
 
 def batched_build(w: np.ndarray, off: np.ndarray):

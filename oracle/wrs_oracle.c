@@ -590,6 +590,164 @@ int or_exact_build(const float* w, int64_t n, double W, uint32_t* rows) {
     return 0;
 }
 
+/* ------------------------------------------------------------------ PSA+ */
+/* PSA+ (AliasTableSplitGpu::psaPlus + PsaPlusNormal::kernel,
+ * construction/aliasTable/buildMethod/AliasTableSplitGpu.cu:342-386,
+ * construction/aliasTable/psaPlus/PsaPlusNormal.cu:12-152): every section is packed locally
+ * first; the items the local pass cannot finish, one of them with a residual weight, go
+ * through the global split/pack. Restated on this library's exact quantities: sections are
+ * tiles of T items, and the lines are those of or_exact_build (the global deficit line A with
+ * its dithering, the corrected excess line E~) restricted to the tile and measured from the
+ * tile's start (A_b, E~_b). In a tile with total deficit D and total excess Et:
+ *   - a light is finished when a heavy of the tile has E > A_i (alias: the first such heavy);
+ *   - a heavy with E_j <= D is finished with r_j = 1 + E_j - A_next (A_next = the first light
+ *     start >= E_j, else D) and aliases the tile's next heavy; the tile's last heavy, if
+ *     finished, keeps r_j as its row probability but waits for its alias: it becomes the
+ *     tile's first leftover light, with deficit A_next - E_j rounded up to the 2^-48 grid;
+ *   - lights starting at or after Et are leftover lights; the first heavy with E_j > D is a
+ *     leftover heavy with residual excess E_j - D, the heavies after it leftover heavies with
+ *     their whole excess.
+ * The leftovers of all tiles, in tile order, are merged as or_exact_build merges lights and
+ * heavies (their excess line corrected for what remains of the mismatch, a rounding residue). */
+typedef struct {
+    uint32_t item;
+    float prob;
+    u128 q;
+} OrLeft;
+
+int or_psa_plus_build(const float* w, int64_t n, double W, int64_t T, uint32_t* rows) {
+    const double W_N = W / (double)n;
+    const double R = 1.0 / W_N;
+    const ClassParams cp = class_params(W_N, R);
+    /* global lines, as or_exact_build */
+    u128 S = 0, L = 0, E = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        float p;
+        uint64_t q;
+        const int k = classify(w[i], &cp, &p, &q);
+        if (k == K_HEAVY) E += (u128)q << 40;
+        else if (k == K_SMALL) S += (u128)q << 16;
+        else L += (u128)q << 16;
+    }
+    const int64_t nfix = excess_correction(S + q_round24(L), E);
+    OrLeft* L2 = (OrLeft*)malloc((size_t)(n + 1) * sizeof(OrLeft));
+    OrLeft* H2 = (OrLeft*)malloc((size_t)(n + 1) * sizeof(OrLeft));
+    u128* A = (u128*)malloc((size_t)(T + 1) * sizeof(u128));
+    u128* Eh = (u128*)malloc((size_t)(T + 1) * sizeof(u128));
+    float* lp = (float*)malloc((size_t)T * sizeof(float));
+    uint32_t* litem = (uint32_t*)malloc((size_t)T * sizeof(uint32_t));
+    uint32_t* hitem = (uint32_t*)malloc((size_t)T * sizeof(uint32_t));
+    int64_t nL2 = 0, nH2 = 0;
+    u128 Sr = 0, Lr = 0, Er = 0;
+    for (int64_t i0 = 0; i0 < n; i0 += T) {
+        const int64_t i1 = (i0 + T < n) ? i0 + T : n;
+        const u128 A_b = Sr + q_round24(Lr);
+        const u128 E_b = q_scale_excess(Er, nfix);
+        int64_t nl = 0, nh = 0;
+        for (int64_t i = i0; i < i1; ++i) {
+            float p;
+            uint64_t q;
+            const int k = classify(w[i], &cp, &p, &q);
+            if (k == K_HEAVY) {
+                Er += (u128)q << 40;
+                Eh[nh] = q_scale_excess(Er, nfix) - E_b;
+                hitem[nh++] = (uint32_t)i;
+            } else {
+                A[nl] = Sr + q_round24(Lr) - A_b;
+                litem[nl] = (uint32_t)i;
+                if (k == K_SMALL) {
+                    lp[nl] = p;
+                    Sr += (u128)q << 16;
+                } else {
+                    lp[nl] = large_light_prob(Lr, q);
+                    Lr += (u128)q << 16;
+                }
+                ++nl;
+            }
+        }
+        const u128 D = Sr + q_round24(Lr) - A_b;
+        A[nl] = D;
+        const u128 Et = q_scale_excess(Er, nfix) - E_b;
+        /* lights */
+        int64_t L0 = nl, j = 0;
+        for (int64_t li = 0; li < nl; ++li) {
+            if (!(A[li] < Et)) {
+                L0 = li;
+                break;
+            }
+            while (Eh[j] <= A[li]) ++j;
+            rows[2 * (int64_t)litem[li]] = f_bits(lp[li]);
+            rows[2 * (int64_t)litem[li] + 1] = hitem[j];
+        }
+        /* heavies */
+        int64_t Js = nh, I = 0;
+        int conv = 0;
+        OrLeft cv = {0, 0.0f, 0};
+        for (int64_t hj = 0; hj < nh; ++hj) {
+            if (Eh[hj] > D) {
+                Js = hj;
+                break;
+            }
+            while (I < nl && A[I] < Eh[hj]) ++I;
+            const u128 A_next = (I < nl) ? A[I] : D;
+            const float pr = heavy_row_prob(q_one() + Eh[hj] - A_next);
+            if (hj + 1 < nh) {
+                rows[2 * (int64_t)hitem[hj]] = f_bits(pr);
+                rows[2 * (int64_t)hitem[hj] + 1] = hitem[hj + 1];
+            } else {
+                const u128 g = ((u128)1 << 16) - 1; /* round up to the 2^-48 grid */
+                conv = 1;
+                cv.item = hitem[hj];
+                cv.prob = pr;
+                cv.q = (A_next - Eh[hj] + g) & ~g;
+            }
+        }
+        if (conv) L2[nL2++] = cv;
+        for (int64_t li = L0; li < nl; ++li) {
+            OrLeft x = {litem[li], lp[li], A[li + 1] - A[li]};
+            L2[nL2++] = x;
+        }
+        for (int64_t hj = Js; hj < nh; ++hj) {
+            OrLeft x = {hitem[hj], 0.0f, hj == Js ? Eh[hj] - D : Eh[hj] - Eh[hj - 1]};
+            H2[nH2++] = x;
+        }
+    }
+    /* global merge of the leftovers */
+    u128 At = 0, Etot = 0;
+    for (int64_t i = 0; i < nL2; ++i) At += L2[i].q;
+    for (int64_t j = 0; j < nH2; ++j) Etot += H2[j].q;
+    const int64_t nfix2 = excess_correction(At, Etot);
+    u128* Ap = (u128*)malloc((size_t)(nL2 + 1) * sizeof(u128));
+    u128* Ep = (u128*)malloc((size_t)(nH2 + 1) * sizeof(u128));
+    u128 run = 0;
+    for (int64_t i = 0; i < nL2; ++i) {
+        Ap[i] = run;
+        run += L2[i].q;
+    }
+    run = 0;
+    for (int64_t j = 0; j < nH2; ++j) {
+        run += H2[j].q;
+        Ep[j] = q_scale_excess(run, nfix2);
+    }
+    int64_t i = 0, j = 0;
+    while (i < nL2 || j < nH2) {
+        if (i < nL2 && (j >= nH2 || Ap[i] < Ep[j])) {
+            const uint32_t al = nH2 == 0 ? L2[i].item : (j < nH2 ? H2[j].item : H2[nH2 - 1].item);
+            rows[2 * (int64_t)L2[i].item] = f_bits(L2[i].prob);
+            rows[2 * (int64_t)L2[i].item + 1] = al;
+            ++i;
+        } else {
+            const u128 A_next = (i < nL2) ? Ap[i] : At;
+            const uint32_t al = (j + 1 < nH2) ? H2[j + 1].item : H2[j].item;
+            rows[2 * (int64_t)H2[j].item] = f_bits(heavy_row_prob(q_one() + Ep[j] - A_next));
+            rows[2 * (int64_t)H2[j].item + 1] = al;
+            ++j;
+        }
+    }
+    free(L2); free(H2); free(A); free(Eh); free(lp); free(litem); free(hitem); free(Ap); free(Ep);
+    return 0;
+}
+
 /* ------------------------------------------------------------------ batched (CSR) */
 /* The batched build gives every table the rows of a single-table build of its weights, so
  * its restatement is a loop of or_exact_build (the reference's batches are such loops). */

@@ -58,6 +58,9 @@ void or_section_counts(int64_t n, uint32_t S, uint64_t m, uint64_t seed, uint64_
 void or_sample_sectioned(const uint32_t* rows, int64_t n, uint64_t m, uint32_t S, uint64_t seed, uint64_t cbase,
                          uint32_t* out, uint64_t* counts);
 
+/* PSA+: tile-local pre-pack over tiles of T items, then the exact merge of the leftovers */
+int or_psa_plus_build(const float* w, int64_t n, double W, int64_t T, uint32_t* rows);
+
 /* batched (CSR): table t owns items [off[t], off[t+1]); its rows (table-local aliases) are
  * or_exact_build of its weights with W = their exact sum (empty tables: no rows). W_out
  * (optional) gets the totals. Returns the number of tables with a zero or invalid total

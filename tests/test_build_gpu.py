@@ -70,6 +70,28 @@ def test_build_is_deterministic(cuda):
     np.testing.assert_array_equal(a, b)
 
 
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("n", [1, 2, 17, 2047, 2049, 100_003, 1 << 20])
+@pytest.mark.parametrize("tile", [1024, 2048, 4096])
+def test_psa_plus_parity(cuda, name, n, tile):
+    """WRS_METHOD_PSA_PLUS: bit-identical to the oracle's PSA+ restatement."""
+    w = gen(name, n)
+    st, rows, W = gpu_build(w, method=wrs.WRS_METHOD_PSA_PLUS, tile_items=tile)
+    assert st == wrs.WRS_SUCCESS, wrs.status_string(st)
+    ref = po.psa_plus_build(w, W, tile)
+    mism = np.nonzero(np.any(rows != ref, axis=1))[0]
+    assert mism.size == 0, f"{mism.size} rows differ, first {mism[:5]}: {rows[mism[:3]]} vs {ref[mism[:3]]}"
+    chk = po.check_table(w, rows)
+    assert chk["bad_rows"] == 0 and chk["zero_mass"] == 0 and chk["max_rel"] <= 2.5e-7, chk
+
+
+def test_psa_plus_rejects_invalid_weights(cuda):
+    w = gen("uniform", 10_000)
+    w[77] = np.nan
+    st, _, _ = gpu_build(w, method=wrs.WRS_METHOD_PSA_PLUS)
+    assert st == wrs.WRS_ERR_INVALID_WEIGHT
+
+
 @pytest.mark.parametrize("bad", [np.nan, -1.0, np.inf, -np.inf])
 def test_build_rejects_invalid_weights_and_recovers(cuda, bad):
     w = gen("uniform", 10_000)

@@ -71,3 +71,29 @@ def test_exact_build_regression_onelight_505711():
     w[0] = 0.5
     chk = po.check_table(w, po.exact_build(w))
     assert chk["max_rel"] <= 2.5e-7
+
+
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("n", [1, 2, 3, 17, 1000, 2049, 100_003])
+@pytest.mark.parametrize("tile", [1024, 2048])
+def test_psa_plus_build_per_item_error(name, n, tile):
+    """The PSA+ restatement (tile-local pre-pack, then the exact merge of the leftovers;
+    AliasTableSplitGpu::psaPlus, AliasTableSplitGpu.cu:342-386) is a valid table with the
+    split method's error bound."""
+    w = gen(name, n)
+    rows = po.psa_plus_build(w, tile=tile)
+    chk = po.check_table(w, rows)
+    assert chk["bad_rows"] == 0 and chk["zero_mass"] == 0
+    assert chk["max_rel"] <= 2.5e-7, chk
+
+
+def test_psa_plus_pairs_locally():
+    """PSA+ resolves most items inside their own tile: the aliases of its light rows point
+    into the same tile far more often than the split method's do."""
+    w = gen("uniform", 1 << 16)
+    W = po.exact_sum(w)
+    n = w.size
+    light = w <= W / n
+    same = lambda rows: np.mean((rows[light, 1] // 2048) == (np.nonzero(light)[0] // 2048))
+    local, split = same(po.psa_plus_build(w, W, 2048)), same(po.exact_build(w, W))
+    assert local > 0.95 and local > split, (local, split)
