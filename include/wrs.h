@@ -78,7 +78,8 @@ typedef struct wrs_alias_row {
 
 typedef enum wrs_build_method {
     WRS_METHOD_SPLIT = 0,     /* split/pack over light/heavy residual prefix sums ("PSA") */
-    WRS_METHOD_PSA_PLUS = 1   /* tile-local greedy pre-pack, leftovers through split/pack */
+    WRS_METHOD_PSA_PLUS = 1   /* tile-local pre-pack, leftovers through split/pack (more scratch:
+                                 query wrs_alias_build_scratch_bytes with the method set) */
 } wrs_build_method;
 
 #define WRS_FLAG_SYNC 1u      /* synchronise the stream and return the device status */
@@ -125,7 +126,8 @@ WRS_API wrs_status wrs_alias_build_f32(const float* d_w, int64_t n, const wrs_bu
  * that forbids cudaMalloc, plugins that must not touch the host process's memory pools,
  * paths that may not block on an allocation). No counterpart in the reference. Its scratch
  * is a fixed 8 MiB device array inside this library (held on every GPU that loads it until
- * the process exits), so it takes n <= 262,144 (2^18) items and rejects larger n with
+ * the process exits), so it takes n <= 262,144 (2^18) items (about 190,000 with
+ * WRS_METHOD_PSA_PLUS, which needs more scratch) and rejects larger n with
  * WRS_ERR_INVALID_ARGUMENT. It calls no allocating routine. The first call on each device
  * looks up the array's device address (make it before any stream capture). All calls on a
  * device share the array, so calls that overlap on the GPU race: serialise them. Device-side
