@@ -199,6 +199,26 @@ def table_error(w: np.ndarray, rows_u32: np.ndarray) -> dict:
             "zero_weight_mass": float(got[~nz].sum()) if (~nz).any() else 0.0}
 
 
+# ---------------------------------------------------------------- multi-GPU replicas
+
+def max_over_ranks(x: float, device) -> float:
+    """The largest value over all ranks (time-like numbers: the job takes the slowest rank);
+    x itself without a process group."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(units_per_rank: int, ms: float, world: int) -> float:
+    """Whole-job throughput in G units/s of `world` replicas that each process
+    `units_per_rank` units, from the slowest rank's time."""
+    return world * units_per_rank / (ms * 1e-3) / 1e9
+
+
 # ---------------------------------------------------------------- our arm
 
 def run_ours(args, rank: int, world: int, local_rank: int):
@@ -271,10 +291,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     total_ms = ev[0][0].elapsed_time(ev[K - 1][2])
     build_ms = statistics.median([e[0].elapsed_time(e[1]) for e in ev])
     sample_ms = statistics.median([e[1].elapsed_time(e[2]) for e in ev])
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, dev)
 
     # sectioned sampling on the same table (reported beside the headline)
     s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -309,10 +326,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / e2e_steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, dev)
 
     if rank != 0:
         return None
@@ -320,7 +334,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     achieved = 12.0 * m / (sample_ms * 1e-3) / 1e9  # GB/s, 12 B per sample (8 B gather + 4 B write)
     build_gbs = 12.0 * n / (build_ms * 1e-3) / 1e9  # 12 B per item (4 B read + 8 B write)
     step_ms = total_ms / K
-    value = world * (n + m) / (step_ms * 1e-3) / 1e9
+    value = replica_value(n + m, step_ms, world)
     cpu = cpu_baseline(w_np, min(n, N_ITEMS), 1 << 22, n, m) if not args.no_cpu_baseline else None
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": K,
@@ -344,7 +358,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                      "algorithmic_bytes": "12 B/sample x 2^30 samples per launch (8 B row gather + 4 B write)"},
         "cpu_baseline": cpu,
         "clocks": clk,
-        "e2e": {"value": round(world * (n + m) / (e2e_ms * 1e-3) / 1e9, 4), "unit": UNIT,
+        "e2e": {"value": round(replica_value(n + m, e2e_ms, world), 4), "unit": UNIT,
                 "ms_per_step": round(e2e_ms, 3), "h2d_bytes_per_step": 4 * n, "d2h_bytes_per_step": 4 * m},
         "gpu_launches": KERNELS_PER_STEP * K,
     }

@@ -1,0 +1,55 @@
+"""The multi-GPU form of the path is replicas (no data-path collective): every rank runs the
+whole step, the job's time is the slowest rank's, and the value is the units all ranks
+processed over that time. The rank reduction of bench.py, run as two gloo processes on CPU."""
+import os
+import socket
+import sys
+
+import pytest
+import torch.multiprocessing as mp
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _rank(rank, world, port, out):
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, REPO)
+    import bench
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        ms = [12.5, 20.0][rank]
+        slowest = bench.max_over_ranks(ms, torch.device("cpu"))
+        dist.barrier()
+        out[rank] = (slowest, bench.replica_value(1 << 20, slowest, world))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_replicas_take_the_slowest_rank_and_sum_the_work():
+    world = 2
+    mgr = mp.Manager()
+    out = mgr.dict()
+    mp.start_processes(_rank, args=(world, _free_port(), out), nprocs=world, start_method="spawn", join=True)
+    for r in range(world):
+        slowest, value = out[r]
+        assert slowest == 20.0
+        assert value == pytest.approx(world * (1 << 20) / 20e-3 / 1e9)
+
+
+def test_single_process_needs_no_group():
+    sys.path.insert(0, REPO)
+    import bench
+    import torch
+    assert bench.max_over_ranks(3.5, torch.device("cpu")) == 3.5
+    assert bench.replica_value(10 ** 9, 1000.0, 1) == pytest.approx(1.0)
