@@ -68,11 +68,12 @@ namespace {
 
 constexpr int64_t kMaxItems = (int64_t)0x7fffffff - 8192;
 
-// Items per tile of the reduce and pack passes (0 = the default 2048).
+// Items per tile of the reduce and pack passes (0 = the default: 2048, and 1024 for PSA+,
+// whose local pass is faster on smaller tiles).
 int64_t tile_items_for(const wrs_build_opts* opts) {
     const uint32_t t = opts ? opts->tile_items : 0u;
     switch (t) {
-        case 0:
+        case 0: return (opts && opts->method == WRS_METHOD_PSA_PLUS) ? 1024 : 2048;
         case 2048: return 2048;
         case 1024: return 1024;
         case 4096: return 4096;

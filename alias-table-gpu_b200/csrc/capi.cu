@@ -1,6 +1,8 @@
 // capi.cu — status strings, device check and version of the C ABI.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "host_util.h"
 
 extern "C" const char* wrs_status_string(wrs_status s) {
@@ -28,3 +30,27 @@ extern "C" wrs_status wrs_check_device(void) {
 }
 
 extern "C" int wrs_version(void) { return WRS_VERSION_MAJOR * 100 + WRS_VERSION_MINOR; }
+
+// The reference's table format (TableStorage, construction/aliasTable/TableStorage.cuh:6-128,
+// structure-of-arrays form): per row an absolute FP64 weight in [0, W/N] and an int alias, so
+// code written against the reference (AliasTable::verifyTableCorrectness, AliasTable.cu:24-65;
+// doSample, sampling/aliasTable/SamplerGpuBasic.cu:28-69) can consume a table built here.
+namespace {
+__global__ void export_reference_kernel(const uint2* __restrict__ table, uint64_t n, double W_N,
+                                        double* __restrict__ weight, int32_t* __restrict__ alias) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint2 r = table[i];
+        weight[i] = (double)__uint_as_float(r.x) * W_N;
+        alias[i] = (int32_t)r.y;
+    }
+}
+}  // namespace
+
+extern "C" wrs_status wrs_export_reference_table(const wrs_alias_row* d_table, int64_t n, double W, double* d_weight,
+                                                 int32_t* d_alias, void* stream) {
+    if (!d_table || !d_weight || !d_alias || n < 1 || n > 0x7fffffffll || !(W > 0.0)) return WRS_ERR_INVALID_ARGUMENT;
+    const uint64_t blocks = std::min<uint64_t>(((uint64_t)n + 255) / 256, 148ull * 32);
+    export_reference_kernel<<<(uint32_t)blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<const uint2*>(d_table), (uint64_t)n, W / (double)n, d_weight, d_alias);
+    return wrs::launch_status();
+}

@@ -80,6 +80,7 @@ _SIGNATURES = {
     "wrs_batched_sample": (ctypes.c_int, [_P, _P, _I64, _P, _U64, _U64, _U64, _P, _P]),
     "wrs_batched_autotune": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _SZ, _P, _P]),
     "wrs_scratch_status": (ctypes.c_int, [_P, _P]),
+    "wrs_export_reference_table": (ctypes.c_int, [_P, _I64, ctypes.c_double, _P, _P, _P]),
     "wrs_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "wrs_check_device": (ctypes.c_int, []),
     "wrs_version": (ctypes.c_int, []),
@@ -213,6 +214,12 @@ def batched_autotune(w, d_offsets, h_offsets, table, scratch, opts: BuildOpts, s
     return lib().wrs_batched_autotune(_ptr(w), _ptr(d_offsets), h.ctypes.data, h.shape[0] - 1, _ptr(table),
                                       _ptr(scratch), scratch.numel() * scratch.element_size(), ctypes.byref(opts),
                                       _stream(stream))
+
+
+def export_reference_table(table, W: float, weight, alias, stream=None) -> int:
+    """The table in the reference's format: FP64 absolute weights (prob * W/n) and int aliases."""
+    return lib().wrs_export_reference_table(_ptr(table), table.numel(), W, _ptr(weight), _ptr(alias),
+                                            _stream(stream))
 
 
 def sum_f32(w, total, scratch, stream=None) -> int:

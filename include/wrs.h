@@ -86,7 +86,7 @@ typedef enum wrs_build_method {
 
 typedef struct wrs_build_opts {
     uint32_t method;            /* wrs_build_method */
-    uint32_t tile_items;        /* 0 = default (2048); 1024, 2048 or 4096 */
+    uint32_t tile_items;        /* 0 = default (2048; 1024 for PSA+); 1024, 2048 or 4096 */
     uint32_t flags;             /* WRS_FLAG_* */
     uint32_t small_table_items; /* batched builds: tables of at most this many items are built
                                    one per warp (0 = default 128; 32, 64, 128, 256 or 512) */
@@ -204,6 +204,15 @@ WRS_API wrs_status wrs_batched_sample(const wrs_alias_row* d_table, const int64_
 WRS_API wrs_status wrs_batched_autotune(const float* d_w, const int64_t* d_offsets, const int64_t* h_offsets,
                                 int64_t num_tables, wrs_alias_row* d_table, void* d_scratch,
                                 size_t scratch_bytes, wrs_build_opts* opts, void* stream);
+
+/* ---- reference table format -------------------------------------------- */
+
+/* Writes the table in the reference's format (TableStorage, construction/aliasTable/
+ * TableStorage.cuh:6-128, structure of arrays): d_weight[i] = prob_i * W / n (absolute FP64
+ * weight in [0, W/n]) and d_alias[i] = alias_i, for code written against the reference
+ * (verifyTableCorrectness, doSample). W is the weight total the build used (its d_W). */
+WRS_API wrs_status wrs_export_reference_table(const wrs_alias_row* d_table, int64_t n, double W,
+                                              double* d_weight, int32_t* d_alias, void* stream);
 
 /* ---- status / misc ------------------------------------------------------ */
 

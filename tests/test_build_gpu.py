@@ -142,3 +142,21 @@ def test_reference_shaped_surface(cuda):
     prob, alias = t.aliasTable
     rows = np.stack([prob.view(np.uint32), alias], axis=1)
     check_parity(w, rows, t.W)
+
+
+@pytest.mark.parametrize("method", [wrs.WRS_METHOD_SPLIT, wrs.WRS_METHOD_PSA_PLUS])
+def test_export_reference_format(cuda, method):
+    """The table in the reference's TableStorage format passes the reference-format check
+    (the per-item restatement of AliasTable::verifyTableCorrectness, AliasTable.cu:24-65)."""
+    w = gen("powerlaw_shuffled", 100_003)
+    st, rows, W = gpu_build(w, method=method)
+    assert st == wrs.WRS_SUCCESS
+    table = torch.from_numpy(rows.view(np.int64).reshape(-1)).cuda()
+    weight = torch.empty(w.size, dtype=torch.float64, device="cuda")
+    alias = torch.empty(w.size, dtype=torch.int32, device="cuda")
+    assert wrs.export_reference_table(table, W, weight, alias) == wrs.WRS_SUCCESS
+    torch.cuda.synchronize()
+    wt, al = weight.cpu().numpy(), alias.cpu().numpy()
+    assert np.array_equal(wt, rows[:, 0].view(np.float32).astype(np.float64) * (W / w.size))
+    chk = po.check_ref_table(w.astype(np.float64), wt, al, W)
+    assert chk["bad_rows"] == 0 and chk["max_rel"] <= 2.5e-7, chk
