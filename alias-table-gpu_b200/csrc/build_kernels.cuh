@@ -607,17 +607,37 @@ __global__ void __launch_bounds__(kReduceThreads) tile_reduce_kernel(const float
     const uint64_t item0 = (uint64_t)tr.local * T + (uint64_t)threadIdx.x * IPT;  // table-local
     uint32_t lbits = 0, sbits = 0, hbits = 0;
     uint64_t S = 0;
+    // p * 2^48 = w * (fl32(N/W) * 2^48) exactly while the scaled factor is finite (a power-of-two
+    // scaling commutes with rounding); small_deficit(p) = 2^48 - rne(p * 2^48).
+    const float R48 = cp.R32 * 281474976710656.0f;
+    if ((uint64_t)(tr.local + 1) * T <= tr.n && R48 < __int_as_float(0x7f800000)) {
+        // a full tile: every item is present
+        uint64_t qsum = 0;
 #pragma unroll
-    for (int k = 0; k < IPT; ++k) {
-        const float wk = x[k];
-        const bool heavy = wk > cp.H1;
-        const bool light = wk >= 0.0f && !heavy;
-        const bool small = wk >= 0.0f && wk < cp.Hh;
-        const uint64_t d = small_deficit(__fmul_rn(wk, cp.R32));
-        S += small ? d : 0ull;
-        lbits |= (uint32_t)light << k;
-        sbits |= (uint32_t)small << k;
-        hbits |= (uint32_t)heavy << k;
+        for (int k = 0; k < IPT; ++k) {
+            const float wk = x[k];
+            const bool heavy = wk > cp.H1;
+            const bool rare = wk >= cp.Hh;
+            const uint64_t qs = __float2ull_rn(__fmul_rn(wk, R48));
+            if (!rare) qsum += qs;
+            hbits |= (uint32_t)heavy << k;
+            sbits |= (uint32_t)!rare << k;
+        }
+        lbits = ~hbits & (IPT == 32 ? 0xffffffffu : ((1u << IPT) - 1u));
+        S = (uint64_t)__popc(sbits) * kOneQ48 - qsum;
+    } else {
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+            const float wk = x[k];
+            const bool heavy = wk > cp.H1;
+            const bool light = wk >= 0.0f && !heavy;
+            const bool small = wk >= 0.0f && wk < cp.Hh;
+            const uint64_t d = small_deficit(__fmul_rn(wk, cp.R32));
+            S += small ? d : 0ull;
+            lbits |= (uint32_t)light << k;
+            sbits |= (uint32_t)small << k;
+            hbits |= (uint32_t)heavy << k;
+        }
     }
     // rare items (large lights and heavies), weights re-read from L1
     uint64_t L = 0, E = 0;
