@@ -912,9 +912,8 @@ __device__ __forceinline__ u128 load_u128(const uint4* p) {
     return q_make(((uint64_t)v.w << 32) | v.z, ((uint64_t)v.y << 32) | v.x);
 }
 
-// Tiles (warps) per CTA of the heavy-list pass: each warp keeps its tile's heavy items in
-// shared memory.
-__host__ __device__ constexpr int heavy_warps(int T) { return T >= 4096 ? 2 : 4; }
+// Tiles (warps) per CTA of the heavy-list pass.
+__host__ __device__ constexpr int heavy_warps(int) { return 4; }
 
 __device__ __forceinline__ uint32_t warp_excl_scan_u32(uint32_t v, uint32_t& total) {
     const int lane = threadIdx.x & 31;
@@ -946,17 +945,19 @@ __global__ void __launch_bounds__(32 * heavy_warps(T)) heavy_list_kernel(const f
                                                                       const uint32_t* __restrict__ hmask,
                                                                       uint32_t num_tiles, uint32_t* heavy_item,
                                                                       uint4* heavy_E, TileMap map) {
-    constexpr int WPT = T / 32;  // mask words per tile
-    constexpr int WPL = WPT / 32;  // mask words per lane
+    constexpr int WPT = T / 32;    // mask words per tile
+    constexpr int WPL = WPT / 32;  // mask words per lane: lane l owns tile items [l*32*WPL, (l+1)*32*WPL)
     static_assert(WPL >= 1 && WPL <= 4, "mask words per lane");
     constexpr int NWARP = heavy_warps(T);
-    __shared__ uint32_t sItem[NWARP][T];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t u = blockIdx.x * NWARP + warp;  // global tile
     if (u >= num_tiles || plan_failed<BATCH>(map)) return;
     const TileRef tr = tile_ref<BATCH>(map, u);
     hdr += tr.table;
     if (earlier_status(hdr) != 0) return;
+    uint32_t wd[WPL];
+#pragma unroll
+    for (int i = 0; i < WPL; ++i) wd[i] = __ldg(hmask + (uint64_t)u * WPT + lane * WPL + i);
     const uint32_t m = __ldcg(&agg[u].nH);
     if (m == 0) return;
     const float* wt = w + tr.item_off;
@@ -966,35 +967,28 @@ __global__ void __launch_bounds__(32 * heavy_warps(T)) heavy_list_kernel(const f
     const int64_t nfix = __ldg(&hdr->nfix);
     const uint32_t g0 = tr.local ? __ldcg(&incl[u - 1].nH) : 0u;
     const u128 Eb = tr.local ? ldcg_E(incl + u - 1) : (u128)0;
-    uint32_t* items = sItem[warp];
-    {
-        // lane l holds mask words l*WPL .. l*WPL + WPL - 1 (consecutive tile items)
-        uint32_t wd[WPL];
-        uint32_t c = 0;
-#pragma unroll
-        for (int i = 0; i < WPL; ++i) {
-            wd[i] = __ldg(hmask + (uint64_t)u * WPT + lane * WPL + i);
-            c += (uint32_t)__popc(wd[i]);
-        }
-        uint32_t ctot;
-        uint32_t o = warp_excl_scan_u32(c, ctot);
-#pragma unroll
-        for (int i = 0; i < WPL; ++i) {
-            const uint32_t ibase = tr.local * (uint32_t)T + (uint32_t)(lane * WPL + i) * 32u;
-            for (uint32_t b = wd[i]; b; b &= b - 1) items[o++] = ibase + (uint32_t)(__ffs(b) - 1);
-        }
-    }
-    __syncwarp();
-    const uint32_t per = (m + 31) / 32;
-    const uint32_t j0 = min(m, (uint32_t)lane * per), j1 = min(m, j0 + per);
+    const uint32_t ibase = tr.local * (uint32_t)T + (uint32_t)lane * WPL * 32u;
+    // this lane's heavies: count and excess sum, then the warp's exclusive prefixes
+    uint32_t c = 0;
     uint64_t hs = 0;
-    for (uint32_t j = j0; j < j1; ++j) hs += rare_q(__ldg(wt + items[j]), true, cp);
+#pragma unroll
+    for (int i = 0; i < WPL; ++i) {
+        c += (uint32_t)__popc(wd[i]);
+        for (uint32_t b = wd[i]; b; b &= b - 1) hs += rare_q(__ldg(wt + ibase + i * 32 + __ffs(b) - 1), true, cp);
+    }
+    uint32_t ctot;
+    uint32_t j = g0 + warp_excl_scan_u32(c, ctot);
     uint64_t htot;
     uint64_t er = warp_excl_scan_u64(hs, htot);
-    for (uint32_t j = j0; j < j1; ++j) {
-        er += rare_q(__ldg(wt + items[j]), true, cp);  // the weight again, from L1
-        heavy_item[g0 + j] = items[j];
-        store_u128(heavy_E + g0 + j, q_scale_excess(Eb + ((u128)er << 40), nfix));
+#pragma unroll
+    for (int i = 0; i < WPL; ++i) {
+        for (uint32_t b = wd[i]; b; b &= b - 1) {
+            const uint32_t item = ibase + i * 32 + (uint32_t)(__ffs(b) - 1);
+            er += rare_q(__ldg(wt + item), true, cp);  // the weight again, from L1
+            heavy_item[j] = item;
+            store_u128(heavy_E + j, q_scale_excess(Eb + ((u128)er << 40), nfix));
+            ++j;
+        }
     }
 }
 
