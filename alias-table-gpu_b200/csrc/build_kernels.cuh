@@ -639,14 +639,28 @@ __global__ void __launch_bounds__(kReduceThreads) tile_reduce_kernel(const float
             hbits |= (uint32_t)heavy << k;
         }
     }
-    // rare items (large lights and heavies), weights re-read from L1
+    // rare items (large lights and heavies): from the weights in registers when a thread has
+    // many (all items predicated), else gathered again from L1 one by one
     uint64_t L = 0, E = 0;
-    for (uint32_t bits = (lbits & ~sbits) | hbits; bits; bits &= bits - 1) {
-        const int k = __ffs(bits) - 1;
-        const bool heavy = (hbits >> k) & 1u;
-        const uint64_t q = rare_q(__ldg(wt + item0 + k), heavy, cp);
-        E += heavy ? q : 0ull;
-        L += heavy ? 0ull : q;
+    const uint32_t rbits = (lbits & ~sbits) | hbits;
+    if ((uint32_t)__popc(rbits) * 4u > (uint32_t)IPT) {
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+            if ((rbits >> k) & 1u) {
+                const bool heavy = (hbits >> k) & 1u;
+                const uint64_t q = rare_q(x[k], heavy, cp);
+                E += heavy ? q : 0ull;
+                L += heavy ? 0ull : q;
+            }
+        }
+    } else {
+        for (uint32_t bits = rbits; bits; bits &= bits - 1) {
+            const int k = __ffs(bits) - 1;
+            const bool heavy = (hbits >> k) & 1u;
+            const uint64_t q = rare_q(__ldg(wt + item0 + k), heavy, cp);
+            E += heavy ? q : 0ull;
+            L += heavy ? 0ull : q;
+        }
     }
     // heavy mask words (32 / IPT lanes per word)
     {
@@ -899,6 +913,12 @@ static __global__ void __launch_bounds__(kPrefixThreads) tile_prefix_kernel(Buil
     }
 }
 
+// Slot of entry i of a shared array that each thread fills at consecutive indices from a
+// scanned start (the light keys of a pack tile, a heavy-list segment): the low four index
+// bits XOR the next four. The threads of a warp start about a thread's item count apart, so
+// without the XOR every lane's store would fall into the same bank (pair).
+__device__ __forceinline__ uint32_t lkey_slot(uint32_t i) { return i ^ ((i >> 4) & 15u); }
+
 // ---------------------------------------------------------------- pass 4: heavy list
 // One tile per warp: the tile's heavies in item order (expanded from its heavy mask), their
 // excess (weights gathered again), and their corrected excess ends E~ (Q64.64), written at
@@ -914,6 +934,18 @@ __device__ __forceinline__ u128 load_u128(const uint4* p) {
 
 // Tiles (warps) per CTA of the heavy-list pass.
 __host__ __device__ constexpr int heavy_warps(int) { return 4; }
+
+// Items per segment of the heavy-list pass: one mask word per lane.
+constexpr int kHeavySeg = 1024;
+// Heavies in a mask word from which a lane loads all of the word's weights.
+constexpr int kDenseWord = 6;
+
+// A warp's staging of one segment's heavies in heavy order: the within-tile inclusive excess
+// prefix (Q40.24) and the item's offset in the segment, at swizzled slots (lkey_slot).
+struct HeavyStage {
+    uint64_t er[kHeavySeg];
+    uint16_t off[kHeavySeg];
+};
 
 __device__ __forceinline__ uint32_t warp_excl_scan_u32(uint32_t v, uint32_t& total) {
     const int lane = threadIdx.x & 31;
@@ -945,19 +977,17 @@ __global__ void __launch_bounds__(32 * heavy_warps(T)) heavy_list_kernel(const f
                                                                       const uint32_t* __restrict__ hmask,
                                                                       uint32_t num_tiles, uint32_t* heavy_item,
                                                                       uint4* heavy_E, TileMap map) {
-    constexpr int WPT = T / 32;    // mask words per tile
-    constexpr int WPL = WPT / 32;  // mask words per lane: lane l owns tile items [l*32*WPL, (l+1)*32*WPL)
-    static_assert(WPL >= 1 && WPL <= 4, "mask words per lane");
+    constexpr int WPT = T / 32;  // mask words per tile
+    constexpr int NSEG = T / kHeavySeg;
+    static_assert(NSEG >= 1 && NSEG * kHeavySeg == T, "segments per tile");
     constexpr int NWARP = heavy_warps(T);
+    __shared__ HeavyStage stage[NWARP];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t u = blockIdx.x * NWARP + warp;  // global tile
     if (u >= num_tiles || plan_failed<BATCH>(map)) return;
     const TileRef tr = tile_ref<BATCH>(map, u);
     hdr += tr.table;
     if (earlier_status(hdr) != 0) return;
-    uint32_t wd[WPL];
-#pragma unroll
-    for (int i = 0; i < WPL; ++i) wd[i] = __ldg(hmask + (uint64_t)u * WPT + lane * WPL + i);
     const uint32_t m = __ldcg(&agg[u].nH);
     if (m == 0) return;
     const float* wt = w + tr.item_off;
@@ -967,28 +997,74 @@ __global__ void __launch_bounds__(32 * heavy_warps(T)) heavy_list_kernel(const f
     const int64_t nfix = __ldg(&hdr->nfix);
     const uint32_t g0 = tr.local ? __ldcg(&incl[u - 1].nH) : 0u;
     const u128 Eb = tr.local ? ldcg_E(incl + u - 1) : (u128)0;
-    const uint32_t ibase = tr.local * (uint32_t)T + (uint32_t)lane * WPL * 32u;
-    // this lane's heavies: count and excess sum, then the warp's exclusive prefixes
-    uint32_t c = 0;
-    uint64_t hs = 0;
+    HeavyStage& sg = stage[warp];
+    uint32_t j0 = g0;  // global heavy index of the segment's first heavy
+    uint64_t e0 = 0;   // excess of the tile's heavies before the segment (Q40.24)
+#pragma unroll 1
+    for (int s = 0; s < NSEG; ++s) {
+        // lane l: the 32 items of mask word l of the segment; their heavies' count and excess
+        const uint32_t wd = __ldg(hmask + (uint64_t)u * WPT + s * 32 + lane);
+        const uint32_t sbase = tr.local * (uint32_t)T + (uint32_t)s * kHeavySeg;
+        const float* wl = wt + sbase + lane * 32;
+        // a dense word loads all of its 32 weights at once (independent loads); a sparse one
+        // gathers its heavies' weights one by one
+        const bool dense = __popc(wd) >= kDenseWord;
+        float xv[32];
+        uint64_t hs = 0;
+        if (dense) {
+            if (((uintptr_t)wl & 15u) == 0) {
 #pragma unroll
-    for (int i = 0; i < WPL; ++i) {
-        c += (uint32_t)__popc(wd[i]);
-        for (uint32_t b = wd[i]; b; b &= b - 1) hs += rare_q(__ldg(wt + ibase + i * 32 + __ffs(b) - 1), true, cp);
-    }
-    uint32_t ctot;
-    uint32_t j = g0 + warp_excl_scan_u32(c, ctot);
-    uint64_t htot;
-    uint64_t er = warp_excl_scan_u64(hs, htot);
+                for (int k = 0; k < 8; ++k) {
+                    const float4 v = __ldg(reinterpret_cast<const float4*>(wl) + k);
+                    xv[4 * k] = v.x;
+                    xv[4 * k + 1] = v.y;
+                    xv[4 * k + 2] = v.z;
+                    xv[4 * k + 3] = v.w;
+                }
+            } else {
 #pragma unroll
-    for (int i = 0; i < WPL; ++i) {
-        for (uint32_t b = wd[i]; b; b &= b - 1) {
-            const uint32_t item = ibase + i * 32 + (uint32_t)(__ffs(b) - 1);
-            er += rare_q(__ldg(wt + item), true, cp);  // the weight again, from L1
-            heavy_item[j] = item;
-            store_u128(heavy_E + j, q_scale_excess(Eb + ((u128)er << 40), nfix));
-            ++j;
+                for (int k = 0; k < 32; ++k) xv[k] = __ldg(wl + k);
+            }
+#pragma unroll
+            for (int k = 0; k < 32; ++k)
+                if ((wd >> k) & 1u) hs += rare_q(xv[k], true, cp);
+        } else {
+            for (uint32_t b = wd; b; b &= b - 1) hs += rare_q(__ldg(wl + __ffs(b) - 1), true, cp);
         }
+        uint32_t ctot;
+        uint64_t htot;
+        uint32_t pos = warp_excl_scan_u32((uint32_t)__popc(wd), ctot);
+        uint64_t er = e0 + warp_excl_scan_u64(hs, htot);
+        // stage them in heavy order, then write the segment's part of the list with
+        // coalesced stores
+        if (dense) {
+#pragma unroll
+            for (int k = 0; k < 32; ++k) {
+                if ((wd >> k) & 1u) {
+                    er += rare_q(xv[k], true, cp);
+                    const uint32_t slot = lkey_slot(pos++);
+                    sg.er[slot] = er;
+                    sg.off[slot] = (uint16_t)(lane * 32 + k);
+                }
+            }
+        } else {
+            for (uint32_t b = wd; b; b &= b - 1) {
+                const uint32_t k = (uint32_t)(__ffs(b) - 1);
+                er += rare_q(__ldg(wl + k), true, cp);  // the weight again, from L1
+                const uint32_t slot = lkey_slot(pos++);
+                sg.er[slot] = er;
+                sg.off[slot] = (uint16_t)(lane * 32 + k);
+            }
+        }
+        __syncwarp();
+        for (uint32_t p = lane; p < ctot; p += 32) {
+            const uint32_t slot = lkey_slot(p);
+            heavy_item[j0 + p] = sbase + sg.off[slot];
+            store_u128(heavy_E + j0 + p, q_scale_excess(Eb + ((u128)sg.er[slot] << 40), nfix));
+        }
+        __syncwarp();  // the next segment reuses the stage
+        j0 += ctot;
+        e0 += htot;
     }
 }
 
@@ -1087,6 +1163,18 @@ struct PackShape<4096> {
 // the chunk arrays (16 * C >= 8 * T bytes).
 __host__ __device__ constexpr int pack_chunk(int T) { return T / 2 > 1024 ? T / 2 : 1024; }
 
+// Heavies that the merge-walk form of the pack kernel holds at once (a u64 key and a u32 item
+// each, in the bytes of the chunk arrays).
+__host__ __device__ constexpr int pack_walk_cap(int T) { return (pack_chunk(T) * 16 / 12) & ~31; }
+
+// A heavy's key in a pack tile's frame: ceil((E~ - A_before) / 2^-48), clamped to
+// [0, 2^64 - 1].
+__device__ __forceinline__ uint64_t pack_heavy_key(u128 Et, u128 A_before) {
+    if (Et <= A_before) return 0;
+    const u128 d = Et - A_before + 0xffff;
+    return (q_hi(d) >> 16) ? ~0ull : (uint64_t)(d >> 16);
+}
+
 // Shared memory of the pack kernel, in this order: light keys (u64 x T; the staged rows at
 // the end), heavy keys (u64 x C), heavy items (u32 x C), heavy ranks (u32 x C).
 __host__ __device__ constexpr size_t pack_smem_bytes(int T) {
@@ -1114,11 +1202,18 @@ __device__ __forceinline__ uint32_t stage_pos(uint32_t i) {
 //      compares indices with ranks.
 //  (3) Light rows, staged in shared memory and written out coalesced (the heavies' rows of
 //      this tile belong to the tiles that own them).
+// When the heavies of (2) fit in shared memory at once (at most pack_walk_cap(T), the common
+// case), (1) and (2) are one merge instead: thread t takes the heavies whose keys lie in
+// [b_t, b_t+1), b_t = its first light's key (a lower bound search), and walks its lights in
+// order: heavies with key <= the light's key rank at that light (their A_next is its key),
+// and the light's alias is the first heavy left. The heavies left after its last light rank
+// at the next thread's first light. No light key goes to shared memory and no heavy searches
+// the lights.
 // In the leftover mode (LEFT, the PSA+ build's second pass) a tile's lights are its leftover
 // lights from the slots (deficits and row probabilities given), and their rows are written
 // at their items.
 template <int NT, int IPT, bool BATCH, bool LEFT>
-__global__ void __launch_bounds__(NT, (NT == 128 && IPT == 16) ? 6 : 1) split_pack_kernel(const float* __restrict__ w,
+__global__ void __launch_bounds__(NT, (NT == 128 && IPT == 16) ? 5 : 1) split_pack_kernel(const float* __restrict__ w,
                                                         const BuildHeader* hdr, const TileVals* incl,
                                                         const TileStart* __restrict__ starts,
                                                         const uint32_t* __restrict__ heavy_item,
@@ -1127,16 +1222,20 @@ __global__ void __launch_bounds__(NT, (NT == 128 && IPT == 16) ? 6 : 1) split_pa
                                                         const LeftSlot* __restrict__ left) {
     constexpr int T = NT * IPT;
     constexpr int C = pack_chunk(T);
+    constexpr int CW = pack_walk_cap(T);
     static_assert(16 * C >= 8 * T, "own-tile slots live in the chunk arrays");
+    static_assert(12 * CW <= 16 * C, "walk arrays live in the chunk arrays");
     static_assert(IPT >= 4 && IPT <= 32 && (IPT & (IPT - 1)) == 0, "items per thread");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint64_t* sLkey = reinterpret_cast<uint64_t*>(smem_raw);
     uint64_t* sHkey = sLkey + T;
     uint32_t* sHitem = reinterpret_cast<uint32_t*>(sHkey + C);
     uint32_t* sHrank = sHitem + C;
-    uint64_t* sSlotQ = sHkey;  // own-tile phase: per item slot
     uint64_t* sStage = sLkey;                                // row phase: staged rows
+    uint64_t* sWk = sHkey;                                   // walk: heavy keys, then A_next keys
+    uint32_t* sWi = reinterpret_cast<uint32_t*>(sWk + CW);   // walk: heavy items
     __shared__ Scan3 s_scan3[NT / 32];
+    __shared__ uint32_t s_wa[NT];
     __shared__ uint32_t s_r0, s_pend_item;
     __shared__ float s_pend_prob;
 
@@ -1163,10 +1262,23 @@ __global__ void __launch_bounds__(NT, (NT == 128 && IPT == 16) ? 6 : 1) split_pa
     const TileStart st0 = starts[tr.tile0 + tr.table + tile], st1 = starts[tr.tile0 + tr.table + tile + 1];
     const u128 A_before = q_make(st0.A_hi, st0.A_lo);
     const u128 A_after = q_make(st1.A_hi, st1.A_lo);
+    const uint32_t g_lo = st0.bound, g_hi = st1.bound;
+    const uint32_t g_end = min(g_hi + 1u, nH);  // the owned heavies and the next one
+    const bool walk = nH != 0 && g_end - g_lo <= (uint32_t)CW;
+    const uint32_t m_w = walk ? g_end - g_lo : 0u;
+    if (walk) {
+#pragma unroll 4
+        for (uint32_t j = tid; j < m_w; j += NT) {
+            sWk[j] = pack_heavy_key(load_u128(heavy_E + g_lo + j), A_before);
+            sWi[j] = __ldg(heavy_item + g_lo + j);
+        }
+    }
+    // own-tile phase: a large light's slot (per item), in whichever array is free
+    uint64_t* sSlotQ = walk ? sStage : sHkey;
     const uint32_t item0 = (uint32_t)((uint64_t)tile * T + (uint64_t)tid * IPT);
     float pk[IPT];
     uint32_t lbits = 0, gbits = 0;  // bit k: item k is a light / a large light
-    uint64_t asum = 0;
+    uint64_t asum = 0, lsum = 0;
 #pragma unroll
     for (int k = 0; k < IPT; ++k) {
         if constexpr (LEFT) {
@@ -1185,7 +1297,8 @@ __global__ void __launch_bounds__(NT, (NT == 128 && IPT == 16) ? 6 : 1) split_pa
         lbits |= (uint32_t)(wk >= 0.0f && !(wk > cp.H1)) << k;
         gbits |= (uint32_t)(wk >= cp.Hh && !(wk > cp.H1)) << k;
     }
-    uint64_t lsum = 0;
+    // large lights' true deficits (weights gathered again from L1), kept in their slots for
+    // the dithering
     for (uint32_t bits = gbits; bits; bits &= bits - 1) {
         const int k = __ffs(bits) - 1;
         const uint64_t q = rare_q(__ldg(w + item0 + k), false, cp);
@@ -1201,30 +1314,22 @@ __global__ void __launch_bounds__(NT, (NT == 128 && IPT == 16) ? 6 : 1) split_pa
     dth.c0 = st0.c0;
     dth.c0h = st0.c0 >> 24;
     const uint64_t D0 = dither_at(dth, ex.b);
-    {
-        // a large light's slot now holds the dithering after it
-        uint64_t lr = ex.b;
-        for (uint32_t bits = gbits; bits; bits &= bits - 1) {
-            const int slot = tid * IPT + __ffs(bits) - 1;
-            lr += sSlotQ[slot];
-            sSlotQ[slot] = dither_at(dth, lr);
-        }
-    }
-    {
-        uint64_t sr = ex.a, D = D0;
+    if (!walk) {
+        uint64_t sr = ex.a, D = D0, lr = ex.b;
         uint32_t li = l0;
 #pragma unroll
         for (int k = 0; k < IPT; ++k) {
             const bool light = (lbits >> k) & 1u;
-            if (light) sLkey[li] = sr + D;
+            if (light) sLkey[lkey_slot(li)] = sr + D;
             li += light ? 1u : 0u;
             if (LEFT) {
                 sr += light ? ls[tid * IPT + k].lo : 0ull;
                 continue;
             }
             sr += (light && !((gbits >> k) & 1u)) ? small_deficit(pk[k]) : 0ull;
-            if ((gbits >> k) & 1u) {
-                const uint64_t D1 = sSlotQ[tid * IPT + k];
+            if ((gbits >> k) & 1u) {  // the dithering after a large light
+                lr += sSlotQ[tid * IPT + k];
+                const uint64_t D1 = dither_at(dth, lr);
                 pk[k] = dithered_prob(D1 - D);
                 D = D1;
             }
@@ -1241,14 +1346,56 @@ __global__ void __launch_bounds__(NT, (NT == 128 && IPT == 16) ? 6 : 1) split_pa
         // no heavy item anywhere: every row keeps itself
 #pragma unroll
         for (int k = 0; k < IPT; ++k) al[k] = LEFT ? (((lbits >> k) & 1u) ? ls[tid * IPT + k].item : 0u) : item0 + k;
+    } else if (walk) {
+        // ---- (1)+(2) as one merge of this thread's lights with the heavies of its key range
+        const uint32_t last_heavy = __ldg(heavy_item + nH - 1);
+        uint32_t a = 0;
+        {
+            const uint64_t b_t = ex.a + D0;  // this thread's first light's key
+            uint32_t hi = m_w;
+            while (a < hi) {
+                const uint32_t mid = (a + hi) >> 1;
+                if (sWk[mid] < b_t) a = mid + 1; else hi = mid;
+            }
+        }
+        s_wa[tid] = a;
+        __syncthreads();  // every range known; from here a thread touches only its own keys
+        const uint32_t a_end = (tid + 1 < NT) ? s_wa[tid + 1] : m_w;
+        uint64_t hk = a < a_end ? sWk[a] : ~0ull;
+        uint64_t sr = ex.a, D = D0, lr = ex.b;
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+            const bool light = (lbits >> k) & 1u;
+            if (light) {
+                const uint64_t key = sr + D;
+                while (hk <= key) {  // heavy a ranks at this light
+                    sWk[a] = key;
+                    ++a;
+                    hk = a < a_end ? sWk[a] : ~0ull;
+                }
+                al[k] = a < m_w ? sWi[a] : last_heavy;
+            }
+            if (LEFT) {
+                sr += light ? ls[tid * IPT + k].lo : 0ull;
+                continue;
+            }
+            sr += (light && !((gbits >> k) & 1u)) ? small_deficit(pk[k]) : 0ull;
+            if ((gbits >> k) & 1u) {  // the dithering after a large light
+                lr += sSlotQ[tid * IPT + k];
+                const uint64_t D1 = dither_at(dth, lr);
+                pk[k] = dithered_prob(D1 - D);
+                D = D1;
+            }
+        }
+        // the heavies left rank at the next thread's first light (or past the tile's lights)
+        const uint64_t nxt = (l0 + nl < nLt) ? sr + D : ~0ull;
+        for (; a < a_end; ++a) sWk[a] = nxt;
     } else {
         // ---- (2) owned heavies and the next one, chunk by chunk
         const uint32_t last_heavy = __ldg(heavy_item + nH - 1);
 #pragma unroll
         for (int k = 0; k < IPT; ++k) al[k] = last_heavy;  // lights past every heavy's excess
                                                             // (rounding residue only)
-        const uint32_t g_lo = st0.bound, g_hi = st1.bound;
-        const uint32_t g_end = min(g_hi + 1u, nH);
         for (uint32_t cs = g_lo; cs < g_end; cs += (uint32_t)C) {
             const uint32_t m = min((uint32_t)C, g_end - cs);
             // state left by the previous chunk (rewritten below only after the next barrier)
@@ -1256,15 +1403,7 @@ __global__ void __launch_bounds__(NT, (NT == 128 && IPT == 16) ? 6 : 1) split_pa
             const uint32_t pend = s_pend_item;
             const float pend_prob = s_pend_prob;
             for (uint32_t j = tid; j < m; j += NT) {
-                const u128 Et = load_u128(heavy_E + cs + j);
-                uint64_t key;
-                if (Et <= A_before) {
-                    key = 0;
-                } else {
-                    const u128 d = Et - A_before + 0xffff;
-                    key = (q_hi(d) >> 16) ? ~0ull : (uint64_t)(d >> 16);
-                }
-                sHkey[j] = key;
+                sHkey[j] = pack_heavy_key(load_u128(heavy_E + cs + j), A_before);
                 sHitem[j] = __ldg(heavy_item + cs + j);
             }
             __syncthreads();
@@ -1282,7 +1421,7 @@ __global__ void __launch_bounds__(NT, (NT == 128 && IPT == 16) ? 6 : 1) split_pa
                 uint32_t lo = r0, hi = nLt;
                 while (lo < hi) {
                     const uint32_t mid = (lo + hi) >> 1;
-                    if (sLkey[mid] < kh) lo = mid + 1; else hi = mid;
+                    if (sLkey[lkey_slot(mid)] < kh) lo = mid + 1; else hi = mid;
                 }
                 sHrank[j] = lo;
             }
@@ -1323,7 +1462,7 @@ __global__ void __launch_bounds__(NT, (NT == 128 && IPT == 16) ? 6 : 1) split_pa
                 }
                 if (g < g_hi) {
                     const u128 Et = load_u128(heavy_E + g);
-                    const u128 A_next = (rk < nLt) ? A_before + ((u128)sLkey[rk] << 16) : A_after;
+                    const u128 A_next = (rk < nLt) ? A_before + ((u128)sLkey[lkey_slot(rk)] << 16) : A_after;
                     const float prob = heavy_row_prob(q_one() + Et - A_next);
                     if (j + 1 < m) {
                         wrs_alias_row r;
@@ -1345,8 +1484,24 @@ __global__ void __launch_bounds__(NT, (NT == 128 && IPT == 16) ? 6 : 1) split_pa
         }
     }
 
+    // rows of the owned heavies of the walk form, once every key left is in place
+    auto walk_heavy_rows = [&]() {
+        const uint32_t m_own = g_hi - g_lo;
+        for (uint32_t j = tid; j < m_own; j += NT) {
+            const uint64_t nk = sWk[j];
+            const u128 A_next = nk == ~0ull ? A_after : A_before + ((u128)nk << 16);
+            wrs_alias_row r;
+            r.prob = heavy_row_prob(q_one() + load_u128(heavy_E + g_lo + j) - A_next);
+            r.alias = (g_lo + j + 1 < nH) ? sWi[j + 1] : sWi[j];  // the last heavy keeps itself
+            table[sWi[j]] = r;
+        }
+    };
     // ---- (3) light rows: staged, then coalesced stores (heavy positions are skipped)
     if constexpr (LEFT) {
+        if (walk) {
+            __syncthreads();
+            walk_heavy_rows();
+        }
 #pragma unroll
         for (int k = 0; k < IPT; ++k) {
             if (!((lbits >> k) & 1u)) continue;
@@ -1363,6 +1518,7 @@ __global__ void __launch_bounds__(NT, (NT == 128 && IPT == 16) ? 6 : 1) split_pa
             sStage[stage_pos<IPT>((uint32_t)(tid * IPT + k))] = row;
         }
         __syncthreads();
+        if (walk) walk_heavy_rows();
         uint64_t* out = reinterpret_cast<uint64_t*>(table) + (uint64_t)tile * T;
         const uint32_t cnt = (uint32_t)min((uint64_t)T, n - (uint64_t)tile * T);
         if (cnt == (uint32_t)T) {

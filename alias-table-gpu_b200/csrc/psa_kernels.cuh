@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(NT) psa_local_kernel(const float* __restrict__
 #pragma unroll
         for (int k = 0; k < IPT; ++k) {
             const bool light = (lbits >> k) & 1u;
-            if (light) sLkey[li] = sr + D;
+            if (light) sLkey[lkey_slot(li)] = sr + D;
             li += light ? 1u : 0u;
             sr += (light && !((gbits >> k) & 1u)) ? small_deficit(pk[k]) : 0ull;
             if ((gbits >> k) & 1u) {
@@ -153,7 +153,7 @@ __global__ void __launch_bounds__(NT) psa_local_kernel(const float* __restrict__
         uint32_t lo = 0, hi = nLt;
         while (lo < hi) {
             const uint32_t mid = (lo + hi) >> 1;
-            if (sLkey[mid] < kEt) lo = mid + 1; else hi = mid;
+            if (sLkey[lkey_slot(mid)] < kEt) lo = mid + 1; else hi = mid;
         }
         L0 = lo;
     }
@@ -176,9 +176,9 @@ __global__ void __launch_bounds__(NT) psa_local_kernel(const float* __restrict__
             const uint64_t kh = sHkey[j];
             while (lo < hi) {
                 const uint32_t mid = (lo + hi) >> 1;
-                if (sLkey[mid] < kh) lo = mid + 1; else hi = mid;
+                if (sLkey[lkey_slot(mid)] < kh) lo = mid + 1; else hi = mid;
             }
-            const u128 A_next = (lo < nLt) ? ((u128)sLkey[lo] << 16) : D128;
+            const u128 A_next = (lo < nLt) ? ((u128)sLkey[lkey_slot(lo)] << 16) : D128;
             const float prob = heavy_row_prob(q_one() + El - A_next);
             if (j + 1 < nHt) {
                 wrs_alias_row r;
@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(NT) psa_local_kernel(const float* __restrict__
         for (int k = 0; k < IPT; ++k) {
             uint64_t row = ~0ull;
             if ((lbits >> k) & 1u) {
-                const uint64_t kl = sLkey[li];
+                const uint64_t kl = sLkey[lkey_slot(li)];
                 if (li < L0) {
                     if (!found) {  // the first heavy whose key exceeds the light's
                         uint32_t lo = 0, hi = nHt;
@@ -228,7 +228,7 @@ __global__ void __launch_bounds__(NT) psa_local_kernel(const float* __restrict__
                     while (sHkey[j] <= kl) ++j;  // a heavy with a larger key exists (li < L0)
                     row = ((uint64_t)sHitem[j] << 32) | __float_as_uint(pk[k]);
                 } else {
-                    const uint64_t kn = (li + 1 < nLt) ? sLkey[li + 1] : D48;
+                    const uint64_t kn = (li + 1 < nLt) ? sLkey[lkey_slot(li + 1)] : D48;
                     LeftSlot sl;
                     sl.item = item0 + k;
                     sl.prob_bits = __float_as_uint(pk[k]);
@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(NT) psa_local_kernel(const float* __restrict__
         if (row != ~0ull) out[i] = row;
     }
     if (tid == 0) {
-        const uint64_t kL0 = (L0 < nLt) ? sLkey[L0] : D48;
+        const uint64_t kL0 = (L0 < nLt) ? sLkey[lkey_slot(L0)] : D48;
         TileVals a;
         a.nL = (conv ? 1u : 0u) + (nLt - L0);
         a.nH = nHt - Js;
