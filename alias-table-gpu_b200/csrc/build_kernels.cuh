@@ -935,10 +935,10 @@ __device__ __forceinline__ u128 load_u128(const uint4* p) {
 // Tiles (warps) per CTA of the heavy-list pass.
 __host__ __device__ constexpr int heavy_warps(int) { return 4; }
 
-// Items per segment of the heavy-list pass: one mask word per lane.
-constexpr int kHeavySeg = 1024;
-// Heavies in a mask word from which a lane loads all of the word's weights.
-constexpr int kDenseWord = 6;
+// Items per segment of the heavy-list pass (16 per lane).
+constexpr int kHeavySeg = 512;
+// Heavies in a lane's 16 items from which it loads all of their weights at once.
+constexpr int kDenseLane = 4;
 
 // A warp's staging of one segment's heavies in heavy order: the within-tile inclusive excess
 // prefix (Q40.24) and the item's offset in the segment, at swizzled slots (lkey_slot).
@@ -977,9 +977,10 @@ __global__ void __launch_bounds__(32 * heavy_warps(T)) heavy_list_kernel(const f
                                                                       const uint32_t* __restrict__ hmask,
                                                                       uint32_t num_tiles, uint32_t* heavy_item,
                                                                       uint4* heavy_E, TileMap map) {
-    constexpr int WPT = T / 32;  // mask words per tile
+    constexpr int WPT = T / 32;    // mask words per tile
+    constexpr int WPL = WPT / 32;  // sparse form: lane l owns tile items [l*32*WPL, (l+1)*32*WPL)
+    static_assert(WPL >= 1 && WPL <= 4, "mask words per lane");
     constexpr int NSEG = T / kHeavySeg;
-    static_assert(NSEG >= 1 && NSEG * kHeavySeg == T, "segments per tile");
     constexpr int NWARP = heavy_warps(T);
     __shared__ HeavyStage stage[NWARP];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -997,24 +998,56 @@ __global__ void __launch_bounds__(32 * heavy_warps(T)) heavy_list_kernel(const f
     const int64_t nfix = __ldg(&hdr->nfix);
     const uint32_t g0 = tr.local ? __ldcg(&incl[u - 1].nH) : 0u;
     const u128 Eb = tr.local ? ldcg_E(incl + u - 1) : (u128)0;
+    if (m * 8u <= (uint32_t)T) {
+        // sparse tile: each lane walks its own items twice around the warp's prefixes and
+        // writes its heavies directly
+        uint32_t wd[WPL];
+#pragma unroll
+        for (int i = 0; i < WPL; ++i) wd[i] = __ldg(hmask + (uint64_t)u * WPT + lane * WPL + i);
+        const uint32_t ibase = tr.local * (uint32_t)T + (uint32_t)lane * WPL * 32u;
+        uint32_t c = 0;
+        uint64_t hs = 0;
+#pragma unroll
+        for (int i = 0; i < WPL; ++i) {
+            c += (uint32_t)__popc(wd[i]);
+            for (uint32_t b = wd[i]; b; b &= b - 1) hs += rare_q(__ldg(wt + ibase + i * 32 + __ffs(b) - 1), true, cp);
+        }
+        uint32_t ctot;
+        uint32_t j = g0 + warp_excl_scan_u32(c, ctot);
+        uint64_t htot;
+        uint64_t er = warp_excl_scan_u64(hs, htot);
+#pragma unroll
+        for (int i = 0; i < WPL; ++i) {
+            for (uint32_t b = wd[i]; b; b &= b - 1) {
+                const uint32_t item = ibase + i * 32 + (uint32_t)(__ffs(b) - 1);
+                er += rare_q(__ldg(wt + item), true, cp);  // the weight again, from L1
+                heavy_item[j] = item;
+                store_u128(heavy_E + j, q_scale_excess(Eb + ((u128)er << 40), nfix));
+                ++j;
+            }
+        }
+        return;
+    }
+    // dense tile: segment by segment, staged in heavy order and written with coalesced stores
     HeavyStage& sg = stage[warp];
     uint32_t j0 = g0;  // global heavy index of the segment's first heavy
     uint64_t e0 = 0;   // excess of the tile's heavies before the segment (Q40.24)
 #pragma unroll 1
     for (int s = 0; s < NSEG; ++s) {
-        // lane l: the 32 items of mask word l of the segment; their heavies' count and excess
-        const uint32_t wd = __ldg(hmask + (uint64_t)u * WPT + s * 32 + lane);
+        // lane l: the 16 items [16 l, 16 l + 16) of the segment
+        const uint32_t word = __ldg(hmask + (uint64_t)u * WPT + s * (kHeavySeg / 32) + (lane >> 1));
+        const uint32_t bits = (word >> ((lane & 1) * 16)) & 0xffffu;
         const uint32_t sbase = tr.local * (uint32_t)T + (uint32_t)s * kHeavySeg;
-        const float* wl = wt + sbase + lane * 32;
-        // a dense word loads all of its 32 weights at once (independent loads); a sparse one
-        // gathers its heavies' weights one by one
-        const bool dense = __popc(wd) >= kDenseWord;
-        float xv[32];
+        const float* wl = wt + sbase + lane * 16;
+        // with many heavies a lane loads all 16 weights at once (independent loads); with few
+        // it gathers its heavies' weights one by one
+        const bool dense = __popc(bits) >= kDenseLane;
+        float xv[16];
         uint64_t hs = 0;
         if (dense) {
             if (((uintptr_t)wl & 15u) == 0) {
 #pragma unroll
-                for (int k = 0; k < 8; ++k) {
+                for (int k = 0; k < 4; ++k) {
                     const float4 v = __ldg(reinterpret_cast<const float4*>(wl) + k);
                     xv[4 * k] = v.x;
                     xv[4 * k + 1] = v.y;
@@ -1023,37 +1056,35 @@ __global__ void __launch_bounds__(32 * heavy_warps(T)) heavy_list_kernel(const f
                 }
             } else {
 #pragma unroll
-                for (int k = 0; k < 32; ++k) xv[k] = __ldg(wl + k);
+                for (int k = 0; k < 16; ++k) xv[k] = __ldg(wl + k);
             }
 #pragma unroll
-            for (int k = 0; k < 32; ++k)
-                if ((wd >> k) & 1u) hs += rare_q(xv[k], true, cp);
+            for (int k = 0; k < 16; ++k)
+                if ((bits >> k) & 1u) hs += rare_q(xv[k], true, cp);
         } else {
-            for (uint32_t b = wd; b; b &= b - 1) hs += rare_q(__ldg(wl + __ffs(b) - 1), true, cp);
+            for (uint32_t b = bits; b; b &= b - 1) hs += rare_q(__ldg(wl + __ffs(b) - 1), true, cp);
         }
         uint32_t ctot;
         uint64_t htot;
-        uint32_t pos = warp_excl_scan_u32((uint32_t)__popc(wd), ctot);
+        uint32_t pos = warp_excl_scan_u32((uint32_t)__popc(bits), ctot);
         uint64_t er = e0 + warp_excl_scan_u64(hs, htot);
-        // stage them in heavy order, then write the segment's part of the list with
-        // coalesced stores
         if (dense) {
 #pragma unroll
-            for (int k = 0; k < 32; ++k) {
-                if ((wd >> k) & 1u) {
+            for (int k = 0; k < 16; ++k) {
+                if ((bits >> k) & 1u) {
                     er += rare_q(xv[k], true, cp);
                     const uint32_t slot = lkey_slot(pos++);
                     sg.er[slot] = er;
-                    sg.off[slot] = (uint16_t)(lane * 32 + k);
+                    sg.off[slot] = (uint16_t)(lane * 16 + k);
                 }
             }
         } else {
-            for (uint32_t b = wd; b; b &= b - 1) {
+            for (uint32_t b = bits; b; b &= b - 1) {
                 const uint32_t k = (uint32_t)(__ffs(b) - 1);
                 er += rare_q(__ldg(wl + k), true, cp);  // the weight again, from L1
                 const uint32_t slot = lkey_slot(pos++);
                 sg.er[slot] = er;
-                sg.off[slot] = (uint16_t)(lane * 32 + k);
+                sg.off[slot] = (uint16_t)(lane * 16 + k);
             }
         }
         __syncwarp();
