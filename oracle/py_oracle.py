@@ -42,6 +42,8 @@ def oracle() -> ctypes.CDLL:
             "or_exact_sum_f32": (_D, [_P, _I64]),
             "or_philox4x32_10": (None, [_P, _P, _P]),
             "or_sweep_build": (_I, [_P, _I64, _P, _P, _P]),
+            "or_sweep_build_f32": (_I, [_P, _I64, _P, _P, _P]),
+            "or_check_ref_table_w": (_I, [_P, _I64, _P, _P, _D, _D, _P]),
             "or_split_build": (_I, [_P, _I64, _I64, _P, _P, _P, _I]),
             "or_check_table": (_I, [_P, _I64, _P, _P, _P]),
             "or_check_ref_table": (_I, [_P, _I64, _P, _P, _D, _P]),
@@ -118,6 +120,30 @@ def sweep_build(w64: np.ndarray):
     W = ctypes.c_double()
     oracle().or_sweep_build(_p(w64), n, _p(wt), _p(al), ctypes.byref(W))
     return wt, al, W.value
+
+
+def sweep_build_f32(w: np.ndarray):
+    """The sweep with every quantity in FP32; returns (row weights, aliases, W_N of the build)."""
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    n = w.size
+    wt = np.zeros(n, dtype=np.float64)
+    al = np.zeros(n, dtype=np.int32)
+    W = ctypes.c_double()
+    oracle().or_sweep_build_f32(_p(w), n, _p(wt), _p(al), ctypes.byref(W))
+    W_N = float(np.float32(W.value) / np.float32(n))
+    return wt, al, W_N
+
+
+def check_ref_table_w(w: np.ndarray, weight: np.ndarray, alias: np.ndarray, W_N_table: float,
+                      W_exact: float) -> dict:
+    """A reference-format table on its own scale W_N_table against n w_i / W_exact."""
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    weight = np.ascontiguousarray(weight, dtype=np.float64)
+    alias = np.ascontiguousarray(alias, dtype=np.int32)
+    st = np.zeros(5, dtype=np.float64)
+    oracle().or_check_ref_table_w(_p(w), w.size, _p(weight), _p(alias), W_N_table, W_exact, _p(st))
+    return {"max_rel": st[0], "p9999_rel": st[1], "worst": int(st[2]), "zero_mass": int(st[3]),
+            "bad_rows": int(st[4])}
 
 
 def split_build(w64: np.ndarray, p: int, threads: int = 1):

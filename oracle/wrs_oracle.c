@@ -158,6 +158,54 @@ int or_sweep_build(const double* win, int64_t n64, double* weight, int32_t* alia
     return 0;
 }
 
+/* The same sweep with every quantity in FP32 (the weights, W summed in input order, W/N, the
+ * running residual w and EPSILON): the "all-FP32" build of the precision comparison. Rows are
+ * returned as doubles on the scale W_f32 / N. */
+int or_sweep_build_f32(const float* win, int64_t n64, double* weight, int32_t* alias, double* W_out) {
+    const int N = (int)n64;
+    float* weights = (float*)malloc((size_t)(N + 2) * sizeof(float));
+    memcpy(weights, win, (size_t)N * sizeof(float));
+    volatile float Wv = 0.0f;  /* no reassociation or wider accumulation */
+    for (int i = 0; i < N; i++) Wv = Wv + weights[i];
+    const float W = Wv;
+    const float WN = W / (float)N;
+    const float eps = (float)EPSILON_REF;
+    weights[N] = INFINITY;
+    weights[N + 1] = 0.0f;
+    for (int i = 0; i < N; ++i) {
+        weight[i] = NAN;
+        alias[i] = -1;
+    }
+    int i = 0;
+    while (weights[i] > WN) i++;
+    int j = 0;
+    while (weights[j] <= WN) j++;
+    volatile float w = weights[j];
+    for (int64_t guard = 0; guard < 4 * (int64_t)N + 16; ++guard) {
+        int exhausted = w <= WN + eps;
+        if (exhausted && j >= N) exhausted = 0;
+        else if (!exhausted && i >= N) exhausted = 1;
+        if (exhausted) {
+            if (j >= N) break;
+            weight[j] = (double)w;
+            int j_ = j;
+            do { j_++; } while (j < N + 2 && weights[j_] <= WN);
+            alias[j] = j_;
+            w = w + (weights[j_] - WN);
+            j = j_;
+        } else {
+            if (i >= N) break;
+            weight[i] = (double)weights[i];
+            alias[i] = j;
+            w = w + (weights[i] - WN);
+            do { i++; } while (i < N + 2 && weights[i] > WN);
+        }
+    }
+    if (W_out) *W_out = (double)W;
+    free(weights);
+    return 0;
+}
+
 typedef struct {
     int i;
     int j;
@@ -341,12 +389,11 @@ static double quantile_sorted_copy(double* v, int64_t m, double q) {
 /* Per-item check: got_i = sum over rows r of [r == i] p_r + [alias_r == i] (1 - p_r), in
  * long double; expected_i = n w_i / W with W the exact sum (AliasTable::verifyTableCorrectness,
  * construction/aliasTable/AliasTable.cu:24-65, with a relative instead of absolute tolerance). */
-static int check_common(const float* w32, const double* w64, int64_t n, const float* probs_or_null,
-                        const uint32_t* rows, const double* ref_weight, const int32_t* ref_alias, double W,
-                        double* stats) {
+static int check_common_w(const float* w32, const double* w64, int64_t n, const float* probs_or_null,
+                          const uint32_t* rows, const double* ref_weight, const int32_t* ref_alias, double W_N,
+                          double W_expect, double* stats) {
     long double* got = (long double*)calloc((size_t)n, sizeof(long double));
     int64_t bad_rows = 0;
-    const double W_N = W / (double)n;
     for (int64_t r = 0; r < n; ++r) {
         long double p;
         int64_t a;
@@ -372,7 +419,7 @@ static int check_common(const float* w32, const double* w64, int64_t n, const fl
     double maxrel = 0.0;
     for (int64_t i = 0; i < n; ++i) {
         long double wi = w32 ? (long double)w32[i] : (long double)w64[i];
-        long double expct = (long double)n * wi / (long double)W;
+        long double expct = (long double)n * wi / (long double)W_expect;
         if (wi == 0.0L) {
             if (got[i] != 0.0L) ++zero_bad;
             continue;
@@ -394,6 +441,19 @@ static int check_common(const float* w32, const double* w64, int64_t n, const fl
     free(rel);
     free(got);
     return 0;
+}
+
+static int check_common(const float* w32, const double* w64, int64_t n, const float* probs_or_null,
+                        const uint32_t* rows, const double* ref_weight, const int32_t* ref_alias, double W,
+                        double* stats) {
+    return check_common_w(w32, w64, n, probs_or_null, rows, ref_weight, ref_alias, W / (double)n, W, stats);
+}
+
+/* A reference-format table whose rows hold weights on its own scale W_N_table (the average
+ * weight its build used), checked against n w_i / W_exact. */
+int or_check_ref_table_w(const float* w, int64_t n, const double* weight, const int32_t* alias, double W_N_table,
+                         double W_exact, double* stats) {
+    return check_common_w(w, NULL, n, NULL, NULL, weight, alias, W_N_table, W_exact, stats);
 }
 
 int or_check_table(const float* w, int64_t n, const uint32_t* rows, double* stats, double* W_used) {

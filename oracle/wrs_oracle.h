@@ -36,6 +36,8 @@ void or_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out
 
 /* reference-format tables: weight (absolute, FP64) + alias (int32) */
 int or_sweep_build(const double* w, int64_t n, double* weight, int32_t* alias, double* W_out);
+/* the same sweep with every quantity in FP32; W_out gets the FP32 total */
+int or_sweep_build_f32(const float* w, int64_t n, double* weight, int32_t* alias, double* W_out);
 int or_split_build(const double* w, int64_t n, int64_t p, double* weight, int32_t* alias, double* W_out,
                    int threads);
 
@@ -47,6 +49,9 @@ int or_check_table(const float* w, int64_t n, const uint32_t* rows, double* stat
 /* same for a reference-format table, prob = weight / (W/N), alias ignored when weight >= W/N */
 int or_check_ref_table(const double* w, int64_t n, const double* weight, const int32_t* alias, double W,
                        double* stats);
+/* a reference-format table on its own scale W_N_table, against n w_i / W_exact */
+int or_check_ref_table_w(const float* w, int64_t n, const double* weight, const int32_t* alias, double W_N_table,
+                         double W_exact, double* stats);
 
 /* the library's exact merge build, sequentially; W = the weight total the build uses */
 int or_exact_build(const float* w, int64_t n, double W, uint32_t* rows);
