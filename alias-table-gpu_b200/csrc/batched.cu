@@ -8,8 +8,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <vector>
 
 #include "batched_kernels.cuh"
+#include "batched_rejection_kernels.cuh"
 #include "host_util.h"
 
 namespace wrs {
@@ -41,17 +43,19 @@ bool shape_of(const wrs_build_opts* opts, Shape* sh) {
     return valid_small(sh->small_max) && valid_tile(sh->tile);
 }
 
-// The host's view of the batch for one shape (from h_offsets).
+// The host's view of the batch for one shape (from h_offsets and h_kinds).
 struct HostPlan {
-    uint32_t small_tables;  // tables with 1 <= n <= small_max
-    uint32_t big_tables;    // tables with n > small_max
+    uint32_t small_tables;  // alias tables with 1 <= n <= small_max
+    uint32_t big_tables;    // alias tables with n > small_max
     uint32_t tiles;         // tiles of the big tables
     uint64_t big_items;
+    uint64_t rej_warp_tables;   // rejection tables with 1 <= n <= kRejWarpMax
+    uint64_t rej_block_tables;  // larger rejection tables
     bool valid;
 };
 
-HostPlan host_plan(const int64_t* h_offsets, int64_t num_tables, const Shape& sh) {
-    HostPlan p{0, 0, 0, 0, true};
+HostPlan host_plan(const int64_t* h_offsets, int64_t num_tables, const Shape& sh, const uint8_t* h_kinds = nullptr) {
+    HostPlan p{0, 0, 0, 0, 0, 0, true};
     if (!h_offsets || num_tables < 1 || h_offsets[0] != 0) {
         p.valid = false;
         return p;
@@ -64,6 +68,12 @@ HostPlan host_plan(const int64_t* h_offsets, int64_t num_tables, const Shape& sh
             return p;
         }
         if (n == 0) continue;
+        const uint8_t kind = h_kinds ? h_kinds[t] : (uint8_t)WRS_TABLE_ALIAS;
+        if (kind == WRS_TABLE_REJECTION) {
+            if (n <= (int64_t)kRejWarpMax) ++p.rej_warp_tables; else ++p.rej_block_tables;
+            continue;
+        }
+        if (kind != WRS_TABLE_ALIAS) continue;
         if (n <= (int64_t)sh.small_max) {
             ++small;
         } else {
@@ -119,8 +129,9 @@ BatchLayout carve_batch(void* scratch, int64_t num_tables, const HostPlan& p, ui
 }
 
 template <int SPL>
-wrs_status launch_small(const float* d_w, const int64_t* d_offsets, int64_t num_tables, wrs_alias_row* d_table,
-                        double* d_W, uint32_t* status, uint32_t small_tables, cudaStream_t stream) {
+wrs_status launch_small(const float* d_w, const int64_t* d_offsets, const uint8_t* d_kinds, int64_t num_tables,
+                        wrs_alias_row* d_table, double* d_W, uint32_t* status, uint32_t small_tables,
+                        cudaStream_t stream) {
     const size_t smem = sizeof(SmallSmem<SPL>) * kSmallWarps;
     cudaError_t e = cudaFuncSetAttribute(small_tables_kernel<SPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
@@ -133,22 +144,22 @@ wrs_status launch_small(const float* d_w, const int64_t* d_offsets, int64_t num_
     const uint64_t want = ((uint64_t)small_tables + kSmallWarps - 1) / kSmallWarps;
     const uint64_t cap = (uint64_t)d.sm_count * per_sm;
     const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min(want, cap));
-    small_tables_kernel<SPL><<<grid, 32 * kSmallWarps, smem, stream>>>(d_w, d_offsets, num_tables, 32u * SPL,
-                                                                        d_table, d_W, status);
+    small_tables_kernel<SPL><<<grid, 32 * kSmallWarps, smem, stream>>>(d_w, d_offsets, d_kinds, num_tables,
+                                                                        32u * SPL, d_table, d_W, status);
     return launch_status();
 }
 
 template <int T>
-wrs_status launch_big(const float* d_w, const int64_t* d_offsets, int64_t num_tables, uint32_t small_max,
-                      wrs_alias_row* d_table, double* d_W, const BatchLayout& L, const HostPlan& p,
-                      cudaStream_t stream) {
+wrs_status launch_big(const float* d_w, const int64_t* d_offsets, const uint8_t* d_kinds, int64_t num_tables,
+                      uint32_t small_max, wrs_alias_row* d_table, double* d_W, const BatchLayout& L,
+                      const HostPlan& p, cudaStream_t stream) {
     constexpr int NT = PackShape<T>::NT, IPT = PackShape<T>::IPT;
     const uint32_t nblk = (uint32_t)((num_tables + kPlanBlock - 1) / kPlanBlock);
     const PlanCounts cap{p.big_tables, p.tiles, p.big_items};
-    plan_count_kernel<<<nblk, kPlanBlock, 0, stream>>>(d_offsets, num_tables, small_max, T, L.blk);
+    plan_count_kernel<<<nblk, kPlanBlock, 0, stream>>>(d_offsets, d_kinds, num_tables, small_max, T, L.blk);
     plan_scan_kernel<<<1, kPlanBlock, 0, stream>>>(L.blk, nblk, cap, L.plan_status);
-    plan_fill_kernel<<<nblk, kPlanBlock, 0, stream>>>(d_offsets, num_tables, small_max, T, L.blk, cap, L.desc,
-                                                      L.tile_table);
+    plan_fill_kernel<<<nblk, kPlanBlock, 0, stream>>>(d_offsets, d_kinds, num_tables, small_max, T, L.blk, cap,
+                                                      L.desc, L.tile_table);
     const TileMap map{L.tile_table, L.desc, L.plan_status, 0, 0};
     const uint32_t nt = p.tiles;
     batch_wsum_kernel<T><<<nt, kBatchWsumThreads, 0, stream>>>(d_w, L.hdrs, L.partials, map, d_W);
@@ -169,10 +180,37 @@ wrs_status launch_big(const float* d_w, const int64_t* d_offsets, int64_t num_ta
     return launch_status();
 }
 
+// Rejection structures of the batch's rejection tables (errors into the batch status word).
+struct RejOut {
+    uint32_t* A;
+    float* frac;
+    uint64_t* a_size;
+};
+
+wrs_status launch_rejection(const float* d_w, const int64_t* d_offsets, const uint8_t* d_kinds, int64_t num_tables,
+                            const HostPlan& p, const RejOut& r, double* d_W, uint32_t* status, cudaStream_t stream) {
+    const DeviceInfo d = device_info();
+    if (p.rej_warp_tables > 0) {
+        const uint64_t want = (p.rej_warp_tables + kRejWarps - 1) / kRejWarps;
+        const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)d.sm_count * 8));
+        rej_warp_tables_kernel<<<grid, 32 * kRejWarps, 0, stream>>>(d_w, d_offsets, d_kinds, num_tables, r.A, r.frac,
+                                                                   r.a_size, d_W, status);
+    }
+    if (p.rej_block_tables > 0) {
+        const uint32_t grid =
+            (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(p.rej_block_tables, (uint64_t)d.sm_count * 2));
+        rej_block_tables_kernel<<<grid, kRejBlockThreads, 0, stream>>>(d_w, d_offsets, d_kinds, num_tables,
+                                                                      kRejWarpMax, r.A, r.frac, r.a_size, d_W,
+                                                                      status);
+    }
+    return launch_status();
+}
+
 wrs_status batched_build(const float* d_w, const int64_t* d_offsets, const int64_t* h_offsets, int64_t num_tables,
                          const Shape& sh, wrs_alias_row* d_table, double* d_W, void* d_scratch, size_t scratch_bytes,
-                         cudaStream_t stream, BatchLayout* out_layout) {
-    const HostPlan p = host_plan(h_offsets, num_tables, sh);
+                         cudaStream_t stream, BatchLayout* out_layout, const uint8_t* d_kinds = nullptr,
+                         const uint8_t* h_kinds = nullptr, const RejOut* rej = nullptr) {
+    const HostPlan p = host_plan(h_offsets, num_tables, sh, h_kinds);
     if (!p.valid) return WRS_ERR_INVALID_ARGUMENT;
     const BatchLayout L = carve_batch(d_scratch, num_tables, p, sh.tile);
     if (scratch_bytes < L.bytes) return WRS_ERR_SCRATCH_TOO_SMALL;
@@ -183,21 +221,24 @@ wrs_status batched_build(const float* d_w, const int64_t* d_offsets, const int64
     if (p.small_tables > 0) {
         uint32_t* status = &L.hdr0->status;
         switch (sh.small_max) {
-            case 32: st = launch_small<1>(d_w, d_offsets, num_tables, d_table, d_W, status, p.small_tables, stream); break;
-            case 64: st = launch_small<2>(d_w, d_offsets, num_tables, d_table, d_W, status, p.small_tables, stream); break;
-            case 128: st = launch_small<4>(d_w, d_offsets, num_tables, d_table, d_W, status, p.small_tables, stream); break;
-            case 256: st = launch_small<8>(d_w, d_offsets, num_tables, d_table, d_W, status, p.small_tables, stream); break;
-            default: st = launch_small<16>(d_w, d_offsets, num_tables, d_table, d_W, status, p.small_tables, stream); break;
+            case 32: st = launch_small<1>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p.small_tables, stream); break;
+            case 64: st = launch_small<2>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p.small_tables, stream); break;
+            case 128: st = launch_small<4>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p.small_tables, stream); break;
+            case 256: st = launch_small<8>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p.small_tables, stream); break;
+            default: st = launch_small<16>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p.small_tables, stream); break;
         }
         if (st != WRS_SUCCESS) return st;
     }
     if (p.big_tables > 0) {
         switch (sh.tile) {
-            case 1024: st = launch_big<1024>(d_w, d_offsets, num_tables, sh.small_max, d_table, d_W, L, p, stream); break;
-            case 4096: st = launch_big<4096>(d_w, d_offsets, num_tables, sh.small_max, d_table, d_W, L, p, stream); break;
-            default: st = launch_big<2048>(d_w, d_offsets, num_tables, sh.small_max, d_table, d_W, L, p, stream); break;
+            case 1024: st = launch_big<1024>(d_w, d_offsets, d_kinds, num_tables, sh.small_max, d_table, d_W, L, p, stream); break;
+            case 4096: st = launch_big<4096>(d_w, d_offsets, d_kinds, num_tables, sh.small_max, d_table, d_W, L, p, stream); break;
+            default: st = launch_big<2048>(d_w, d_offsets, d_kinds, num_tables, sh.small_max, d_table, d_W, L, p, stream); break;
         }
+        if (st != WRS_SUCCESS) return st;
     }
+    if (rej && (p.rej_warp_tables > 0 || p.rej_block_tables > 0))
+        st = launch_rejection(d_w, d_offsets, d_kinds, num_tables, p, *rej, d_W, &L.hdr0->status, stream);
     return st;
 }
 
@@ -251,7 +292,8 @@ extern "C" wrs_status wrs_batched_sample(const wrs_alias_row* d_table, const int
     const uint64_t grid = (total_samples + per_cta - 1) / per_cta;
     if (grid > 0x7fffffffull) return WRS_ERR_INVALID_ARGUMENT;
     batch_sample_kernel<<<(uint32_t)grid, kBatchSampleThreads, 0, stream>>>(
-        d_table, d_offsets, num_tables, d_sample_offsets, total_samples, seed, counter_base, d_out, nullptr);
+        d_table, d_offsets, num_tables, d_sample_offsets, total_samples, seed, counter_base, d_out, nullptr, nullptr,
+        nullptr, nullptr, nullptr, 0u);
     return launch_status();
 }
 
@@ -303,5 +345,175 @@ extern "C" wrs_status wrs_batched_autotune(const float* d_w, const int64_t* d_of
     if (result != WRS_SUCCESS) return result;
     opts->small_table_items = best.small_max;
     opts->tile_items = best.tile;
+    return WRS_SUCCESS;
+}
+
+// ---------------------------------------------------------------- mixed batches
+namespace wrs {
+namespace {
+
+size_t mixed_scratch_bytes(const int64_t* h_offsets, const uint8_t* h_kinds, int64_t num_tables,
+                           const wrs_build_opts* opts) {
+    if (opts) {
+        Shape sh;
+        if (!shape_of(opts, &sh)) return 0;
+        const HostPlan p = host_plan(h_offsets, num_tables, sh, h_kinds);
+        return p.valid ? carve_batch(nullptr, num_tables, p, sh.tile).bytes : 0;
+    }
+    size_t best = 0;
+    for (uint32_t s : kSmallChoices)
+        for (uint32_t t : kTileChoices) {
+            const Shape sh{s, t};
+            const HostPlan p = host_plan(h_offsets, num_tables, sh, h_kinds);
+            if (!p.valid) return 0;
+            best = std::max(best, carve_batch(nullptr, num_tables, p, t).bytes);
+        }
+    return best;
+}
+
+wrs_status launch_mixed_sample(const wrs_alias_row* d_table, const uint32_t* d_A, const float* d_frac,
+                               const uint64_t* d_a_size, const int64_t* d_offsets, const uint8_t* d_kinds,
+                               int64_t num_tables, const int64_t* d_sample_offsets, uint64_t total_samples,
+                               uint64_t seed, uint64_t counter_base, uint32_t max_tries, uint32_t* d_out,
+                               uint32_t* d_status, cudaStream_t stream) {
+    if (total_samples == 0) return WRS_SUCCESS;
+    const uint64_t per_cta = (uint64_t)kBatchSampleThreads * kBatchSamplePer;
+    const uint64_t grid = (total_samples + per_cta - 1) / per_cta;
+    if (grid > 0x7fffffffull) return WRS_ERR_INVALID_ARGUMENT;
+    batch_sample_kernel<<<(uint32_t)grid, kBatchSampleThreads, 0, stream>>>(
+        d_table, d_offsets, num_tables, d_sample_offsets, total_samples, seed, counter_base, d_out, d_status, d_kinds,
+        d_A, d_frac, d_a_size, max_tries ? max_tries : 64u);
+    return launch_status();
+}
+
+// Size class of a table of n >= 1 items: ceil(log2 n).
+int size_class(int64_t n) { return n <= 1 ? 0 : 64 - __builtin_clzll((unsigned long long)(n - 1)); }
+
+}  // namespace
+}  // namespace wrs
+
+extern "C" size_t wrs_batched_mixed_build_scratch_bytes(const int64_t* h_offsets, const uint8_t* h_kinds,
+                                                        int64_t num_tables, const wrs_build_opts* opts) {
+    return mixed_scratch_bytes(h_offsets, h_kinds, num_tables, opts);
+}
+
+extern "C" wrs_status wrs_batched_mixed_build_f32(const float* d_w, const int64_t* d_offsets,
+                                                  const int64_t* h_offsets, const uint8_t* d_kinds,
+                                                  const uint8_t* h_kinds, int64_t num_tables,
+                                                  const wrs_build_opts* opts, wrs_alias_row* d_table, uint32_t* d_A,
+                                                  float* d_frac, uint64_t* d_a_size, double* d_W, void* d_scratch,
+                                                  size_t scratch_bytes, void* stream_) {
+    if (!d_w || !d_offsets || !h_offsets || !d_scratch || num_tables < 1) return WRS_ERR_INVALID_ARGUMENT;
+    if ((d_kinds == nullptr) != (h_kinds == nullptr)) return WRS_ERR_INVALID_ARGUMENT;
+    Shape sh;
+    if (!shape_of(opts, &sh)) return WRS_ERR_INVALID_ARGUMENT;
+    if (opts && opts->method != WRS_METHOD_SPLIT) return WRS_ERR_UNSUPPORTED;
+    const HostPlan p = host_plan(h_offsets, num_tables, sh, h_kinds);
+    if (!p.valid) return WRS_ERR_INVALID_ARGUMENT;
+    if ((p.small_tables > 0 || p.big_tables > 0) && !d_table) return WRS_ERR_INVALID_ARGUMENT;
+    if ((p.rej_warp_tables > 0 || p.rej_block_tables > 0) && (!d_A || !d_frac || !d_a_size))
+        return WRS_ERR_INVALID_ARGUMENT;
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+    const RejOut r{d_A, d_frac, d_a_size};
+    BatchLayout L;
+    const wrs_status st = batched_build(d_w, d_offsets, h_offsets, num_tables, sh, d_table, d_W, d_scratch,
+                                        scratch_bytes, stream, &L, d_kinds, h_kinds, &r);
+    if (st != WRS_SUCCESS) return st;
+    if (opts && (opts->flags & WRS_FLAG_SYNC)) return read_device_status(&L.hdr0->status, stream);
+    return WRS_SUCCESS;
+}
+
+extern "C" wrs_status wrs_batched_mixed_sample(const wrs_alias_row* d_table, const uint32_t* d_A,
+                                               const float* d_frac, const uint64_t* d_a_size,
+                                               const int64_t* d_offsets, const uint8_t* d_kinds, int64_t num_tables,
+                                               const int64_t* d_sample_offsets, uint64_t total_samples, uint64_t seed,
+                                               uint64_t counter_base, uint32_t max_tries, uint32_t* d_out,
+                                               uint32_t* d_status, void* stream_) {
+    if (!d_offsets || !d_sample_offsets || !d_out || num_tables < 1) return WRS_ERR_INVALID_ARGUMENT;
+    if (!d_kinds && !d_table) return WRS_ERR_INVALID_ARGUMENT;
+    if (d_kinds && (!d_A || !d_frac || !d_a_size)) return WRS_ERR_INVALID_ARGUMENT;
+    return launch_mixed_sample(d_table, d_A, d_frac, d_a_size, d_offsets, d_kinds, num_tables, d_sample_offsets,
+                               total_samples, seed, counter_base, max_tries, d_out, d_status,
+                               static_cast<cudaStream_t>(stream_));
+}
+
+extern "C" wrs_status wrs_batched_autotune_kinds(const float* d_w, const int64_t* d_offsets,
+                                                 const int64_t* h_offsets, int64_t num_tables,
+                                                 const int64_t* d_sample_offsets, const int64_t* h_sample_offsets,
+                                                 const wrs_build_opts* opts, wrs_alias_row* d_table, uint32_t* d_A,
+                                                 float* d_frac, uint64_t* d_a_size, uint8_t* d_kinds_tmp,
+                                                 uint32_t* d_out, void* d_scratch, size_t scratch_bytes,
+                                                 uint8_t* h_kinds_out, uint8_t* class_kinds, void* stream_) {
+    if (!d_w || !d_offsets || !h_offsets || !d_sample_offsets || !h_sample_offsets || !d_table || !d_A || !d_frac ||
+        !d_a_size || !d_kinds_tmp || !d_out || !d_scratch || !h_kinds_out || num_tables < 1)
+        return WRS_ERR_INVALID_ARGUMENT;
+    Shape sh;
+    if (!shape_of(opts, &sh)) return WRS_ERR_INVALID_ARGUMENT;
+    if (opts && opts->method != WRS_METHOD_SPLIT) return WRS_ERR_UNSUPPORTED;
+    const HostPlan p_all = host_plan(h_offsets, num_tables, sh, nullptr);
+    if (!p_all.valid) return WRS_ERR_INVALID_ARGUMENT;
+    if (scratch_bytes < mixed_scratch_bytes(h_offsets, nullptr, num_tables, opts)) return WRS_ERR_SCRATCH_TOO_SMALL;
+    const int64_t total_i = h_sample_offsets[num_tables];
+    if (h_sample_offsets[0] != 0 || total_i < 0) return WRS_ERR_INVALID_ARGUMENT;
+    const uint64_t total = (uint64_t)total_i;
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+    constexpr int kClasses = 33;
+    std::vector<int> cls((size_t)num_tables);
+    bool present[kClasses] = {};
+    for (int64_t t = 0; t < num_tables; ++t) {
+        const int64_t n = h_offsets[t + 1] - h_offsets[t];
+        cls[(size_t)t] = n > 0 ? size_class(n) : -1;
+        if (n > 0) present[cls[(size_t)t]] = true;
+    }
+    uint8_t choice[kClasses];
+    for (int c = 0; c < kClasses; ++c) choice[c] = WRS_TABLE_SKIP;
+    std::vector<uint8_t> kinds((size_t)num_tables);
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess) return WRS_ERR_CUDA;
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return WRS_ERR_CUDA;
+    }
+    const RejOut r{d_A, d_frac, d_a_size};
+    wrs_status result = WRS_SUCCESS;
+    for (int c = 0; c < kClasses && result == WRS_SUCCESS; ++c) {
+        if (!present[c]) continue;
+        float ms_of[2] = {1e30f, 1e30f};
+        for (int m = 0; m < 2 && result == WRS_SUCCESS; ++m) {
+            const uint8_t kind = m == 0 ? (uint8_t)WRS_TABLE_ALIAS : (uint8_t)WRS_TABLE_REJECTION;
+            for (int64_t t = 0; t < num_tables; ++t) kinds[(size_t)t] = cls[(size_t)t] == c ? kind : WRS_TABLE_SKIP;
+            if (cudaMemcpyAsync(d_kinds_tmp, kinds.data(), (size_t)num_tables, cudaMemcpyHostToDevice, stream) !=
+                cudaSuccess) {
+                result = WRS_ERR_CUDA;
+                break;
+            }
+            for (int rep = 0; rep < 3; ++rep) {  // the first run warms up
+                BatchLayout L;
+                cudaEventRecord(e0, stream);
+                wrs_status st = batched_build(d_w, d_offsets, h_offsets, num_tables, sh, d_table, nullptr, d_scratch,
+                                              scratch_bytes, stream, &L, d_kinds_tmp, kinds.data(), &r);
+                if (st == WRS_SUCCESS)
+                    st = launch_mixed_sample(d_table, d_A, d_frac, d_a_size, d_offsets, d_kinds_tmp, num_tables,
+                                             d_sample_offsets, total, 0x5A5A5A5Aull, 0, 0, d_out, nullptr, stream);
+                cudaEventRecord(e1, stream);
+                if (st == WRS_SUCCESS) st = read_device_status(&L.hdr0->status, stream);
+                if (st != WRS_SUCCESS) {
+                    result = st;
+                    break;
+                }
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (rep > 0) ms_of[m] = std::min(ms_of[m], ms);
+            }
+        }
+        choice[c] = ms_of[0] <= ms_of[1] ? (uint8_t)WRS_TABLE_ALIAS : (uint8_t)WRS_TABLE_REJECTION;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (result != WRS_SUCCESS) return result;
+    for (int64_t t = 0; t < num_tables; ++t)
+        h_kinds_out[t] = cls[(size_t)t] < 0 ? (uint8_t)WRS_TABLE_SKIP : choice[cls[(size_t)t]];
+    if (class_kinds)
+        for (int c = 0; c < kClasses; ++c) class_kinds[c] = choice[c];
     return WRS_SUCCESS;
 }

@@ -28,6 +28,13 @@ namespace wrs {
 // in the plan status, and the batched passes then do nothing.
 constexpr int kPlanBlock = 1024;
 
+// Per-table method of a mixed batch (kinds[t]; a null kinds array means every table is an
+// alias table). The alias passes build only WRS_TABLE_ALIAS tables, the rejection passes only
+// WRS_TABLE_REJECTION ones; a table of any other kind is skipped by both.
+__device__ __forceinline__ bool kind_is(const uint8_t* kinds, int64_t t, uint8_t k) {
+    return kinds ? __ldg(kinds + t) == k : k == WRS_TABLE_ALIAS;
+}
+
 struct PlanCounts {
     uint32_t tables;
     uint32_t tiles;
@@ -72,11 +79,11 @@ __device__ __forceinline__ PlanCounts pc_block_scan(const PlanCounts v, PlanCoun
     return pc_sub(pc_add(warp ? base : zero, inc), v);
 }
 
-__device__ __forceinline__ PlanCounts plan_of(const int64_t* offsets, int64_t num_tables, int64_t t,
-                                             uint32_t small_max, uint32_t tile_items, int64_t* n_out) {
+__device__ __forceinline__ PlanCounts plan_of(const int64_t* offsets, const uint8_t* kinds, int64_t num_tables,
+                                             int64_t t, uint32_t small_max, uint32_t tile_items, int64_t* n_out) {
     PlanCounts c{0u, 0u, 0ull};
     int64_t n = 0;
-    if (t < num_tables) {
+    if (t < num_tables && kind_is(kinds, t, WRS_TABLE_ALIAS)) {
         n = offsets[t + 1] - offsets[t];
         if (n > (int64_t)small_max) c = PlanCounts{1u, (uint32_t)((n + tile_items - 1) / tile_items), (uint64_t)n};
     }
@@ -85,12 +92,13 @@ __device__ __forceinline__ PlanCounts plan_of(const int64_t* offsets, int64_t nu
 }
 
 __global__ void __launch_bounds__(kPlanBlock) plan_count_kernel(const int64_t* __restrict__ offsets,
-                                                               int64_t num_tables, uint32_t small_max,
+                                                               const uint8_t* kinds, int64_t num_tables,
+                                                               uint32_t small_max,
                                                                uint32_t tile_items, PlanCounts* blk) {
     __shared__ PlanCounts s[32];
     int64_t n;
     const PlanCounts c =
-        plan_of(offsets, num_tables, (int64_t)blockIdx.x * kPlanBlock + threadIdx.x, small_max, tile_items, &n);
+        plan_of(offsets, kinds, num_tables, (int64_t)blockIdx.x * kPlanBlock + threadIdx.x, small_max, tile_items, &n);
     PlanCounts tot;
     pc_block_scan(c, s, &tot);
     if (threadIdx.x == 0) blk[blockIdx.x] = tot;
@@ -115,13 +123,14 @@ __global__ void __launch_bounds__(kPlanBlock) plan_scan_kernel(PlanCounts* blk, 
 }
 
 __global__ void __launch_bounds__(kPlanBlock) plan_fill_kernel(const int64_t* __restrict__ offsets,
-                                                              int64_t num_tables, uint32_t small_max,
+                                                              const uint8_t* kinds, int64_t num_tables,
+                                                              uint32_t small_max,
                                                               uint32_t tile_items, const PlanCounts* blk,
                                                               PlanCounts cap, TableDesc* desc, uint32_t* tile_table) {
     __shared__ PlanCounts s[32];
     const int64_t t = (int64_t)blockIdx.x * kPlanBlock + threadIdx.x;
     int64_t n;
-    const PlanCounts c = plan_of(offsets, num_tables, t, small_max, tile_items, &n);
+    const PlanCounts c = plan_of(offsets, kinds, num_tables, t, small_max, tile_items, &n);
     PlanCounts tot;
     const PlanCounts ex = pc_add(blk[blockIdx.x], pc_block_scan(c, s, &tot));
     if (c.tables == 0) return;
@@ -313,7 +322,8 @@ struct SmallSmem {
 template <int SPL>
 __global__ void __launch_bounds__(32 * kSmallWarps) small_tables_kernel(const float* __restrict__ w,
                                                                        const int64_t* __restrict__ offsets,
-                                                                       int64_t num_tables, uint32_t small_max,
+                                                                       const uint8_t* kinds, int64_t num_tables,
+                                                                       uint32_t small_max,
                                                                        wrs_alias_row* __restrict__ table,
                                                                        double* W_out, uint32_t* status) {
     constexpr int CAP = 32 * SPL;
@@ -324,7 +334,7 @@ __global__ void __launch_bounds__(32 * kSmallWarps) small_tables_kernel(const fl
     for (int64_t t = (int64_t)blockIdx.x * kSmallWarps + warp; t < num_tables; t += nwarps) {
         const int64_t off = offsets[t];
         const int64_t nn = offsets[t + 1] - off;
-        if (nn < 1 || nn > (int64_t)small_max || nn > CAP) continue;
+        if (nn < 1 || nn > (int64_t)small_max || nn > CAP || !kind_is(kinds, t, WRS_TABLE_ALIAS)) continue;
         const uint32_t n = (uint32_t)nn;
         const uint32_t ipl = (n + 31) / 32;
         const float* wt = w + off;
@@ -475,13 +485,18 @@ __global__ void __launch_bounds__(32 * kSmallWarps) small_tables_kernel(const fl
 // coin = (x_second >> 8) * 2^-24, result = coin < prob[row] ? row : alias[row]. Every thread
 // takes kBatchSamplePer consecutive positions: it finds the table of its first one by a
 // binary search of the sample offsets and walks forward from there.
+// In a mixed batch (kinds not null) a rejection table's positions follow the rejection
+// contract instead (rejection_sample_kernel: b = counter_base + s, two tries per Philox
+// block, slot and acceptance from the table's own slot range), and the positions of a
+// skipped table are left as they are.
 constexpr int kBatchSampleThreads = 256;
 constexpr int kBatchSamplePer = 8;
 
 __global__ void __launch_bounds__(kBatchSampleThreads) batch_sample_kernel(
     const wrs_alias_row* __restrict__ table, const int64_t* __restrict__ offsets, int64_t num_tables,
     const int64_t* __restrict__ sample_offsets, uint64_t total, uint64_t seed, uint64_t counter_base,
-    uint32_t* __restrict__ out, uint32_t* status) {
+    uint32_t* __restrict__ out, uint32_t* status, const uint8_t* kinds, const uint32_t* __restrict__ A,
+    const float* __restrict__ frac, const uint64_t* __restrict__ a_size, uint32_t max_tries) {
     const uint64_t s0 = ((uint64_t)blockIdx.x * kBatchSampleThreads + threadIdx.x) * kBatchSamplePer;
     if (s0 >= total) return;
     // the last table whose sample range starts at or before s0
@@ -500,6 +515,35 @@ __global__ void __launch_bounds__(kBatchSampleThreads) batch_sample_kernel(
         while (s >= s_end_t && t + 1 < num_tables) {
             ++t;
             s_end_t = (uint64_t)__ldg(sample_offsets + t + 1);
+        }
+        const uint8_t kind = kinds ? __ldg(kinds + t) : (uint8_t)WRS_TABLE_ALIAS;
+        if (kind != WRS_TABLE_ALIAS && s < s_end_t) {
+            if (kind != WRS_TABLE_REJECTION) continue;  // a skipped table
+            const int64_t off = __ldg(offsets + t);
+            const uint64_t asz = __ldg(a_size + t);
+            if (asz == 0 || asz > 0xffffffffull) {
+                out[s] = 0xffffffffu;
+                if (status) record_status(status, WRS_ERR_INVALID_ARGUMENT);
+                continue;
+            }
+            const uint32_t* At = A + 2 * off;
+            const uint64_t b = counter_base + s;
+            uint32_t res = 0xffffffffu;
+            Philox4 r{};
+            for (uint32_t tr = 0; tr < max_tries; ++tr) {
+                if ((tr & 1u) == 0)
+                    r = philox4x32_10((uint32_t)b, (uint32_t)(b >> 32), tr >> 1, 0x52454a00u, k0, k1);
+                const uint32_t xs = r.x[(tr & 1u) * 2], xc = r.x[(tr & 1u) * 2 + 1];
+                const uint32_t e = __ldg(At + scale_u32(xs, (uint32_t)asz));
+                const uint32_t item = e & 0x7fffffffu;
+                if ((e >> 31) == 0u || coin24(xc) < __ldg(frac + off + item)) {
+                    res = item;
+                    break;
+                }
+            }
+            if (res == 0xffffffffu && status) record_status(status, kErrTooManyTries);
+            out[s] = res;
+            continue;
         }
         const uint64_t b = counter_base + (s >> 1);
         if (b != have) {

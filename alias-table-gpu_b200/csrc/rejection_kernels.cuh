@@ -35,14 +35,6 @@ __device__ __forceinline__ void store_release_u64(uint64_t* p, uint64_t v) {
     asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-// Slot count and first-slot acceptance of one item (same FP64 expression as the reference).
-__device__ __forceinline__ void rej_item(float wf, double nd, double W, uint32_t& c, float& fr) {
-    const double x = __ddiv_rn(__dmul_rn(nd, (double)wf), W);
-    const double fl = floor(x);
-    c = (uint32_t)fl + 1u;
-    fr = __double2float_rn(x - fl);
-}
-
 // Tile look-back words: (flag << 62) | value, flag 1 = aggregate, 2 = inclusive.
 template <int IPT>
 __global__ void __launch_bounds__(kBuildThreads) rejection_tile_kernel(

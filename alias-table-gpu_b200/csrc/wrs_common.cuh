@@ -33,6 +33,16 @@ __device__ __forceinline__ void record_status(uint32_t* status, uint32_t code) {
     atomicCAS(status, 0u, code);
 }
 
+// Rejection slots of one item: c = floor(n w / W) + 1 and the first slot's acceptance
+// frac(n w / W), with the FP64 expression of the reference's CalcNumOccurrencesOperator
+// (construction/rejectionSampling/RejectionSampling.cu:26-33).
+__device__ __forceinline__ void rej_item(float wf, double nd, double W, uint32_t& c, float& fr) {
+    const double x = __ddiv_rn(__dmul_rn(nd, (double)wf), W);
+    const double fl = floor(x);
+    c = (uint32_t)fl + 1u;
+    fr = __double2float_rn(x - fl);
+}
+
 __device__ __forceinline__ uint32_t load_acquire(const uint32_t* p) {
     uint32_t v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");

@@ -79,6 +79,12 @@ _SIGNATURES = {
     "wrs_batched_build_f32": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P, _SZ, _P]),
     "wrs_batched_sample": (ctypes.c_int, [_P, _P, _I64, _P, _U64, _U64, _U64, _P, _P]),
     "wrs_batched_autotune": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _SZ, _P, _P]),
+    "wrs_batched_mixed_build_scratch_bytes": (_SZ, [_P, _P, _I64, _P]),
+    "wrs_batched_mixed_build_f32": (ctypes.c_int, [_P, _P, _P, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _SZ, _P]),
+    "wrs_batched_mixed_sample": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _I64, _P, _U64, _U64, _U64, _U32, _P, _P,
+                                                _P]),
+    "wrs_batched_autotune_kinds": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _SZ,
+                                                  _P, _P, _P]),
     "wrs_scratch_status": (ctypes.c_int, [_P, _P]),
     "wrs_export_reference_table": (ctypes.c_int, [_P, _I64, ctypes.c_double, _P, _P, _P]),
     "wrs_status_string": (ctypes.c_char_p, [ctypes.c_int]),
@@ -214,6 +220,60 @@ def batched_autotune(w, d_offsets, h_offsets, table, scratch, opts: BuildOpts, s
     return lib().wrs_batched_autotune(_ptr(w), _ptr(d_offsets), h.ctypes.data, h.shape[0] - 1, _ptr(table),
                                       _ptr(scratch), scratch.numel() * scratch.element_size(), ctypes.byref(opts),
                                       _stream(stream))
+
+
+WRS_TABLE_ALIAS = 0
+WRS_TABLE_REJECTION = 1
+WRS_TABLE_SKIP = 2
+
+
+def _host_u8(a) -> Optional[np.ndarray]:
+    return None if a is None else np.ascontiguousarray(np.asarray(a, dtype=np.uint8))
+
+
+def batched_mixed_build_scratch_bytes(h_offsets, h_kinds=None, opts: Optional[BuildOpts] = None) -> int:
+    """Scratch of a mixed build (h_kinds None: enough for any kinds)."""
+    h = _host_i64(h_offsets)
+    k = _host_u8(h_kinds)
+    return lib().wrs_batched_mixed_build_scratch_bytes(h.ctypes.data, None if k is None else k.ctypes.data,
+                                                       h.shape[0] - 1, ctypes.byref(opts) if opts else None)
+
+
+def batched_mixed_build(w, d_offsets, h_offsets, d_kinds, h_kinds, table, A, frac, a_size, scratch,
+                        opts: Optional[BuildOpts] = None, W_out=None, stream=None) -> int:
+    """Builds each table by its kind: alias rows into `table`, rejection slots into `A`
+    (table t at A[2 off[t]:]), acceptances into `frac`, |A_t| into `a_size`."""
+    h = _host_i64(h_offsets)
+    k = _host_u8(h_kinds)
+    return lib().wrs_batched_mixed_build_f32(_ptr(w), _ptr(d_offsets), h.ctypes.data, _ptr(d_kinds),
+                                             None if k is None else k.ctypes.data, h.shape[0] - 1,
+                                             ctypes.byref(opts) if opts else None, _ptr(table), _ptr(A), _ptr(frac),
+                                             _ptr(a_size), _ptr(W_out), _ptr(scratch),
+                                             scratch.numel() * scratch.element_size(), _stream(stream))
+
+
+def batched_mixed_sample(table, A, frac, a_size, d_offsets, d_kinds, num_tables: int, d_sample_offsets, total: int,
+                         seed: int, out, counter_base: int = 0, max_tries: int = 0, status=None, stream=None) -> int:
+    return lib().wrs_batched_mixed_sample(_ptr(table), _ptr(A), _ptr(frac), _ptr(a_size), _ptr(d_offsets),
+                                          _ptr(d_kinds), num_tables, _ptr(d_sample_offsets), total,
+                                          seed & (2**64 - 1), counter_base & (2**64 - 1), max_tries, _ptr(out),
+                                          _ptr(status), _stream(stream))
+
+
+def batched_autotune_kinds(w, d_offsets, h_offsets, d_sample_offsets, h_sample_offsets, table, A, frac, a_size,
+                           d_kinds_tmp, out, scratch, opts: Optional[BuildOpts] = None, stream=None):
+    """Alias or rejection per size class (ceil(log2 n)), timed on this batch. Returns
+    (status, kinds per table, kinds per class)."""
+    h = _host_i64(h_offsets)
+    hs = _host_i64(h_sample_offsets)
+    kinds = np.zeros(h.shape[0] - 1, dtype=np.uint8)
+    cls = np.zeros(33, dtype=np.uint8)
+    st = lib().wrs_batched_autotune_kinds(_ptr(w), _ptr(d_offsets), h.ctypes.data, h.shape[0] - 1,
+                                          _ptr(d_sample_offsets), hs.ctypes.data, ctypes.byref(opts) if opts else None,
+                                          _ptr(table), _ptr(A), _ptr(frac), _ptr(a_size), _ptr(d_kinds_tmp), _ptr(out),
+                                          _ptr(scratch), scratch.numel() * scratch.element_size(),
+                                          kinds.ctypes.data, cls.ctypes.data, _stream(stream))
+    return st, kinds, cls
 
 
 def export_reference_table(table, W: float, weight, alias, stream=None) -> int:

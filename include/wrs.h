@@ -205,6 +205,62 @@ WRS_API wrs_status wrs_batched_autotune(const float* d_w, const int64_t* d_offse
                                 int64_t num_tables, wrs_alias_row* d_table, void* d_scratch,
                                 size_t scratch_bytes, wrs_build_opts* opts, void* stream);
 
+/* ---- mixed batches: alias or rejection per table ----------------------- */
+
+/* Method of each table of a mixed batch, one byte per table (d_kinds in device memory,
+ * h_kinds the same array in host memory). A table of any other kind is skipped: it gets no
+ * rows and no slots, and its sample positions are left as they are. */
+#define WRS_TABLE_ALIAS 0u
+#define WRS_TABLE_REJECTION 1u
+#define WRS_TABLE_SKIP 2u
+
+/* Builds every table by its kind. Alias tables as wrs_batched_build_f32 does (their rows in
+ * d_table at the table's items, table-local aliases). Rejection tables as
+ * wrs_rejection_build_f32 does for their weights: c_i = floor(n w_i / W) + 1 slots per item,
+ * the table's slots at d_A[2 * offsets[t] ...] (|A_t| <= 2 n_t, in d_a_size[t]), first-slot
+ * acceptances at d_frac[offsets[t] ...], table-local items. d_A holds 2 * offsets[num_tables]
+ * slots, d_frac offsets[num_tables] floats, d_a_size num_tables u64 (written for rejection
+ * tables only). h_kinds sizes the launches, as h_offsets does; a NULL kinds pair makes every
+ * table an alias table. The scratch query with h_kinds = NULL covers every choice of kinds.
+ * Replaces a loop of AliasTableSplitGpu and RejectionSampling objects, one per table
+ * (AliasTableSplitGpu.cu:388-468, RejectionSampling.cu:35-56). */
+WRS_API size_t     wrs_batched_mixed_build_scratch_bytes(const int64_t* h_offsets, const uint8_t* h_kinds,
+                                                         int64_t num_tables, const wrs_build_opts* opts);
+WRS_API wrs_status wrs_batched_mixed_build_f32(const float* d_w, const int64_t* d_offsets, const int64_t* h_offsets,
+                                               const uint8_t* d_kinds, const uint8_t* h_kinds, int64_t num_tables,
+                                               const wrs_build_opts* opts, wrs_alias_row* d_table, uint32_t* d_A,
+                                               float* d_frac, uint64_t* d_a_size, double* d_W /* optional */,
+                                               void* d_scratch, size_t scratch_bytes, void* stream);
+/* One launch for the whole batch: output position s of table t follows table t's kind.
+ * Alias tables: the contract of wrs_batched_sample. Rejection tables: the contract of
+ * wrs_rejection_sample over the global position s (b = counter_base + s, at most max_tries
+ * tries, 0 = 64), the result a table-local item. A table without items (or without slots)
+ * and a rejection sample that runs out of tries write 0xFFFFFFFF and record the error in
+ * *d_status (optional, device). */
+WRS_API wrs_status wrs_batched_mixed_sample(const wrs_alias_row* d_table, const uint32_t* d_A, const float* d_frac,
+                                            const uint64_t* d_a_size, const int64_t* d_offsets,
+                                            const uint8_t* d_kinds, int64_t num_tables,
+                                            const int64_t* d_sample_offsets, uint64_t total_samples, uint64_t seed,
+                                            uint64_t counter_base, uint32_t max_tries, uint32_t* d_out,
+                                            uint32_t* d_status, void* stream);
+/* The autotuner's choice of method per size class; class c holds the tables with
+ * 2^(c-1) < n <= 2^c (class 0: n = 1). For every class present it times the mixed build and
+ * the mixed sample of that class's tables alone (every other table skipped), once as alias
+ * and once as rejection tables, with the batch's sample counts (h_sample_offsets is the host
+ * copy of d_sample_offsets), and writes the faster kind for each table into h_kinds_out
+ * (empty tables: WRS_TABLE_SKIP) and, if class_kinds is not NULL, the choice per class into
+ * class_kinds[0..32] (WRS_TABLE_SKIP for absent classes). Synchronous. d_kinds_tmp (num_tables
+ * bytes) and d_out (the batch's samples) are working buffers on the device; the other buffers
+ * are those of wrs_batched_mixed_build_f32, with the scratch of its query for h_kinds = NULL.
+ * This replaces the reference's compile-time choice of one method for every table. */
+WRS_API wrs_status wrs_batched_autotune_kinds(const float* d_w, const int64_t* d_offsets, const int64_t* h_offsets,
+                                              int64_t num_tables, const int64_t* d_sample_offsets,
+                                              const int64_t* h_sample_offsets, const wrs_build_opts* opts,
+                                              wrs_alias_row* d_table, uint32_t* d_A, float* d_frac,
+                                              uint64_t* d_a_size, uint8_t* d_kinds_tmp, uint32_t* d_out,
+                                              void* d_scratch, size_t scratch_bytes, uint8_t* h_kinds_out,
+                                              uint8_t* class_kinds, void* stream);
+
 /* ---- reference table format -------------------------------------------- */
 
 /* Writes the table in the reference's format (TableStorage, construction/aliasTable/

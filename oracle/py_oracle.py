@@ -58,6 +58,8 @@ def oracle() -> ctypes.CDLL:
             "or_batched_build": (_I, [_P, _P, _I64, _P, _P]),
             "or_psa_plus_build": (_I, [_P, _I64, _D, _I64, _P]),
             "or_batched_sample": (None, [_P, _P, _I64, _P, _U64, _U64, _P]),
+            "or_batched_mixed_build": (_I, [_P, _P, _I64, _P, _P, _P, _P, _P, _P]),
+            "or_batched_mixed_sample": (_I, [_P, _P, _P, _P, _P, _I64, _P, _P, _U64, _U64, _U32, _P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -343,3 +345,36 @@ def ref_sampler_cpu(weight, alias, W: float, num_samples: int, want_out: bool = 
     out = np.zeros(num_samples, dtype=np.int32) if want_out else None
     sec = ref().ref_sampler_cpu(_p(weight), _p(alias), weight.size, W, num_samples, _p(out) if want_out else None)
     return sec, out
+
+
+def batched_mixed_build(w: np.ndarray, off: np.ndarray, kinds: np.ndarray):
+    """Mixed batch: returns (rows (n, 2) u32, A (2n) u32, frac (n) f32, a_size u64, W, bad)."""
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    off = np.ascontiguousarray(off, dtype=np.int64)
+    kinds = np.ascontiguousarray(kinds, dtype=np.uint8)
+    n = int(off[-1])
+    rows = np.zeros((max(n, 1), 2), dtype=np.uint32)
+    A = np.zeros(max(2 * n, 1), dtype=np.uint32)
+    frac = np.zeros(max(n, 1), dtype=np.float32)
+    a_size = np.zeros(kinds.size, dtype=np.uint64)
+    W = np.zeros(kinds.size, dtype=np.float64)
+    bad = oracle().or_batched_mixed_build(_p(w), _p(off), kinds.size, _p(kinds), _p(rows), _p(A), _p(frac),
+                                          _p(a_size), _p(W))
+    return rows[:n], A[:2 * n], frac[:n], a_size, W, bad
+
+
+def batched_mixed_sample(rows, A, frac, a_size, off, kinds, soff, seed: int, cbase: int = 0, max_tries: int = 0,
+                         out: np.ndarray | None = None):
+    rows = np.ascontiguousarray(rows, dtype=np.uint32)
+    A = np.ascontiguousarray(A, dtype=np.uint32)
+    frac = np.ascontiguousarray(frac, dtype=np.float32)
+    a_size = np.ascontiguousarray(a_size, dtype=np.uint64)
+    off = np.ascontiguousarray(off, dtype=np.int64)
+    kinds = np.ascontiguousarray(kinds, dtype=np.uint8)
+    soff = np.ascontiguousarray(soff, dtype=np.int64)
+    if out is None:
+        out = np.zeros(max(int(soff[-1]), 1), dtype=np.uint32)
+    failed = oracle().or_batched_mixed_sample(_p(rows), _p(A), _p(frac), _p(a_size), _p(off), kinds.size, _p(kinds),
+                                              _p(soff), seed, cbase, max_tries, _p(out))
+    return out[:int(soff[-1])], failed
+

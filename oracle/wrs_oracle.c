@@ -860,6 +860,75 @@ void or_batched_sample(const uint32_t* rows, const int64_t* off, int64_t num_tab
     }
 }
 
+/* Mixed batch (kinds[t]: 0 alias, 1 rejection, other: skipped). Alias tables get the rows of
+ * or_batched_build; rejection table t gets or_rejection_build's slots at A + 2 off[t] (capacity
+ * 2 n_t), its acceptances at frac + off[t] and |A_t| in a_size[t]; both with W the exact sum.
+ * Returns the number of tables with invalid or all-zero weights. */
+int or_batched_mixed_build(const float* w, const int64_t* off, int64_t num_tables, const uint8_t* kinds,
+                           uint32_t* rows, uint32_t* A, float* frac, uint64_t* a_size, double* W_out) {
+    int bad = 0;
+    for (int64_t t = 0; t < num_tables; ++t) {
+        const int64_t n = off[t + 1] - off[t];
+        if (n <= 0 || kinds[t] > 1) continue;
+        const double W = or_exact_sum_f32(w + off[t], n);
+        if (W_out) W_out[t] = W;
+        if (!(W > 0.0) || isinf(W)) {
+            ++bad;
+            continue;
+        }
+        if (kinds[t] == 0) {
+            or_exact_build(w + off[t], n, W, rows + 2 * off[t]);
+        } else {
+            const uint64_t asz = or_rejection_build(w + off[t], n, W, A + 2 * off[t], 2 * (uint64_t)n, frac + off[t]);
+            a_size[t] = asz > 2 * (uint64_t)n ? 0 : asz;
+        }
+    }
+    return bad;
+}
+
+/* The mixed sampler: alias positions as or_batched_sample, rejection positions as
+ * or_rejection_sample over the global position s (b = cbase + s); skipped tables' positions
+ * are left as they are. Returns 1 if a rejection sample ran out of tries. */
+int or_batched_mixed_sample(const uint32_t* rows, const uint32_t* A, const float* frac, const uint64_t* a_size,
+                            const int64_t* off, int64_t num_tables, const uint8_t* kinds, const int64_t* soff,
+                            uint64_t seed, uint64_t cbase, uint32_t max_tries, uint32_t* out) {
+    int failed = 0;
+    const uint32_t tries = max_tries ? max_tries : 64u;
+    for (int64_t t = 0; t < num_tables; ++t) {
+        const uint64_t n = (uint64_t)(off[t + 1] - off[t]);
+        for (int64_t s = soff[t]; s < soff[t + 1]; ++s) {
+            uint32_t x[4];
+            if (kinds[t] == 0) {
+                philox_block(cbase + ((uint64_t)s >> 1), 0, 0, seed, x);
+                const uint32_t xr = (s & 1) ? x[2] : x[0], xc = (s & 1) ? x[3] : x[1];
+                out[s] = n == 0 ? 0xffffffffu : do_sample(rows + 2 * off[t], scale_u32(xr, (uint32_t)n), xc);
+            } else if (kinds[t] == 1) {
+                const uint64_t asz = n ? a_size[t] : 0;
+                if (asz == 0) {
+                    out[s] = 0xffffffffu;
+                    continue;
+                }
+                const uint32_t* At = A + 2 * off[t];
+                const uint64_t b = cbase + (uint64_t)s;
+                uint32_t res = 0xffffffffu;
+                for (uint32_t tr = 0; tr < tries; ++tr) {
+                    if ((tr & 1u) == 0) philox_block(b, tr >> 1, 0x52454a00u, seed, x);
+                    const uint32_t xs = x[(tr & 1u) * 2], xc = x[(tr & 1u) * 2 + 1];
+                    const uint32_t e = At[scale_u32(xs, (uint32_t)asz)];
+                    const uint32_t item = e & 0x7fffffffu;
+                    if ((e >> 31) == 0u || coin24(xc) < frac[off[t] + item]) {
+                        res = item;
+                        break;
+                    }
+                }
+                if (res == 0xffffffffu) failed = 1;
+                out[s] = res;
+            }
+        }
+    }
+    return failed;
+}
+
 double or_sample_plain_timed(const uint32_t* rows, int64_t n, uint64_t m, uint64_t seed, int threads, uint32_t* out) {
     struct timespec t0, t1;
     clock_gettime(CLOCK_MONOTONIC, &t0);

@@ -80,6 +80,12 @@ void or_batched_sample(const uint32_t* rows, const int64_t* off, int64_t num_tab
 uint64_t or_rejection_build(const float* w, int64_t n, double W, uint32_t* A, uint64_t a_capacity, float* frac);
 int or_rejection_sample(const uint32_t* A, uint64_t a_size, const float* frac, uint64_t m, uint64_t seed,
                         uint64_t cbase, uint32_t max_tries, uint32_t* out);
+/* mixed batch (kinds: 0 alias, 1 rejection, else skipped); rejection slots at A + 2 off[t] */
+int or_batched_mixed_build(const float* w, const int64_t* off, int64_t num_tables, const uint8_t* kinds,
+                           uint32_t* rows, uint32_t* A, float* frac, uint64_t* a_size, double* W_out);
+int or_batched_mixed_sample(const uint32_t* rows, const uint32_t* A, const float* frac, const uint64_t* a_size,
+                            const int64_t* off, int64_t num_tables, const uint8_t* kinds, const int64_t* soff,
+                            uint64_t seed, uint64_t cbase, uint32_t max_tries, uint32_t* out);
 
 /* reference CPU sampler restatement with the Philox contract, all cores; returns samples/s */
 double or_sample_plain_timed(const uint32_t* rows, int64_t n, uint64_t m, uint64_t seed, int threads,
