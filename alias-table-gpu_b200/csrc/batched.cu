@@ -443,7 +443,8 @@ extern "C" wrs_status wrs_batched_autotune_kinds(const float* d_w, const int64_t
                                                  const wrs_build_opts* opts, wrs_alias_row* d_table, uint32_t* d_A,
                                                  float* d_frac, uint64_t* d_a_size, uint8_t* d_kinds_tmp,
                                                  uint32_t* d_out, void* d_scratch, size_t scratch_bytes,
-                                                 uint8_t* h_kinds_out, uint8_t* class_kinds, void* stream_) {
+                                                 uint8_t* h_kinds_out, uint8_t* class_kinds, float* class_ms,
+                                                 void* stream_) {
     if (!d_w || !d_offsets || !h_offsets || !d_sample_offsets || !h_sample_offsets || !d_table || !d_A || !d_frac ||
         !d_a_size || !d_kinds_tmp || !d_out || !d_scratch || !h_kinds_out || num_tables < 1)
         return WRS_ERR_INVALID_ARGUMENT;
@@ -467,6 +468,8 @@ extern "C" wrs_status wrs_batched_autotune_kinds(const float* d_w, const int64_t
     }
     uint8_t choice[kClasses];
     for (int c = 0; c < kClasses; ++c) choice[c] = WRS_TABLE_SKIP;
+    if (class_ms)
+        for (int c = 0; c < 2 * kClasses; ++c) class_ms[c] = 0.0f;
     std::vector<uint8_t> kinds((size_t)num_tables);
     cudaEvent_t e0, e1;
     if (cudaEventCreate(&e0) != cudaSuccess) return WRS_ERR_CUDA;
@@ -507,6 +510,10 @@ extern "C" wrs_status wrs_batched_autotune_kinds(const float* d_w, const int64_t
             }
         }
         choice[c] = ms_of[0] <= ms_of[1] ? (uint8_t)WRS_TABLE_ALIAS : (uint8_t)WRS_TABLE_REJECTION;
+        if (class_ms) {
+            class_ms[2 * c] = ms_of[0];
+            class_ms[2 * c + 1] = ms_of[1];
+        }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -84,7 +84,7 @@ _SIGNATURES = {
     "wrs_batched_mixed_sample": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _I64, _P, _U64, _U64, _U64, _U32, _P, _P,
                                                 _P]),
     "wrs_batched_autotune_kinds": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _SZ,
-                                                  _P, _P, _P]),
+                                                  _P, _P, _P, _P]),
     "wrs_scratch_status": (ctypes.c_int, [_P, _P]),
     "wrs_export_reference_table": (ctypes.c_int, [_P, _I64, ctypes.c_double, _P, _P, _P]),
     "wrs_status_string": (ctypes.c_char_p, [ctypes.c_int]),
@@ -263,17 +263,18 @@ def batched_mixed_sample(table, A, frac, a_size, d_offsets, d_kinds, num_tables:
 def batched_autotune_kinds(w, d_offsets, h_offsets, d_sample_offsets, h_sample_offsets, table, A, frac, a_size,
                            d_kinds_tmp, out, scratch, opts: Optional[BuildOpts] = None, stream=None):
     """Alias or rejection per size class (ceil(log2 n)), timed on this batch. Returns
-    (status, kinds per table, kinds per class)."""
+    (status, kinds per table, kinds per class, ms per class as (alias, rejection) pairs)."""
     h = _host_i64(h_offsets)
     hs = _host_i64(h_sample_offsets)
     kinds = np.zeros(h.shape[0] - 1, dtype=np.uint8)
     cls = np.zeros(33, dtype=np.uint8)
+    ms = np.zeros((33, 2), dtype=np.float32)
     st = lib().wrs_batched_autotune_kinds(_ptr(w), _ptr(d_offsets), h.ctypes.data, h.shape[0] - 1,
                                           _ptr(d_sample_offsets), hs.ctypes.data, ctypes.byref(opts) if opts else None,
                                           _ptr(table), _ptr(A), _ptr(frac), _ptr(a_size), _ptr(d_kinds_tmp), _ptr(out),
                                           _ptr(scratch), scratch.numel() * scratch.element_size(),
-                                          kinds.ctypes.data, cls.ctypes.data, _stream(stream))
-    return st, kinds, cls
+                                          kinds.ctypes.data, cls.ctypes.data, ms.ctypes.data, _stream(stream))
+    return st, kinds, cls, ms
 
 
 def export_reference_table(table, W: float, weight, alias, stream=None) -> int:

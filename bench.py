@@ -396,17 +396,19 @@ def batch_config5():
     w = np.concatenate([w_small, w_large])
     counts = 4 * sizes
     what = (f"10^6 tables of U{{1..64}} items, w~Exp(1), and 100 tables of 2^20 items, w~Pareto(1.5) "
-            f"({int(sizes.sum())} items); build + 4 x size samples per table; alias tables for every size "
-            f"class (the alias-vs-rejection choice per class is not built)")
+            f"({int(sizes.sum())} items); build + 4 x size samples per table; alias or rejection per size "
+            f"class (ceil(log2 n)), chosen by the autotuner on this batch")
     return sizes, w, counts, what, [(np.arange(BATCH_PER_TABLE_SAMPLE), sizes <= 64),
                                     (np.arange(1_000_000, 1_000_004), sizes > 64)]
 
 
-def batched_phase(dev, make=batch_config4) -> dict:
+def batched_phase(dev, make=batch_config4, mixed: bool = False) -> dict:
     """A batched-tables configuration: the batched build and sample (autotuned launch shape,
     captured in one CUDA graph) against the plain single-table entry points called once per
     table, timed on samples of each size class and scaled to all tables of the class by count
-    (each call pays the same launch sequence)."""
+    (each call pays the same launch sequence). With `mixed`, the autotuner also picks alias or
+    rejection per size class, and the timed graph is the mixed build and sampler with those
+    kinds (the all-alias graph is timed beside it)."""
     import torch
     import wrs
 
@@ -467,6 +469,48 @@ def batched_phase(dev, make=batch_config4) -> dict:
     torch.cuda.synchronize()
     batched_ms = e0.elapsed_time(e1) / reps
     batched_wall_ms = (time.perf_counter() - t0) * 1e3 / reps
+    mixed_info = None
+    if mixed:
+        A = torch.empty(2 * items, dtype=torch.int32, device=dev)
+        frac = torch.empty(items, dtype=torch.float32, device=dev)
+        a_size = torch.empty(nt, dtype=torch.int64, device=dev)
+        kt = torch.empty(nt, dtype=torch.uint8, device=dev)
+        scr_m = torch.empty(wrs.batched_mixed_build_scratch_bytes(off, None, opts), dtype=torch.uint8, device=dev)
+        st, kinds, cls, cms = wrs.batched_autotune_kinds(w, d_off, off, d_soff, soff, table, A, frac, a_size, kt,
+                                                         out, scr_m, opts)
+        if st:
+            raise wrs.WrsError(st, "kinds autotune")
+        d_kinds = torch.from_numpy(kinds).to(dev)
+        st = wrs.batched_mixed_build(w, d_off, off, d_kinds, kinds, table, A, frac, a_size, scr_m,
+                                     wrs.build_opts(0, opts.tile_items, True, opts.small_table_items))
+        if st:
+            raise wrs.WrsError(st, "mixed build")
+        gm = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(s):
+            gm.capture_begin()
+            wrs.batched_mixed_build(w, d_off, off, d_kinds, kinds, table, A, frac, a_size, scr_m, opts, stream=s)
+            wrs.batched_mixed_sample(table, A, frac, a_size, d_off, d_kinds, nt, d_soff, total, SEED_SAMPLES, out, 0,
+                                     stream=s)
+            gm.capture_end()
+        torch.cuda.current_stream(dev).wait_stream(s)
+        for _ in range(3):
+            gm.replay()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0.record()
+        for _ in range(reps):
+            gm.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        present = sorted(set(int(c) for c in np.where(sizes <= 1, 0, np.ceil(np.log2(np.maximum(sizes, 2))))))
+        names = {wrs.WRS_TABLE_ALIAS: "alias", wrs.WRS_TABLE_REJECTION: "rejection"}
+        mixed_info = {"all_alias_ms": round(batched_ms, 4),
+                      "kinds_by_size_class": {f"n<=2^{c}": names.get(int(cls[c]), "skip") for c in present},
+                      "class_ms_alias_vs_rejection": {f"n<=2^{c}": [round(float(cms[c, 0]), 3),
+                                                                     round(float(cms[c, 1]), 3)] for c in present},
+                      "rejection_tables": int((kinds == wrs.WRS_TABLE_REJECTION).sum())}
+        batched_ms = e0.elapsed_time(e1) / reps
+        batched_wall_ms = (time.perf_counter() - t0) * 1e3 / reps
 
     # per-table launches: build + the table's samples, one call each, per size class
     L = wrs.lib()
@@ -508,6 +552,7 @@ def batched_phase(dev, make=batch_config4) -> dict:
         "per_table_sample": "timed on " + ", ".join(timed) + " per size class, scaled by table count",
         "speedup": round(per_ms / batched_ms, 1),
         "tables_equal_to_single_builds": f"{int(check.size) if exact else 0} of {int(check.size)} checked",
+        **({"mixed": mixed_info} if mixed_info else {}),
     }
 
 
@@ -516,7 +561,8 @@ def run_batched_only(args, rank: int, local_rank: int):
     if rank != 0:
         return None
     torch.cuda.set_device(local_rank)
-    b = batched_phase(torch.device("cuda", local_rank), batch_config5 if args.config == "5" else batch_config4)
+    b = batched_phase(torch.device("cuda", local_rank), batch_config5 if args.config == "5" else batch_config4,
+                      mixed=args.config == "5")
     items_samples = b["items"] + b["samples"]
     return {"metric": METRIC, "value": b["batched_g_items_plus_samples_s"], "unit": UNIT, "n_gpus": 1,
             "steps": 20, "warmup": 3, "ms_per_step": b["batched_ms"], "higher_is_better": True, "scaling": "weak",

@@ -249,7 +249,9 @@ WRS_API wrs_status wrs_batched_mixed_sample(const wrs_alias_row* d_table, const 
  * and once as rejection tables, with the batch's sample counts (h_sample_offsets is the host
  * copy of d_sample_offsets), and writes the faster kind for each table into h_kinds_out
  * (empty tables: WRS_TABLE_SKIP) and, if class_kinds is not NULL, the choice per class into
- * class_kinds[0..32] (WRS_TABLE_SKIP for absent classes). Synchronous. d_kinds_tmp (num_tables
+ * class_kinds[0..32] (WRS_TABLE_SKIP for absent classes), and if class_ms is not NULL the
+ * timings behind the choice into class_ms[0..65] (class c: [2c] as alias, [2c+1] as rejection,
+ * in ms; 0 for absent classes). Synchronous. d_kinds_tmp (num_tables
  * bytes) and d_out (the batch's samples) are working buffers on the device; the other buffers
  * are those of wrs_batched_mixed_build_f32, with the scratch of its query for h_kinds = NULL.
  * This replaces the reference's compile-time choice of one method for every table. */
@@ -259,7 +261,7 @@ WRS_API wrs_status wrs_batched_autotune_kinds(const float* d_w, const int64_t* d
                                               wrs_alias_row* d_table, uint32_t* d_A, float* d_frac,
                                               uint64_t* d_a_size, uint8_t* d_kinds_tmp, uint32_t* d_out,
                                               void* d_scratch, size_t scratch_bytes, uint8_t* h_kinds_out,
-                                              uint8_t* class_kinds, void* stream);
+                                              uint8_t* class_kinds, float* class_ms, void* stream);
 
 /* ---- reference table format -------------------------------------------- */
 

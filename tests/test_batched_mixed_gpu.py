@@ -177,12 +177,15 @@ def test_autotune_kinds(cuda):
     kt = torch.empty(off.size - 1, dtype=torch.uint8, device="cuda")
     out = torch.empty(int(soff[-1]), dtype=torch.int32, device="cuda")
     scratch = alloc_scratch(wrs.batched_mixed_build_scratch_bytes(off, None, None))
-    st, kinds, cls = wrs.batched_autotune_kinds(d_w, d_off, off, d_soff, soff, table, A, frac, a_size, kt, out,
-                                                scratch)
+    st, kinds, cls, ms = wrs.batched_autotune_kinds(d_w, d_off, off, d_soff, soff, table, A, frac, a_size, kt,
+                                                    out, scratch)
     assert st == wrs.WRS_SUCCESS, wrs.status_string(st)
     sizes = off[1:] - off[:-1]
     c = np.where(sizes <= 1, 0, np.ceil(np.log2(np.maximum(sizes, 2))).astype(int))
     assert np.all(kinds == cls[c]), "a table's kind is not its class's"
+    for k in np.unique(c):
+        assert ms[k, 0] > 0 and ms[k, 1] > 0
+        assert cls[k] == (wrs.WRS_TABLE_ALIAS if ms[k, 0] <= ms[k, 1] else wrs.WRS_TABLE_REJECTION)
     assert set(np.unique(cls[c]).tolist()) <= {wrs.WRS_TABLE_ALIAS, wrs.WRS_TABLE_REJECTION}
     st, got = run_mixed_build(w, off, kinds)
     assert st == wrs.WRS_SUCCESS
