@@ -9,6 +9,8 @@
 //                            (sampling/rejectionSampling/SamplerRejection.cu:63-72)
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "host_util.h"
 #include "rejection_kernels.cuh"
 #include "sample_kernels.cuh"
@@ -75,6 +77,56 @@ extern "C" wrs_status wrs_alias_sample(const wrs_alias_row* d_table, int64_t n, 
     if (st != WRS_SUCCESS) return st;
     if (opts && (opts->flags & WRS_FLAG_SYNC)) return cuda_status(cudaStreamSynchronize(stream));
     return WRS_SUCCESS;
+}
+
+// ---------------------------------------------------------------- sampling into host memory
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_copy_mu;
+cudaStream_t g_copy_stream[kMaxDevices] = {};
+
+// The library's device-to-host copy stream of the current device (created on first use).
+wrs_status copy_stream(cudaStream_t* out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return WRS_ERR_CUDA;
+    std::lock_guard<std::mutex> lock(g_copy_mu);
+    if (!g_copy_stream[dev] && cudaStreamCreateWithFlags(&g_copy_stream[dev], cudaStreamNonBlocking) != cudaSuccess) {
+        g_copy_stream[dev] = nullptr;
+        return WRS_ERR_CUDA;
+    }
+    *out = g_copy_stream[dev];
+    return WRS_SUCCESS;
+}
+}  // namespace
+
+extern "C" wrs_status wrs_alias_sample_to_host(const wrs_alias_row* d_table, int64_t n, uint64_t num_samples,
+                                               uint64_t seed, uint64_t counter_base, uint64_t chunk_samples,
+                                               uint32_t* d_out, uint32_t* h_out, void* stream_) {
+    if (!d_table || n < 1 || n > kMaxItems || (num_samples > 0 && (!d_out || !h_out))) return WRS_ERR_INVALID_ARGUMENT;
+    if (num_samples == 0) return WRS_SUCCESS;
+    uint64_t chunk = chunk_samples ? chunk_samples : (1ull << 25);
+    chunk += chunk & 1u;  // chunks start at even positions: a Philox block serves positions 2b, 2b + 1
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+    cudaStream_t copy = nullptr;
+    wrs_status st = copy_stream(&copy);
+    if (st != WRS_SUCCESS) return st;
+    cudaEvent_t ev = nullptr;
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return WRS_ERR_CUDA;
+    for (uint64_t s0 = 0; s0 < num_samples && st == WRS_SUCCESS; s0 += chunk) {
+        const uint64_t c = num_samples - s0 < chunk ? num_samples - s0 : chunk;
+        st = wrs_alias_sample(d_table, n, c, seed, counter_base + s0 / 2, nullptr, d_out + s0, nullptr, stream_);
+        if (st != WRS_SUCCESS) break;
+        // the copy stream takes the chunk once it is written (a wait binds the latest record)
+        if (cudaEventRecord(ev, stream) != cudaSuccess || cudaStreamWaitEvent(copy, ev, 0) != cudaSuccess ||
+            cudaMemcpyAsync(h_out + s0, d_out + s0, c * sizeof(uint32_t), cudaMemcpyDeviceToHost, copy) !=
+                cudaSuccess)
+            st = WRS_ERR_CUDA;
+    }
+    // later work on `stream` (and a later call reusing d_out) waits for every copy
+    if (cudaEventRecord(ev, copy) != cudaSuccess || cudaStreamWaitEvent(stream, ev, 0) != cudaSuccess)
+        st = st == WRS_SUCCESS ? WRS_ERR_CUDA : st;
+    cudaEventDestroy(ev);
+    return st;
 }
 
 // ---------------------------------------------------------------- rejection

@@ -72,6 +72,7 @@ _SIGNATURES = {
     "wrs_alias_build_f32": (ctypes.c_int, [_P, _I64, _P, _P, _P, _P, _SZ, _P]),
     "wrs_alias_build_f32_static_scratch": (ctypes.c_int, [_P, _I64, _P, _P, _P, _P]),
     "wrs_alias_sample": (ctypes.c_int, [_P, _I64, _U64, _U64, _U64, _P, _P, _P, _P]),
+    "wrs_alias_sample_to_host": (ctypes.c_int, [_P, _I64, _U64, _U64, _U64, _U64, _P, _P, _P]),
     "wrs_rejection_build_scratch_bytes": (_SZ, [_I64]),
     "wrs_rejection_build_f32": (ctypes.c_int, [_P, _I64, _P, _U64, _P, _P, _P, _P, _SZ, _U32, _P]),
     "wrs_rejection_sample": (ctypes.c_int, [_P, _P, _P, _I64, _U64, _U64, _U64, _U32, _P, _P, _U32, _P]),
@@ -166,6 +167,14 @@ def alias_sample(table, n: int, num_samples: int, seed: int, out, counter_base: 
     opts = SampleOpts(mode, section_items, WRS_FLAG_SYNC if sync else 0, 0)
     return lib().wrs_alias_sample(_ptr(table), n, num_samples, seed & (2**64 - 1), counter_base & (2**64 - 1),
                                   ctypes.byref(opts), _ptr(out), _ptr(section_counts), _stream(stream))
+
+
+def alias_sample_to_host(table, n: int, num_samples: int, seed: int, out, host_out, counter_base: int = 0,
+                         chunk_samples: int = 0, stream=None) -> int:
+    """Plain samples into `host_out` (a pinned CPU tensor), produced chunk by chunk in `out`
+    on the device while the copies of finished chunks run on the library's copy stream."""
+    return lib().wrs_alias_sample_to_host(_ptr(table), n, num_samples, seed & (2**64 - 1), counter_base & (2**64 - 1),
+                                          chunk_samples, _ptr(out), host_out.data_ptr(), _stream(stream))
 
 
 def rejection_build_scratch_bytes(n: int) -> int:

@@ -147,6 +147,18 @@ WRS_API wrs_status wrs_alias_build_f32_static_scratch(const float* d_w, int64_t 
 WRS_API wrs_status wrs_alias_sample(const wrs_alias_row* d_table, int64_t n, uint64_t num_samples,
                             uint64_t seed, uint64_t counter_base, const wrs_sample_opts* opts,
                             uint32_t* d_out, uint64_t* d_section_counts, void* stream);
+/* Plain sampling with the samples delivered to host memory: the samples of wrs_alias_sample
+ * (PLAIN, same seed and counter_base) are produced chunk by chunk into d_out on `stream`, and
+ * an internal copy stream of the library moves each finished chunk to h_out (num_samples u32;
+ * pinned host memory, or the copies do not overlap), so the transfer overlaps the sampling
+ * of the next chunk. Work enqueued on `stream` after the call waits for every copy.
+ * chunk_samples: 0 = 2^25 (rounded up to an even count). The copy stream is created on the
+ * first call on a device: make that call outside stream capture. The reference's samplers
+ * keep no output (SamplerGpuBasic.cu:77-133); this is the transfer a caller of its
+ * getSamplingDistribution pays for, overlapped. */
+WRS_API wrs_status wrs_alias_sample_to_host(const wrs_alias_row* d_table, int64_t n, uint64_t num_samples,
+                                            uint64_t seed, uint64_t counter_base, uint64_t chunk_samples,
+                                            uint32_t* d_out, uint32_t* h_out, void* stream);
 
 /* ---- rejection sampling ------------------------------------------------- */
 

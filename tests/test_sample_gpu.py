@@ -74,3 +74,20 @@ def test_reference_shaped_samplers(cuda):
         assert dist.sum() == 2_000_000
         assert chi2_pvalue(dist, w / w.sum(dtype=np.float64) * 2_000_000) > 1e-6
         assert s.benchmarkSampling(1 << 20) > 0
+
+
+@pytest.mark.parametrize("m,chunk,cbase", [(1, 0, 0), (1001, 64, 7), (1001, 63, 8), ((1 << 20) + 5, 1 << 17, 99),
+                                           (3 << 20, 0, (1 << 40) + 1)])
+def test_sample_to_host_bit_exact(tables, m, chunk, cbase):
+    # chunked sampling with overlapped copies gives the plain sampler's stream, in pinned memory;
+    # two calls in a row on the same buffers (the second must wait for the first's copies)
+    w, rows = tables["powerlaw_shuffled"]
+    table = torch.from_numpy(np.ascontiguousarray(rows).view(np.int64).reshape(-1)).cuda()
+    out = torch.empty(m, dtype=torch.int32, device="cuda")
+    host = torch.full((m,), -1, dtype=torch.int32).pin_memory()
+    for rep in range(2):
+        c = cbase + rep * m
+        st = wrs.alias_sample_to_host(table, rows.shape[0], m, SEED, out, host, c, chunk)
+        assert st == 0
+        torch.cuda.current_stream().synchronize()
+        np.testing.assert_array_equal(host.numpy().view(np.uint32), po.sample_plain(rows, m, SEED, c))
