@@ -1183,7 +1183,7 @@ struct PackShape<1024> {
 };
 template <>
 struct PackShape<2048> {
-    static constexpr int NT = 128, IPT = 16;
+    static constexpr int NT = 256, IPT = 8;
 };
 template <>
 struct PackShape<4096> {
@@ -1244,7 +1244,7 @@ __device__ __forceinline__ uint32_t stage_pos(uint32_t i) {
 // lights from the slots (deficits and row probabilities given), and their rows are written
 // at their items.
 template <int NT, int IPT, bool BATCH, bool LEFT>
-__global__ void __launch_bounds__(NT, (NT == 128 && IPT == 16) ? 5 : 1) split_pack_kernel(const float* __restrict__ w,
+__global__ void __launch_bounds__(NT, (NT == 256 && IPT == 8) ? 4 : 1) split_pack_kernel(const float* __restrict__ w,
                                                         const BuildHeader* hdr, const TileVals* incl,
                                                         const TileStart* __restrict__ starts,
                                                         const uint32_t* __restrict__ heavy_item,
