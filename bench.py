@@ -185,6 +185,31 @@ def table_error_gpu(w, table) -> dict:
     return {"max_rel": float(top[0].item()), "p9999_rel": float(top[-1].item()), "zero_weight_mass": zm}
 
 
+def chi2_gpu(w, samples, min_expected: float = 32.0) -> dict:
+    """Chi-square goodness of fit of the samples against w_i / W, on the device. Items are
+    grouped, in index order, into bins of at least `min_expected` expected samples (the
+    cumulative expected count cut every `min_expected`); the p-value of the statistic with
+    bins - 1 degrees of freedom uses the Wilson-Hilferty normal approximation."""
+    import torch
+    m = samples.numel()
+    wd = w.double()
+    expected = wd * (m / wd.sum())
+    cum = torch.cumsum(expected, 0)
+    bin_of = torch.clamp((cum - expected * 0.5) / min_expected, min=0).long()
+    nbins = int(bin_of[-1].item()) + 1
+    del cum
+    counts = torch.bincount(samples, minlength=w.numel()).double()
+    obs = torch.zeros(nbins, dtype=torch.float64, device=w.device).index_add_(0, bin_of, counts)
+    exp_b = torch.zeros(nbins, dtype=torch.float64, device=w.device).index_add_(0, bin_of, expected)
+    del counts, bin_of, expected
+    keep = exp_b > 0
+    stat = float((((obs - exp_b) ** 2)[keep] / exp_b[keep]).sum().item())
+    df = int(keep.sum().item()) - 1
+    z = ((stat / df) ** (1.0 / 3.0) - (1.0 - 2.0 / (9.0 * df))) / math.sqrt(2.0 / (9.0 * df))
+    return {"samples": m, "bins": df + 1, "min_expected_per_bin": min_expected, "stat": round(stat, 1), "df": df,
+            "stat_over_df": round(stat / df, 6), "p_value": 0.5 * math.erfc(z / math.sqrt(2.0))}
+
+
 def table_error(w: np.ndarray, rows_u32: np.ndarray) -> dict:
     """Per-item relative error of the table against w_i / W (W summed in FP64 pairwise)."""
     n = w.size
@@ -306,6 +331,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     torch.cuda.synchronize()
     sect_ms = s0.elapsed_time(s1) / reps
 
+    # goodness of fit of the last timed step's samples (outside every timed region)
+    chi2 = chi2_gpu(w, out) if rank == 0 else None
+
     # end to end through the API with host buffers: H2D weights, build, sample, D2H samples
     out_host = torch.empty(m, dtype=torch.int32).pin_memory()
     e2e_steps = max(3, min(K, 10))
@@ -356,6 +384,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                    "sectioned_gsamples_s": round(m / sect_ms / 1e6, 3),
                    "section_items": SECTION_ITEMS},
         "prob_error": err,
+        "chi_square": chi2,
         "roofline": {"kernel": "sample_plain_kernel", "bound": "hbm", "achieved": round(achieved, 1),
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "traffic": ncu_traffic() if args.config == "2" else None,
