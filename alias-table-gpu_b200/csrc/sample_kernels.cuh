@@ -23,6 +23,16 @@ __device__ __forceinline__ uint32_t alias_pick(const uint2 row, uint32_t r, uint
     return coin24(coin_bits) < __uint_as_float(row.x) ? r : row.y;
 }
 
+// A random row gather that asks L2 to fetch 64 bytes around the row (the prefetch-size
+// qualifier of ld): without it a random 8-byte gather from a table larger than L2 cost about
+// 107 bytes of DRAM reads (3.6 sectors), with it about 58. The sampling rate is the same
+// either way (the random DRAM access rate bounds it), at half the DRAM traffic.
+__device__ __forceinline__ uint2 ld_row_64B(const uint2* p) {
+    uint2 v;
+    asm("ld.global.nc.L2::64B.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "l"(p));
+    return v;
+}
+
 // Plain sampling: each thread handles octets of consecutive output positions (4 Philox
 // blocks, 8 independent gathers in flight, two 16-byte stores).
 __global__ void __launch_bounds__(256) sample_plain_kernel(const uint2* __restrict__ table, uint32_t n, uint64_t m,
@@ -45,7 +55,7 @@ __global__ void __launch_bounds__(256) sample_plain_kernel(const uint2* __restri
         }
         uint2 v[8];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) v[j] = __ldg(table + rows[j]);
+        for (int j = 0; j < 8; ++j) v[j] = ld_row_64B(table + rows[j]);
         uint32_t res[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) res[j] = alias_pick(v[j], rows[j], coins[j]);
