@@ -87,14 +87,17 @@ __global__ void __launch_bounds__(NT) psa_local_kernel(const float* __restrict__
         gbits |= (uint32_t)(wk >= cp.Hh && !(wk > cp.H1)) << k;
         hbits |= (uint32_t)(wk > cp.H1) << k;
     }
+    // the rare items' FP64 quantities, from the weights in registers
     uint64_t lsum = 0, hsum = 0;
-    for (uint32_t bits = gbits; bits; bits &= bits - 1) {
-        const int k = __ffs(bits) - 1;
-        const uint64_t q = rare_q(__ldg(w + item0 + k), false, cp);
-        sSlotQ[tid * IPT + k] = q;
-        lsum += q;
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+        if ((gbits >> k) & 1u) {
+            const uint64_t q = rare_q(x[k], false, cp);
+            sSlotQ[tid * IPT + k] = q;
+            lsum += q;
+        }
+        if ((hbits >> k) & 1u) hsum += rare_q(x[k], true, cp);
     }
-    for (uint32_t bits = hbits; bits; bits &= bits - 1) hsum += rare_q(__ldg(w + item0 + __ffs(bits) - 1), true, cp);
     const uint32_t nl = (uint32_t)__popc(lbits), nh = (uint32_t)__popc(hbits);
     Scan3 tot_l, tot_h;
     const Scan3 ex = block_scan3<NT>(Scan3{nl, asum, lsum}, s_scan3, tot_l);
@@ -104,15 +107,7 @@ __global__ void __launch_bounds__(NT) psa_local_kernel(const float* __restrict__
     Dither dth = make_dither(before.L);
     const uint64_t D0 = dither_at(dth, ex.b);
     {
-        uint64_t lr = ex.b;
-        for (uint32_t bits = gbits; bits; bits &= bits - 1) {
-            const int slot = tid * IPT + __ffs(bits) - 1;
-            lr += sSlotQ[slot];
-            sSlotQ[slot] = dither_at(dth, lr);
-        }
-    }
-    {
-        uint64_t sr = ex.a, D = D0;
+        uint64_t sr = ex.a, D = D0, lr = ex.b;
         uint32_t li = l0;
 #pragma unroll
         for (int k = 0; k < IPT; ++k) {
@@ -120,8 +115,9 @@ __global__ void __launch_bounds__(NT) psa_local_kernel(const float* __restrict__
             if (light) sLkey[lkey_slot(li)] = sr + D;
             li += light ? 1u : 0u;
             sr += (light && !((gbits >> k) & 1u)) ? small_deficit(pk[k]) : 0ull;
-            if ((gbits >> k) & 1u) {
-                const uint64_t D1 = sSlotQ[tid * IPT + k];
+            if ((gbits >> k) & 1u) {  // the dithering after a large light
+                lr += sSlotQ[tid * IPT + k];
+                const uint64_t D1 = dither_at(dth, lr);
                 pk[k] = dithered_prob(D1 - D);
                 D = D1;
             }
@@ -132,9 +128,10 @@ __global__ void __launch_bounds__(NT) psa_local_kernel(const float* __restrict__
     {
         uint64_t er = exh.a;
         uint32_t hj = exh.c;
-        for (uint32_t bits = hbits; bits; bits &= bits - 1) {
-            const int k = __ffs(bits) - 1;
-            er += rare_q(__ldg(w + item0 + k), true, cp);
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+            if (!((hbits >> k) & 1u)) continue;
+            er += rare_q(x[k], true, cp);
             const u128 El = q_scale_excess(before.E + ((u128)er << 40), nfix) - Eb;
             sHe[hj] = El;
             sHkey[hj] = excess_key(El);
