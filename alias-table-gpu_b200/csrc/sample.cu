@@ -35,7 +35,7 @@ extern "C" wrs_status wrs_alias_sample(const wrs_alias_row* d_table, int64_t n, 
     cudaStream_t stream = static_cast<cudaStream_t>(stream_);
     const DeviceInfo dev = device_info();
     const uint2* table = reinterpret_cast<const uint2*>(d_table);
-    if (mode == WRS_SAMPLE_PLAIN) {
+    if (mode == WRS_SAMPLE_PLAIN || mode == WRS_SAMPLE_HISTOGRAM || mode == WRS_SAMPLE_DISCARD) {
         if (num_samples == 0) return WRS_SUCCESS;
         const uint64_t noct = (num_samples + 7) / 8;
         const uint32_t threads = (opts && opts->threads) ? opts->threads : 256u;
@@ -43,8 +43,15 @@ extern "C" wrs_status wrs_alias_sample(const wrs_alias_row* d_table, int64_t n, 
         uint64_t grid = (noct + threads - 1) / threads;
         const uint64_t cap = (uint64_t)dev.sm_count * 16;
         if (grid > cap) grid = cap;
-        sample_plain_kernel<<<(uint32_t)grid, threads, 0, stream>>>(table, (uint32_t)n, num_samples, seed_k0(seed),
-                                                                   seed_k1(seed), counter_base, d_out);
+        if (mode == WRS_SAMPLE_HISTOGRAM)
+            sample_plain_kernel<1><<<(uint32_t)grid, threads, 0, stream>>>(
+                table, (uint32_t)n, num_samples, seed_k0(seed), seed_k1(seed), counter_base, d_out);
+        else if (mode == WRS_SAMPLE_DISCARD)
+            sample_plain_kernel<2><<<(uint32_t)grid, threads, 0, stream>>>(
+                table, (uint32_t)n, num_samples, seed_k0(seed), seed_k1(seed), counter_base, d_out);
+        else
+            sample_plain_kernel<0><<<(uint32_t)grid, threads, 0, stream>>>(
+                table, (uint32_t)n, num_samples, seed_k0(seed), seed_k1(seed), counter_base, d_out);
     } else if (mode == WRS_SAMPLE_SECTIONED) {
         const uint32_t S = (opts && opts->section_items) ? opts->section_items : kDefaultSection;
         if (S < 2 || (S & 1u)) return WRS_ERR_INVALID_ARGUMENT;

@@ -35,12 +35,16 @@ __device__ __forceinline__ uint2 ld_row_64B(const uint2* p) {
 
 // Plain sampling: each thread handles octets of consecutive output positions (4 Philox
 // blocks, 8 independent gathers in flight, two 16-byte stores).
+// MODE 0 writes sample s at out[s]; MODE 1 counts the samples instead (out[row] += 1 per
+// sample); MODE 2 folds them into out[0] ^= (the XOR of all samples).
+template <int MODE>
 __global__ void __launch_bounds__(256) sample_plain_kernel(const uint2* __restrict__ table, uint32_t n, uint64_t m,
                                                            uint32_t k0, uint32_t k1, uint64_t cbase,
                                                            uint32_t* __restrict__ out) {
     const uint64_t noct = (m + 7) >> 3;
     const uint64_t gsize = (uint64_t)gridDim.x * blockDim.x;
     const bool out_aligned = ((uintptr_t)out & 15u) == 0;
+    uint32_t fold = 0;
     for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < noct; g += gsize) {
         const uint64_t b = cbase + 4 * g;
         uint32_t rows[8], coins[8];
@@ -60,6 +64,25 @@ __global__ void __launch_bounds__(256) sample_plain_kernel(const uint2* __restri
 #pragma unroll
         for (int j = 0; j < 8; ++j) res[j] = alias_pick(v[j], rows[j], coins[j]);
         const uint64_t s0 = 8 * g;
+        if constexpr (MODE == 2) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) fold ^= (s0 + j < m) ? res[j] : 0u;
+            continue;
+        }
+        if constexpr (MODE == 1) {
+            // lanes of the warp that drew the same row add together: one atomic per distinct
+            // row (hot rows of skewed weights would otherwise serialise on one counter)
+            const uint32_t act = __activemask();
+            const int lane = threadIdx.x & 31;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const bool valid = s0 + j < m;
+                const uint32_t key = valid ? res[j] : 0xffffffffu;
+                const uint32_t peers = __match_any_sync(act, key);
+                if (valid && lane == __ffs(peers) - 1) atomicAdd(out + res[j], (uint32_t)__popc(peers));
+            }
+            continue;
+        }
         if (out_aligned && s0 + 8 <= m) {
             uint4* o4 = reinterpret_cast<uint4*>(out + s0);
             __stcs(o4, make_uint4(res[0], res[1], res[2], res[3]));
@@ -68,6 +91,17 @@ __global__ void __launch_bounds__(256) sample_plain_kernel(const uint2* __restri
 #pragma unroll
             for (int j = 0; j < 8; ++j)
                 if (s0 + j < m) out[s0 + j] = res[j];
+        }
+    }
+    if constexpr (MODE == 2) {
+        __shared__ uint32_t s_fold[8];
+        fold = __reduce_xor_sync(0xffffffffu, fold);
+        if ((threadIdx.x & 31) == 0) s_fold[threadIdx.x >> 5] = fold;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t f = 0;
+            for (int i = 0; i < (int)(blockDim.x >> 5); ++i) f ^= s_fold[i];
+            atomicXor(out, f);
         }
     }
 }

@@ -40,6 +40,8 @@ WRS_METHOD_PSA_PLUS = 1
 WRS_FLAG_SYNC = 1
 WRS_SAMPLE_PLAIN = 0
 WRS_SAMPLE_SECTIONED = 1
+WRS_SAMPLE_HISTOGRAM = 2
+WRS_SAMPLE_DISCARD = 3
 
 
 class BuildOpts(ctypes.Structure):
@@ -430,6 +432,11 @@ class Sampler:
         return torch.bincount(out.long(), minlength=self.algorithm.N).cpu().numpy()
 
 
+def alias_histogram(table, n: int, num_samples: int, seed: int, counts, counter_base: int = 0, stream=None) -> int:
+    """Adds the plain samples' per-row counts to `counts` (n int32 on the device)."""
+    return alias_sample(table, n, num_samples, seed, counts, counter_base, mode=WRS_SAMPLE_HISTOGRAM, stream=stream)
+
+
 class SamplerGpuBasic(Sampler):
     def name(self) -> str:
         return "SamplerGpuBasic"
@@ -442,6 +449,15 @@ class SamplerGpuBasic(Sampler):
         _check(alias_sample(a.table, a.N, numSamples, self.seed, out, self.counter), "plain sample")
         self.counter += (numSamples + 1) // 2
         return out
+
+    def getSamplingDistribution(self, numSamples: int) -> np.ndarray:
+        """Per-item counts of numSamples plain samples, counted on the device (no sample list)."""
+        import torch
+        a = self.algorithm
+        counts = torch.zeros(a.N, dtype=torch.int32, device=a.device)
+        _check(alias_histogram(a.table, a.N, numSamples, self.seed, counts, self.counter), "plain histogram")
+        self.counter += (numSamples + 1) // 2
+        return counts.cpu().numpy().astype(np.int64)
 
 
 class SamplerGpuSectioned(Sampler):

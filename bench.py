@@ -331,6 +331,34 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     torch.cuda.synchronize()
     sect_ms = s0.elapsed_time(s1) / reps
 
+    # histogram mode: the same plain samples counted per row instead of written (the
+    # reference's GPU samplers write no samples); the counts are zeroed inside the timed loop
+    counts = torch.empty(n, dtype=torch.int32, device=dev)
+    st = wrs.alias_histogram(table, n, m, SEED_SAMPLES, counts.zero_(), 0, stream=sp)
+    torch.cuda.synchronize()
+    s0.record(stream)
+    for r in range(reps):
+        counts.zero_()
+        st |= wrs.alias_histogram(table, n, m, SEED_SAMPLES, counts, (r + 1) * (m // 2), stream=sp)
+    s1.record(stream)
+    torch.cuda.synchronize()
+    if st:
+        raise wrs.WrsError(st, "histogram")
+    hist_ms = s0.elapsed_time(s1) / reps
+    del counts
+    # discard mode: the same plain samples drawn and folded into one word (the reference's GPU
+    # samplers keep no samples: the like-for-like timing)
+    fold = torch.zeros(1, dtype=torch.int32, device=dev)
+    s0.record(stream)
+    for r in range(reps):
+        st |= wrs.alias_sample(table, n, m, SEED_SAMPLES, fold, (r + 1) * (m // 2), mode=wrs.WRS_SAMPLE_DISCARD,
+                               stream=sp)
+    s1.record(stream)
+    torch.cuda.synchronize()
+    if st:
+        raise wrs.WrsError(st, "discard")
+    discard_ms = s0.elapsed_time(s1) / reps
+
     # goodness of fit of the last timed step's samples (outside every timed region)
     chi2 = chi2_gpu(w, out) if rank == 0 else None
 
@@ -382,6 +410,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                    "sample_ms": round(sample_ms, 4), "sample_gsamples_s": round(m / sample_ms / 1e6, 3),
                    "sectioned_sample_ms": round(sect_ms, 4),
                    "sectioned_gsamples_s": round(m / sect_ms / 1e6, 3),
+                   "histogram_sample_ms": round(hist_ms, 4), "histogram_gsamples_s": round(m / hist_ms / 1e6, 3),
+                   "discard_sample_ms": round(discard_ms, 4), "discard_gsamples_s": round(m / discard_ms / 1e6, 3),
                    "section_items": SECTION_ITEMS},
         "prob_error": err,
         "chi_square": chi2,

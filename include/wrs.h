@@ -94,8 +94,15 @@ typedef struct wrs_build_opts {
 
 typedef enum wrs_sample_mode {
     WRS_SAMPLE_PLAIN = 0,     /* sample s at output position s, any row */
-    WRS_SAMPLE_SECTIONED = 1  /* rows cut into sections; per-section counts from an exact
+    WRS_SAMPLE_SECTIONED = 1, /* rows cut into sections; per-section counts from an exact
                                  binomial tree; output grouped by section */
+    WRS_SAMPLE_HISTOGRAM = 2, /* the PLAIN samples counted instead of written: d_out holds n u32
+                                 counters that the call adds to (the caller zeroes them); the
+                                 reference's samplers write no samples, and its
+                                 getSamplingDistribution returns these counts */
+    WRS_SAMPLE_DISCARD = 3    /* the PLAIN samples drawn and folded into d_out[0] ^= (the XOR of
+                                 all of them): the like-for-like timing of the reference's
+                                 samplers, which keep nothing (SamplerGpuBasic.cu:77-107) */
 } wrs_sample_mode;
 
 typedef struct wrs_sample_opts {

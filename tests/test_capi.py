@@ -79,3 +79,15 @@ def test_argument_checks_before_any_device_work():
     assert L.wrs_rejection_sample(None, None, None, 10, 10, 0, 0, 0, None, None, 0, None) == \
         wrs.WRS_ERR_INVALID_ARGUMENT
     assert L.wrs_scratch_status(None, None) == wrs.WRS_ERR_INVALID_ARGUMENT
+
+
+def test_header_compiles_as_c_and_cxx():
+    # the boundary header must parse for C and C++ callers (FFI binders include it as is)
+    import shutil
+    import subprocess
+    hdr = HEADER
+    for cc, lang in (("gcc", "c"), ("g++", "c++")):
+        if shutil.which(cc) is None:
+            continue
+        r = subprocess.run([cc, "-fsyntax-only", "-Wall", "-x", lang, hdr], capture_output=True, text=True)
+        assert r.returncode == 0, f"{cc}: {r.stderr}"

@@ -91,3 +91,30 @@ def test_sample_to_host_bit_exact(tables, m, chunk, cbase):
         assert st == 0
         torch.cuda.current_stream().synchronize()
         np.testing.assert_array_equal(host.numpy().view(np.uint32), po.sample_plain(rows, m, SEED, c))
+
+
+@pytest.mark.parametrize("m,cbase", [(1, 0), (1001, 7), ((1 << 20) + 5, 99)])
+def test_histogram_mode_counts_plain_samples(tables, m, cbase):
+    # the counts of the histogram mode are the bin counts of the plain sampler's output
+    w, rows = tables["powerlaw_shuffled"]
+    n = rows.shape[0]
+    table = torch.from_numpy(np.ascontiguousarray(rows).view(np.int64).reshape(-1)).cuda()
+    counts = torch.zeros(n, dtype=torch.int32, device="cuda")
+    assert wrs.alias_histogram(table, n, m, SEED, counts, cbase) == 0
+    torch.cuda.synchronize()
+    ref = np.bincount(po.sample_plain(rows, m, SEED, cbase), minlength=n)
+    np.testing.assert_array_equal(counts.cpu().numpy(), ref)
+
+
+@pytest.mark.parametrize("m,cbase", [(1, 0), (1001, 7), ((1 << 20) + 5, 99)])
+def test_discard_mode_folds_plain_samples(tables, m, cbase):
+    # the discard mode draws the plain samples and keeps only their XOR (folded into out[0])
+    w, rows = tables["uniform"]
+    n = rows.shape[0]
+    table = torch.from_numpy(np.ascontiguousarray(rows).view(np.int64).reshape(-1)).cuda()
+    out = torch.full((2,), 0x1234, dtype=torch.int32, device="cuda")
+    assert wrs.alias_sample(table, n, m, SEED, out[:1], cbase, mode=wrs.WRS_SAMPLE_DISCARD) == 0
+    torch.cuda.synchronize()
+    ref = np.bitwise_xor.reduce(po.sample_plain(rows, m, SEED, cbase).astype(np.uint32)) ^ np.uint32(0x1234)
+    got = out.cpu().numpy().view(np.uint32)
+    assert got[0] == ref and got[1] == 0x1234
