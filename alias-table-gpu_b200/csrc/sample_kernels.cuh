@@ -32,6 +32,17 @@ __device__ __forceinline__ uint2 ld_row_64B(const uint2* p) {
     asm("ld.global.nc.L2::64B.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "l"(p));
     return v;
 }
+// The same for the rejection sampler's random slot and acceptance gathers.
+__device__ __forceinline__ uint32_t ld_u32_64B(const uint32_t* p) {
+    uint32_t v;
+    asm("ld.global.nc.L2::64B.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ float ld_f32_64B(const float* p) {
+    float v;
+    asm("ld.global.nc.L2::64B.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
 
 // Plain sampling: each thread handles octets of consecutive output positions (4 Philox
 // blocks, 8 independent gathers in flight, two 16-byte stores).
@@ -223,9 +234,9 @@ __global__ void __launch_bounds__(256) rejection_sample_kernel(const uint32_t* _
         for (uint32_t t = 0; t < max_tries; ++t) {
             if ((t & 1u) == 0) r = philox4x32_10((uint32_t)b, (uint32_t)(b >> 32), t >> 1, 0x52454a00u, k0, k1);
             const uint32_t xs = r.x[(t & 1u) * 2], xc = r.x[(t & 1u) * 2 + 1];
-            const uint32_t e = __ldg(A + scale_u32(xs, asz));
+            const uint32_t e = ld_u32_64B(A + scale_u32(xs, asz));
             const uint32_t item = e & 0x7fffffffu;
-            if ((e >> 31) == 0u || coin24(xc) < __ldg(frac + item)) {
+            if ((e >> 31) == 0u || coin24(xc) < ld_f32_64B(frac + item)) {
                 res = item;
                 break;
             }

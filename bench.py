@@ -358,6 +358,32 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     if st:
         raise wrs.WrsError(st, "discard")
     discard_ms = s0.elapsed_time(s1) / reps
+    # rejection sampling on the same weights (build: W, slot counts, slot fill; then samples)
+    A = torch.empty(2 * n, dtype=torch.int32, device=dev)
+    frac = torch.empty(n, dtype=torch.float32, device=dev)
+    a_size = torch.zeros(1, dtype=torch.int64, device=dev)
+    rscr = torch.empty(wrs.rejection_build_scratch_bytes(n), dtype=torch.uint8, device=dev)
+    rstat = torch.zeros(1, dtype=torch.int32, device=dev)
+    st = wrs.rejection_build(w, A, frac, a_size, rscr, sync=True, stream=sp)
+    rm = min(m, 1 << 28)
+    st |= wrs.rejection_sample(A, a_size, frac, n, rm, SEED_SAMPLES, out, 0, 0, rstat, stream=sp)
+    torch.cuda.synchronize()
+    s0.record(stream)
+    for r in range(reps):
+        st |= wrs.rejection_build(w, A, frac, a_size, rscr, stream=sp)
+    s1.record(stream)
+    torch.cuda.synchronize()
+    rej_build_ms = s0.elapsed_time(s1) / reps
+    s0.record(stream)
+    for r in range(reps):
+        st |= wrs.rejection_sample(A, a_size, frac, n, rm, SEED_SAMPLES, out, (r + 1) * rm, 0, rstat, stream=sp)
+    s1.record(stream)
+    torch.cuda.synchronize()
+    rej_sample_ms = s0.elapsed_time(s1) / reps
+    if st or int(rstat.item()) or wrs.scratch_status(rscr, sp):
+        raise wrs.WrsError(st or int(rstat.item()) or 1, "rejection")
+    rej_slots = int(a_size.item())
+    del A, frac, rscr
 
     # goodness of fit of the last timed step's samples (outside every timed region)
     chi2 = chi2_gpu(w, out) if rank == 0 else None
@@ -412,6 +438,10 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                    "sectioned_gsamples_s": round(m / sect_ms / 1e6, 3),
                    "histogram_sample_ms": round(hist_ms, 4), "histogram_gsamples_s": round(m / hist_ms / 1e6, 3),
                    "discard_sample_ms": round(discard_ms, 4), "discard_gsamples_s": round(m / discard_ms / 1e6, 3),
+                   "rejection_build_ms": round(rej_build_ms, 4), "rejection_slots": rej_slots,
+                   "rejection_build_gitems_s": round(n / rej_build_ms / 1e6, 3),
+                   "rejection_samples": rm, "rejection_sample_ms": round(rej_sample_ms, 4),
+                   "rejection_gsamples_s": round(rm / rej_sample_ms / 1e6, 3),
                    "section_items": SECTION_ITEMS},
         "prob_error": err,
         "chi_square": chi2,
