@@ -103,7 +103,8 @@ struct __align__(16) BuildHeader {
     float Hh;
     uint32_t pad0;
     int64_t nfix;       // excess correction, set with the tile prefixes
-    uint64_t pad[5];
+    uint64_t huge_count; // rejection: number of deferred items filled by the whole grid
+    uint64_t pad[4];
 };
 static_assert(sizeof(BuildHeader) == 128, "header layout");
 

@@ -221,10 +221,12 @@ __global__ void __launch_bounds__(kBuildThreads) rejection_tile_kernel(
     }
 }
 
-// Deferred items: warp per item up to kRejHugeSlots slots, whole grid for larger ones.
-__global__ void __launch_bounds__(256) rejection_big_kernel(const BuildHeader* hdr, const RejBigEntry* big_list,
+// Deferred items: a warp per item up to kRejHugeSlots slots; larger ones go to the huge list
+// (their index in the deferred list) for rejection_huge_kernel.
+__global__ void __launch_bounds__(256) rejection_big_kernel(BuildHeader* hdr, const RejBigEntry* big_list,
                                                             uint64_t big_capacity, uint32_t* __restrict__ A,
-                                                            uint64_t a_capacity) {
+                                                            uint64_t a_capacity, uint32_t* huge_idx,
+                                                            uint64_t huge_capacity) {
     const uint64_t cnt_raw = hdr->big_count;
     const uint64_t cnt = cnt_raw < big_capacity ? cnt_raw : big_capacity;
     if (cnt == 0) return;
@@ -233,20 +235,37 @@ __global__ void __launch_bounds__(256) rejection_big_kernel(const BuildHeader* h
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t e = warp_g; e < cnt; e += nwarps) {
         const RejBigEntry be = big_list[e];
-        if (be.count > kRejHugeSlots) continue;
+        if (be.count > kRejHugeSlots) {
+            if (lane == 0) {
+                const uint64_t h = atomicAdd((unsigned long long*)&hdr->huge_count, 1ull);
+                if (h < huge_capacity) huge_idx[h] = (uint32_t)e;
+            }
+            continue;
+        }
         for (uint32_t i = lane; i < be.count; i += 32) {
             const uint64_t slot = be.start + i;
             if (slot < a_capacity) A[slot] = be.item | (i == 0 ? 0x80000000u : 0u);
         }
     }
-    const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint64_t gsize = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t e = 0; e < cnt; ++e) {
-        const RejBigEntry be = big_list[e];
-        if (be.count <= kRejHugeSlots) continue;
-        for (uint64_t i = gtid; i < be.count; i += gsize) {
-            const uint64_t slot = be.start + i;
-            if (slot < a_capacity) A[slot] = be.item | (i == 0 ? 0x80000000u : 0u);
+}
+
+// The huge deferred items (more than kRejHugeSlots slots each, at most 2n / kRejHugeSlots of
+// them): each item's slots in chunks of kRejChunk, block b taking chunks b, b + gridDim.x, ...
+constexpr uint32_t kRejChunk = 4096;
+__global__ void __launch_bounds__(256) rejection_huge_kernel(const BuildHeader* hdr, const RejBigEntry* big_list,
+                                                             const uint32_t* huge_idx, uint64_t huge_capacity,
+                                                             uint32_t* __restrict__ A, uint64_t a_capacity) {
+    const uint64_t cnt_raw = hdr->huge_count;
+    const uint64_t cnt = cnt_raw < huge_capacity ? cnt_raw : huge_capacity;
+    for (uint64_t h = 0; h < cnt; ++h) {
+        const RejBigEntry be = big_list[huge_idx[h]];
+        const uint32_t chunks = (be.count + kRejChunk - 1) / kRejChunk;
+        for (uint32_t c = blockIdx.x; c < chunks; c += gridDim.x) {
+            const uint32_t j1 = min(be.count, (c + 1) * kRejChunk);
+            for (uint32_t j = c * kRejChunk + threadIdx.x; j < j1; j += blockDim.x) {
+                const uint64_t slot = be.start + j;
+                if (slot < a_capacity) A[slot] = be.item | (j == 0 ? 0x80000000u : 0u);
+            }
         }
     }
 }

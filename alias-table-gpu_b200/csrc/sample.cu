@@ -144,6 +144,8 @@ struct RejLayout {
     uint64_t* tile_words;
     RejBigEntry* big;
     uint64_t big_capacity;
+    uint32_t* huge;
+    uint64_t huge_capacity;
     size_t bytes;
 };
 constexpr int kRejIpt = 8;
@@ -157,6 +159,8 @@ RejLayout carve_rej(void* scratch, uint64_t n) {
     L.tile_words = c.take<uint64_t>(nt);
     L.big_capacity = (2 * n) / kRejBig + 16;
     L.big = c.take<RejBigEntry>(L.big_capacity);
+    L.huge_capacity = (2 * n) / kRejHugeSlots + 16;
+    L.huge = c.take<uint32_t>(L.huge_capacity);
     L.bytes = c.off;
     return L;
 }
@@ -182,7 +186,10 @@ extern "C" wrs_status wrs_rejection_build_f32(const float* d_w, int64_t n, uint3
     rejection_tile_kernel<kRejIpt><<<(uint32_t)nt, kBuildThreads, 0, stream>>>(
         d_w, (uint64_t)n, L.hdr, L.tile_words, (uint32_t)nt, d_A, a_capacity, d_frac, L.big, L.big_capacity, d_A_size);
     const DeviceInfo dev = device_info();
-    rejection_big_kernel<<<(uint32_t)dev.sm_count * 4, 256, 0, stream>>>(L.hdr, L.big, L.big_capacity, d_A, a_capacity);
+    rejection_big_kernel<<<(uint32_t)dev.sm_count * 4, 256, 0, stream>>>(L.hdr, L.big, L.big_capacity, d_A, a_capacity,
+                                                                      L.huge, L.huge_capacity);
+    rejection_huge_kernel<<<(uint32_t)dev.sm_count * 4, 256, 0, stream>>>(L.hdr, L.big, L.huge, L.huge_capacity, d_A,
+                                                                       a_capacity);
     const wrs_status st = launch_status();
     if (st != WRS_SUCCESS) return st;
     if (flags & WRS_FLAG_SYNC) return read_device_status(&L.hdr->status, stream);

@@ -34,7 +34,15 @@ def big_items(n):
     return w
 
 
-@pytest.mark.parametrize("maker", [lambda: gen("uniform", 1000), lambda: gen("pareto", 100_003),
+def many_huge_items(n):
+    # several items of more than 2^16 slots (chunked over the grid) and of 2^16 or fewer
+    w = np.random.default_rng(6).random(n, dtype=np.float32)
+    for k, v in enumerate([4e5, 2e5, 1.5e5, 9e4, 7e4, 2e4, 5e3]):
+        w[(k * 7919) % n] = v
+    return w
+
+
+@pytest.mark.parametrize("maker", [lambda: gen("uniform", 1000), lambda: many_huge_items(500_000), lambda: gen("pareto", 100_003),
                                    lambda: gen("zeros_mix", 50_000), lambda: gen("powerlaw_shuffled", 1 << 20),
                                    lambda: big_items(300_000), lambda: np.ones(1, np.float32)])
 def test_rejection_build_bit_exact(cuda, maker):
