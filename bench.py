@@ -50,6 +50,11 @@ FALLBACK_HBM_GBS = 6650.0
 # kernels one step launches: wsum, tile_reduce, tile_prefix, heavy_list, tile_link, split_pack
 # (the build) and sample_plain
 KERNELS_PER_STEP = 7
+# kernels one replay of the batched graph launches when the batch has both one-warp tables
+# and tiled tables: plan_count, plan_scan, plan_fill, batch_wsum, tile_reduce, batch_prefix,
+# heavy_list, tile_link, split_pack, batch_status, small_tables (the build) and batch_sample;
+# a mixed batch with rejection tables adds one or two rejection kernels
+BATCHED_KERNELS_PER_REPLAY = 12
 BATCH_TABLES = 1 << 17
 BATCH_SAMPLES_PER_TABLE = 64
 BATCH_PER_TABLE_SAMPLE = 4096  # tables timed one call at a time (the per-table baseline)
@@ -661,7 +666,8 @@ def run_batched_only(args, rank: int, local_rank: int):
             "steps": 20, "warmup": 3, "ms_per_step": b["batched_ms"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": b["workload"], "items": b["items"], "samples": b["samples"]},
-            "batched": b, "gpu_launches": None,
+            "batched": b,
+            "gpu_launches": (BATCHED_KERNELS_PER_REPLAY + (2 if b.get("mixed", {}).get("rejection_tables") else 0)) * 20,
             "e2e": None, "note": f"{items_samples} items+samples per graph replay"}
 
 
