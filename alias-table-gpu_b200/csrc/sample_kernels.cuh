@@ -127,8 +127,11 @@ __global__ void __launch_bounds__(256) sample_plain_kernel(const uint2* __restri
 // consecutive Philox blocks at a time (eight gathers in flight).
 constexpr int kSectThreads = 512;
 
+// The staged form runs two CTAs per SM (at most 64 registers: the once-per-section binomial
+// walk may spill, the sampling loop does not); the L2 form one CTA per SM, so that the
+// sections in flight stay in L2.
 template <bool STAGE>
-__global__ void __launch_bounds__(kSectThreads) sample_sectioned_kernel(const uint2* __restrict__ table, uint32_t n,
+__global__ void __launch_bounds__(kSectThreads, STAGE ? 2 : 1) sample_sectioned_kernel(const uint2* __restrict__ table, uint32_t n,
                                                                         uint64_t m, uint32_t S, uint32_t K,
                                                                         uint32_t k0, uint32_t k1, uint64_t cbase,
                                                                         uint32_t* __restrict__ out,
