@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "batched_kernels.cuh"
@@ -18,6 +19,23 @@ namespace wrs {
 namespace {
 
 constexpr uint32_t kDefaultSmall = 128;
+
+// The library's side stream of the current device (created on first use): the one-warp
+// tables of a batch are built there while `stream` runs the tiled passes.
+constexpr int kMaxDevices = 64;
+std::mutex g_side_mu;
+cudaStream_t g_side[kMaxDevices] = {};
+wrs_status side_stream(cudaStream_t* out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return WRS_ERR_CUDA;
+    std::lock_guard<std::mutex> lock(g_side_mu);
+    if (!g_side[dev] && cudaStreamCreateWithFlags(&g_side[dev], cudaStreamNonBlocking) != cudaSuccess) {
+        g_side[dev] = nullptr;
+        return WRS_ERR_CUDA;
+    }
+    *out = g_side[dev];
+    return WRS_SUCCESS;
+}
 const uint32_t kSmallChoices[] = {32, 64, 128, 256, 512};
 const uint32_t kTileChoices[] = {1024, 2048, 4096};
 
@@ -218,8 +236,25 @@ wrs_status batched_build(const float* d_w, const int64_t* d_offsets, const int64
     if (cudaMemsetAsync(L.hdr0, 0, sizeof(BuildHeader) * (2 + (size_t)p.big_tables), stream) != cudaSuccess)
         return WRS_ERR_CUDA;
     wrs_status st = WRS_SUCCESS;
+    // the one-warp tables and the tiled tables are independent: with both present the former
+    // run on the side stream, forked from `stream` and joined back into it by events (which a
+    // stream capture records as a fork and a join)
+    cudaStream_t small_stream = stream;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    const bool fork = p.small_tables > 0 && p.big_tables > 0;
+    if (fork) {
+        if (side_stream(&small_stream) != WRS_SUCCESS ||
+            cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventRecord(ev_fork, stream) != cudaSuccess || cudaStreamWaitEvent(small_stream, ev_fork, 0) != cudaSuccess) {
+            if (ev_fork) cudaEventDestroy(ev_fork);
+            if (ev_join) cudaEventDestroy(ev_join);
+            return WRS_ERR_CUDA;
+        }
+    }
     if (p.small_tables > 0) {
         uint32_t* status = &L.hdr0->status;
+        const cudaStream_t stream = small_stream;  // the launches below
         switch (sh.small_max) {
             case 32: st = launch_small<1>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p.small_tables, stream); break;
             case 64: st = launch_small<2>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p.small_tables, stream); break;
@@ -227,16 +262,22 @@ wrs_status batched_build(const float* d_w, const int64_t* d_offsets, const int64
             case 256: st = launch_small<8>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p.small_tables, stream); break;
             default: st = launch_small<16>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p.small_tables, stream); break;
         }
-        if (st != WRS_SUCCESS) return st;
     }
-    if (p.big_tables > 0) {
+    if (st == WRS_SUCCESS && p.big_tables > 0) {
         switch (sh.tile) {
             case 1024: st = launch_big<1024>(d_w, d_offsets, d_kinds, num_tables, sh.small_max, d_table, d_W, L, p, stream); break;
             case 4096: st = launch_big<4096>(d_w, d_offsets, d_kinds, num_tables, sh.small_max, d_table, d_W, L, p, stream); break;
             default: st = launch_big<2048>(d_w, d_offsets, d_kinds, num_tables, sh.small_max, d_table, d_W, L, p, stream); break;
         }
-        if (st != WRS_SUCCESS) return st;
     }
+    if (fork) {  // joined whatever happened above, so that a capture stays well formed
+        if ((cudaEventRecord(ev_join, small_stream) != cudaSuccess ||
+             cudaStreamWaitEvent(stream, ev_join, 0) != cudaSuccess) && st == WRS_SUCCESS)
+            st = WRS_ERR_CUDA;
+        cudaEventDestroy(ev_fork);
+        cudaEventDestroy(ev_join);
+    }
+    if (st != WRS_SUCCESS) return st;
     if (rej && (p.rej_warp_tables > 0 || p.rej_block_tables > 0))
         st = launch_rejection(d_w, d_offsets, d_kinds, num_tables, p, *rej, d_W, &L.hdr0->status, stream);
     return st;
