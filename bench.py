@@ -500,7 +500,7 @@ def batch_config5():
                                     (np.arange(1_000_000, 1_000_004), sizes > 64)]
 
 
-def batched_phase(dev, make=batch_config4, mixed: bool = False) -> dict:
+def batched_phase(dev, make=batch_config4, mixed: bool = False, shape: str = "") -> dict:
     """A batched-tables configuration: the batched build and sample (autotuned launch shape,
     captured in one CUDA graph) against the plain single-table entry points called once per
     table, timed on samples of each size class and scaled to all tables of the class by count
@@ -524,10 +524,14 @@ def batched_phase(dev, make=batch_config4, mixed: bool = False) -> dict:
     total = int(soff[-1])
     d_soff = torch.from_numpy(soff).to(dev)
     out = torch.empty(total, dtype=torch.int32, device=dev)
-    opts = wrs.build_opts()
-    st = wrs.batched_autotune(w, d_off, off, table, scratch, opts)
-    if st:
-        raise wrs.WrsError(st, "batched autotune")
+    if shape:
+        small, tile = (int(x) for x in shape.split(","))
+        opts = wrs.build_opts(0, tile, False, small)
+    else:
+        opts = wrs.build_opts()
+        st = wrs.batched_autotune(w, d_off, off, table, scratch, opts)
+        if st:
+            raise wrs.WrsError(st, "batched autotune")
     # the batch's rows equal single-table builds of the same weights (a sample of tables,
     # the largest ones included; the tests check every table against the oracle)
     st = wrs.batched_build(w, d_off, off, table, scratch, wrs.build_opts(0, opts.tile_items, True,
@@ -654,13 +658,41 @@ def batched_phase(dev, make=batch_config4, mixed: bool = False) -> dict:
     }
 
 
+def batched_once(args, dev) -> dict:
+    """One batched build and one batched sampling call of configuration 4 or 5 with a fixed
+    launch shape (alias tables only), for profiler captures."""
+    import torch
+    import wrs
+    sizes, w_np, counts, what, _ = (batch_config5 if args.config == "5" else batch_config4)()
+    nt = sizes.size
+    off = np.zeros(nt + 1, dtype=np.int64)
+    np.cumsum(sizes, out=off[1:])
+    soff = np.zeros(nt + 1, dtype=np.int64)
+    np.cumsum(counts, out=soff[1:])
+    small, tile = (int(x) for x in (args.shape or "128,1024").split(","))
+    opts = wrs.build_opts(0, tile, True, small)
+    w = torch.from_numpy(w_np).to(dev)
+    d_off, d_soff = torch.from_numpy(off).to(dev), torch.from_numpy(soff).to(dev)
+    table = torch.empty(int(off[-1]), dtype=torch.int64, device=dev)
+    out = torch.empty(int(soff[-1]), dtype=torch.int32, device=dev)
+    scratch = torch.empty(wrs.batched_build_scratch_bytes(off, opts), dtype=torch.uint8, device=dev)
+    st = wrs.batched_build(w, d_off, off, table, scratch, opts)
+    st = st or wrs.batched_sample(table, d_off, nt, d_soff, int(soff[-1]), SEED_SAMPLES, out, 0)
+    torch.cuda.synchronize()
+    if st:
+        raise wrs.WrsError(st, "batched once")
+    return {"workload": what, "shape": [small, tile], "items": int(off[-1]), "samples": int(soff[-1])}
+
+
 def run_batched_only(args, rank: int, local_rank: int):
     import torch
     if rank != 0:
         return None
     torch.cuda.set_device(local_rank)
+    if args.once:
+        return {"once": batched_once(args, torch.device("cuda", local_rank))}
     b = batched_phase(torch.device("cuda", local_rank), batch_config5 if args.config == "5" else batch_config4,
-                      mixed=args.config == "5")
+                      mixed=args.config == "5", shape=args.shape)
     items_samples = b["items"] + b["samples"]
     return {"metric": METRIC, "value": b["batched_g_items_plus_samples_s"], "unit": UNIT, "n_gpus": 1,
             "steps": 20, "warmup": 3, "ms_per_step": b["batched_ms"], "higher_is_better": True, "scaling": "weak",
@@ -752,6 +784,10 @@ def main():
     ap.add_argument("--config", default="2", choices=sorted(CONFIGS) + ["4", "5"],
                     help="BASELINE configuration: 2 (default, headline; includes the batched phase), 1, 3, "
                          "or 4 / 5 (batched tables only)")
+    ap.add_argument("--shape", default="",
+                    help="batched configurations: small_table_items,tile_items instead of the autotuner's")
+    ap.add_argument("--once", action="store_true",
+                    help="batched configurations: one build and one sampling call, no timing (profiler captures)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
