@@ -44,8 +44,11 @@ __global__ void __launch_bounds__(kBuildThreads) rejection_tile_kernel(
     constexpr int T = kBuildThreads * IPT;
     __shared__ uint32_t s_tile;
     __shared__ int s_abort;
-    __shared__ uint32_t s_small_incl[T];   // inclusive prefix of small-item slot counts
-    __shared__ uint32_t s_off[T];          // exclusive prefix of all slot counts (tile-local)
+    // inclusive prefix of small-item slot counts | exclusive prefix of all slot counts (tile-
+    // local); in the staged form the tile's slots themselves
+    __shared__ uint32_t s_buf[2 * T];
+    uint32_t* s_small_incl = s_buf;
+    uint32_t* s_off = s_buf + T;
     __shared__ uint64_t s_warp64[kBuildThreads / 32 + 1];
     __shared__ uint32_t s_warp32[kBuildThreads / 32 + 1];
     __shared__ uint64_t s_base;
@@ -170,6 +173,23 @@ __global__ void __launch_bounds__(kBuildThreads) rejection_tile_kernel(
                 if (asz > a_capacity) record_status(&hdr->status, kErrCapacity);
             }
         }
+    }
+    // a tile without deferred items and with at most 2T slots is staged: each thread writes its
+    // items' slots at their tile offsets, then the tile's slots go out with coalesced stores
+    const bool staged = tile_total <= (uint64_t)(2 * T) && (uint64_t)small_total == tile_total;
+    if (staged) {
+        uint32_t o = (uint32_t)ex64;
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+            const uint32_t item = (uint32_t)(item0 + k);
+            for (uint32_t j = 0; j < cs[k]; ++j) s_buf[o + j] = item | (j == 0 ? 0x80000000u : 0u);
+            o += cs[k];
+        }
+        __syncthreads();
+        const uint64_t base = s_base;
+        for (uint32_t q = threadIdx.x; q < (uint32_t)tile_total; q += kBuildThreads)
+            if (base + q < a_capacity) A[base + q] = s_buf[q];
+        return;
     }
     // per-item offsets and the small-slot prefix into shared memory
     {
