@@ -254,13 +254,13 @@ wrs_status batched_build(const float* d_w, const int64_t* d_offsets, const int64
     }
     if (p.small_tables > 0) {
         uint32_t* status = &L.hdr0->status;
-        const cudaStream_t stream = small_stream;  // the launches below
+        const cudaStream_t ss = small_stream;
         switch (sh.small_max) {
-            case 32: st = launch_small<1>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p.small_tables, stream); break;
-            case 64: st = launch_small<2>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p.small_tables, stream); break;
-            case 128: st = launch_small<4>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p.small_tables, stream); break;
-            case 256: st = launch_small<8>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p.small_tables, stream); break;
-            default: st = launch_small<16>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p.small_tables, stream); break;
+            case 32: st = launch_small<1>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p.small_tables, ss); break;
+            case 64: st = launch_small<2>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p.small_tables, ss); break;
+            case 128: st = launch_small<4>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p.small_tables, ss); break;
+            case 256: st = launch_small<8>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p.small_tables, ss); break;
+            default: st = launch_small<16>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p.small_tables, ss); break;
         }
     }
     if (st == WRS_SUCCESS && p.big_tables > 0) {
