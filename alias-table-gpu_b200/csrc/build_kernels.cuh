@@ -1394,18 +1394,22 @@ __global__ void __launch_bounds__(NT, (NT == 256 && IPT == 8) ? 4 : 1) split_pac
         __syncthreads();  // every range known; from here a thread touches only its own keys
         const uint32_t a_end = (tid + 1 < NT) ? s_wa[tid + 1] : m_w;
         uint64_t hk = a < a_end ? sWk[a] : ~0ull;
+        uint32_t cur = a < m_w ? sWi[a] : last_heavy;  // the first heavy left: the lights' alias
         uint64_t sr = ex.a, D = D0, lr = ex.b;
 #pragma unroll
         for (int k = 0; k < IPT; ++k) {
             const bool light = (lbits >> k) & 1u;
             if (light) {
                 const uint64_t key = sr + D;
-                while (hk <= key) {  // heavy a ranks at this light
-                    sWk[a] = key;
-                    ++a;
-                    hk = a < a_end ? sWk[a] : ~0ull;
+                if (hk <= key) {
+                    do {  // heavy a ranks at this light
+                        sWk[a] = key;
+                        ++a;
+                        hk = a < a_end ? sWk[a] : ~0ull;
+                    } while (hk <= key);
+                    cur = a < m_w ? sWi[a] : last_heavy;
                 }
-                al[k] = a < m_w ? sWi[a] : last_heavy;
+                al[k] = cur;
             }
             if (LEFT) {
                 sr += light ? ls[tid * IPT + k].lo : 0ull;

@@ -390,6 +390,20 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     rej_slots = int(a_size.item())
     del A, frac, rscr
 
+    # the random-access bound of the plain sampler: a library gather (torch index_select) of
+    # random 8-byte rows from the same table, with precomputed uniform row indices
+    g_n = 1 << 27
+    gidx = torch.randint(0, n, (g_n,), dtype=torch.int64, device=dev)
+    gout = torch.index_select(table, 0, gidx)
+    torch.cuda.synchronize()
+    s0.record(stream)
+    for r in range(reps):
+        torch.index_select(table, 0, gidx, out=gout)
+    s1.record(stream)
+    torch.cuda.synchronize()
+    gather_ms = s0.elapsed_time(s1) / reps
+    del gidx, gout
+
     # goodness of fit of the last timed step's samples (outside every timed region)
     chi2 = chi2_gpu(w, out) if rank == 0 else None
 
@@ -470,7 +484,12 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "roofline": {"kernel": "sample_plain_kernel", "bound": "hbm", "achieved": round(achieved, 1),
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "traffic": ncu_traffic() if args.config == "2" else None,
-                     "algorithmic_bytes": "12 B/sample x 2^30 samples per launch (8 B row gather + 4 B write)"},
+                     "algorithmic_bytes": "12 B/sample x 2^30 samples per launch (8 B row gather + 4 B write)",
+                     "random_access_bound": {
+                         "probe": "torch index_select of 2^27 random 8-byte rows of the same table (index read "
+                                  "and row write included)",
+                         "gathers_per_s_g": round(g_n / gather_ms / 1e6, 2),
+                         "sampler_over_probe": round((m / sample_ms) / (g_n / gather_ms), 3)}},
         "cpu_baseline": cpu,
         "clocks": clk,
         "e2e": {"value": round(replica_value(n + m, e2e_ms, world), 4), "unit": UNIT,
