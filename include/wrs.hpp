@@ -13,6 +13,9 @@
  *   SamplerGpuBasic, SamplerGpuSectioned, SamplerRejection
  *                       <- sampling/aliasTable/SamplerGpuBasic.cuh, SamplerGpuSectioned.cuh,
  *                          sampling/rejectionSampling/SamplerRejection.cuh
+ *   BatchedAliasTablesGpu, SamplerBatched
+ *                       <- a loop of AliasTableSplitGpu / SamplerGpuBasic objects, one per table
+ *                          (the reference has no batched form)
  *
  * Differences, as in the C ABI: weights are FP32 (the reference holds FP64 host weights), the
  * table rows are {float prob, uint32 alias} on the device, and samples are a function of
@@ -310,6 +313,101 @@ protected:
     int64_t items() const override { return r_.N; }
     RejectionSamplingGpu& r_;
     uint32_t tries_;
+};
+
+// ---------------------------------------------------------------- batches
+
+// Many alias tables at once (CSR offsets into one weight array): the batched form of
+// AliasTableSplitGpu (the reference builds one object per table). autotune() picks the
+// launch shape on this batch; the table's rows land at their items with table-local aliases.
+class BatchedAliasTablesGpu {
+public:
+    BatchedAliasTablesGpu(std::vector<float> w, std::vector<int64_t> offsets, cudaStream_t stream = nullptr)
+        : weights(std::move(w)), offsets(std::move(offsets)), stream_(stream) {
+        opts_.method = WRS_METHOD_SPLIT;
+        opts_.tile_items = 0;
+        opts_.flags = 0;
+        opts_.small_table_items = 0;
+    }
+    std::string name() { return "BatchedAliasTablesGpu"; }
+    int64_t numTables() const { return (int64_t)offsets.size() - 1; }
+    void preBuild() {
+        w_dev_.resize(weights.size());
+        if (!weights.empty())
+            check_cuda(cudaMemcpyAsync(w_dev_.get(), weights.data(), w_dev_.bytes(), cudaMemcpyHostToDevice, stream_),
+                       "weights upload");
+        off_dev_.resize(offsets.size());
+        check_cuda(cudaMemcpyAsync(off_dev_.get(), offsets.data(), off_dev_.bytes(), cudaMemcpyHostToDevice, stream_),
+                   "offsets upload");
+        table_.resize(weights.empty() ? 1 : weights.size());
+        W_dev_.resize((size_t)numTables());
+        scratch_.resize(wrs_batched_build_scratch_bytes(offsets.data(), numTables(), nullptr));
+    }
+    void autotune() {
+        check(wrs_batched_autotune(w_dev_.get(), off_dev_.get(), offsets.data(), numTables(), table_.get(),
+                                   scratch_.get(), scratch_.bytes(), &opts_, stream_), "batched autotune");
+    }
+    void build() {
+        check(wrs_batched_build_f32(w_dev_.get(), off_dev_.get(), offsets.data(), numTables(), &opts_, table_.get(),
+                                    W_dev_.get(), scratch_.get(), scratch_.bytes(), stream_), "batched build");
+    }
+    bool postBuild() {
+        check(wrs_scratch_status(scratch_.get(), stream_), "batched build (device)");
+        W = W_dev_.to_host(stream_);
+        return true;
+    }
+    bool fullBuild() {
+        preBuild();
+        build();
+        return postBuild();
+    }
+    const wrs_alias_row* deviceTable() const { return table_.get(); }
+    const int64_t* deviceOffsets() const { return off_dev_.get(); }
+    std::vector<wrs_alias_row> hostTable() const { return table_.to_host(stream_); }
+    cudaStream_t stream() const { return stream_; }
+
+    std::vector<float> weights;
+    std::vector<int64_t> offsets;
+    std::vector<double> W;  // per-table weight totals
+
+private:
+    cudaStream_t stream_;
+    wrs_build_opts opts_{};
+    DeviceArray<float> w_dev_;
+    DeviceArray<int64_t> off_dev_;
+    DeviceArray<wrs_alias_row> table_;
+    DeviceArray<double> W_dev_;
+    DeviceArray<unsigned char> scratch_;
+};
+
+// Per-table sample counts over a batch: table t's table-local samples at
+// [sampleOffsets[t], sampleOffsets[t + 1]) of the output.
+class SamplerBatched {
+public:
+    explicit SamplerBatched(BatchedAliasTablesGpu& b, uint64_t seed = 0x5EED) : b_(b), seed_(seed) {}
+    std::string name() { return "SamplerBatched"; }
+    // counts (host, one per table) -> samples (host); sampleOffsets receives the CSR offsets
+    std::vector<uint32_t> sample(const std::vector<int64_t>& counts, std::vector<int64_t>* sampleOffsets = nullptr) {
+        std::vector<int64_t> soff(counts.size() + 1, 0);
+        for (size_t t = 0; t < counts.size(); ++t) soff[t + 1] = soff[t] + counts[t];
+        const uint64_t total = (uint64_t)soff.back();
+        DeviceArray<int64_t> d_soff(soff.size());
+        check_cuda(cudaMemcpyAsync(d_soff.get(), soff.data(), d_soff.bytes(), cudaMemcpyHostToDevice, b_.stream()),
+                   "sample offsets upload");
+        DeviceArray<uint32_t> out(total ? total : 1);
+        check(wrs_batched_sample(b_.deviceTable(), b_.deviceOffsets(), b_.numTables(), d_soff.get(), total, seed_,
+                                 counter, out.get(), b_.stream()), "batched sample");
+        counter += (total + 1) / 2;
+        std::vector<uint32_t> h = out.to_host(b_.stream());
+        h.resize(total);
+        if (sampleOffsets) *sampleOffsets = soff;
+        return h;
+    }
+    uint64_t counter = 0;
+
+private:
+    BatchedAliasTablesGpu& b_;
+    uint64_t seed_;
 };
 
 }  // namespace wrs

@@ -53,6 +53,14 @@ int main(int argc, char** argv) {
         rs.sample(m, d.get());
         write_file(out + "_rej.bin", d.to_host());
 
+        // the same weights cut into three tables, built as a batch and sampled 1000 times each
+        const int64_t n = (int64_t)w.size();
+        wrs::BatchedAliasTablesGpu batch(w, {0, n / 3, n / 2, n});
+        if (!batch.fullBuild()) return 1;
+        write_file(out + "_batch_rows.bin", batch.hostTable());
+        wrs::SamplerBatched bs(batch, seed);
+        write_file(out + "_batch_samples.bin", bs.sample({1000, 1000, 1000}));
+
         const double gs = wrs::SamplerGpuBasic(alias, seed).benchmarkSampling(m);
         std::printf("{\"alias\": \"%s\", \"W\": %.17g, \"rejection\": \"%s\", \"slots\": %llu, \"sampler\": \"%s\", "
                     "\"gsamples_per_s\": %.3f}\n",

@@ -2,7 +2,8 @@
 
 tests/cpp/shim_check.cpp uses it as code written against the reference's classes would:
 AliasTableSplitGpu / RejectionSamplingGpu with fullBuild(), SamplerGpuBasic (sample,
-getSamplingDistribution, benchmarkSampling), SamplerGpuSectioned and SamplerRejection. On the
+getSamplingDistribution, benchmarkSampling), SamplerGpuSectioned, SamplerRejection, and the
+batched form (BatchedAliasTablesGpu, SamplerBatched). On the
 CPU the program must compile and link against the library; on the GPU its tables and samples
 must equal the oracle's (the same contracts as the C ABI tests)."""
 import json
@@ -70,3 +71,10 @@ def test_shim_matches_oracle(cuda, tmp_path, kind, n):
     rej, failed = po.rejection_sample(A, frac, m, seed, 0)
     assert failed == 0
     assert np.array_equal(np.fromfile(prefix + "_rej.bin", dtype=np.uint32), rej)
+    off = np.array([0, n // 3, n // 2, n], dtype=np.int64)
+    brows = np.fromfile(prefix + "_batch_rows.bin", dtype=np.uint32).reshape(-1, 2)
+    ref_b, _, _ = po.batched_build(w, off)
+    assert np.array_equal(brows, ref_b)
+    soff = np.array([0, 1000, 2000, 3000], dtype=np.int64)
+    assert np.array_equal(np.fromfile(prefix + "_batch_samples.bin", dtype=np.uint32),
+                          po.batched_sample(brows, off, soff, seed, 0))
