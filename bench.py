@@ -607,6 +607,28 @@ def batched_phase(dev, make=batch_config4, mixed: bool = False, shape: str = "")
     torch.cuda.synchronize()
     batched_ms = e0.elapsed_time(e1) / reps
     batched_wall_ms = (time.perf_counter() - t0) * 1e3 / reps
+    # end to end: the weights and both offset arrays copied up from pinned host memory, the
+    # graph replayed, the samples copied down
+    w_h = torch.from_numpy(w_np).pin_memory()
+    off_h, soff_h = torch.from_numpy(off).pin_memory(), torch.from_numpy(soff).pin_memory()
+    out_h = torch.empty(total, dtype=torch.int32).pin_memory()
+
+    def e2e_once():
+        w.copy_(w_h, non_blocking=True)
+        d_off.copy_(off_h, non_blocking=True)
+        d_soff.copy_(soff_h, non_blocking=True)
+        g.replay()
+        out_h.copy_(out, non_blocking=True)
+
+    e2e_once()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        e2e_once()
+    e1.record()
+    torch.cuda.synchronize()
+    batched_e2e_ms = e0.elapsed_time(e1) / reps
+    h2d_bytes = 4 * items + 8 * (nt + 1) * 2
     mixed_info = None
     if mixed:
         A = torch.empty(2 * items, dtype=torch.int32, device=dev)
@@ -685,6 +707,9 @@ def batched_phase(dev, make=batch_config4, mixed: bool = False, shape: str = "")
         "workload": what, "items": items, "samples": total,
         "autotuned": {"small_table_items": int(opts.small_table_items), "tile_items": int(opts.tile_items)},
         "batched_ms": round(batched_ms, 4), "batched_wall_ms": round(batched_wall_ms, 4),
+        "e2e": {"value": round((items + total) / (batched_e2e_ms * 1e-3) / 1e9, 3), "unit": UNIT,
+                "ms_per_step": round(batched_e2e_ms, 4), "h2d_bytes_per_step": h2d_bytes,
+                "d2h_bytes_per_step": 4 * total, "path": "all-alias graph"},
         "batched_g_items_plus_samples_s": round((items + total) / (batched_ms * 1e-3) / 1e9, 3),
         "per_table_ms": round(per_ms, 2), "per_table_wall_ms": round(per_wall_ms, 2),
         "per_table_sample": "timed on " + ", ".join(timed) + " per size class, scaled by table count",
@@ -736,7 +761,7 @@ def run_batched_only(args, rank: int, local_rank: int):
             "config": {"workload": b["workload"], "items": b["items"], "samples": b["samples"]},
             "batched": b,
             "gpu_launches": (BATCHED_KERNELS_PER_REPLAY + (2 if b.get("mixed", {}).get("rejection_tables") else 0)) * 20,
-            "e2e": None, "note": f"{items_samples} items+samples per graph replay"}
+            "e2e": b["e2e"], "note": f"{items_samples} items+samples per graph replay"}
 
 
 # ---------------------------------------------------------------- reference CPU
