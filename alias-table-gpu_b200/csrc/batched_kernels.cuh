@@ -486,8 +486,8 @@ __global__ void __launch_bounds__(32 * kSmallWarps) small_tables_kernel(const fl
 // takes kBatchSamplePer consecutive positions: it finds the table of its first one by a
 // binary search of the sample offsets and walks forward from there.
 // In a mixed batch (kinds not null) a rejection table's positions follow the rejection
-// contract instead (rejection_sample_kernel: b = counter_base + s, two tries per Philox
-// block, slot and acceptance from the table's own slot range), and the positions of a
+// contract instead (rejection_sample_kernel: b = counter_base + s, one try per Philox block,
+// a 64-bit slot uniform and the acceptance from the table's own slot range), and the positions of a
 // skipped table are left as they are.
 constexpr int kBatchSampleThreads = 256;
 constexpr int kBatchSamplePer = 8;
@@ -529,12 +529,11 @@ __global__ void __launch_bounds__(kBatchSampleThreads) batch_sample_kernel(
             const uint32_t* At = A + 2 * off;
             const uint64_t b = counter_base + s;
             uint32_t res = 0xffffffffu;
-            Philox4 r{};
             for (uint32_t tr = 0; tr < max_tries; ++tr) {
-                if ((tr & 1u) == 0)
-                    r = philox4x32_10((uint32_t)b, (uint32_t)(b >> 32), tr >> 1, 0x52454a00u, k0, k1);
-                const uint32_t xs = r.x[(tr & 1u) * 2], xc = r.x[(tr & 1u) * 2 + 1];
-                const uint32_t e = __ldg(At + scale_u32(xs, (uint32_t)asz));
+                const Philox4 r = philox4x32_10((uint32_t)b, (uint32_t)(b >> 32), tr, 0x52454a00u, k0, k1);
+                const uint32_t xc = r.x[2];
+                const uint32_t e =
+                    __ldg(At + (uint32_t)__umul64hi(((uint64_t)r.x[1] << 32) | r.x[0], (uint64_t)asz));
                 const uint32_t item = e & 0x7fffffffu;
                 if ((e >> 31) == 0u || coin24(xc) < __ldg(frac + off + item)) {
                     res = item;

@@ -371,7 +371,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     rstat = torch.zeros(1, dtype=torch.int32, device=dev)
     st = wrs.rejection_build(w, A, frac, a_size, rscr, sync=True, stream=sp)
     rm = min(m, 1 << 28)
-    st |= wrs.rejection_sample(A, a_size, frac, n, rm, SEED_SAMPLES, out, 0, 0, rstat, stream=sp)
+    rout = torch.empty(rm, dtype=torch.int32, device=dev)
+    st |= wrs.rejection_sample(A, a_size, frac, n, rm, SEED_SAMPLES, rout, 0, 0, rstat, stream=sp)
     torch.cuda.synchronize()
     s0.record(stream)
     for r in range(reps):
@@ -381,7 +382,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     rej_build_ms = s0.elapsed_time(s1) / reps
     s0.record(stream)
     for r in range(reps):
-        st |= wrs.rejection_sample(A, a_size, frac, n, rm, SEED_SAMPLES, out, (r + 1) * rm, 0, rstat, stream=sp)
+        st |= wrs.rejection_sample(A, a_size, frac, n, rm, SEED_SAMPLES, rout, (r + 1) * rm, 0, rstat, stream=sp)
     s1.record(stream)
     torch.cuda.synchronize()
     rej_sample_ms = s0.elapsed_time(s1) / reps
@@ -389,6 +390,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         raise wrs.WrsError(st or int(rstat.item()) or 1, "rejection")
     rej_slots = int(a_size.item())
     del A, frac, rscr
+    rej_chi2 = chi2_gpu(w, rout) if rank == 0 else None
+    del rout
 
     # the random-access bound of the plain sampler: a library gather (torch index_select) of
     # random 8-byte rows from the same table, with precomputed uniform row indices
@@ -481,6 +484,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                    "section_items": SECTION_ITEMS},
         "prob_error": err,
         "chi_square": chi2,
+        "rejection_chi_square": rej_chi2,
         "roofline": {"kernel": "sample_plain_kernel", "bound": "hbm", "achieved": round(achieved, 1),
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "traffic": ncu_traffic() if args.config == "2" else None,

@@ -148,6 +148,9 @@ WRS_API wrs_status wrs_alias_build_f32_static_scratch(const float* d_w, int64_t 
  *   odd s reads (x2, x3). row = floor(x_first * len / 2^32) + offset (PLAIN: len = n,
  *   offset = 0; SECTIONED: the section of s), coin = (x_second >> 8) * 2^-24,
  *   result = coin < prob[row] ? row : alias[row].
+ *   The row map gives every row floor or ceil of 2^32 / len of the 2^32 values of x_first:
+ *   exact when len is a power of two, otherwise each row's share is within len / 2^32
+ *   (relative) of 1 / len.
  * SECTIONED derives the per-section counts from a binomial tree keyed by the same
  * (seed, counter_base). d_section_counts (optional, device, ceil(n/section_items) u64)
  * receives them. */
@@ -178,10 +181,10 @@ WRS_API wrs_status wrs_rejection_build_f32(const float* d_w, int64_t n, uint32_t
                                    float* d_frac, uint64_t* d_A_size, double* d_W,
                                    void* d_scratch, size_t scratch_bytes, uint32_t flags,
                                    void* stream);
-/* Sample s, try t uses Philox counter (lo32(b), hi32(b), t >> 1, 0x52454a00) with
- * b = counter_base + s and words (x0, x1) for even t, (x2, x3) for odd t:
- * slot = floor(x_first * |A| / 2^32); a first slot is accepted iff
- * (x_second >> 8) * 2^-24 < frac[item]; other slots always accept.
+/* Sample s, try t uses Philox counter (lo32(b), hi32(b), t, 0x52454a00) with
+ * b = counter_base + s: slot = floor(u * |A| / 2^64) for the 64-bit uniform u = x1:x0 (every
+ * slot's share is exact to |A| / 2^64); a first slot is accepted iff
+ * (x2 >> 8) * 2^-24 < frac[item]; other slots always accept.
  * After max_tries (0 = 64) failed tries the output is 0xFFFFFFFF and *d_status
  * (optional, device u32) gets WRS_ERR_TOO_MANY_TRIES. */
 WRS_API wrs_status wrs_rejection_sample(const uint32_t* d_A, const uint64_t* d_A_size, const float* d_frac,

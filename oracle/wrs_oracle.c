@@ -102,6 +102,10 @@ static inline void philox_block(uint64_t b, uint32_t c2, uint32_t c3, uint64_t s
 }
 
 static inline uint32_t scale_u32(uint32_t x, uint32_t len) { return (uint32_t)(((uint64_t)x * len) >> 32); }
+/* a rejection try's slot: floor(u |A| / 2^64) for the 64-bit uniform u = x1:x0 */
+static inline uint32_t slot_of(uint32_t x0, uint32_t x1, uint64_t asz) {
+    return (uint32_t)((((unsigned __int128)(((uint64_t)x1 << 32) | x0)) * asz) >> 64);
+}
 static inline float coin24(uint32_t x) { return (float)(x >> 8) * 5.9604644775390625e-8f; }
 static inline float bits_f(uint32_t b) {
     float f;
@@ -912,9 +916,9 @@ int or_batched_mixed_sample(const uint32_t* rows, const uint32_t* A, const float
                 const uint64_t b = cbase + (uint64_t)s;
                 uint32_t res = 0xffffffffu;
                 for (uint32_t tr = 0; tr < tries; ++tr) {
-                    if ((tr & 1u) == 0) philox_block(b, tr >> 1, 0x52454a00u, seed, x);
-                    const uint32_t xs = x[(tr & 1u) * 2], xc = x[(tr & 1u) * 2 + 1];
-                    const uint32_t e = At[scale_u32(xs, (uint32_t)asz)];
+                    philox_block(b, tr, 0x52454a00u, seed, x);
+                    const uint32_t xc = x[2];
+                    const uint32_t e = At[slot_of(x[0], x[1], asz)];
                     const uint32_t item = e & 0x7fffffffu;
                     if ((e >> 31) == 0u || coin24(xc) < frac[off[t] + item]) {
                         res = item;
@@ -1195,9 +1199,9 @@ int or_rejection_sample(const uint32_t* A, uint64_t a_size, const float* frac, u
         uint64_t b = cbase + s;
         uint32_t res = 0xffffffffu, x[4];
         for (uint32_t t = 0; t < tries; ++t) {
-            if ((t & 1u) == 0) philox_block(b, t >> 1, 0x52454a00u, seed, x);
-            uint32_t xs = x[(t & 1u) * 2], xc = x[(t & 1u) * 2 + 1];
-            uint32_t e = A[scale_u32(xs, (uint32_t)a_size)];
+            philox_block(b, t, 0x52454a00u, seed, x);
+            uint32_t xc = x[2];
+            uint32_t e = A[slot_of(x[0], x[1], a_size)];
             uint32_t item = e & 0x7fffffffu;
             if ((e >> 31) == 0u || coin24(xc) < frac[item]) {
                 res = item;
