@@ -481,8 +481,8 @@ __global__ void __launch_bounds__(32 * kSmallWarps) small_tables_kernel(const fl
 // ---------------------------------------------------------------- batched plain sampling
 // Output position s of the batch belongs to table t with sample_offsets[t] <= s <
 // sample_offsets[t + 1] and follows the plain contract over the global position s:
-// Philox counter counter_base + floor(s / 2), row = floor(x_first * n_t / 2^32) (table-local),
-// coin = (x_second >> 8) * 2^-24, result = coin < prob[row] ? row : alias[row]. Every thread
+// Philox counter counter_base + s, row = floor((x1:x0) * n_t / 2^64) (table-local),
+// coin = (x2 >> 8) * 2^-24, result = coin < prob[row] ? row : alias[row]. Every thread
 // takes kBatchSamplePer consecutive positions: it finds the table of its first one by a
 // binary search of the sample offsets and walks forward from there.
 // In a mixed batch (kinds not null) a rejection table's positions follow the rejection
@@ -509,8 +509,6 @@ __global__ void __launch_bounds__(kBatchSampleThreads) batch_sample_kernel(
     uint64_t s_end_t = (uint64_t)__ldg(sample_offsets + t + 1);
     const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
     const uint64_t s1 = min(total, s0 + kBatchSamplePer);
-    Philox4 x{};
-    uint64_t have = ~0ull;
     for (uint64_t s = s0; s < s1; ++s) {
         while (s >= s_end_t && t + 1 < num_tables) {
             ++t;
@@ -532,8 +530,7 @@ __global__ void __launch_bounds__(kBatchSampleThreads) batch_sample_kernel(
             for (uint32_t tr = 0; tr < max_tries; ++tr) {
                 const Philox4 r = philox4x32_10((uint32_t)b, (uint32_t)(b >> 32), tr, 0x52454a00u, k0, k1);
                 const uint32_t xc = r.x[2];
-                const uint32_t e =
-                    __ldg(At + (uint32_t)__umul64hi(((uint64_t)r.x[1] << 32) | r.x[0], (uint64_t)asz));
+                const uint32_t e = __ldg(At + scale_u64(r.x[0], r.x[1], (uint32_t)asz));
                 const uint32_t item = e & 0x7fffffffu;
                 if ((e >> 31) == 0u || coin24(xc) < __ldg(frac + off + item)) {
                     res = item;
@@ -544,13 +541,8 @@ __global__ void __launch_bounds__(kBatchSampleThreads) batch_sample_kernel(
             out[s] = res;
             continue;
         }
-        const uint64_t b = counter_base + (s >> 1);
-        if (b != have) {
-            x = philox4x32_10((uint32_t)b, (uint32_t)(b >> 32), 0u, 0u, k0, k1);
-            have = b;
-        }
-        const uint32_t xr = (s & 1) ? x.x[2] : x.x[0];
-        const uint32_t xc = (s & 1) ? x.x[3] : x.x[1];
+        const uint64_t b = counter_base + s;
+        const Philox4 x = philox4x32_10((uint32_t)b, (uint32_t)(b >> 32), 0u, 0u, k0, k1);
         const int64_t off = __ldg(offsets + t);
         const uint64_t n = (uint64_t)(__ldg(offsets + t + 1) - off);
         if (n == 0 || n > 0xffffffffull || s >= s_end_t) {
@@ -558,9 +550,9 @@ __global__ void __launch_bounds__(kBatchSampleThreads) batch_sample_kernel(
             if (status) record_status(status, WRS_ERR_INVALID_ARGUMENT);
             continue;
         }
-        const uint32_t row = scale_u32(xr, (uint32_t)n);
+        const uint32_t row = scale_u64(x.x[0], x.x[1], (uint32_t)n);
         const uint2 e = __ldg(reinterpret_cast<const uint2*>(table + off) + row);
-        out[s] = coin24(xc) < __uint_as_float(e.x) ? row : e.y;
+        out[s] = coin24(x.x[2]) < __uint_as_float(e.x) ? row : e.y;
     }
 }
 

@@ -112,7 +112,6 @@ extern "C" wrs_status wrs_alias_sample_to_host(const wrs_alias_row* d_table, int
     if (!d_table || n < 1 || n > kMaxItems || (num_samples > 0 && (!d_out || !h_out))) return WRS_ERR_INVALID_ARGUMENT;
     if (num_samples == 0) return WRS_SUCCESS;
     uint64_t chunk = chunk_samples ? chunk_samples : (1ull << 25);
-    chunk += chunk & 1u;  // chunks start at even positions: a Philox block serves positions 2b, 2b + 1
     cudaStream_t stream = static_cast<cudaStream_t>(stream_);
     cudaStream_t copy = nullptr;
     wrs_status st = copy_stream(&copy);
@@ -121,7 +120,7 @@ extern "C" wrs_status wrs_alias_sample_to_host(const wrs_alias_row* d_table, int
     if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return WRS_ERR_CUDA;
     for (uint64_t s0 = 0; s0 < num_samples && st == WRS_SUCCESS; s0 += chunk) {
         const uint64_t c = num_samples - s0 < chunk ? num_samples - s0 : chunk;
-        st = wrs_alias_sample(d_table, n, c, seed, counter_base + s0 / 2, nullptr, d_out + s0, nullptr, stream_);
+        st = wrs_alias_sample(d_table, n, c, seed, counter_base + s0, nullptr, d_out + s0, nullptr, stream_);
         if (st != WRS_SUCCESS) break;
         // the copy stream takes the chunk once it is written (a wait binds the latest record)
         if (cudaEventRecord(ev, stream) != cudaSuccess || cudaStreamWaitEvent(copy, ev, 0) != cudaSuccess ||

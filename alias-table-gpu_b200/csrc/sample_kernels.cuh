@@ -5,9 +5,9 @@
 // The reference draws an FP64 uniform u from clock-seeded XORWOW, takes row = (int)(u*N) and
 // compares W/N * frac(u*N) with the row weight; it writes no output. Here every sample is
 // a pure function of (seed, counter_base, output position) through Philox4x32-10:
-//   block b = counter_base + s/2 gives words x0..x3; sample s uses (x0, x1) if s is even,
-//   (x2, x3) if odd; row = floor(x_first * len / 2^32) + offset, coin = (x_second >> 8) 2^-24,
-//   result = coin < prob[row] ? row : alias[row]
+//   block b = counter_base + s gives words x0..x3; row = floor((x1:x0) * len / 2^64) + offset
+//   (a 64-bit uniform, so every row's share is exact to within len / 2^64),
+//   coin = (x2 >> 8) 2^-24, result = coin < prob[row] ? row : alias[row]
 // — the reference's decision (SamplerGpuBasic.cu:48-69) with frac := coin and
 // weight := prob * W/N. Each sample is one 8-byte gather of a packed {prob, alias} row.
 #pragma once
@@ -44,7 +44,7 @@ __device__ __forceinline__ float ld_f32_64B(const float* p) {
     return v;
 }
 
-// Plain sampling: each thread handles octets of consecutive output positions (4 Philox
+// Plain sampling: each thread handles octets of consecutive output positions (8 Philox
 // blocks, 8 independent gathers in flight, two 16-byte stores).
 // MODE 0 writes sample s at out[s]; MODE 1 counts the samples instead (out[row] += 1 per
 // sample); MODE 2 folds them into out[0] ^= (the XOR of all samples).
@@ -57,16 +57,14 @@ __global__ void __launch_bounds__(256) sample_plain_kernel(const uint2* __restri
     const bool out_aligned = ((uintptr_t)out & 15u) == 0;
     uint32_t fold = 0;
     for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < noct; g += gsize) {
-        const uint64_t b = cbase + 4 * g;
+        const uint64_t b = cbase + 8 * g;
         uint32_t rows[8], coins[8];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < 8; ++j) {
             const uint64_t bj = b + j;
             const Philox4 r = philox4x32_10((uint32_t)bj, (uint32_t)(bj >> 32), 0u, 0u, k0, k1);
-            rows[2 * j] = scale_u32(r.x[0], n);
-            coins[2 * j] = r.x[1];
-            rows[2 * j + 1] = scale_u32(r.x[2], n);
-            coins[2 * j + 1] = r.x[3];
+            rows[j] = scale_u64(r.x[0], r.x[1], n);
+            coins[j] = r.x[2];
         }
         uint2 v[8];
 #pragma unroll
@@ -123,8 +121,8 @@ __global__ void __launch_bounds__(256) sample_plain_kernel(const uint2* __restri
 // being sampled at any moment (grid size x section bytes) stay inside L2; with STAGE each
 // section is first copied into shared memory and gathered from there. The counts and offsets
 // of a CTA's sections are computed up front, one thread per section (each a walk down the
-// binomial tree), so no thread waits for them between sections. Each thread draws four
-// consecutive Philox blocks at a time (eight gathers in flight).
+// binomial tree), so no thread waits for them between sections. Each thread draws eight
+// consecutive output positions at a time (eight Philox blocks, eight gathers in flight).
 constexpr int kSectThreads = 512;
 
 // The staged form runs two CTAs per SM (at most 64 registers: the once-per-section binomial
@@ -168,22 +166,19 @@ __global__ void __launch_bounds__(kSectThreads, STAGE ? 2 : 1) sample_sectioned_
             }
             const uint64_t cnt = s_cnt[ii], off = s_off[ii];
             if (cnt > 0) {
-                // Philox blocks covering output positions [off, off + cnt), in groups of four
-                // aligned to the global block index
-                const uint64_t b_lo = off >> 1, b_hi = (off + cnt - 1) >> 1;
-                const uint64_t g_lo = b_lo & ~3ull;
-                const uint64_t ng = ((b_hi - g_lo) >> 2) + 1;
+                // output positions [off, off + cnt) in groups of eight aligned to the global
+                // position (position p draws Philox block cbase + p)
+                const uint64_t p_lo = off & ~7ull;
+                const uint64_t ng = ((off + cnt - 1 - p_lo) >> 3) + 1;
                 for (uint64_t gi = threadIdx.x; gi < ng; gi += blockDim.x) {
-                    const uint64_t blk0 = g_lo + 4 * gi;
+                    const uint64_t s0 = p_lo + 8 * gi;  // output position of res[0]
                     uint32_t rows[8], coins[8];
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const uint64_t bb = cbase + blk0 + j;
+                    for (int j = 0; j < 8; ++j) {
+                        const uint64_t bb = cbase + s0 + j;
                         const Philox4 r = philox4x32_10((uint32_t)bb, (uint32_t)(bb >> 32), 0u, 0u, k0, k1);
-                        rows[2 * j] = scale_u32(r.x[0], len);
-                        coins[2 * j] = r.x[1];
-                        rows[2 * j + 1] = scale_u32(r.x[2], len);
-                        coins[2 * j + 1] = r.x[3];
+                        rows[j] = scale_u64(r.x[0], r.x[1], len);
+                        coins[j] = r.x[2];
                     }
                     uint2 v[8];
 #pragma unroll
@@ -191,7 +186,6 @@ __global__ void __launch_bounds__(kSectThreads, STAGE ? 2 : 1) sample_sectioned_
                     uint32_t res[8];
 #pragma unroll
                     for (int j = 0; j < 8; ++j) res[j] = alias_pick(v[j], start + rows[j], coins[j]);
-                    const uint64_t s0 = 2 * blk0;  // output position of res[0]
                     if (s0 >= off && s0 + 8 <= off + cnt && out16) {
                         uint4* o4 = reinterpret_cast<uint4*>(out + s0);
                         __stcs(o4, make_uint4(res[0], res[1], res[2], res[3]));
@@ -212,9 +206,7 @@ __global__ void __launch_bounds__(kSectThreads, STAGE ? 2 : 1) sample_sectioned_
 // Slot of a try: floor(u * |A| / 2^64) for the 64-bit uniform u = x1:x0, so that every slot
 // of a large array gets its share to within |A| / 2^64 (a 32-bit uniform would leave shares
 // differing by up to |A| / 2^32 relative: about 3% at 1.3e8 slots).
-__device__ __forceinline__ uint32_t slot_of(uint32_t x0, uint32_t x1, uint32_t asz) {
-    return (uint32_t)__umul64hi(((uint64_t)x1 << 32) | x0, (uint64_t)asz);
-}
+__device__ __forceinline__ uint32_t slot_of(uint32_t x0, uint32_t x1, uint32_t asz) { return scale_u64(x0, x1, asz); }
 
 // ---------------------------------------------------------------- rejection sampling
 // Replaces SamplerRejection::sample / SamplerRejectionGiveUp::sample

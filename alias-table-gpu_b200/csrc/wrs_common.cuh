@@ -210,6 +210,17 @@ __host__ __device__ __forceinline__ uint32_t scale_u32(uint32_t x, uint32_t len)
     return (uint32_t)(((uint64_t)x * (uint64_t)len) >> 32);
 }
 
+// index in [0, len) from the 64-bit uniform u = x1:x0, exactly floor(u * len / 2^64): every
+// index gets its share to within len / 2^64 (a 32-bit uniform would leave shares differing by
+// up to len / 2^32 relative, about 2% at 1e8 rows).
+__host__ __device__ __forceinline__ uint32_t scale_u64(uint32_t x0, uint32_t x1, uint32_t len) {
+#ifdef __CUDA_ARCH__
+    return (uint32_t)__umul64hi(((uint64_t)x1 << 32) | x0, (uint64_t)len);
+#else
+    return (uint32_t)(((unsigned __int128)((((uint64_t)x1) << 32) | x0) * len) >> 64);
+#endif
+}
+
 // coin in [0, 1) with 24 random bits.
 __host__ __device__ __forceinline__ float coin24(uint32_t x) {
     return (float)(x >> 8) * 5.9604644775390625e-8f;  // 2^-24

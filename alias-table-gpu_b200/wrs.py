@@ -447,7 +447,7 @@ class SamplerGpuBasic(Sampler):
         if out is None:
             out = torch.empty(numSamples, dtype=torch.int32, device=a.device)
         _check(alias_sample(a.table, a.N, numSamples, self.seed, out, self.counter), "plain sample")
-        self.counter += (numSamples + 1) // 2
+        self.counter += numSamples
         return out
 
     def getSamplingDistribution(self, numSamples: int) -> np.ndarray:
@@ -456,7 +456,7 @@ class SamplerGpuBasic(Sampler):
         a = self.algorithm
         counts = torch.zeros(a.N, dtype=torch.int32, device=a.device)
         _check(alias_histogram(a.table, a.N, numSamples, self.seed, counts, self.counter), "plain histogram")
-        self.counter += (numSamples + 1) // 2
+        self.counter += numSamples
         return counts.cpu().numpy().astype(np.int64)
 
 
@@ -475,7 +475,7 @@ class SamplerGpuSectioned(Sampler):
             out = torch.empty(numSamples, dtype=torch.int32, device=a.device)
         _check(alias_sample(a.table, a.N, numSamples, self.seed, out, self.counter, mode=WRS_SAMPLE_SECTIONED,
                             section_items=self.itemsPerSection), "sectioned sample")
-        self.counter += (numSamples + 1) // 2
+        self.counter += numSamples
         return out
 
 
@@ -569,5 +569,5 @@ class SamplerBatched:
             out = torch.empty(max(1, total), dtype=torch.int32, device=t.device)
         _check(batched_sample(t.table, t.offsetsGpu, t.num_tables, d_soff, total, self.seed, out, self.counter),
                "batched sample")
-        self.counter += (total + 1) // 2
+        self.counter += total
         return out[:total], soff

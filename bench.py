@@ -292,7 +292,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
     for i in range(args.warmup):
         build()
-        sample(i * (m // 2))
+        sample(i * m)
     torch.cuda.synchronize()
 
     K = args.steps
@@ -313,7 +313,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         ev[k][0].record(stream)
         build()
         ev[k][1].record(stream)
-        sample((args.warmup + k) * (m // 2))
+        sample((args.warmup + k) * m)
         ev[k][2].record(stream)
     torch.cuda.synchronize()
     if world > 1:
@@ -331,7 +331,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     reps = 5
     s0.record(stream)
     for r in range(reps):
-        sample((r + 1) * (m // 2), wrs.WRS_SAMPLE_SECTIONED, SECTION_ITEMS)
+        sample((r + 1) * m, wrs.WRS_SAMPLE_SECTIONED, SECTION_ITEMS)
     s1.record(stream)
     torch.cuda.synchronize()
     sect_ms = s0.elapsed_time(s1) / reps
@@ -344,7 +344,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     s0.record(stream)
     for r in range(reps):
         counts.zero_()
-        st |= wrs.alias_histogram(table, n, m, SEED_SAMPLES, counts, (r + 1) * (m // 2), stream=sp)
+        st |= wrs.alias_histogram(table, n, m, SEED_SAMPLES, counts, (r + 1) * m, stream=sp)
     s1.record(stream)
     torch.cuda.synchronize()
     if st:
@@ -356,7 +356,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     fold = torch.zeros(1, dtype=torch.int32, device=dev)
     s0.record(stream)
     for r in range(reps):
-        st |= wrs.alias_sample(table, n, m, SEED_SAMPLES, fold, (r + 1) * (m // 2), mode=wrs.WRS_SAMPLE_DISCARD,
+        st |= wrs.alias_sample(table, n, m, SEED_SAMPLES, fold, (r + 1) * m, mode=wrs.WRS_SAMPLE_DISCARD,
                                stream=sp)
     s1.record(stream)
     torch.cuda.synchronize()
@@ -439,7 +439,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             if i + 1 < steps:
                 h2d.wait_event(built)
                 load_weights()
-            sample_to_host(cbase0 + i * (m // 2))  # chunks copied down while the next ones are drawn
+            sample_to_host(cbase0 + i * m)  # chunks copied down while the next ones are drawn
 
     e2e_steps_run(2, 0)
     torch.cuda.synchronize()

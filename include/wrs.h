@@ -144,13 +144,11 @@ WRS_API wrs_status wrs_alias_build_f32_static_scratch(const float* d_w, int64_t 
 
 /* Sampling-input contract (bit-exact, see the oracle):
  *   output position s uses Philox4x32-10 with key (lo32(seed), hi32(seed)) and counter
- *   (lo32(b), hi32(b), 0, 0), b = counter_base + floor(s / 2); even s reads words (x0, x1),
- *   odd s reads (x2, x3). row = floor(x_first * len / 2^32) + offset (PLAIN: len = n,
- *   offset = 0; SECTIONED: the section of s), coin = (x_second >> 8) * 2^-24,
- *   result = coin < prob[row] ? row : alias[row].
- *   The row map gives every row floor or ceil of 2^32 / len of the 2^32 values of x_first:
- *   exact when len is a power of two, otherwise each row's share is within len / 2^32
- *   (relative) of 1 / len.
+ *   (lo32(b), hi32(b), 0, 0), b = counter_base + s, giving words x0..x3.
+ *   row = floor(u * len / 2^64) + offset for the 64-bit uniform u = x1 * 2^32 + x0 (PLAIN:
+ *   len = n, offset = 0; SECTIONED: the section of s), coin = (x2 >> 8) * 2^-24,
+ *   result = coin < prob[row] ? row : alias[row]. x3 is unused.
+ *   Every row's share of the 2^64 values of u is within len / 2^64 (relative) of 1 / len.
  * SECTIONED derives the per-section counts from a binomial tree keyed by the same
  * (seed, counter_base). d_section_counts (optional, device, ceil(n/section_items) u64)
  * receives them. */
@@ -162,7 +160,7 @@ WRS_API wrs_status wrs_alias_sample(const wrs_alias_row* d_table, int64_t n, uin
  * an internal copy stream of the library moves each finished chunk to h_out (num_samples u32;
  * pinned host memory, or the copies do not overlap), so the transfer overlaps the sampling
  * of the next chunk. Work enqueued on `stream` after the call waits for every copy.
- * chunk_samples: 0 = 2^25 (rounded up to an even count). The copy stream is created on the
+ * chunk_samples: 0 = 2^25. The copy stream is created on the
  * first call on a device: make that call outside stream capture. The reference's samplers
  * keep no output (SamplerGpuBasic.cu:77-133); this is the transfer a caller of its
  * getSamplingDistribution pays for, overlapped. */
@@ -214,7 +212,7 @@ WRS_API wrs_status wrs_batched_build_f32(const float* d_w, const int64_t* d_offs
                                  void* d_scratch, size_t scratch_bytes, void* stream);
 /* Table t draws d_sample_offsets[t+1] - d_sample_offsets[t] samples, written (as table-local
  * row indices) at d_out[d_sample_offsets[t] ...]. Output position s of table t uses the
- * plain contract with b = counter_base + floor(s / 2) over the global position s. */
+ * plain contract with b = counter_base + s over the global position s. */
 WRS_API wrs_status wrs_batched_sample(const wrs_alias_row* d_table, const int64_t* d_offsets,
                               int64_t num_tables, const int64_t* d_sample_offsets,
                               uint64_t total_samples, uint64_t seed, uint64_t counter_base,

@@ -258,7 +258,7 @@ public:
         wrs_sample_opts o{WRS_SAMPLE_PLAIN, 0u, 0u, 0u};
         check(wrs_alias_sample(a_.deviceTable(), a_.N, numSamples, seed_, counter, &o, d_out, nullptr, a_.stream()),
               "plain sample");
-        counter += (numSamples + 1) / 2;
+        counter += numSamples;
     }
     // counted on the device (the histogram mode), without a sample list
     std::vector<int64_t> getSamplingDistribution(uint64_t numSamples) override {
@@ -267,7 +267,7 @@ public:
         wrs_sample_opts o{WRS_SAMPLE_HISTOGRAM, 0u, 0u, 0u};
         check(wrs_alias_sample(a_.deviceTable(), a_.N, numSamples, seed_, counter, &o, counts.get(), nullptr,
                                a_.stream()), "plain histogram");
-        counter += (numSamples + 1) / 2;
+        counter += numSamples;
         const std::vector<uint32_t> h = counts.to_host(a_.stream());
         return std::vector<int64_t>(h.begin(), h.end());
     }
@@ -287,7 +287,7 @@ public:
         wrs_sample_opts o{WRS_SAMPLE_SECTIONED, section_, 0u, 0u};
         check(wrs_alias_sample(a_.deviceTable(), a_.N, numSamples, seed_, counter, &o, d_out, nullptr, a_.stream()),
               "sectioned sample");
-        counter += (numSamples + 1) / 2;
+        counter += numSamples;
     }
 
 protected:
@@ -397,7 +397,7 @@ public:
         DeviceArray<uint32_t> out(total ? total : 1);
         check(wrs_batched_sample(b_.deviceTable(), b_.deviceOffsets(), b_.numTables(), d_soff.get(), total, seed_,
                                  counter, out.get(), b_.stream()), "batched sample");
-        counter += (total + 1) / 2;
+        counter += total;
         std::vector<uint32_t> h = out.to_host(b_.stream());
         h.resize(total);
         if (sampleOffsets) *sampleOffsets = soff;

@@ -102,6 +102,10 @@ static inline void philox_block(uint64_t b, uint32_t c2, uint32_t c3, uint64_t s
 }
 
 static inline uint32_t scale_u32(uint32_t x, uint32_t len) { return (uint32_t)(((uint64_t)x * len) >> 32); }
+/* an alias row: floor(u len / 2^64) for the 64-bit uniform u = x1:x0 */
+static inline uint32_t row_of(const uint32_t x[4], uint64_t len) {
+    return (uint32_t)((((unsigned __int128)(((uint64_t)x[1] << 32) | x[0])) * len) >> 64);
+}
 /* a rejection try's slot: floor(u |A| / 2^64) for the 64-bit uniform u = x1:x0 */
 static inline uint32_t slot_of(uint32_t x0, uint32_t x1, uint64_t asz) {
     return (uint32_t)((((unsigned __int128)(((uint64_t)x1 << 32) | x0)) * asz) >> 64);
@@ -838,12 +842,13 @@ static inline uint32_t do_sample(const uint32_t* rows, uint32_t row, uint32_t co
     return coin24(coin_bits) < bits_f(rows[2 * (uint64_t)row]) ? row : rows[2 * (uint64_t)row + 1];
 }
 
+/* The sampling contract: output position s uses Philox block counter_base + s; the row from
+ * the 64-bit uniform x1:x0, the coin from x2. */
 void or_sample_plain(const uint32_t* rows, int64_t n, uint64_t m, uint64_t seed, uint64_t cbase, uint32_t* out) {
-    for (uint64_t s = 0; s < m; s += 2) {
+    for (uint64_t s = 0; s < m; ++s) {
         uint32_t x[4];
-        philox_block(cbase + (s >> 1), 0, 0, seed, x);
-        out[s] = do_sample(rows, scale_u32(x[0], (uint32_t)n), x[1]);
-        if (s + 1 < m) out[s + 1] = do_sample(rows, scale_u32(x[2], (uint32_t)n), x[3]);
+        philox_block(cbase + s, 0, 0, seed, x);
+        out[s] = do_sample(rows, row_of(x, (uint64_t)n), x[2]);
     }
 }
 
@@ -853,13 +858,12 @@ void or_batched_sample(const uint32_t* rows, const int64_t* off, int64_t num_tab
         const uint64_t n = (uint64_t)(off[t + 1] - off[t]);
         for (int64_t s = soff[t]; s < soff[t + 1]; ++s) {
             uint32_t x[4];
-            philox_block(cbase + ((uint64_t)s >> 1), 0, 0, seed, x);
-            const uint32_t xr = (s & 1) ? x[2] : x[0], xc = (s & 1) ? x[3] : x[1];
+            philox_block(cbase + (uint64_t)s, 0, 0, seed, x);
             if (n == 0) {
                 out[s] = 0xffffffffu;
                 continue;
             }
-            out[s] = do_sample(rows + 2 * off[t], scale_u32(xr, (uint32_t)n), xc);
+            out[s] = do_sample(rows + 2 * off[t], row_of(x, n), x[2]);
         }
     }
 }
@@ -903,9 +907,8 @@ int or_batched_mixed_sample(const uint32_t* rows, const uint32_t* A, const float
         for (int64_t s = soff[t]; s < soff[t + 1]; ++s) {
             uint32_t x[4];
             if (kinds[t] == 0) {
-                philox_block(cbase + ((uint64_t)s >> 1), 0, 0, seed, x);
-                const uint32_t xr = (s & 1) ? x[2] : x[0], xc = (s & 1) ? x[3] : x[1];
-                out[s] = n == 0 ? 0xffffffffu : do_sample(rows + 2 * off[t], scale_u32(xr, (uint32_t)n), xc);
+                philox_block(cbase + (uint64_t)s, 0, 0, seed, x);
+                out[s] = n == 0 ? 0xffffffffu : do_sample(rows + 2 * off[t], row_of(x, n), x[2]);
             } else if (kinds[t] == 1) {
                 const uint64_t asz = n ? a_size[t] : 0;
                 if (asz == 0) {
@@ -936,16 +939,13 @@ int or_batched_mixed_sample(const uint32_t* rows, const uint32_t* A, const float
 double or_sample_plain_timed(const uint32_t* rows, int64_t n, uint64_t m, uint64_t seed, int threads, uint32_t* out) {
     struct timespec t0, t1;
     clock_gettime(CLOCK_MONOTONIC, &t0);
-    const int64_t npair = (int64_t)((m + 1) / 2);
 #ifdef _OPENMP
 #pragma omp parallel for num_threads(threads > 0 ? threads : 1) schedule(static)
 #endif
-    for (int64_t q = 0; q < npair; ++q) {
+    for (int64_t q = 0; q < (int64_t)m; ++q) {
         uint32_t x[4];
-        uint64_t s = 2 * (uint64_t)q;
         philox_block((uint64_t)q, 0, 0, seed, x);
-        out[s] = do_sample(rows, scale_u32(x[0], (uint32_t)n), x[1]);
-        if (s + 1 < m) out[s + 1] = do_sample(rows, scale_u32(x[2], (uint32_t)n), x[3]);
+        out[q] = do_sample(rows, row_of(x, (uint64_t)n), x[2]);
     }
     (void)threads;
     clock_gettime(CLOCK_MONOTONIC, &t1);
@@ -1163,10 +1163,8 @@ void or_sample_sectioned(const uint32_t* rows, int64_t n, uint64_t m, uint32_t S
         uint32_t len = (uint32_t)section_rows(k, k + 1, S, (uint64_t)n);
         for (uint64_t s = off; s < off + counts[k]; ++s) {
             uint32_t x[4];
-            philox_block(cbase + (s >> 1), 0, 0, seed, x);
-            int h = (int)(s & 1);
-            uint32_t r = start + scale_u32(x[2 * h], len);
-            out[s] = do_sample(rows, r, x[2 * h + 1]);
+            philox_block(cbase + s, 0, 0, seed, x);
+            out[s] = do_sample(rows, start + row_of(x, len), x[2]);
         }
         off += counts[k];
     }

@@ -41,7 +41,7 @@ int main(int argc, char** argv) {
         wrs::DeviceArray<uint32_t> d(m);
         basic.sample(m, d.get());  // counter 0
         write_file(out + "_plain.bin", d.to_host());
-        write_file(out + "_hist.bin", basic.getSamplingDistribution(m));  // counter (m + 1) / 2
+        write_file(out + "_hist.bin", basic.getSamplingDistribution(m));  // counter m
 
         wrs::SamplerGpuSectioned sect(alias, 4096, seed);
         sect.sample(m, d.get());

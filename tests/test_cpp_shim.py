@@ -63,7 +63,7 @@ def test_shim_matches_oracle(cuda, tmp_path, kind, n):
     assert np.array_equal(rows, po.exact_build(w, W))
     assert np.array_equal(np.fromfile(prefix + "_plain.bin", dtype=np.uint32), po.sample_plain(rows, m, seed, 0))
     hist = np.fromfile(prefix + "_hist.bin", dtype=np.int64)
-    assert np.array_equal(hist, np.bincount(po.sample_plain(rows, m, seed, (m + 1) // 2), minlength=n))
+    assert np.array_equal(hist, np.bincount(po.sample_plain(rows, m, seed, m), minlength=n))
     sect, _ = po.sample_sectioned(rows, m, 4096, seed, 0)
     assert np.array_equal(np.fromfile(prefix + "_sect.bin", dtype=np.uint32), sect)
     A, frac = po.rejection_build(w, W)

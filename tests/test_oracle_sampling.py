@@ -100,7 +100,7 @@ def test_plain_sampler_counter_continuation():
     rows = po.exact_build(w)
     a = po.sample_plain(rows, 1000, SEED, 0)
     b = po.sample_plain(rows, 600, SEED, 0)
-    c = po.sample_plain(rows, 400, SEED, 300)
+    c = po.sample_plain(rows, 400, SEED, 600)
     np.testing.assert_array_equal(a, np.concatenate([b, c]))
 
 
@@ -184,7 +184,7 @@ def test_batched_oracle_matches_per_table_oracle():
     r = rows[off[4]:off[5]]
     assert np.array_equal(po.batched_sample(r, np.array([0, 700]), np.array([0, 1001]), 99, 5),
                           po.sample_plain(r, 1001, 99, 5))
-    # odd split points keep the global Philox pairing
+    # odd split points: position s draws Philox block s, whichever table it falls in
     counts = np.array([7, 0, 9, 1, 33, 2], dtype=np.int64)
     soff = np.zeros(sizes.size + 1, dtype=np.int64)
     np.cumsum(counts, out=soff[1:])
@@ -192,10 +192,8 @@ def test_batched_oracle_matches_per_table_oracle():
     for t in range(sizes.size):
         n = int(sizes[t])
         for s in range(soff[t], soff[t + 1]):
-            b = s >> 1
-            x = po.philox([b & 0xffffffff, b >> 32, 0, 0], [5, 0])
-            xr, xc = (x[2], x[3]) if s & 1 else (x[0], x[1])
-            row = (int(xr) * n) >> 32
+            x = po.philox([s & 0xffffffff, s >> 32, 0, 0], [5, 0])
+            row = (((int(x[1]) << 32) | int(x[0])) * n) >> 64
             p = rows[off[t] + row, 0].view(np.float32)
-            coin = np.float32((int(xc) >> 8) * 2.0 ** -24)
+            coin = np.float32((int(x[2]) >> 8) * 2.0 ** -24)
             assert out[s] == (row if coin < p else rows[off[t] + row, 1])
