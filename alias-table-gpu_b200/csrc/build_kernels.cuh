@@ -1213,11 +1213,14 @@ __host__ __device__ constexpr size_t pack_smem_bytes(int T) {
     return (size_t)T * sizeof(uint64_t) + (size_t)pack_chunk(T) * (sizeof(uint64_t) + 2 * sizeof(uint32_t));
 }
 
-// Staged row position of tile item i (XOR swizzle of the IPT items of a thread, so that
-// neither the per-thread writes nor the per-warp reads of the stage conflict on banks).
+// Staged row position of tile item i: an XOR swizzle inside each thread's IPT items, keyed by
+// i / max(IPT, 16), so that a warp's 8-byte stores of its threads' k-th items cover all 16
+// bank pairs twice (two wavefronts; keyed by the thread index alone, IPT = 8 would hit 8 bank
+// pairs four times) and its reads of 32 consecutive rows stay a permutation (two wavefronts).
 template <int IPT>
 __device__ __forceinline__ uint32_t stage_pos(uint32_t i) {
-    return (i & ~(uint32_t)(IPT - 1)) | ((i ^ (i / IPT)) & (uint32_t)(IPT - 1));
+    constexpr uint32_t kKey = IPT > 16 ? IPT : 16;
+    return (i & ~(uint32_t)(IPT - 1)) | ((i ^ (i / kKey)) & (uint32_t)(IPT - 1));
 }
 
 // One light tile per CTA of NT threads, IPT consecutive items per thread.

@@ -44,34 +44,49 @@ __device__ __forceinline__ float ld_f32_64B(const float* p) {
     return v;
 }
 
+// The rows and coins of the eight consecutive output positions whose Philox blocks start at b.
+__device__ __forceinline__ void draw_octet(uint64_t b, uint32_t n, uint32_t k0, uint32_t k1, uint32_t (&rows)[8],
+                                           uint32_t (&coins)[8]) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const uint64_t bj = b + j;
+        const Philox4 r = philox4x32_10((uint32_t)bj, (uint32_t)(bj >> 32), 0u, 0u, k0, k1);
+        rows[j] = scale_u64(r.x[0], r.x[1], n);
+        coins[j] = r.x[2];
+    }
+}
+
 // Plain sampling: each thread handles octets of consecutive output positions (8 Philox
-// blocks, 8 independent gathers in flight, two 16-byte stores).
+// blocks, 8 independent gathers in flight, two 16-byte stores). The next octet's Philox
+// blocks are drawn while the current octet's gathers are in flight (drawn just before them,
+// 2^28 samples from a 2^26-row table took 5.80 ms instead of 5.13 ms). The launch bounds allow
+// about 60 registers (four CTAs per SM), with which the fold mode takes 4.73 ms instead of 5.26.
 // MODE 0 writes sample s at out[s]; MODE 1 counts the samples instead (out[row] += 1 per
 // sample); MODE 2 folds them into out[0] ^= (the XOR of all samples).
 template <int MODE>
-__global__ void __launch_bounds__(256) sample_plain_kernel(const uint2* __restrict__ table, uint32_t n, uint64_t m,
+__global__ void __launch_bounds__(256, 4) sample_plain_kernel(const uint2* __restrict__ table, uint32_t n, uint64_t m,
                                                            uint32_t k0, uint32_t k1, uint64_t cbase,
                                                            uint32_t* __restrict__ out) {
     const uint64_t noct = (m + 7) >> 3;
     const uint64_t gsize = (uint64_t)gridDim.x * blockDim.x;
     const bool out_aligned = ((uintptr_t)out & 15u) == 0;
     uint32_t fold = 0;
-    for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < noct; g += gsize) {
-        const uint64_t b = cbase + 8 * g;
-        uint32_t rows[8], coins[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const uint64_t bj = b + j;
-            const Philox4 r = philox4x32_10((uint32_t)bj, (uint32_t)(bj >> 32), 0u, 0u, k0, k1);
-            rows[j] = scale_u64(r.x[0], r.x[1], n);
-            coins[j] = r.x[2];
-        }
+    uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t rows[8], coins[8];
+    if (g < noct) draw_octet(cbase + 8 * g, n, k0, k1, rows, coins);
+    for (; g < noct; g += gsize) {
         uint2 v[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) v[j] = ld_row_64B(table + rows[j]);
+        uint32_t rows_n[8], coins_n[8];
+        draw_octet(cbase + 8 * (g + gsize), n, k0, k1, rows_n, coins_n);  // unused past the last octet
         uint32_t res[8];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) res[j] = alias_pick(v[j], rows[j], coins[j]);
+        for (int j = 0; j < 8; ++j) {
+            res[j] = alias_pick(v[j], rows[j], coins[j]);
+            rows[j] = rows_n[j];
+            coins[j] = coins_n[j];
+        }
         const uint64_t s0 = 8 * g;
         if constexpr (MODE == 2) {
 #pragma unroll
