@@ -96,13 +96,17 @@ def measured_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def ncu_traffic():
-    """DRAM bytes per launch of the plain sampler from the committed ncu summary, if any."""
+def ncu_traffic(n, m):
+    """DRAM bytes of one plain-sampler launch of m samples from an n-row table, from the
+    committed ncu summary (bytes per sample of a capture on a table of the same size; the
+    gathers are random, so the bytes grow in proportion to the samples), if there is one."""
     path = os.path.join(REPO, "profiles", "traffic.json")
     try:
         with open(path) as f:
             d = json.load(f)
-        return d.get("sample_plain_kernel_bytes_per_launch")
+        if int(d["table_rows"]) != n:
+            return None
+        return int(round(d["sample_plain_kernel_bytes_per_sample"] * m))
     except Exception:
         return None
 
@@ -487,8 +491,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "rejection_chi_square": rej_chi2,
         "roofline": {"kernel": "sample_plain_kernel", "bound": "hbm", "achieved": round(achieved, 1),
                      "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                     "traffic": ncu_traffic() if args.config == "2" else None,
-                     "algorithmic_bytes": "12 B/sample x 2^30 samples per launch (8 B row gather + 4 B write)",
+                     "traffic": ncu_traffic(n, m),
+                     "algorithmic_bytes": "12 B/sample x 2^%d samples per launch (8 B row gather + 4 B write)"
+                                          % (m.bit_length() - 1),
                      "random_access_bound": {
                          "probe": "torch index_select of 2^27 random 8-byte rows of the same table (index read "
                                   "and row write included)",
