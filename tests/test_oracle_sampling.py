@@ -104,6 +104,38 @@ def test_plain_sampler_counter_continuation():
     np.testing.assert_array_equal(a, np.concatenate([b, c]))
 
 
+def _contract_sample(rows, start, length, b, seed):
+    """One output position of the sampling contract in include/wrs.h, in plain Python:
+    Philox block b, row = floor((x1:x0) * length / 2^64) + start, coin = (x2 >> 8) 2^-24."""
+    x = po.philox([b & 0xFFFFFFFF, b >> 32, 0, 0], [seed & 0xFFFFFFFF, seed >> 32])
+    row = start + ((((int(x[1]) << 32) | int(x[0])) * length) >> 64)
+    p = rows[row, 0].view(np.float32)
+    coin = np.float32((int(x[2]) >> 8) * 2.0 ** -24)
+    return row if coin < p else int(rows[row, 1])
+
+
+@pytest.mark.parametrize("n", [1, 7, 5003])
+def test_plain_and_sectioned_follow_the_written_contract(n):
+    """The oracle's samplers against a plain-Python reading of the contract, on table sizes that
+    are not powers of two (where a 32-bit row uniform would be biased)."""
+    rng = np.random.default_rng(n)
+    w = rng.random(n, dtype=np.float32) + np.float32(0.01)
+    rows = po.exact_build(w)
+    seed, cbase, m = 0x1234_5678_9ABC_DEF0, (1 << 32) - 5, 300
+    out = po.sample_plain(rows, m, seed, cbase)
+    assert [int(v) for v in out] == [_contract_sample(rows, 0, n, cbase + s, seed) for s in range(m)]
+    S = 64
+    sect, counts = po.sample_sectioned(rows, m, S, seed, cbase)
+    assert int(counts.sum()) == m
+    s = 0
+    for k, c in enumerate(counts):
+        start = k * S
+        length = min(S, n - start)
+        for _ in range(int(c)):
+            assert int(sect[s]) == _contract_sample(rows, start, length, cbase + s, seed)
+            s += 1
+
+
 def test_sectioned_sampler_distribution():
     w = _weights(5000)
     rows = po.exact_build(w)
