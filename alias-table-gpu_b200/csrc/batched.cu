@@ -500,6 +500,7 @@ extern "C" wrs_status wrs_batched_autotune_kinds(const float* d_w, const int64_t
     const uint64_t total = (uint64_t)total_i;
     cudaStream_t stream = static_cast<cudaStream_t>(stream_);
     constexpr int kClasses = 33;
+    constexpr float kRejectionWins = 0.95f;  // rejection's time over alias's below which it is chosen
     std::vector<int> cls((size_t)num_tables);
     bool present[kClasses] = {};
     for (int64_t t = 0; t < num_tables; ++t) {
@@ -550,7 +551,11 @@ extern "C" wrs_status wrs_batched_autotune_kinds(const float* d_w, const int64_t
                 if (rep > 0) ms_of[m] = std::min(ms_of[m], ms);
             }
         }
-        choice[c] = ms_of[0] <= ms_of[1] ? (uint8_t)WRS_TABLE_ALIAS : (uint8_t)WRS_TABLE_REJECTION;
+        // rejection only where it wins clearly: a class timed alone does not carry the rejection
+        // kernels' cost to the rest of the batch (on 10^6 tables of 1..64 items, classes whose
+        // two timings were within 1.2% chose rejection and the batch took 7.58 ms, 7.10 ms as
+        // all alias)
+        choice[c] = ms_of[1] < kRejectionWins * ms_of[0] ? (uint8_t)WRS_TABLE_REJECTION : (uint8_t)WRS_TABLE_ALIAS;
         if (class_ms) {
             class_ms[2 * c] = ms_of[0];
             class_ms[2 * c + 1] = ms_of[1];

@@ -267,8 +267,9 @@ WRS_API wrs_status wrs_batched_mixed_sample(const wrs_alias_row* d_table, const 
  * 2^(c-1) < n <= 2^c (class 0: n = 1). For every class present it times the mixed build and
  * the mixed sample of that class's tables alone (every other table skipped), once as alias
  * and once as rejection tables, with the batch's sample counts (h_sample_offsets is the host
- * copy of d_sample_offsets), and writes the faster kind for each table into h_kinds_out
- * (empty tables: WRS_TABLE_SKIP) and, if class_kinds is not NULL, the choice per class into
+ * copy of d_sample_offsets). A class takes rejection where that took under 0.95 of alias's
+ * time, else alias. It writes each table's kind into h_kinds_out (empty tables:
+ * WRS_TABLE_SKIP) and, if class_kinds is not NULL, the choice per class into
  * class_kinds[0..32] (WRS_TABLE_SKIP for absent classes), and if class_ms is not NULL the
  * timings behind the choice into class_ms[0..65] (class c: [2c] as alias, [2c+1] as rejection,
  * in ms; 0 for absent classes). Synchronous. d_kinds_tmp (num_tables
