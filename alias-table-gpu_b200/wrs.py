@@ -479,6 +479,23 @@ class SamplerGpuSectioned(Sampler):
         return out
 
 
+class SamplerGpuSectionedShared(SamplerGpuSectioned):
+    """SamplerGpuSectionedShared (sampling/aliasTable/SamplerGpuSectionedShared.cu:3-111): every
+    section staged in shared memory. alias_sample stages sections of at most 12,288 rows (96 KiB),
+    so this is the sectioned sampler with the reference's default of 3000 rows per section; a
+    section too large to stage raises, as the reference asserts."""
+    MAX_STAGED_ROWS = 12288
+
+    def __init__(self, algorithm: SamplingAlgorithm, itemsPerSection: int = 3000, seed: int = 0x5EED):
+        if not (2 <= itemsPerSection <= self.MAX_STAGED_ROWS) or itemsPerSection % 2:
+            raise WrsError(WRS_ERR_INVALID_ARGUMENT, "SamplerGpuSectionedShared: itemsPerSection must be even, "
+                                                     "in [2, 12288]")
+        super().__init__(algorithm, itemsPerSection, seed)
+
+    def name(self) -> str:
+        return "SamplerGpuSectionedShared"
+
+
 class SamplerRejection(Sampler):
     def __init__(self, algorithm: RejectionSamplingGpu, seed: int = 0x5EED, max_tries: int = 0):
         super().__init__(algorithm, seed)
@@ -496,6 +513,17 @@ class SamplerRejection(Sampler):
                                 self.max_tries), "rejection sample")
         self.counter += numSamples
         return out
+
+
+class SamplerRejectionGiveUp(SamplerRejection):
+    """SamplerRejectionGiveUp (sampling/rejectionSampling/SamplerRejectionGiveUp.cu:17-37, MAX_TRIES 8):
+    at most 8 tries per sample; a sample that runs out of tries is written as 0xFFFFFFFF."""
+
+    def __init__(self, algorithm: RejectionSamplingGpu, seed: int = 0x5EED):
+        super().__init__(algorithm, seed, max_tries=8)
+
+    def name(self) -> str:
+        return "SamplerRejectionGiveUp"
 
 
 class BatchedAliasTablesGpu:

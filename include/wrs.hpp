@@ -297,6 +297,21 @@ protected:
     uint32_t section_;
 };
 
+// SamplerGpuSectionedShared (sampling/aliasTable/SamplerGpuSectionedShared.cu:3-111): each section is
+// staged in shared memory before it is sampled. wrs_alias_sample stages every section of at most
+// 12,288 rows (96 KiB), so this is the sectioned sampler with the reference's default of 3000 rows
+// per section; a section too large to stage is an error, as the reference asserts.
+class SamplerGpuSectionedShared : public SamplerGpuSectioned {
+public:
+    static constexpr uint32_t kMaxStagedRows = 12288;
+    explicit SamplerGpuSectionedShared(AliasTableSplitGpu& a, uint32_t itemsPerSection = 3000, uint64_t seed = 0x5EED)
+        : SamplerGpuSectioned(a, itemsPerSection, seed) {
+        if (itemsPerSection < 2 || itemsPerSection > kMaxStagedRows || (itemsPerSection & 1u))
+            throw Error(WRS_ERR_INVALID_ARGUMENT, "SamplerGpuSectionedShared: itemsPerSection must be even, in [2, 12288]");
+    }
+    std::string name() override { return "SamplerGpuSectionedShared"; }
+};
+
 class SamplerRejection : public Sampler {
 public:
     explicit SamplerRejection(RejectionSamplingGpu& r, uint64_t seed = 0x5EED, uint32_t maxTries = 0)
@@ -313,6 +328,14 @@ protected:
     int64_t items() const override { return r_.N; }
     RejectionSamplingGpu& r_;
     uint32_t tries_;
+};
+
+// SamplerRejectionGiveUp (sampling/rejectionSampling/SamplerRejectionGiveUp.cu:17-37,
+// MAX_TRIES 8 in SamplerRejectionGiveUp.cuh): at most 8 tries per sample; a sample that runs
+// out of tries is written as 0xFFFFFFFF (the reference gives up on it the same way).
+class SamplerRejectionGiveUp : public SamplerRejection {
+public:
+    explicit SamplerRejectionGiveUp(RejectionSamplingGpu& r, uint64_t seed = 0x5EED) : SamplerRejection(r, seed, 8u) {}
 };
 
 // ---------------------------------------------------------------- batches

@@ -91,3 +91,19 @@ def test_header_compiles_as_c_and_cxx():
             continue
         r = subprocess.run([cc, "-fsyntax-only", "-Wall", "-x", lang, hdr], capture_output=True, text=True)
         assert r.returncode == 0, f"{cc}: {r.stderr}"
+
+
+def test_reference_named_sampler_variants():
+    """SamplerGpuSectionedShared / SamplerRejectionGiveUp: the reference's other sampler names,
+    as the sectioned sampler with staged 3000-row sections and rejection with at most 8 tries."""
+    class Table:  # stands in for a built table: the constructors only keep the reference
+        N, device = 10, "cpu"
+
+    s = wrs.SamplerGpuSectionedShared(Table())
+    assert s.name() == "SamplerGpuSectionedShared" and s.itemsPerSection == 3000 and s.counter == 0
+    for bad in (0, 3001, 12290):
+        with pytest.raises(wrs.WrsError) as e:
+            wrs.SamplerGpuSectionedShared(Table(), bad)
+        assert e.value.status == wrs.WRS_ERR_INVALID_ARGUMENT
+    g = wrs.SamplerRejectionGiveUp(Table())
+    assert g.name() == "SamplerRejectionGiveUp" and g.max_tries == 8

@@ -22,13 +22,13 @@ LIB_DIR = os.path.join(REPO, "alias-table-gpu_b200")
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 
 
-def compile_shim(tmp_path):
+def compile_shim(tmp_path, src=SRC):
     cxx = shutil.which("g++")
     if cxx is None or not os.path.exists(os.path.join(CUDA, "include", "cuda_runtime.h")):
         pytest.skip("needs g++ and the CUDA headers")
-    exe = str(tmp_path / "shim_check")
+    exe = str(tmp_path / os.path.splitext(os.path.basename(src))[0])
     cmd = [cxx, "-std=c++17", "-O2", "-Wall", "-Werror", "-I", os.path.join(REPO, "include"),
-           "-I", os.path.join(CUDA, "include"), SRC, "-o", exe, "-L", LIB_DIR, "-lwrs",
+           "-I", os.path.join(CUDA, "include"), src, "-o", exe, "-L", LIB_DIR, "-lwrs",
            "-L", os.path.join(CUDA, "lib64"), "-lcudart",
            f"-Wl,-rpath,{LIB_DIR}:{os.path.join(CUDA, 'lib64')}"]
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -38,6 +38,12 @@ def compile_shim(tmp_path):
 
 def test_shim_compiles_and_links(tmp_path):
     compile_shim(tmp_path)
+
+
+def test_shim_reference_named_variants_compile_and_link(tmp_path):
+    """SamplerGpuSectionedShared and SamplerRejectionGiveUp, the reference's other sampler names."""
+    exe = compile_shim(tmp_path, os.path.join(REPO, "tests", "cpp", "shim_names.cpp"))
+    assert subprocess.run([exe], timeout=60).returncode == 0  # no arguments: touches no device
 
 
 @pytest.mark.gpu
