@@ -205,11 +205,6 @@ __host__ __device__ __forceinline__ Philox4 philox4x32_10(uint32_t c0, uint32_t 
     return r;
 }
 
-// row in [0, len) from 32 random bits, exactly floor(x * len / 2^32).
-__host__ __device__ __forceinline__ uint32_t scale_u32(uint32_t x, uint32_t len) {
-    return (uint32_t)(((uint64_t)x * (uint64_t)len) >> 32);
-}
-
 // index in [0, len) from the 64-bit uniform u = x1:x0, exactly floor(u * len / 2^64): every
 // index gets its share to within len / 2^64 (a 32-bit uniform would leave shares differing by
 // up to len / 2^32 relative, about 2% at 1e8 rows).

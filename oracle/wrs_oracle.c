@@ -101,7 +101,6 @@ static inline void philox_block(uint64_t b, uint32_t c2, uint32_t c3, uint64_t s
     or_philox4x32_10(ctr, key, out);
 }
 
-static inline uint32_t scale_u32(uint32_t x, uint32_t len) { return (uint32_t)(((uint64_t)x * len) >> 32); }
 /* an alias row: floor(u len / 2^64) for the 64-bit uniform u = x1:x0 */
 static inline uint32_t row_of(const uint32_t x[4], uint64_t len) {
     return (uint32_t)((((unsigned __int128)(((uint64_t)x[1] << 32) | x[0])) * len) >> 64);
