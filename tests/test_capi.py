@@ -107,3 +107,25 @@ def test_reference_named_sampler_variants():
         assert e.value.status == wrs.WRS_ERR_INVALID_ARGUMENT
     g = wrs.SamplerRejectionGiveUp(Table())
     assert g.name() == "SamplerRejectionGiveUp" and g.max_tries == 8
+
+
+def test_batched_scratch_queries_plan_on_the_host():
+    """The batched and mixed scratch queries run the host plan alone: valid CSR offsets give a
+    size, offsets that do not start at 0 or that decrease give 0 (the builds then refuse)."""
+    import numpy as np
+    ok = np.array([0, 3, 3, 10, 5000, 5001], dtype=np.int64)
+    a = wrs.batched_build_scratch_bytes(ok)
+    assert a > 0
+    # the default query covers every launch shape the autotuner may pick
+    for small in (32, 64, 128, 256, 512):
+        for tile in (1024, 2048, 4096):
+            s = wrs.batched_build_scratch_bytes(ok, wrs.build_opts(tile_items=tile, small_table_items=small))
+            assert 0 < s <= a
+    assert wrs.batched_build_scratch_bytes(np.array([1, 3, 10], dtype=np.int64)) == 0
+    assert wrs.batched_build_scratch_bytes(np.array([0, 5, 3], dtype=np.int64)) == 0
+    kinds = np.array([wrs.WRS_TABLE_ALIAS, wrs.WRS_TABLE_REJECTION, wrs.WRS_TABLE_SKIP, wrs.WRS_TABLE_ALIAS,
+                      wrs.WRS_TABLE_REJECTION], dtype=np.uint8)
+    m_any = wrs.batched_mixed_build_scratch_bytes(ok)
+    m_kinds = wrs.batched_mixed_build_scratch_bytes(ok, kinds)
+    assert 0 < m_kinds <= m_any
+    assert wrs.batched_mixed_build_scratch_bytes(np.array([0, 5, 3], dtype=np.int64)) == 0
