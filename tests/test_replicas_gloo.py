@@ -53,3 +53,14 @@ def test_single_process_needs_no_group():
     import torch
     assert bench.max_over_ranks(3.5, torch.device("cpu")) == 3.5
     assert bench.replica_value(10 ** 9, 1000.0, 1) == pytest.approx(1.0)
+
+
+def test_reference_arm_runs_on_rank_zero_only():
+    """Under torchrun the reference arm (the reference's CPU path) runs and prints on rank 0;
+    every other rank exits 0 without work or output."""
+    import subprocess
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1", MASTER_ADDR="127.0.0.1")
+    r = subprocess.run([sys.executable, os.path.join(REPO, "bench.py"), "--impl", "reference", "--gpus", "2",
+                        "--steps", "1", "--warmup", "3"], env=env, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.strip() == ""
