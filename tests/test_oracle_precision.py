@@ -97,3 +97,32 @@ def test_psa_plus_pairs_locally():
     same = lambda rows: np.mean((rows[light, 1] // 2048) == (np.nonzero(light)[0] // 2048))
     local, split = same(po.psa_plus_build(w, W, 2048)), same(po.exact_build(w, W))
     assert local > 0.95 and local > split, (local, split)
+
+
+@pytest.mark.skipif(not po.ref_available(debug=True), reason="the compiled reference (oracle/_ref) is not built")
+@pytest.mark.parametrize("name,n", [("uniform", 10_000), ("powerlaw_shuffled", 100_003), ("loguniform", 50_000),
+                                    ("one_heavy", 4097), ("one_light", 505_711), ("zeros_mix", 30_000),
+                                    ("pareto", 65_536), ("all_equal", 1000)])
+def test_reference_verifier_accepts_the_tables(name, n):
+    """The reference's own AliasTable::verifyTableCorrectness (AliasTable.cu:24-65, compiled from
+    its sources, debug build) accepts this library's tables in the reference's row format
+    (weight = prob * W/N in FP64, as wrs_export_reference_table writes them). The tables are the
+    oracle's, which the GPU build reproduces bit for bit. The reference's check is absolute
+    (every item within max(N 1e-8, 1e-3) of its weight), so the log-uniform weights, which reach
+    1e8, are scaled to mean 1 first: at their own scale no FP32-probability table passes it."""
+    w = gen(name, n)
+    if name == "loguniform":
+        w = (w.astype(np.float64) / w.astype(np.float64).mean()).astype(np.float32)
+    rows = po.exact_build(w)
+    W = po.exact_sum(w)
+    weight = rows[:, 0].view(np.float32).astype(np.float64) * (W / n)
+    alias = rows[:, 1].astype(np.int32)
+    assert po.ref_verify(w.astype(np.float64), weight, alias, W)
+    # the verifier is live: a quarter of a donating row's mass moved to its alias fails it
+    # (where W/N is large enough for the absolute tolerance to notice)
+    donors = np.nonzero((alias != np.arange(n)) & (weight > 0.5 * W / n))[0]
+    if W / n >= 0.1 and donors.size:
+        j = int(donors[0])
+        bad = weight.copy()
+        bad[j] *= 0.75
+        assert not po.ref_verify(w.astype(np.float64), bad, alias, W)
