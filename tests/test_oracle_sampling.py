@@ -229,3 +229,20 @@ def test_batched_oracle_matches_per_table_oracle():
             p = rows[off[t] + row, 0].view(np.float32)
             coin = np.float32((int(x[2]) >> 8) * 2.0 ** -24)
             assert out[s] == (row if coin < p else rows[off[t] + row, 1])
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="the compiled reference (oracle/_ref) is not built")
+def test_reference_sampler_draws_from_the_tables():
+    """The reference's own CPU sampler (SamplerCpu::sample, SamplerCpu.cu:12-18, compiled from its
+    sources) driven by this library's table in the reference's row format draws from w_i / W."""
+    rng = np.random.default_rng(31)
+    n = 1000
+    w = (rng.pareto(1.5, n) + 1.0).astype(np.float32)
+    rows = po.exact_build(w)
+    W = po.exact_sum(w)
+    weight = rows[:, 0].view(np.float32).astype(np.float64) * (W / n)
+    alias = rows[:, 1].astype(np.int32)
+    _, out = po.ref_sampler_cpu(weight, alias, W, 1_000_000, want_out=True)
+    assert out.min() >= 0 and out.max() < n
+    counts = np.bincount(out, minlength=n)
+    assert chi2_pvalue(counts, w.astype(np.float64) / W * out.size) > 1e-4
