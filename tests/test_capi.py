@@ -129,3 +129,16 @@ def test_batched_scratch_queries_plan_on_the_host():
     m_kinds = wrs.batched_mixed_build_scratch_bytes(ok, kinds)
     assert 0 < m_kinds <= m_any
     assert wrs.batched_mixed_build_scratch_bytes(np.array([0, 5, 3], dtype=np.int64)) == 0
+
+
+def test_missing_library_fails_loudly():
+    """Without the built CUDA library every entry point raises: there is no CPU fallback."""
+    import subprocess
+    import sys
+    pkg = os.path.dirname(wrs.__file__)
+    code = ("import sys; sys.path.insert(0, %r); import wrs; wrs.LIB_PATH = '/nonexistent/libwrs.so'\n"
+            "try:\n    wrs.alias_build_scratch_bytes(1000)\nexcept RuntimeError as e:\n    print('raised', e)\n"
+            "else:\n    print('no error')\n") % pkg
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.startswith("raised") and "libwrs.so not built" in r.stdout
