@@ -316,7 +316,7 @@ class SamplerRejection : public Sampler {
 public:
     explicit SamplerRejection(RejectionSamplingGpu& r, uint64_t seed = 0x5EED, uint32_t maxTries = 0)
         : Sampler(seed), r_(r), tries_(maxTries) {}
-    std::string name() override { return tries_ ? "SamplerRejectionGiveUp" : "SamplerRejection"; }
+    std::string name() override { return "SamplerRejection"; }
     void sample(uint64_t numSamples, uint32_t* d_out) override {
         check(wrs_rejection_sample(r_.deviceA(), r_.deviceASize(), r_.deviceFrac(), r_.N, numSamples, seed_, counter,
                                    tries_, d_out, nullptr, 0u, r_.stream()), "rejection sample");
@@ -336,6 +336,7 @@ protected:
 class SamplerRejectionGiveUp : public SamplerRejection {
 public:
     explicit SamplerRejectionGiveUp(RejectionSamplingGpu& r, uint64_t seed = 0x5EED) : SamplerRejection(r, seed, 8u) {}
+    std::string name() override { return "SamplerRejectionGiveUp"; }
 };
 
 // ---------------------------------------------------------------- batches
