@@ -126,7 +126,8 @@ wrs_status launch_build(const float* d_w, uint64_t n, uint32_t method, wrs_alias
     const TileMap map{nullptr, nullptr, nullptr, n, (uint32_t)num_tiles};
     tile_reduce_kernel<T, false><<<(uint32_t)num_tiles, kReduceThreads, 0, stream>>>(d_w, L.hdr, L.agg, L.hmask, map);
     tile_prefix_kernel<<<(uint32_t)L.num_blocks, kPrefixThreads, 0, stream>>>(L.hdr, L.agg, L.incl, L.blocks,
-                                                                               (uint32_t)num_tiles);
+                                                                               (uint32_t)num_tiles,
+                                                                               current_wait_cfg());
     heavy_list_kernel<T, false><<<(uint32_t)((num_tiles + heavy_warps(T) - 1) / heavy_warps(T)), 32 * heavy_warps(T),
                                   0, stream>>>(d_w, L.hdr, L.agg, L.incl, L.hmask, (uint32_t)num_tiles, L.heavy_item,
                                                L.heavy_E, map);
@@ -199,7 +200,8 @@ wrs_status launch_psa(const float* d_w, uint64_t n, wrs_alias_row* d_table, doub
                                                                      d_W);
     const TileMap map{nullptr, nullptr, nullptr, n, nt};
     tile_reduce_kernel<T, false><<<nt, kReduceThreads, 0, stream>>>(d_w, L.hdr, L.agg, L.hmask, map);
-    tile_prefix_kernel<<<(uint32_t)L.num_blocks, kPrefixThreads, 0, stream>>>(L.hdr, L.agg, L.incl, L.blocks, nt);
+    const WaitCfg wc = current_wait_cfg();
+    tile_prefix_kernel<<<(uint32_t)L.num_blocks, kPrefixThreads, 0, stream>>>(L.hdr, L.agg, L.incl, L.blocks, nt, wc);
     {
         const size_t smem = psa_local_smem_bytes(T);
         if (cudaFuncSetAttribute(psa_local_kernel<NT, IPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
@@ -207,7 +209,8 @@ wrs_status launch_psa(const float* d_w, uint64_t n, wrs_alias_row* d_table, doub
             return WRS_ERR_CUDA;
         psa_local_kernel<NT, IPT><<<nt, NT, smem, stream>>>(d_w, n, L.hdr, L.incl, d_table, L.slots, L.agg2, L.hdr2);
     }
-    tile_prefix_kernel<<<(uint32_t)L.num_blocks, kPrefixThreads, 0, stream>>>(L.hdr2, L.agg2, L.incl2, L.blocks2, nt);
+    tile_prefix_kernel<<<(uint32_t)L.num_blocks, kPrefixThreads, 0, stream>>>(L.hdr2, L.agg2, L.incl2, L.blocks2, nt,
+                                                                               wc);
     psa_heavy_list_kernel<T><<<(nt + 3) / 4, 128, 0, stream>>>(L.hdr2, L.agg2, L.incl2, L.slots, nt, L.heavy_item2,
                                                                L.heavy_E2);
     tile_link_kernel<false><<<(nt + 1 + 255) / 256, 256, 0, stream>>>(L.hdr2, L.incl2, nt, 1u, L.heavy_E2, L.starts2,

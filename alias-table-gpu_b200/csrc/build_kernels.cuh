@@ -780,7 +780,7 @@ struct __align__(16) BlockWord {  // look-back record of one prefix CTA
 
 static __global__ void __launch_bounds__(kPrefixThreads) tile_prefix_kernel(BuildHeader* hdr, const TileVals* agg,
                                                                      TileVals* incl, BlockWord* blocks,
-                                                                     uint32_t num_tiles) {
+                                                                     uint32_t num_tiles, WaitCfg wc) {
     __shared__ uint32_t s_blk;
     __shared__ PVals s_warp[kPrefixThreads / 32 + 1];
     __shared__ PVals s_base;
@@ -791,8 +791,9 @@ static __global__ void __launch_bounds__(kPrefixThreads) tile_prefix_kernel(Buil
     }
     __syncthreads();
     const uint32_t blk = s_blk;
+    const bool publish = blk != wc.hold;  // a held block (failure-detection tests) publishes nothing
     if (s_abort) {
-        if (threadIdx.x == 0) store_release(&blocks[blk].flag, 2u);
+        if (threadIdx.x == 0 && publish) store_release(&blocks[blk].flag, 2u);
         return;
     }
     const uint32_t t0 = blk * kPrefixTiles + threadIdx.x * kPrefixPerThread;
@@ -835,13 +836,13 @@ static __global__ void __launch_bounds__(kPrefixThreads) tile_prefix_kernel(Buil
     if (warp == 0) {
         PVals excl = pv_zero();
         if (blk == 0) {
-            if (lane == 0) {
+            if (lane == 0 && publish) {
                 blocks[0].agg = btot;
                 blocks[0].incl = btot;
                 store_release(&blocks[0].flag, 2u);
             }
         } else {
-            if (lane == 0) {
+            if (lane == 0 && publish) {
                 blocks[blk].agg = btot;
                 store_release(&blocks[blk].flag, 1u);
             }
@@ -857,7 +858,7 @@ static __global__ void __launch_bounds__(kPrefixThreads) tile_prefix_kernel(Buil
                     while ((fl = load_acquire(&blocks[p].flag)) == 0u) {
                         __nanosleep(20);
                         if ((++spins & 255u) == 0u) {
-                            if (global_ns() - t_start > kWaitLimitNs || load_relaxed(&hdr->status) != 0) {
+                            if (wait_expired(t_start, wc) || load_relaxed(&hdr->status) != 0) {
                                 timed_out = true;
                                 break;
                             }
@@ -888,7 +889,7 @@ static __global__ void __launch_bounds__(kPrefixThreads) tile_prefix_kernel(Buil
                 if (incl_mask) break;
                 pred -= 32;
             }
-            if (lane == 0) {
+            if (lane == 0 && publish) {
                 blocks[blk].incl = pv_add(excl, btot);
                 store_release(&blocks[blk].flag, 2u);
             }

@@ -2,8 +2,37 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 
 #include "host_util.h"
+
+namespace {
+std::atomic<uint64_t> g_wait_limit_ns{0};      // 0: the default, wrs::kWaitLimitNs
+std::atomic<uint32_t> g_hold{0xffffffffu};     // ~0u: no look-back block is held
+}  // namespace
+
+namespace wrs {
+WaitCfg current_wait_cfg() {
+    WaitCfg c;
+    const uint64_t l = g_wait_limit_ns.load(std::memory_order_relaxed);
+    c.limit_ns = l ? l : kWaitLimitNs;
+    c.hold = g_hold.load(std::memory_order_relaxed);
+    c.pad = 0;
+    return c;
+}
+}  // namespace wrs
+
+extern "C" wrs_status wrs_set_device_wait_limit(uint64_t limit_ns) {
+    if (limit_ns > 60ull * 1000000000ull) return WRS_ERR_INVALID_ARGUMENT;
+    g_wait_limit_ns.store(limit_ns, std::memory_order_relaxed);
+    return WRS_SUCCESS;
+}
+
+extern "C" wrs_status wrs_debug_hold_lookback(int64_t block) {
+    if (block < -1 || block >= 0xffffffffll) return WRS_ERR_INVALID_ARGUMENT;
+    g_hold.store(block < 0 ? 0xffffffffu : (uint32_t)block, std::memory_order_relaxed);
+    return WRS_SUCCESS;
+}
 
 extern "C" const char* wrs_status_string(wrs_status s) {
     switch (s) {

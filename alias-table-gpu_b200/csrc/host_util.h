@@ -6,8 +6,12 @@
 #include <cuda_runtime.h>
 
 #include "wrs.h"
+#include "wrs_common.cuh"
 
 namespace wrs {
+
+// The wait limits of launches made now (wrs_set_device_wait_limit, wrs_debug_hold_lookback).
+WaitCfg current_wait_cfg();
 
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 

@@ -40,7 +40,7 @@ template <int IPT>
 __global__ void __launch_bounds__(kBuildThreads) rejection_tile_kernel(
     const float* __restrict__ w, uint64_t n, BuildHeader* hdr, uint64_t* tile_words, uint32_t num_tiles,
     uint32_t* __restrict__ A, uint64_t a_capacity, float* __restrict__ frac, RejBigEntry* big_list,
-    uint64_t big_capacity, uint64_t* a_size_out) {
+    uint64_t big_capacity, uint64_t* a_size_out, WaitCfg wc) {
     constexpr int T = kBuildThreads * IPT;
     __shared__ uint32_t s_tile;
     __shared__ int s_abort;
@@ -60,8 +60,9 @@ __global__ void __launch_bounds__(kBuildThreads) rejection_tile_kernel(
     __syncthreads();
     const uint32_t tile = s_tile;
     if (tile >= num_tiles) return;
+    const bool publish = tile != wc.hold;  // a held tile (failure-detection tests) publishes nothing
     if (s_abort) {
-        if (threadIdx.x == 0) store_release_u64(&tile_words[tile], (2ull << 62));
+        if (threadIdx.x == 0 && publish) store_release_u64(&tile_words[tile], (2ull << 62));
         return;
     }
     const double W = hdr->W_hi;
@@ -126,9 +127,9 @@ __global__ void __launch_bounds__(kBuildThreads) rejection_tile_kernel(
     if (threadIdx.x < 32) {
         uint64_t excl = 0;
         if (tile == 0) {
-            if (lane == 0) store_release_u64(&tile_words[0], (2ull << 62) | tile_total);
+            if (lane == 0 && publish) store_release_u64(&tile_words[0], (2ull << 62) | tile_total);
         } else {
-            if (lane == 0) store_release_u64(&tile_words[tile], (1ull << 62) | tile_total);
+            if (lane == 0 && publish) store_release_u64(&tile_words[tile], (1ull << 62) | tile_total);
             int64_t pred = (int64_t)tile - 1;
             bool timed_out = false;
             const uint64_t t_start = global_ns();
@@ -140,7 +141,7 @@ __global__ void __launch_bounds__(kBuildThreads) rejection_tile_kernel(
                     while (((word = load_acquire_u64(&tile_words[p])) >> 62) == 0u) {
                         __nanosleep(32);
                         if ((++spins & 255u) == 0u) {
-                            if (global_ns() - t_start > kWaitLimitNs || load_relaxed(&hdr->status) != 0) {
+                            if (wait_expired(t_start, wc) || load_relaxed(&hdr->status) != 0) {
                                 timed_out = true;
                                 break;
                             }
@@ -161,7 +162,7 @@ __global__ void __launch_bounds__(kBuildThreads) rejection_tile_kernel(
                 if (mask) break;
                 pred -= 32;
             }
-            if (lane == 0) store_release_u64(&tile_words[tile], (2ull << 62) | (excl + tile_total));
+            if (lane == 0 && publish) store_release_u64(&tile_words[tile], (2ull << 62) | (excl + tile_total));
         }
         if (lane == 0) {
             s_base = excl;

@@ -183,7 +183,8 @@ extern "C" wrs_status wrs_rejection_build_f32(const float* d_w, int64_t n, uint3
     wsum_kernel<kWsumBlock><<<wsum_grid((uint64_t)n), kWsumBlock, 0, stream>>>(
         d_w, (uint64_t)n, L.hdr, L.partials, reinterpret_cast<uint32_t*>(L.tile_words), 2 * nt, d_W);
     rejection_tile_kernel<kRejIpt><<<(uint32_t)nt, kBuildThreads, 0, stream>>>(
-        d_w, (uint64_t)n, L.hdr, L.tile_words, (uint32_t)nt, d_A, a_capacity, d_frac, L.big, L.big_capacity, d_A_size);
+        d_w, (uint64_t)n, L.hdr, L.tile_words, (uint32_t)nt, d_A, a_capacity, d_frac, L.big, L.big_capacity, d_A_size,
+        current_wait_cfg());
     const DeviceInfo dev = device_info();
     rejection_big_kernel<<<(uint32_t)dev.sm_count * 4, 256, 0, stream>>>(L.hdr, L.big, L.big_capacity, d_A, a_capacity,
                                                                       L.huge, L.huge_capacity);

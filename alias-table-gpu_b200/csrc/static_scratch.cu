@@ -5,15 +5,21 @@
 // touch the host process's memory pools, or paths that may not block on an allocation.
 // wrs_alias_build_f32_static_scratch builds tables of up to kStaticMaxItems items with
 // its scratch in a fixed device array of kStaticScratchBytes (8 MiB) that lives in this
-// library: every GPU that loads the library holds that array until the process exits.
+// library: every GPU that loads the library holds that array until the process exits. The
+// driver reserves it when it loads this library's device code on a device, which with lazy
+// module loading (the CUDA default) is the first call of any entry point on that device.
 // The caller still passes the weights, the table and the optional W output.
 //
 // The array's name is only a host-side stand-in in host code, so its device address is
-// looked up with cudaGetSymbolAddress, once per device, with that device current; the
-// first call on each device does this set-up (make it before any stream capture).
-// All calls on a device share the one array: calls that overlap on the GPU race and
-// corrupt each other's results, so serialise them (one stream, or events). The build
-// itself clears what must start at zero (the scratch header) on every call.
+// looked up with cudaGetSymbolAddress, with the device current, at the first call on each
+// device (make that call before any stream capture). The address is kept per device and
+// per CUDA context: after a device reset (a new primary context) the next call looks it up
+// again. All calls on a device share the one array: calls that overlap on the GPU race and
+// corrupt each other's results, so serialise them (one stream, or events). The build itself
+// clears what must start at zero (the scratch header) on every call; the header's status
+// word then keeps the last call's device-side status until the next call on that device
+// (wrs_static_scratch_status reads it).
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -28,21 +34,49 @@ constexpr size_t kStaticScratchBytes = (size_t)8 << 20;  // 8 MiB (>= the build'
 
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+
+struct DeviceSlot {
+    CUcontext ctx = nullptr;  // the context the address belongs to
+    void* ptr = nullptr;      // device address of g_static_scratch in that context
+};
+
 std::mutex g_mu;
-std::vector<void*> g_dev_ptr;  // per device ordinal: device address of g_static_scratch
+std::vector<DeviceSlot> g_slots;  // per device ordinal
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+bool g_ctx_fn_looked_up = false;
+
+// The current CUDA context, through the driver entry point the runtime hands out (this
+// library links only the CUDA runtime). nullptr when the driver does not provide it.
+CUcontext current_context() {
+    if (!g_ctx_fn_looked_up) {
+        g_ctx_fn_looked_up = true;
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(fn);
+    }
+    CUcontext c = nullptr;
+    if (g_ctx_get_current == nullptr || g_ctx_get_current(&c) != CUDA_SUCCESS) return nullptr;
+    return c;
+}
 
 wrs_status static_scratch_address(void** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return WRS_ERR_CUDA;
     std::lock_guard<std::mutex> lock(g_mu);
-    if ((int)g_dev_ptr.size() <= dev) g_dev_ptr.resize(dev + 1, nullptr);
-    if (g_dev_ptr[dev] == nullptr) {
+    if ((int)g_slots.size() <= dev) g_slots.resize(dev + 1);
+    DeviceSlot& s = g_slots[dev];
+    const CUcontext ctx = current_context();
+    if (s.ptr == nullptr || ctx == nullptr || ctx != s.ctx) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
         if (e != cudaSuccess || p == nullptr) return WRS_ERR_CUDA;
-        g_dev_ptr[dev] = p;
+        s.ptr = p;
+        s.ctx = ctx;
     }
-    *out = g_dev_ptr[dev];
+    *out = s.ptr;
     return WRS_SUCCESS;
 }
 
@@ -57,4 +91,11 @@ extern "C" wrs_status wrs_alias_build_f32_static_scratch(const float* d_w, int64
     const wrs_status st = static_scratch_address(&scratch);
     if (st != WRS_SUCCESS) return st;
     return wrs_alias_build_f32(d_w, n, opts, d_table, d_W, scratch, kStaticScratchBytes, stream);
+}
+
+extern "C" wrs_status wrs_static_scratch_status(void* stream) {
+    void* scratch = nullptr;
+    const wrs_status st = static_scratch_address(&scratch);
+    if (st != WRS_SUCCESS) return st;
+    return wrs_scratch_status(scratch, stream);
 }

@@ -241,4 +241,17 @@ __device__ __forceinline__ uint64_t global_ns() {
 }
 constexpr uint64_t kWaitLimitNs = 2000000000ull;  // 2 s: far above any legitimate wait
 
+// Limits of the bounded device waits, passed to every kernel that waits: a look-back wait
+// gives up after limit_ns (records WRS_ERR_DEVICE_TIMEOUT and returns); look-back block or
+// tile `hold` (~0u: none) publishes nothing, so that its successors' waits run out — the
+// failure-detection tests' way of making a wait that nothing ends.
+struct WaitCfg {
+    uint64_t limit_ns;
+    uint32_t hold;
+    uint32_t pad;
+};
+__device__ __forceinline__ bool wait_expired(uint64_t t_start, const WaitCfg& wc) {
+    return global_ns() - t_start > wc.limit_ns;
+}
+
 }  // namespace wrs

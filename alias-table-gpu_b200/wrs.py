@@ -89,6 +89,9 @@ _SIGNATURES = {
     "wrs_batched_autotune_kinds": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _SZ,
                                                   _P, _P, _P, _P]),
     "wrs_scratch_status": (ctypes.c_int, [_P, _P]),
+    "wrs_static_scratch_status": (ctypes.c_int, [_P]),
+    "wrs_set_device_wait_limit": (ctypes.c_int, [_U64]),
+    "wrs_debug_hold_lookback": (ctypes.c_int, [_I64]),
     "wrs_export_reference_table": (ctypes.c_int, [_P, _I64, ctypes.c_double, _P, _P, _P]),
     "wrs_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "wrs_check_device": (ctypes.c_int, []),
@@ -161,6 +164,23 @@ def alias_build_static_scratch(w, table, opts: Optional[BuildOpts] = None, W_out
     memory; the scratch is a fixed array inside the library, shared by all calls on a device."""
     return lib().wrs_alias_build_f32_static_scratch(_ptr(w), w.numel(), ctypes.byref(opts) if opts else None,
                                                     _ptr(table), _ptr(W_out), _stream(stream))
+
+
+def set_device_wait_limit(limit_ns: int) -> int:
+    """Limit of every bounded device wait of later launches (0 = the default, 2 s)."""
+    return lib().wrs_set_device_wait_limit(limit_ns)
+
+
+def debug_hold_lookback(block: int) -> int:
+    """Failure-detection tests: look-back block `block` of later builds publishes nothing
+    (-1 = off), so its successors' waits run out."""
+    return lib().wrs_debug_hold_lookback(block)
+
+
+def static_scratch_status(stream=None) -> int:
+    """Device status of the last allocation-free build on the current device (synchronises
+    `stream`); valid until the next such build on that device."""
+    return lib().wrs_static_scratch_status(_stream(stream))
 
 
 def alias_sample(table, n: int, num_samples: int, seed: int, out, counter_base: int = 0,

@@ -132,15 +132,24 @@ WRS_API wrs_status wrs_alias_build_f32(const float* d_w, int64_t n, const wrs_bu
 /* The same build for callers that cannot allocate device memory (code under an allocator
  * that forbids cudaMalloc, plugins that must not touch the host process's memory pools,
  * paths that may not block on an allocation). No counterpart in the reference. Its scratch
- * is a fixed 8 MiB device array inside this library (held on every GPU that loads it until
- * the process exits), so it takes n <= 262,144 (2^18) items (about 190,000 with
- * WRS_METHOD_PSA_PLUS, which needs more scratch) and rejects larger n with
- * WRS_ERR_INVALID_ARGUMENT. It calls no allocating routine. The first call on each device
- * looks up the array's device address (make it before any stream capture). All calls on a
- * device share the array, so calls that overlap on the GPU race: serialise them. Device-side
- * errors are returned when opts->flags has WRS_FLAG_SYNC. */
+ * is a fixed 8 MiB device array inside this library, so it takes n <= 262,144 (2^18) items
+ * (about 190,000 with WRS_METHOD_PSA_PLUS, which needs more scratch) and rejects larger n
+ * with WRS_ERR_INVALID_ARGUMENT. It calls no allocating routine itself, but the driver
+ * reserves the array on a device when it loads this library's device code there: with lazy
+ * module loading (the CUDA default) that is the first call of any wrs_* entry point on that
+ * device, so make one warm-up call (or set CUDA_MODULE_LOADING=EAGER) before entering a
+ * region that must not allocate or a stream capture. The array stays reserved on every GPU
+ * that loaded it until the process exits. The first call on each device (and the first after
+ * a device reset, which makes a new context) looks up the array's device address. All calls
+ * on a device share the array, so calls that overlap on the GPU race: serialise them.
+ * Device-side errors are returned when opts->flags has WRS_FLAG_SYNC; without it,
+ * wrs_static_scratch_status reads them afterwards. */
 WRS_API wrs_status wrs_alias_build_f32_static_scratch(const float* d_w, int64_t n, const wrs_build_opts* opts,
                                                       wrs_alias_row* d_table, double* d_W, void* stream);
+/* Reads (synchronising `stream`) the device status word of the current device's static
+ * scratch array: the status of the last wrs_alias_build_f32_static_scratch call on this
+ * device, valid until the next such call. No counterpart in the reference. */
+WRS_API wrs_status wrs_static_scratch_status(void* stream);
 
 /* Sampling-input contract (bit-exact, see the oracle):
  *   output position s uses Philox4x32-10 with key (lo32(seed), hi32(seed)) and counter
@@ -294,6 +303,18 @@ WRS_API wrs_status wrs_export_reference_table(const wrs_alias_row* d_table, int6
                                               double* d_weight, int32_t* d_alias, void* stream);
 
 /* ---- status / misc ------------------------------------------------------ */
+
+/* Bounded device waits. Every device-side wait of the library (the decoupled look-back scans
+ * of the builds) gives up after a time limit, records WRS_ERR_DEVICE_TIMEOUT in the status
+ * word and returns, so a wait never hangs the GPU. This sets the limit for launches this
+ * process makes from now on: limit_ns = 0 restores the default (2 s); at most 60 s. No
+ * counterpart in the reference (its kernels never wait on one another). */
+WRS_API wrs_status wrs_set_device_wait_limit(uint64_t limit_ns);
+/* For failure-detection tests: look-back block or tile `block` (its index in launch order) of
+ * the builds launched from now on publishes nothing, so that the waits of the blocks after it
+ * run out at the limit and the build reports WRS_ERR_DEVICE_TIMEOUT (its outputs are then
+ * invalid); block = -1 turns this off. No counterpart in the reference. */
+WRS_API wrs_status wrs_debug_hold_lookback(int64_t block);
 
 /* Reads (synchronising `stream`) the device status word of a build scratch buffer. */
 WRS_API wrs_status wrs_scratch_status(const void* d_scratch, void* stream);

@@ -16,6 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libref.so")
 REF_DBG_SO = os.path.join(HERE, "_ref", "libref_dbg.so")
+REF_GPU_SO = os.path.join(HERE, "_ref", "libref_gpu.so")
 
 _P = ctypes.c_void_p
 _I64 = ctypes.c_int64
@@ -49,6 +50,7 @@ def oracle() -> ctypes.CDLL:
             "or_check_ref_table": (_I, [_P, _I64, _P, _P, _D, _P]),
             "or_exact_build": (_I, [_P, _I64, _D, _P]),
             "or_sample_plain": (None, [_P, _I64, _U64, _U64, _U64, _P]),
+            "or_plain_replay_uniforms": (None, [_I64, _U64, _U64, _U64, _P, _P, _P]),
             "or_binomial": (_U64, [_U64, _D, _U32, _U32, _U64, _U32]),
             "or_section_counts": (None, [_I64, _U32, _U64, _U64, _U64, _P]),
             "or_sample_sectioned": (None, [_P, _I64, _U64, _U32, _U64, _U64, _P, _P]),
@@ -93,6 +95,29 @@ def ref(debug: bool = False) -> ctypes.CDLL:
             f.argtypes = args
         _ref[key] = L
     return _ref[key]
+
+
+def ref_gpu_available() -> bool:
+    return os.path.exists(REF_GPU_SO)
+
+
+def ref_gpu() -> ctypes.CDLL:
+    """The reference's own GPU code (doSample, the rejection build and acceptance), compiled
+    from its sources for sm_100a (test infrastructure; needs a GPU to call)."""
+    if "gpu" not in _ref:
+        L = ctypes.CDLL(REF_GPU_SO)
+        sig = {
+            "ref_gpu_do_sample_aos": (_I, [_P, _P, _I, _D, _P, _P, _I]),
+            "ref_gpu_do_sample_soa": (_I, [_P, _P, _I, _D, _P, _P, _I]),
+            "ref_gpu_rejection_build": (_I, [_P, _I, _D, _P, ctypes.c_longlong, _P]),
+            "ref_gpu_rejection_fraction": (_I, [_P, _I, _D, _P]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _ref["gpu"] = L
+    return _ref["gpu"]
 
 
 def _p(a: np.ndarray) -> int:
@@ -193,6 +218,16 @@ def sample_plain(rows: np.ndarray, m: int, seed: int, cbase: int = 0) -> np.ndar
     out = np.zeros(m, dtype=np.uint32)
     oracle().or_sample_plain(_p(rows), rows.shape[0], m, seed, cbase, _p(out))
     return out
+
+
+def plain_replay_uniforms(n: int, m: int, seed: int, cbase: int = 0):
+    """u = (row + coin) / n for output positions 0..m-1 of the plain contract, with the
+    (row, coin) pairs themselves."""
+    u = np.zeros(m, dtype=np.float64)
+    rows = np.zeros(m, dtype=np.uint32)
+    coins = np.zeros(m, dtype=np.float32)
+    oracle().or_plain_replay_uniforms(n, m, seed & (2**64 - 1), cbase & (2**64 - 1), _p(u), _p(rows), _p(coins))
+    return u, rows, coins
 
 
 def psa_plus_build(w: np.ndarray, W: float | None = None, tile: int = 2048) -> np.ndarray:

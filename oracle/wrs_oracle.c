@@ -851,6 +851,24 @@ void or_sample_plain(const uint32_t* rows, int64_t n, uint64_t m, uint64_t seed,
     }
 }
 
+/* The uniforms that make the reference's doSample (SamplerGpuBasic.cu:28-69: rand = u * N,
+ * row = (int)rand, frac = rand - row) decide on the contract's (row, coin) of output position
+ * s: u = (row + coin) / n in FP64. For power-of-two n <= 2^29, u * n = row + coin exactly
+ * (24 + 29 bits fit in 53), so (int)(u * n) = row and u * n - row = coin. rows_out and
+ * coins_out (optional) receive the pair itself. */
+void or_plain_replay_uniforms(int64_t n, uint64_t m, uint64_t seed, uint64_t cbase, double* u, uint32_t* rows_out,
+                              float* coins_out) {
+    for (uint64_t s = 0; s < m; ++s) {
+        uint32_t x[4];
+        philox_block(cbase + s, 0, 0, seed, x);
+        const uint32_t row = row_of(x, (uint64_t)n);
+        const float c = coin24(x[2]);
+        u[s] = ((double)row + (double)c) / (double)n;
+        if (rows_out) rows_out[s] = row;
+        if (coins_out) coins_out[s] = c;
+    }
+}
+
 void or_batched_sample(const uint32_t* rows, const int64_t* off, int64_t num_tables, const int64_t* soff,
                        uint64_t seed, uint64_t cbase, uint32_t* out) {
     for (int64_t t = 0; t < num_tables; ++t) {

@@ -58,6 +58,8 @@ int or_exact_build(const float* w, int64_t n, double W, uint32_t* rows);
 
 /* sampling contract */
 void or_sample_plain(const uint32_t* rows, int64_t n, uint64_t m, uint64_t seed, uint64_t cbase, uint32_t* out);
+void or_plain_replay_uniforms(int64_t n, uint64_t m, uint64_t seed, uint64_t cbase, double* u, uint32_t* rows_out,
+                              float* coins_out);
 uint64_t or_binomial(uint64_t n, double p, uint32_t k0, uint32_t k1, uint64_t cbase, uint32_t node);
 void or_section_counts(int64_t n, uint32_t S, uint64_t m, uint64_t seed, uint64_t cbase, uint64_t* counts);
 void or_sample_sectioned(const uint32_t* rows, int64_t n, uint64_t m, uint32_t S, uint64_t seed, uint64_t cbase,

@@ -142,3 +142,11 @@ def test_missing_library_fails_loudly():
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stderr
     assert r.stdout.startswith("raised") and "libwrs.so not built" in r.stdout
+
+
+def test_wait_limit_setters_check_their_arguments():
+    assert wrs.set_device_wait_limit(0) == wrs.WRS_SUCCESS
+    assert wrs.set_device_wait_limit(61 * 10 ** 9) == wrs.WRS_ERR_INVALID_ARGUMENT
+    assert wrs.debug_hold_lookback(-2) == wrs.WRS_ERR_INVALID_ARGUMENT
+    assert wrs.debug_hold_lookback(3) == wrs.WRS_SUCCESS
+    assert wrs.debug_hold_lookback(-1) == wrs.WRS_SUCCESS

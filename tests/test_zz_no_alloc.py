@@ -43,7 +43,7 @@ def static_build(w, opts):
     return st, table.cpu().numpy(), W.item()
 
 
-@pytest.mark.parametrize("tile", [0, 1024])
+@pytest.mark.parametrize("tile", [0, 1024, 4096])
 def test_static_scratch_build_matches_regular_build_twice(cuda, tile):
     opts = wrs.build_opts(tile_items=tile, sync=True)
     cases = [("powerlaw", MAX_ITEMS, 11), ("uniform", 100_003, 12)]  # two calls in a row
@@ -72,3 +72,38 @@ def test_static_scratch_build_reports_device_errors_with_sync(cuda):
     assert st == wrs.WRS_SUCCESS
     ref, _ = regular_build(w, wrs.build_opts(sync=True))
     np.testing.assert_array_equal(got, ref)
+
+
+def test_static_scratch_psa_plus_matches_regular_build(cuda):
+    """PSA+ through the allocation-free entry point, below its documented limit (about
+    190,000 items): two calls in a row, each bit for bit the regular PSA+ build."""
+    opts = wrs.build_opts(method=wrs.WRS_METHOD_PSA_PLUS, sync=True)
+    for kind, n, seed in [("uniform", 150_000, 21), ("powerlaw", 65_537, 22)]:
+        w = torch.from_numpy(weights(kind, n, seed)).cuda()
+        st, got, W_got = static_build(w, opts)
+        assert st == wrs.WRS_SUCCESS, wrs.status_string(st)
+        ref, W_ref = regular_build(w, opts)
+        assert W_got == W_ref
+        np.testing.assert_array_equal(got, ref)
+
+
+def test_static_scratch_psa_plus_rejects_tables_whose_scratch_exceeds_the_array(cuda):
+    """n = 2^18 is within the item limit, but PSA+ needs more than the 8 MiB array holds."""
+    opts = wrs.build_opts(method=wrs.WRS_METHOD_PSA_PLUS, sync=True)
+    assert wrs.alias_build_scratch_bytes(MAX_ITEMS, opts) > 8 << 20
+    w = torch.ones(MAX_ITEMS, dtype=torch.float32, device="cuda")
+    table = torch.empty(MAX_ITEMS, dtype=torch.int64, device="cuda")
+    assert wrs.alias_build_static_scratch(w, table, opts) == wrs.WRS_ERR_INVALID_ARGUMENT
+
+
+def test_static_scratch_status_reports_an_error_without_sync(cuda):
+    """Without WRS_FLAG_SYNC the call returns at once; the device-side error of that build is
+    read afterwards from the library's array, and the next build clears it."""
+    w = torch.ones(5000, dtype=torch.float32, device="cuda")
+    w[17] = float("nan")
+    table = torch.empty(5000, dtype=torch.int64, device="cuda")
+    assert wrs.alias_build_static_scratch(w, table) == wrs.WRS_SUCCESS
+    assert wrs.static_scratch_status() == wrs.WRS_ERR_INVALID_WEIGHT
+    w[17] = 2.0
+    assert wrs.alias_build_static_scratch(w, table) == wrs.WRS_SUCCESS
+    assert wrs.static_scratch_status() == wrs.WRS_SUCCESS
