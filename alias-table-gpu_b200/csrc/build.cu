@@ -6,8 +6,8 @@
 //
 // Unlike the reference build (>= 5 blocking device-to-host copies and >= 3 cudaMalloc/cudaFree
 // pairs inside build()), the whole build is stream-ordered work on caller memory: a 128-byte
-// memset of the scratch header, then the wsum, tile_reduce, tile_prefix, heavy_list,
-// tile_link and split_pack kernels.
+// memset of the scratch header, then the wsum, scan, link and pack kernels (split method), or
+// the wsum, tile_reduce, tile_prefix, psa_local and leftover passes (PSA+).
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -15,6 +15,7 @@
 
 #include "build_kernels.cuh"
 #include "psa_kernels.cuh"
+#include "split_kernels.cuh"
 #include "host_util.h"
 
 namespace wrs {
@@ -68,12 +69,12 @@ namespace {
 
 constexpr int64_t kMaxItems = (int64_t)0x7fffffff - 8192;
 
-// Items per tile of the reduce and pack passes (0 = the default: 2048, and 1024 for PSA+,
-// whose local pass is faster on smaller tiles).
+// Items per tile of the scan and pack passes (0 = the default: 4096, and 1024 for PSA+, whose
+// local pass is faster on smaller tiles).
 int64_t tile_items_for(const wrs_build_opts* opts) {
     const uint32_t t = opts ? opts->tile_items : 0u;
     switch (t) {
-        case 0: return (opts && opts->method == WRS_METHOD_PSA_PLUS) ? 1024 : 2048;
+        case 0: return (opts && opts->method == WRS_METHOD_PSA_PLUS) ? 1024 : 4096;
         case 2048: return 2048;
         case 1024: return 1024;
         case 4096: return 4096;
@@ -81,65 +82,78 @@ int64_t tile_items_for(const wrs_build_opts* opts) {
     }
 }
 
-struct BuildLayout {
+// The split method: wsum (W, class thresholds, look-back flags cleared), scan (tile sums,
+// look-back prefixes, tile starts, compact heavy list), link (the split search per tile
+// boundary), pack_walk (the merge, walk form) and split_pack's chunked form for the tiles whose
+// heavies exceed the walk arrays.
+struct SplitLayout {
     BuildHeader* hdr;
     double2* partials;
-    BlockWord* blocks;
-    uint64_t num_blocks;
-    TileVals* agg;
-    TileVals* incl;
+    ScanRecs rec;
     TileStart* starts;
-    uint32_t* hmask;
     uint32_t* heavy_item;
-    uint4* heavy_E;
+    uint64_t* heavy_E;
     size_t bytes;
 };
 
-BuildLayout carve_build(void* scratch, uint64_t n, uint64_t num_tiles, uint64_t tile_items) {
+SplitLayout carve_split(void* scratch, uint64_t n, uint64_t num_tiles) {
     Carver c(scratch);
-    BuildLayout L;
+    SplitLayout L;
     L.hdr = c.take<BuildHeader>(1);
     L.partials = c.take<double2>(kWsumMaxGrid);
-    L.num_blocks = (num_tiles + kPrefixTiles - 1) / kPrefixTiles;
-    L.blocks = c.take<BlockWord>(L.num_blocks);
-    L.agg = c.take<TileVals>(num_tiles);
-    L.incl = c.take<TileVals>(num_tiles);
+    L.rec.flag = c.take<uint32_t>(num_tiles);
+    L.rec.agg = c.take<ScanVals>(num_tiles);
+    L.rec.incl = c.take<ScanVals>(num_tiles);
     L.starts = c.take<TileStart>(num_tiles + 1);
-    L.hmask = c.take<uint32_t>(num_tiles * (tile_items / 32));
     L.heavy_item = c.take<uint32_t>(n);
-    L.heavy_E = c.take<uint4>(n);
+    L.heavy_E = c.take<uint64_t>(n);
     L.bytes = c.off;
     return L;
 }
 
 template <int T>
-wrs_status launch_build(const float* d_w, uint64_t n, uint32_t method, wrs_alias_row* d_table, double* d_W,
-                        const BuildLayout& L, uint64_t num_tiles, cudaStream_t stream) {
-    constexpr int NT = PackShape<T>::NT, IPT = PackShape<T>::IPT;
-    (void)method;
-    cudaError_t e = cudaMemsetAsync(L.hdr, 0, sizeof(BuildHeader), stream);
-    if (e != cudaSuccess) return WRS_ERR_CUDA;
-    const uint32_t g = wsum_grid(n);
-    const uint64_t zero_words = L.num_blocks * sizeof(BlockWord) / sizeof(uint32_t);
-    wsum_kernel<kWsumBlock><<<g, kWsumBlock, 0, stream>>>(d_w, n, L.hdr, L.partials,
-                                                          reinterpret_cast<uint32_t*>(L.blocks), zero_words, d_W);
-    const TileMap map{nullptr, nullptr, nullptr, n, (uint32_t)num_tiles};
-    tile_reduce_kernel<T, false><<<(uint32_t)num_tiles, kReduceThreads, 0, stream>>>(d_w, L.hdr, L.agg, L.hmask, map);
-    tile_prefix_kernel<<<(uint32_t)L.num_blocks, kPrefixThreads, 0, stream>>>(L.hdr, L.agg, L.incl, L.blocks,
-                                                                               (uint32_t)num_tiles,
-                                                                               current_wait_cfg());
-    heavy_list_kernel<T, false><<<(uint32_t)((num_tiles + heavy_warps(T) - 1) / heavy_warps(T)), 32 * heavy_warps(T),
-                                  0, stream>>>(d_w, L.hdr, L.agg, L.incl, L.hmask, (uint32_t)num_tiles, L.heavy_item,
-                                               L.heavy_E, map);
-    tile_link_kernel<false><<<(uint32_t)((num_tiles + 1 + 255) / 256), 256, 0, stream>>>(
-        L.hdr, L.incl, (uint32_t)num_tiles, 1u, L.heavy_E, L.starts, map);
+struct SplitShape;
+template <>
+struct SplitShape<1024> {
+    static constexpr int SCAN_IPT = 4, NT = 128, IPT = 8;
+};
+template <>
+struct SplitShape<2048> {
+    static constexpr int SCAN_IPT = 8, NT = 256, IPT = 8;
+};
+template <>
+struct SplitShape<4096> {
+    static constexpr int SCAN_IPT = 16, NT = 256, IPT = 16;
+};
+
+template <int T>
+wrs_status launch_split(const float* d_w, uint64_t n, wrs_alias_row* d_table, double* d_W, const SplitLayout& L,
+                        uint64_t num_tiles, cudaStream_t stream) {
+    using S = SplitShape<T>;
+    static_assert(S::NT * S::IPT == T && kScanThreads * S::SCAN_IPT == T, "tile shapes");
+    const uint32_t nt = (uint32_t)num_tiles;
+    if (cudaMemsetAsync(L.hdr, 0, sizeof(BuildHeader), stream) != cudaSuccess) return WRS_ERR_CUDA;
+    wsum_kernel<kWsumBlock><<<wsum_grid(n), kWsumBlock, 0, stream>>>(d_w, n, L.hdr, L.partials, L.rec.flag, nt, d_W);
+    scan_kernel<S::SCAN_IPT><<<nt, kScanThreads, 0, stream>>>(d_w, n, L.hdr, L.rec, nt, L.starts, L.heavy_item,
+                                                                L.heavy_E, current_wait_cfg());
+    if (nt > 1) link_kernel<<<(nt - 1 + 255) / 256, 256, 0, stream>>>(L.hdr, nt, L.heavy_E, L.starts);
     {
+        const size_t smem = pack_walk_smem_bytes(T);
+        if (cudaFuncSetAttribute(pack_walk_kernel<S::NT, S::IPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem) != cudaSuccess)
+            return WRS_ERR_CUDA;
+        pack_walk_kernel<S::NT, S::IPT><<<nt, S::NT, smem, stream>>>(d_w, n, L.hdr, L.starts, L.heavy_item,
+                                                                      L.heavy_E, nt, d_table);
+    }
+    {
+        constexpr int NT = PackShape<T>::NT, IPT = PackShape<T>::IPT;
         const size_t smem = pack_smem_bytes(T);
-        e = cudaFuncSetAttribute(split_pack_kernel<NT, IPT, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
-        if (e != cudaSuccess) return WRS_ERR_CUDA;
-        split_pack_kernel<NT, IPT, false, false><<<(uint32_t)num_tiles, NT, smem, stream>>>(
-            d_w, L.hdr, L.incl, L.starts, L.heavy_item, L.heavy_E, (uint32_t)num_tiles, d_table, map, nullptr);
+        if (cudaFuncSetAttribute(split_pack_kernel<NT, IPT, false, false, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return WRS_ERR_CUDA;
+        const TileMap map{nullptr, nullptr, nullptr, n, nt};
+        split_pack_kernel<NT, IPT, false, false, true><<<nt, NT, smem, stream>>>(
+            d_w, L.hdr, nullptr, L.starts, L.heavy_item, L.heavy_E, nt, d_table, map, nullptr);
     }
     return launch_status();
 }
@@ -260,7 +274,7 @@ extern "C" size_t wrs_alias_build_scratch_bytes(int64_t n, const wrs_build_opts*
     if (n < 1 || T < 0) return 0;
     const uint64_t nt = ((uint64_t)n + T - 1) / T;
     if (opts && opts->method == WRS_METHOD_PSA_PLUS) return carve_psa(nullptr, (uint64_t)n, nt, T).bytes;
-    return carve_build(nullptr, (uint64_t)n, nt, T).bytes;
+    return carve_split(nullptr, (uint64_t)n, nt).bytes;
 }
 
 extern "C" wrs_status wrs_alias_build_f32(const float* d_w, int64_t n, const wrs_build_opts* opts,
@@ -285,14 +299,14 @@ extern "C" wrs_status wrs_alias_build_f32(const float* d_w, int64_t n, const wrs
         if (opts->flags & WRS_FLAG_SYNC) return read_device_status(&L.hdr->status, stream);
         return WRS_SUCCESS;
     }
-    if (scratch_bytes < carve_build(nullptr, (uint64_t)n, nt, T).bytes) return WRS_ERR_SCRATCH_TOO_SMALL;
+    if (scratch_bytes < carve_split(nullptr, (uint64_t)n, nt).bytes) return WRS_ERR_SCRATCH_TOO_SMALL;
     cudaStream_t stream = static_cast<cudaStream_t>(stream_);
-    const BuildLayout L = carve_build(d_scratch, (uint64_t)n, nt, T);
+    const SplitLayout L = carve_split(d_scratch, (uint64_t)n, nt);
     wrs_status st;
     switch (T) {
-        case 1024: st = launch_build<1024>(d_w, (uint64_t)n, method, d_table, d_W, L, nt, stream); break;
-        case 4096: st = launch_build<4096>(d_w, (uint64_t)n, method, d_table, d_W, L, nt, stream); break;
-        default: st = launch_build<2048>(d_w, (uint64_t)n, method, d_table, d_W, L, nt, stream); break;
+        case 1024: st = launch_split<1024>(d_w, (uint64_t)n, d_table, d_W, L, nt, stream); break;
+        case 2048: st = launch_split<2048>(d_w, (uint64_t)n, d_table, d_W, L, nt, stream); break;
+        default: st = launch_split<4096>(d_w, (uint64_t)n, d_table, d_W, L, nt, stream); break;
     }
     if (st != WRS_SUCCESS) return st;
     if (opts && (opts->flags & WRS_FLAG_SYNC)) return read_device_status(&L.hdr->status, stream);

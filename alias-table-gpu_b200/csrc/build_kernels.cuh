@@ -101,7 +101,7 @@ struct __align__(16) BuildHeader {
     float R32;          // class thresholds (ClassParams), set with W
     float H1;
     float Hh;
-    uint32_t pad0;
+    uint32_t nH_total;  // split build: number of heavy items, set by the scan pass
     int64_t nfix;       // excess correction, set with the tile prefixes
     uint64_t huge_count; // rejection: number of deferred items filled by the whole grid
     uint64_t pad[4];
@@ -1208,6 +1208,31 @@ __device__ __forceinline__ uint64_t pack_heavy_key(u128 Et, u128 A_before) {
     return (q_hi(d) >> 16) ? ~0ull : (uint64_t)(d >> 16);
 }
 
+// A heavy's corrected excess end (Q64.64) from its stored end E (Q40.24): the compact heavy
+// list of the split build's scan pass keeps E uncorrected.
+__device__ __forceinline__ u128 corrected_end(uint64_t E, int64_t nfix) { return q_scale_excess((u128)E << 40, nfix); }
+
+// The pack kernel's view of the heavy list's excess ends: corrected Q64.64 ends (uint4 each;
+// the reduce/prefix/heavy-list passes) or compact Q40.24 ends corrected on load (u64 each;
+// the split build's scan pass).
+template <bool E64>
+struct HeavyEnds;
+template <>
+struct HeavyEnds<false> {
+    const uint4* p;
+    __device__ __forceinline__ u128 at(uint32_t g) const { return load_u128(p + g); }
+};
+template <>
+struct HeavyEnds<true> {
+    const uint64_t* p;
+    int64_t nfix;
+    __device__ __forceinline__ u128 at(uint32_t g) const { return corrected_end(__ldg(p + g), nfix); }
+};
+
+// Heavies that the split build's walk-form pack kernel (pack_walk_kernel) holds at once for T
+// items per tile; tiles with more take split_pack_kernel's chunked form.
+__host__ __device__ constexpr int walk_cap(int T) { return T / 2; }
+
 // Shared memory of the pack kernel, in this order: light keys (u64 x T; the staged rows at
 // the end), heavy keys (u64 x C), heavy items (u32 x C), heavy ranks (u32 x C).
 __host__ __device__ constexpr size_t pack_smem_bytes(int T) {
@@ -1248,12 +1273,15 @@ __device__ __forceinline__ uint32_t stage_pos(uint32_t i) {
 // In the leftover mode (LEFT, the PSA+ build's second pass) a tile's lights are its leftover
 // lights from the slots (deficits and row probabilities given), and their rows are written
 // at their items.
-template <int NT, int IPT, bool BATCH, bool LEFT>
+// E64 (the split build's compact heavy list): the heavy count comes from the header, and the
+// kernel builds only the tiles whose heavies exceed walk_cap(T) (pack_walk_kernel builds the
+// others).
+template <int NT, int IPT, bool BATCH, bool LEFT, bool E64 = false>
 __global__ void __launch_bounds__(NT, (NT == 256 && IPT == 8) ? 4 : 1) split_pack_kernel(const float* __restrict__ w,
                                                         const BuildHeader* hdr, const TileVals* incl,
                                                         const TileStart* __restrict__ starts,
                                                         const uint32_t* __restrict__ heavy_item,
-                                                        const uint4* __restrict__ heavy_E, uint32_t num_tiles,
+                                                        const void* __restrict__ heavy_E_raw, uint32_t num_tiles,
                                                         wrs_alias_row* __restrict__ table, TileMap map,
                                                         const LeftSlot* __restrict__ left) {
     constexpr int T = NT * IPT;
@@ -1280,21 +1308,35 @@ __global__ void __launch_bounds__(NT, (NT == 256 && IPT == 8) ? 4 : 1) split_pac
                                                         // the last tiles, still in L2
     if (plan_failed<BATCH>(map)) return;
     const TileRef tr = tile_ref<BATCH>(map, gtile);
+    if constexpr (E64) {
+        // only the tiles whose heavies exceed walk_cap(T), decided before any weight is read
+        if (earlier_status(hdr) != 0) return;
+        const uint32_t nH0 = __ldg(&hdr->nH_total);
+        const uint32_t lo = starts[tr.local].bound, hi = starts[tr.local + 1].bound;
+        if (hi < lo || hi > nH0) return;  // bounds out of order: an earlier pass failed
+        if (nH0 == 0 || min(hi + 1u, nH0) - lo <= (uint32_t)walk_cap(NT * IPT)) return;
+    }
     const uint32_t tile = tr.local;
     const uint64_t n = tr.n;
     w += tr.item_off;
     table += tr.item_off;
     heavy_item += tr.heavy_off;
-    heavy_E += tr.heavy_off;
     // ---- (1) own tile (the weights' loads go out first: they do not depend on the header)
     float x[IPT];
     if (!LEFT) load_items<NT, IPT>(w, n, tile, tid, x);
     hdr += tr.table;
     if (earlier_status(hdr) != 0) return;
+    HeavyEnds<E64> he;
+    if constexpr (E64) {
+        he.p = static_cast<const uint64_t*>(heavy_E_raw) + tr.heavy_off;
+        he.nfix = __ldg(&hdr->nfix);
+    } else {
+        he.p = static_cast<const uint4*>(heavy_E_raw) + tr.heavy_off;
+    }
     const LeftSlot* ls = LEFT ? left + (uint64_t)tile * T : nullptr;
     const uint32_t nvalid = LEFT ? __ldcg(&incl[tile].nL) - (tile ? __ldcg(&incl[tile - 1].nL) : 0u) : 0u;
     const ClassParams cp = load_class_params(hdr);
-    const uint32_t nH = __ldg(&incl[tr.tile0 + tr.ntiles - 1].nH);
+    const uint32_t nH = E64 ? __ldg(&hdr->nH_total) : __ldg(&incl[tr.tile0 + tr.ntiles - 1].nH);
     const TileStart st0 = starts[tr.tile0 + tr.table + tile], st1 = starts[tr.tile0 + tr.table + tile + 1];
     const u128 A_before = q_make(st0.A_hi, st0.A_lo);
     const u128 A_after = q_make(st1.A_hi, st1.A_lo);
@@ -1305,7 +1347,7 @@ __global__ void __launch_bounds__(NT, (NT == 256 && IPT == 8) ? 4 : 1) split_pac
     if (walk) {
 #pragma unroll 4
         for (uint32_t j = tid; j < m_w; j += NT) {
-            sWk[j] = pack_heavy_key(load_u128(heavy_E + g_lo + j), A_before);
+            sWk[j] = pack_heavy_key(he.at(g_lo + j), A_before);
             sWi[j] = __ldg(heavy_item + g_lo + j);
         }
     }
@@ -1443,7 +1485,7 @@ __global__ void __launch_bounds__(NT, (NT == 256 && IPT == 8) ? 4 : 1) split_pac
             const uint32_t pend = s_pend_item;
             const float pend_prob = s_pend_prob;
             for (uint32_t j = tid; j < m; j += NT) {
-                sHkey[j] = pack_heavy_key(load_u128(heavy_E + cs + j), A_before);
+                sHkey[j] = pack_heavy_key(he.at(cs + j), A_before);
                 sHitem[j] = __ldg(heavy_item + cs + j);
             }
             __syncthreads();
@@ -1452,7 +1494,7 @@ __global__ void __launch_bounds__(NT, (NT == 256 && IPT == 8) ? 4 : 1) split_pac
                 wrs_alias_row r;
                 r.prob = pend_prob;
                 r.alias = sHitem[0];
-                table[pend] = r;
+                if (pend < n) table[pend] = r;
             }
             // ranks: the index of the first light whose key is not below the heavy's
             // (all heavies of this chunk rank at r0 or later)
@@ -1501,14 +1543,14 @@ __global__ void __launch_bounds__(NT, (NT == 256 && IPT == 8) ? 4 : 1) split_pac
                     s_pend_item = 0xffffffffu;
                 }
                 if (g < g_hi) {
-                    const u128 Et = load_u128(heavy_E + g);
+                    const u128 Et = he.at(g);
                     const u128 A_next = (rk < nLt) ? A_before + ((u128)sLkey[lkey_slot(rk)] << 16) : A_after;
                     const float prob = heavy_row_prob(q_one() + Et - A_next);
                     if (j + 1 < m) {
                         wrs_alias_row r;
                         r.prob = prob;
                         r.alias = sHitem[j + 1];
-                        table[sHitem[j]] = r;
+                        if (sHitem[j] < n) table[sHitem[j]] = r;
                     } else if (g + 1 < nH) {
                         s_pend_item = sHitem[j];  // its alias opens the next chunk
                         s_pend_prob = prob;
@@ -1516,7 +1558,7 @@ __global__ void __launch_bounds__(NT, (NT == 256 && IPT == 8) ? 4 : 1) split_pac
                         wrs_alias_row r;  // the last heavy of the table keeps itself
                         r.prob = prob;
                         r.alias = sHitem[j];
-                        table[sHitem[j]] = r;
+                        if (sHitem[j] < n) table[sHitem[j]] = r;
                     }
                 }
             }
@@ -1531,9 +1573,9 @@ __global__ void __launch_bounds__(NT, (NT == 256 && IPT == 8) ? 4 : 1) split_pac
             const uint64_t nk = sWk[j];
             const u128 A_next = nk == ~0ull ? A_after : A_before + ((u128)nk << 16);
             wrs_alias_row r;
-            r.prob = heavy_row_prob(q_one() + load_u128(heavy_E + g_lo + j) - A_next);
+            r.prob = heavy_row_prob(q_one() + he.at(g_lo + j) - A_next);
             r.alias = (g_lo + j + 1 < nH) ? sWi[j + 1] : sWi[j];  // the last heavy keeps itself
-            table[sWi[j]] = r;
+            if (sWi[j] < n) table[sWi[j]] = r;
         }
     };
     // ---- (3) light rows: staged, then coalesced stores (heavy positions are skipped)

@@ -26,8 +26,8 @@ def short_waits(cuda):
 
 
 def test_split_build_lookback_wait_times_out(short_waits):
-    # 2^22 + 5 items = 2049 tiles of 2048: three prefix blocks of 1024 tiles; block 0 is held,
-    # so blocks 1 and 2 wait on a flag that nothing sets
+    # 2^22 + 5 items: over a thousand tiles, each looking back over its predecessors; tile 0 is
+    # held, so the tiles after it wait on a flag that nothing sets
     n = (1 << 22) + 5
     w = np.random.default_rng(3).random(n, dtype=np.float32)
     assert wrs.debug_hold_lookback(0) == wrs.WRS_SUCCESS
