@@ -192,7 +192,7 @@ wrs_status launch_big(const float* d_w, const int64_t* d_offsets, const uint8_t*
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return WRS_ERR_CUDA;
     split_pack_kernel<NT, IPT, true, false><<<nt, NT, smem, stream>>>(d_w, L.hdrs, L.incl, L.starts, L.heavy_item,
-                                                                L.heavy_E, nt, d_table, map, nullptr);
+                                                                L.heavy_E, nt, d_table, map, nullptr, nullptr);
     batch_status_kernel<<<(p.big_tables + 1 + 255) / 256, 256, 0, stream>>>(L.hdr0 + 1, p.big_tables + 1,
                                                                            &L.hdr0->status);
     return launch_status();

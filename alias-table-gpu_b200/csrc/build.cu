@@ -10,6 +10,7 @@
 // the wsum, tile_reduce, tile_prefix, psa_local and leftover passes (PSA+).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <mutex>
 #include <vector>
 
@@ -69,12 +70,12 @@ namespace {
 
 constexpr int64_t kMaxItems = (int64_t)0x7fffffff - 8192;
 
-// Items per tile of the scan and pack passes (0 = the default: 4096, and 1024 for PSA+, whose
+// Items per tile of the scan and pack passes (0 = the default: 2048, and 1024 for PSA+, whose
 // local pass is faster on smaller tiles).
 int64_t tile_items_for(const wrs_build_opts* opts) {
     const uint32_t t = opts ? opts->tile_items : 0u;
     switch (t) {
-        case 0: return (opts && opts->method == WRS_METHOD_PSA_PLUS) ? 1024 : 4096;
+        case 0: return (opts && opts->method == WRS_METHOD_PSA_PLUS) ? 1024 : 2048;
         case 2048: return 2048;
         case 1024: return 1024;
         case 4096: return 4096;
@@ -83,14 +84,20 @@ int64_t tile_items_for(const wrs_build_opts* opts) {
 }
 
 // The split method: wsum (W, class thresholds, look-back flags cleared), scan (tile sums,
-// look-back prefixes, tile starts, compact heavy list), link (the split search per tile
-// boundary), pack_walk (the merge, walk form) and split_pack's chunked form for the tiles whose
-// heavies exceed the walk arrays.
+// look-back prefixes over groups of tiles, tile starts, compact heavy list), link (the split
+// search per tile boundary), pack_walk (the merge, walk form; it lists the tiles whose heavies
+// exceed its arrays) and split_pack's chunked form over that list.
 struct SplitLayout {
     BuildHeader* hdr;
     double2* partials;
-    ScanRecs rec;
+    LbWord* lb;          // scan: look-back word per group of tiles
+    BlockWord* blocks;   // tile_prefix: look-back record per block of tiles
+    uint64_t num_groups;
+    uint64_t num_blocks;
+    TileVals* agg;
+    TileVals* incl;
     TileStart* starts;
+    uint32_t* chunk_list;
     uint32_t* heavy_item;
     uint64_t* heavy_E;
     size_t bytes;
@@ -101,10 +108,14 @@ SplitLayout carve_split(void* scratch, uint64_t n, uint64_t num_tiles) {
     SplitLayout L;
     L.hdr = c.take<BuildHeader>(1);
     L.partials = c.take<double2>(kWsumMaxGrid);
-    L.rec.flag = c.take<uint32_t>(num_tiles);
-    L.rec.agg = c.take<ScanVals>(num_tiles);
-    L.rec.incl = c.take<ScanVals>(num_tiles);
+    L.num_groups = (num_tiles + kScanGroup - 1) / kScanGroup;
+    L.num_blocks = (num_tiles + kPrefixTiles - 1) / kPrefixTiles;
+    L.lb = c.take<LbWord>(L.num_groups);
+    L.blocks = c.take<BlockWord>(L.num_blocks);  // right after lb: one zeroing covers both
+    L.agg = c.take<TileVals>(num_tiles);
+    L.incl = c.take<TileVals>(num_tiles);
     L.starts = c.take<TileStart>(num_tiles + 1);
+    L.chunk_list = c.take<uint32_t>(num_tiles);
     L.heavy_item = c.take<uint32_t>(n);
     L.heavy_E = c.take<uint64_t>(n);
     L.bytes = c.off;
@@ -133,17 +144,24 @@ wrs_status launch_split(const float* d_w, uint64_t n, wrs_alias_row* d_table, do
     static_assert(S::NT * S::IPT == T && kScanThreads * S::SCAN_IPT == T, "tile shapes");
     const uint32_t nt = (uint32_t)num_tiles;
     if (cudaMemsetAsync(L.hdr, 0, sizeof(BuildHeader), stream) != cudaSuccess) return WRS_ERR_CUDA;
-    wsum_kernel<kWsumBlock><<<wsum_grid(n), kWsumBlock, 0, stream>>>(d_w, n, L.hdr, L.partials, L.rec.flag, nt, d_W);
-    scan_kernel<S::SCAN_IPT><<<nt, kScanThreads, 0, stream>>>(d_w, n, L.hdr, L.rec, nt, L.starts, L.heavy_item,
-                                                                L.heavy_E, current_wait_cfg());
-    if (nt > 1) link_kernel<<<(nt - 1 + 255) / 256, 256, 0, stream>>>(L.hdr, nt, L.heavy_E, L.starts);
+    // wsum clears the look-back words of scan and tile_prefix (adjacent in the scratch)
+    const uint64_t zero_words =
+        (uint64_t)(reinterpret_cast<const char*>(L.blocks + L.num_blocks) - reinterpret_cast<const char*>(L.lb)) / 4;
+    wsum_kernel<kWsumBlock><<<wsum_grid(n), kWsumBlock, 0, stream>>>(d_w, n, L.hdr, L.partials,
+                                                                     reinterpret_cast<uint32_t*>(L.lb), zero_words,
+                                                                     d_W);
+    const WaitCfg wc = current_wait_cfg();
+    scan_kernel<S::SCAN_IPT><<<(uint32_t)L.num_groups, kScanThreads, 0, stream>>>(d_w, n, L.hdr, L.lb, nt, L.agg,
+                                                                                   L.heavy_item, L.heavy_E, wc);
+    tile_prefix_kernel<<<(uint32_t)L.num_blocks, kPrefixThreads, 0, stream>>>(L.hdr, L.agg, L.incl, L.blocks, nt, wc);
+    link_kernel<<<(nt + 1 + 255) / 256, 256, 0, stream>>>(L.hdr, L.incl, nt, L.heavy_E, L.starts);
     {
-        const size_t smem = pack_walk_smem_bytes(T);
+        const size_t smem = pack_walk_smem_bytes(T, S::IPT);
         if (cudaFuncSetAttribute(pack_walk_kernel<S::NT, S::IPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem) != cudaSuccess)
             return WRS_ERR_CUDA;
         pack_walk_kernel<S::NT, S::IPT><<<nt, S::NT, smem, stream>>>(d_w, n, L.hdr, L.starts, L.heavy_item,
-                                                                      L.heavy_E, nt, d_table);
+                                                                      L.heavy_E, nt, d_table, L.chunk_list);
     }
     {
         constexpr int NT = PackShape<T>::NT, IPT = PackShape<T>::IPT;
@@ -152,8 +170,10 @@ wrs_status launch_split(const float* d_w, uint64_t n, wrs_alias_row* d_table, do
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
             return WRS_ERR_CUDA;
         const TileMap map{nullptr, nullptr, nullptr, n, nt};
-        split_pack_kernel<NT, IPT, false, false, true><<<nt, NT, smem, stream>>>(
-            d_w, L.hdr, nullptr, L.starts, L.heavy_item, L.heavy_E, nt, d_table, map, nullptr);
+        // the tiles pack_walk listed; a small grid, so that an empty list costs one short launch
+        const uint32_t grid = std::min<uint32_t>(nt, (uint32_t)device_info().sm_count * 2u);
+        split_pack_kernel<NT, IPT, false, false, true><<<grid, NT, smem, stream>>>(
+            d_w, L.hdr, nullptr, L.starts, L.heavy_item, L.heavy_E, nt, d_table, map, nullptr, L.chunk_list);
     }
     return launch_status();
 }
@@ -236,7 +256,7 @@ wrs_status launch_psa(const float* d_w, uint64_t n, wrs_alias_row* d_table, doub
             return WRS_ERR_CUDA;
         split_pack_kernel<NT, IPT, false, true><<<nt, NT, smem, stream>>>(d_w, L.hdr2, L.incl2, L.starts2,
                                                                           L.heavy_item2, L.heavy_E2, nt, d_table, map,
-                                                                          L.slots);
+                                                                          L.slots, nullptr);
     }
     copy_status_kernel<<<1, 1, 0, stream>>>(L.hdr2, L.hdr);
     return launch_status();
@@ -305,8 +325,8 @@ extern "C" wrs_status wrs_alias_build_f32(const float* d_w, int64_t n, const wrs
     wrs_status st;
     switch (T) {
         case 1024: st = launch_split<1024>(d_w, (uint64_t)n, d_table, d_W, L, nt, stream); break;
-        case 2048: st = launch_split<2048>(d_w, (uint64_t)n, d_table, d_W, L, nt, stream); break;
-        default: st = launch_split<4096>(d_w, (uint64_t)n, d_table, d_W, L, nt, stream); break;
+        case 4096: st = launch_split<4096>(d_w, (uint64_t)n, d_table, d_W, L, nt, stream); break;
+        default: st = launch_split<2048>(d_w, (uint64_t)n, d_table, d_W, L, nt, stream); break;
     }
     if (st != WRS_SUCCESS) return st;
     if (opts && (opts->flags & WRS_FLAG_SYNC)) return read_device_status(&L.hdr->status, stream);

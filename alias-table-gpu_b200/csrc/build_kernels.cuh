@@ -104,7 +104,9 @@ struct __align__(16) BuildHeader {
     uint32_t nH_total;  // split build: number of heavy items, set by the scan pass
     int64_t nfix;       // excess correction, set with the tile prefixes
     uint64_t huge_count; // rejection: number of deferred items filled by the whole grid
-    uint64_t pad[4];
+    uint32_t chunk_count; // split build: tiles pack_walk_kernel left to the chunked form
+    uint32_t pad1;
+    uint64_t pad[3];
 };
 static_assert(sizeof(BuildHeader) == 128, "header layout");
 
@@ -263,6 +265,24 @@ __global__ void __launch_bounds__(BLOCK) wsum_kernel(const float* __restrict__ w
         const float4* w4 = reinterpret_cast<const float4*>(w);
         const int64_t gs = (int64_t)gsize;
         int64_t q = n4 - 1 - (int64_t)gtid;
+        // four independent 16-byte loads in flight per thread, summed into two accumulators
+        DD acc2 = {0.0, 0.0};
+        for (; q - 3 * gs >= 0; q -= 4 * gs) {
+            float4 v[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) v[j] = __ldg(w4 + q - j * gs);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                bad |= weight_invalid(v[j].x) | weight_invalid(v[j].y) | weight_invalid(v[j].z) |
+                       weight_invalid(v[j].w);
+                DD& a = (j & 1) ? acc2 : acc;
+                a = dd_add_d(a, (double)v[j].x);
+                a = dd_add_d(a, (double)v[j].y);
+                a = dd_add_d(a, (double)v[j].z);
+                a = dd_add_d(a, (double)v[j].w);
+            }
+        }
+        acc = dd_add(acc, acc2);
         for (; q - gs >= 0; q -= 2 * gs) {
             const float4 a = __ldg(w4 + q);
             const float4 b = __ldg(w4 + q - gs);
@@ -1230,8 +1250,9 @@ struct HeavyEnds<true> {
 };
 
 // Heavies that the split build's walk-form pack kernel (pack_walk_kernel) holds at once for T
-// items per tile; tiles with more take split_pack_kernel's chunked form.
-__host__ __device__ constexpr int walk_cap(int T) { return T / 2; }
+// items per tile (a light tile of uniform weights owns about T/2 heavies, with a wide spread);
+// tiles with more take split_pack_kernel's chunked form.
+__host__ __device__ constexpr int walk_cap(int T) { return T; }
 
 // Shared memory of the pack kernel, in this order: light keys (u64 x T; the staged rows at
 // the end), heavy keys (u64 x C), heavy items (u32 x C), heavy ranks (u32 x C).
@@ -1274,16 +1295,15 @@ __device__ __forceinline__ uint32_t stage_pos(uint32_t i) {
 // lights from the slots (deficits and row probabilities given), and their rows are written
 // at their items.
 // E64 (the split build's compact heavy list): the heavy count comes from the header, and the
-// kernel builds only the tiles whose heavies exceed walk_cap(T) (pack_walk_kernel builds the
-// others).
-template <int NT, int IPT, bool BATCH, bool LEFT, bool E64 = false>
-__global__ void __launch_bounds__(NT, (NT == 256 && IPT == 8) ? 4 : 1) split_pack_kernel(const float* __restrict__ w,
-                                                        const BuildHeader* hdr, const TileVals* incl,
-                                                        const TileStart* __restrict__ starts,
-                                                        const uint32_t* __restrict__ heavy_item,
-                                                        const void* __restrict__ heavy_E_raw, uint32_t num_tiles,
-                                                        wrs_alias_row* __restrict__ table, TileMap map,
-                                                        const LeftSlot* __restrict__ left) {
+// kernel builds only the tiles that pack_walk_kernel listed (their heavies exceed walk_cap(T);
+// the list's length in the header's chunk_count), CTA b taking entries b, b + gridDim.x, ...
+template <int NT, int IPT, bool BATCH, bool LEFT, bool E64>
+__device__ __forceinline__ void split_pack_tile(const float* __restrict__ w, const BuildHeader* hdr,
+                                                const TileVals* incl, const TileStart* __restrict__ starts,
+                                                const uint32_t* __restrict__ heavy_item,
+                                                const void* __restrict__ heavy_E_raw, uint32_t gtile,
+                                                wrs_alias_row* __restrict__ table, TileMap map,
+                                                const LeftSlot* __restrict__ left) {
     constexpr int T = NT * IPT;
     constexpr int C = pack_chunk(T);
     constexpr int CW = pack_walk_cap(T);
@@ -1304,8 +1324,6 @@ __global__ void __launch_bounds__(NT, (NT == 256 && IPT == 8) ? 4 : 1) split_pac
     __shared__ float s_pend_prob;
 
     const int tid = threadIdx.x;
-    const uint32_t gtile = num_tiles - 1 - blockIdx.x;  // descending: the previous passes ended at
-                                                        // the last tiles, still in L2
     if (plan_failed<BATCH>(map)) return;
     const TileRef tr = tile_ref<BATCH>(map, gtile);
     if constexpr (E64) {
@@ -1448,11 +1466,11 @@ __global__ void __launch_bounds__(NT, (NT == 256 && IPT == 8) ? 4 : 1) split_pac
             if (light) {
                 const uint64_t key = sr + D;
                 if (hk <= key) {
-                    do {  // heavy a ranks at this light
+                    do {  // heavy a ranks at this light (a < a_end bounds the loop whatever the keys)
                         sWk[a] = key;
                         ++a;
                         hk = a < a_end ? sWk[a] : ~0ull;
-                    } while (hk <= key);
+                    } while (a < a_end && hk <= key);
                     cur = a < m_w ? sWi[a] : last_heavy;
                 }
                 al[k] = cur;
@@ -1616,6 +1634,29 @@ __global__ void __launch_bounds__(NT, (NT == 256 && IPT == 8) ? 4 : 1) split_pac
                 if (row != ~0ull) out[i] = row;
             }
         }
+    }
+}
+
+template <int NT, int IPT, bool BATCH, bool LEFT, bool E64 = false>
+__global__ void __launch_bounds__(NT, (NT == 256 && IPT == 8) ? 4 : 1) split_pack_kernel(const float* __restrict__ w,
+                                                        const BuildHeader* hdr, const TileVals* incl,
+                                                        const TileStart* __restrict__ starts,
+                                                        const uint32_t* __restrict__ heavy_item,
+                                                        const void* __restrict__ heavy_E_raw, uint32_t num_tiles,
+                                                        wrs_alias_row* __restrict__ table, TileMap map,
+                                                        const LeftSlot* __restrict__ left,
+                                                        const uint32_t* __restrict__ tile_list) {
+    if constexpr (E64) {
+        const uint32_t count = min(__ldg(&hdr->chunk_count), num_tiles);
+        for (uint32_t i = blockIdx.x; i < count; i += gridDim.x) {
+            split_pack_tile<NT, IPT, BATCH, LEFT, E64>(w, hdr, incl, starts, heavy_item, heavy_E_raw,
+                                                       __ldg(tile_list + i), table, map, left);
+            __syncthreads();  // the next tile reuses the shared arrays
+        }
+    } else {
+        // descending: the previous passes ended at the last tiles, still in L2
+        split_pack_tile<NT, IPT, BATCH, LEFT, E64>(w, hdr, incl, starts, heavy_item, heavy_E_raw,
+                                                   num_tiles - 1 - blockIdx.x, table, map, left);
     }
 }
 

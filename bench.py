@@ -47,9 +47,9 @@ METRIC = "build Gitems/s + Gsamples/s, batched vs per-table, %HBM peak, at ≤1e
 UNIT = "G(items+samples)/s"
 WORKLOAD = "single large table: n=2^26 w=(i+1)^-1.1 permuted; split build + 2^30 plain samples per step"
 FALLBACK_HBM_GBS = 6650.0
-# kernels one step launches: wsum, scan, link, pack_walk, split_pack (the chunked form's
-# launch; its CTAs return at once when every tile's heavies fit the walk arrays) and the sampler
-KERNELS_PER_STEP = 6
+# kernels one step launches: wsum, scan, tile_prefix, link, pack_walk, split_pack (the chunked
+# form over the tiles pack_walk listed; an empty list costs one short launch) and the sampler
+KERNELS_PER_STEP = 7
 # kernels one replay of the batched graph launches when the batch has both one-warp tables
 # and tiled tables: plan_count, plan_scan, plan_fill, batch_wsum, tile_reduce, batch_prefix,
 # heavy_list, tile_link, split_pack, batch_status, small_tables (the build) and batch_sample;
