@@ -17,6 +17,7 @@
 #include "build_kernels.cuh"
 #include "psa_kernels.cuh"
 #include "split_kernels.cuh"
+#include "precision_kernels.cuh"
 #include "host_util.h"
 
 namespace wrs {
@@ -178,6 +179,58 @@ wrs_status launch_split(const float* d_w, uint64_t n, wrs_alias_row* d_table, do
     return launch_status();
 }
 
+// The comparison builds in one floating-point type R (WRS_PRECISION_FP64 / _FP32): weight tile
+// sums, the total W, deficit/excess tile sums, the tiles' line bases, the two lines in item
+// order, and the merge.
+template <typename R>
+struct PrecLayout {
+    BuildHeader* hdr;
+    PrecTile<R>* tiles;
+    PrecTile<R>* prefix;  // num_tiles + 1: the last holds the totals
+    R* Lkey;
+    uint32_t* Litem;
+    float* Lprob;
+    R* Hkey;
+    uint32_t* Hitem;
+    size_t bytes;
+};
+
+template <typename R>
+PrecLayout<R> carve_prec(void* scratch, uint64_t n) {
+    const uint64_t nt = (n + kPrecTile - 1) / kPrecTile;
+    Carver c(scratch);
+    PrecLayout<R> L;
+    L.hdr = c.take<BuildHeader>(1);
+    L.tiles = c.take<PrecTile<R>>(nt);
+    L.prefix = c.take<PrecTile<R>>(nt + 1);
+    L.Lkey = c.take<R>(n);
+    L.Litem = c.take<uint32_t>(n);
+    L.Lprob = c.take<float>(n);
+    L.Hkey = c.take<R>(n);
+    L.Hitem = c.take<uint32_t>(n);
+    L.bytes = c.off;
+    return L;
+}
+
+template <typename R>
+wrs_status launch_prec(const float* d_w, uint64_t n, wrs_alias_row* d_table, double* d_W, const PrecLayout<R>& L,
+                       cudaStream_t stream) {
+    const uint32_t nt = (uint32_t)((n + kPrecTile - 1) / kPrecTile);
+    if (cudaMemsetAsync(L.hdr, 0, sizeof(BuildHeader), stream) != cudaSuccess) return WRS_ERR_CUDA;
+    prec_weight_tiles_kernel<R><<<nt, kPrecThreads, 0, stream>>>(d_w, n, L.hdr, L.tiles);
+    prec_weight_total_kernel<R><<<1, kPrecScanThreads, 0, stream>>>(L.hdr, L.tiles, nt, n, d_W);
+    const uint32_t lgrid = (nt + 127) / 128;
+    prec_lines_kernel<R, false><<<lgrid, 128, 0, stream>>>(d_w, n, L.hdr, L.tiles, nullptr, nt, nullptr, nullptr,
+                                                           nullptr, nullptr, nullptr);
+    prec_line_bases_kernel<R><<<1, 32, 0, stream>>>(L.hdr, L.tiles, L.prefix, nt);
+    prec_lines_kernel<R, true><<<lgrid, 128, 0, stream>>>(d_w, n, L.hdr, L.tiles, L.prefix, nt, L.Lkey, L.Litem,
+                                                          L.Lprob, L.Hkey, L.Hitem);
+    const uint64_t threads = (n + kPrecMergeChunk - 1) / kPrecMergeChunk;
+    prec_merge_kernel<R><<<(uint32_t)((threads + 255) / 256), 256, 0, stream>>>(
+        L.hdr, L.prefix + nt, L.Lkey, L.Litem, L.Lprob, L.Hkey, L.Hitem, n, d_table);
+    return launch_status();
+}
+
 // PSA+: the split passes up to the tile prefixes, the local pass, and the split passes again
 // over the leftovers (second header, prefix records, tile starts and heavy list).
 struct PsaLayout {
@@ -292,6 +345,12 @@ extern "C" wrs_status wrs_sum_f32(const float* d_w, int64_t n, double* d_total, 
 extern "C" size_t wrs_alias_build_scratch_bytes(int64_t n, const wrs_build_opts* opts) {
     const int64_t T = tile_items_for(opts);
     if (n < 1 || T < 0) return 0;
+    const uint32_t prec = opts ? opts->precision : WRS_PRECISION_MIXED;
+    if (prec != WRS_PRECISION_MIXED) {
+        if (prec > WRS_PRECISION_FP32 || opts->method != WRS_METHOD_SPLIT) return 0;
+        return prec == WRS_PRECISION_FP64 ? carve_prec<double>(nullptr, (uint64_t)n).bytes
+                                          : carve_prec<float>(nullptr, (uint64_t)n).bytes;
+    }
     const uint64_t nt = ((uint64_t)n + T - 1) / T;
     if (opts && opts->method == WRS_METHOD_PSA_PLUS) return carve_psa(nullptr, (uint64_t)n, nt, T).bytes;
     return carve_split(nullptr, (uint64_t)n, nt).bytes;
@@ -305,6 +364,27 @@ extern "C" wrs_status wrs_alias_build_f32(const float* d_w, int64_t n, const wrs
     const uint32_t method = opts ? opts->method : WRS_METHOD_SPLIT;
     if (T < 0 || method > WRS_METHOD_PSA_PLUS) return WRS_ERR_INVALID_ARGUMENT;
     const uint64_t nt = ((uint64_t)n + T - 1) / T;
+    const uint32_t prec = opts ? opts->precision : WRS_PRECISION_MIXED;
+    if (prec != WRS_PRECISION_MIXED) {
+        if (prec > WRS_PRECISION_FP32 || method != WRS_METHOD_SPLIT) return WRS_ERR_INVALID_ARGUMENT;
+        cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+        wrs_status st;
+        BuildHeader* hdr;
+        if (prec == WRS_PRECISION_FP64) {
+            if (scratch_bytes < carve_prec<double>(nullptr, (uint64_t)n).bytes) return WRS_ERR_SCRATCH_TOO_SMALL;
+            const PrecLayout<double> L = carve_prec<double>(d_scratch, (uint64_t)n);
+            hdr = L.hdr;
+            st = launch_prec<double>(d_w, (uint64_t)n, d_table, d_W, L, stream);
+        } else {
+            if (scratch_bytes < carve_prec<float>(nullptr, (uint64_t)n).bytes) return WRS_ERR_SCRATCH_TOO_SMALL;
+            const PrecLayout<float> L = carve_prec<float>(d_scratch, (uint64_t)n);
+            hdr = L.hdr;
+            st = launch_prec<float>(d_w, (uint64_t)n, d_table, d_W, L, stream);
+        }
+        if (st != WRS_SUCCESS) return st;
+        if (opts->flags & WRS_FLAG_SYNC) return read_device_status(&hdr->status, stream);
+        return WRS_SUCCESS;
+    }
     if (method == WRS_METHOD_PSA_PLUS) {
         if (scratch_bytes < carve_psa(nullptr, (uint64_t)n, nt, T).bytes) return WRS_ERR_SCRATCH_TOO_SMALL;
         cudaStream_t stream = static_cast<cudaStream_t>(stream_);

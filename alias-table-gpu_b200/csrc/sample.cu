@@ -218,3 +218,17 @@ extern "C" wrs_status wrs_rejection_sample(const uint32_t* d_A, const uint64_t* 
     }
     return WRS_SUCCESS;
 }
+
+extern "C" wrs_status wrs_random_gather_probe(const wrs_alias_row* d_table, int64_t n, uint64_t num_gathers,
+                                              uint64_t seed, uint32_t* d_sink, void* stream_) {
+    if (!d_table || !d_sink || n < 1 || n > kMaxItems) return WRS_ERR_INVALID_ARGUMENT;
+    if (((uintptr_t)d_table & 7u) != 0 || ((uintptr_t)d_sink & 3u) != 0) return WRS_ERR_INVALID_ARGUMENT;
+    if (num_gathers == 0) return WRS_SUCCESS;
+    const DeviceInfo dev = device_info();
+    uint64_t grid = ((num_gathers + 7) / 8 + 255) / 256;
+    const uint64_t cap = (uint64_t)dev.sm_count * 16;
+    if (grid > cap) grid = cap;
+    gather_probe_kernel<<<(uint32_t)grid, 256, 0, static_cast<cudaStream_t>(stream_)>>>(
+        reinterpret_cast<const uint2*>(d_table), (uint32_t)n, num_gathers, seed, d_sink);
+    return launch_status();
+}

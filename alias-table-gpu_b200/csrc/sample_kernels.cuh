@@ -130,6 +130,33 @@ __global__ void __launch_bounds__(256, 4) sample_plain_kernel(const uint2* __res
     }
 }
 
+// The random-access ceiling of the plain sampler's table: the same 8-byte row gathers (with the
+// .L2::64B prefetch size), eight in flight per thread, at rows from a cheap integer hash instead
+// of Philox and with nothing written but one XOR word per CTA. A diagnostic, timed beside the
+// sampler.
+__device__ __forceinline__ uint32_t probe_row(uint64_t s, uint32_t n) {
+    uint64_t z = s * 0x9E3779B97F4A7C15ull;
+    z ^= z >> 29;
+    z *= 0xBF58476D1CE4E5B9ull;
+    z ^= z >> 32;
+    return (uint32_t)__umul64hi(z, (uint64_t)n);
+}
+__global__ void __launch_bounds__(256, 4) gather_probe_kernel(const uint2* __restrict__ table, uint32_t n, uint64_t m,
+                                                              uint64_t seed, uint32_t* __restrict__ sink) {
+    const uint64_t noct = (m + 7) >> 3;
+    const uint64_t gsize = (uint64_t)gridDim.x * blockDim.x;
+    uint32_t acc = 0;
+    for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < noct; g += gsize) {
+        uint2 v[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] = ld_row_64B(table + probe_row(seed + 8 * g + j, n));
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc ^= v[j].x ^ v[j].y;
+    }
+    acc = __reduce_xor_sync(0xffffffffu, acc);
+    if ((threadIdx.x & 31) == 0) atomicXor(sink, acc);
+}
+
 // Sectioned sampling: rows cut into K sections of S rows; section k receives an exact
 // multinomial share of the m samples (binomial tree, section_count) and writes them at its
 // output offset. CTA c handles sections c, c + gridDim.x, ... in that order, so the sections

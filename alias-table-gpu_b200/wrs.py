@@ -37,6 +37,9 @@ WRS_ERR_CAPACITY = 9
 
 WRS_METHOD_SPLIT = 0
 WRS_METHOD_PSA_PLUS = 1
+WRS_PRECISION_MIXED = 0
+WRS_PRECISION_FP64 = 1
+WRS_PRECISION_FP32 = 2
 WRS_FLAG_SYNC = 1
 WRS_SAMPLE_PLAIN = 0
 WRS_SAMPLE_SECTIONED = 1
@@ -46,7 +49,8 @@ WRS_SAMPLE_DISCARD = 3
 
 class BuildOpts(ctypes.Structure):
     _fields_ = [("method", ctypes.c_uint32), ("tile_items", ctypes.c_uint32),
-                ("flags", ctypes.c_uint32), ("small_table_items", ctypes.c_uint32)]
+                ("flags", ctypes.c_uint32), ("small_table_items", ctypes.c_uint32),
+                ("precision", ctypes.c_uint32)]
 
 
 class SampleOpts(ctypes.Structure):
@@ -75,6 +79,7 @@ _SIGNATURES = {
     "wrs_alias_build_f32_static_scratch": (ctypes.c_int, [_P, _I64, _P, _P, _P, _P]),
     "wrs_alias_sample": (ctypes.c_int, [_P, _I64, _U64, _U64, _U64, _P, _P, _P, _P]),
     "wrs_alias_sample_to_host": (ctypes.c_int, [_P, _I64, _U64, _U64, _U64, _U64, _P, _P, _P]),
+    "wrs_random_gather_probe": (ctypes.c_int, [_P, _I64, _U64, _U64, _P, _P]),
     "wrs_rejection_build_scratch_bytes": (_SZ, [_I64]),
     "wrs_rejection_build_f32": (ctypes.c_int, [_P, _I64, _P, _U64, _P, _P, _P, _P, _SZ, _U32, _P]),
     "wrs_rejection_sample": (ctypes.c_int, [_P, _P, _P, _I64, _U64, _U64, _U64, _U32, _P, _P, _U32, _P]),
@@ -143,8 +148,8 @@ def _stream(stream) -> Optional[int]:
 # ---------------------------------------------------------------- C ABI wrappers
 
 def build_opts(method: int = WRS_METHOD_SPLIT, tile_items: int = 0, sync: bool = False,
-               small_table_items: int = 0) -> BuildOpts:
-    return BuildOpts(method, tile_items, WRS_FLAG_SYNC if sync else 0, small_table_items)
+               small_table_items: int = 0, precision: int = 0) -> BuildOpts:
+    return BuildOpts(method, tile_items, WRS_FLAG_SYNC if sync else 0, small_table_items, precision)
 
 
 def alias_build_scratch_bytes(n: int, opts: Optional[BuildOpts] = None) -> int:
@@ -189,6 +194,13 @@ def alias_sample(table, n: int, num_samples: int, seed: int, out, counter_base: 
     opts = SampleOpts(mode, section_items, WRS_FLAG_SYNC if sync else 0, 0)
     return lib().wrs_alias_sample(_ptr(table), n, num_samples, seed & (2**64 - 1), counter_base & (2**64 - 1),
                                   ctypes.byref(opts), _ptr(out), _ptr(section_counts), _stream(stream))
+
+
+def random_gather_probe(table, n: int, num_gathers: int, seed: int, sink, stream=None) -> int:
+    """num_gathers random 8-byte row gathers of the table, XOR-folded into sink[0] (a diagnostic
+    of the random-access rate)."""
+    return lib().wrs_random_gather_probe(_ptr(table), n, num_gathers, seed & (2**64 - 1), _ptr(sink),
+                                         _stream(stream))
 
 
 def alias_sample_to_host(table, n: int, num_samples: int, seed: int, out, host_out, counter_base: int = 0,

@@ -410,6 +410,16 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     torch.cuda.synchronize()
     gather_ms = s0.elapsed_time(s1) / reps
     del gidx, gout
+    # ... and the library's own probe: the sampler's row gathers (same load form, eight in
+    # flight per thread) at hashed rows, nothing written: the table's random-access ceiling
+    sink = torch.zeros(1, dtype=torch.int32, device=dev)
+    assert wrs.random_gather_probe(table, n, m, 7, sink, sp) == 0
+    s0.record(stream)
+    for r in range(reps):
+        assert wrs.random_gather_probe(table, n, m, 8 + r, sink, sp) == 0
+    s1.record(stream)
+    torch.cuda.synchronize()
+    probe_ms = s0.elapsed_time(s1) / reps
 
     # goodness of fit of the last timed step's samples (outside every timed region)
     chi2 = chi2_gpu(w, out) if rank == 0 else None
@@ -495,10 +505,12 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                      "algorithmic_bytes": "12 B/sample x 2^%d samples per launch (8 B row gather + 4 B write)"
                                           % (m.bit_length() - 1),
                      "random_access_bound": {
-                         "probe": "torch index_select of 2^27 random 8-byte rows of the same table (index read "
-                                  "and row write included)",
-                         "gathers_per_s_g": round(g_n / gather_ms / 1e6, 2),
-                         "sampler_over_probe": round((m / sample_ms) / (g_n / gather_ms), 3)}},
+                         "probe": "wrs_random_gather_probe: the sampler's 8-byte row gathers (.L2::64B, 8 in "
+                                  "flight per thread) at hashed rows of the same table, nothing written, "
+                                  "%d gathers" % m,
+                         "gathers_per_s_g": round(m / probe_ms / 1e6, 2),
+                         "sampler_over_probe": round((m / sample_ms) / (m / probe_ms), 3),
+                         "torch_index_select_gathers_per_s_g": round(g_n / gather_ms / 1e6, 2)}},
         "cpu_baseline": cpu,
         "clocks": clk,
         "e2e": {"value": round(replica_value(n + m, e2e_ms, world), 4), "unit": UNIT,
@@ -507,7 +519,108 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     }
     if not args.no_batched and args.config == "2":
         line["batched"] = batched_phase(dev)
+    if not args.no_side and args.config == "2" and world == 1:
+        del w, table, scratch, out
+        torch.cuda.empty_cache()
+        line["side_configs"] = side_configs(dev)
     return line
+
+
+def single_table_summary(dev, cfg: dict, steps: int = 20) -> dict:
+    """Split build and plain sampling of one configuration's table (median of `steps` CUDA-event
+    timings each, after warm-up), with the table's per-item error."""
+    import torch
+    import wrs
+
+    n, m = 1 << cfg["log2n"], 1 << cfg["log2m"]
+    w = torch.from_numpy(cfg["make"](n)).to(dev)
+    opts = wrs.build_opts()
+    table = torch.empty(n, dtype=torch.int64, device=dev)
+    scratch = torch.empty(wrs.alias_build_scratch_bytes(n, opts), dtype=torch.uint8, device=dev)
+    out = torch.empty(m, dtype=torch.int32, device=dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3 * steps)]
+    for r in range(3):
+        assert wrs.alias_build(w, table, scratch, opts) == 0
+        assert wrs.alias_sample(table, n, m, SEED_SAMPLES, out, r * m) == 0
+    torch.cuda.synchronize()
+    for r in range(steps):
+        ev[3 * r].record()
+        assert wrs.alias_build(w, table, scratch, opts) == 0
+        ev[3 * r + 1].record()
+        assert wrs.alias_sample(table, n, m, SEED_SAMPLES, out, (3 + r) * m) == 0
+        ev[3 * r + 2].record()
+    torch.cuda.synchronize()
+    if wrs.scratch_status(scratch) != 0:
+        raise RuntimeError("build failed on the device")
+    b = statistics.median([ev[3 * r].elapsed_time(ev[3 * r + 1]) for r in range(steps)])
+    smp = statistics.median([ev[3 * r + 1].elapsed_time(ev[3 * r + 2]) for r in range(steps)])
+    return {"workload": cfg["workload"], "build_ms": round(b, 4), "build_gitems_s": round(n / b / 1e6, 2),
+            "sample_ms": round(smp, 4), "sample_gsamples_s": round(m / smp / 1e6, 2),
+            "value": round((n + m) / (b + smp) / 1e6, 3), "unit": UNIT, "prob_error": table_error_gpu(w, table)}
+
+
+def precision_summary(dev, reps: int = 3) -> dict:
+    """The precision stress configuration (n = 2^28 log-uniform weights over 16 decades): the
+    default build (exact fixed-point lines, compensated W, FP32 stored probabilities) against
+    the all-FP64 and all-FP32 builds, each timed (median of `reps`) with its per-item error
+    against n w_i / W on the device; then 2^28 plain samples of the default table."""
+    import torch
+    import wrs
+
+    cfg = CONFIGS["3"]
+    n, m = 1 << cfg["log2n"], 1 << cfg["log2m"]
+    w = torch.from_numpy(cfg["make"](n)).to(dev)
+    table = torch.empty(n, dtype=torch.int64, device=dev)
+    modes = [("mixed", wrs.WRS_PRECISION_MIXED), ("fp64", wrs.WRS_PRECISION_FP64), ("fp32", wrs.WRS_PRECISION_FP32)]
+    need = max(wrs.alias_build_scratch_bytes(n, wrs.build_opts(precision=p)) for _, p in modes)
+    scratch = torch.empty(need, dtype=torch.uint8, device=dev)
+    res = {"workload": cfg["workload"] + "; builds in the three precisions"}
+    for name, p in modes:
+        opts = wrs.build_opts(precision=p)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * reps)]
+        assert wrs.alias_build(w, table, scratch, opts) == 0
+        torch.cuda.synchronize()
+        for r in range(reps):
+            ev[2 * r].record()
+            assert wrs.alias_build(w, table, scratch, opts) == 0
+            ev[2 * r + 1].record()
+        torch.cuda.synchronize()
+        if wrs.scratch_status(scratch) != 0:
+            raise RuntimeError(f"{name} build failed on the device")
+        ms = statistics.median([ev[2 * r].elapsed_time(ev[2 * r + 1]) for r in range(reps)])
+        res[name] = {"build_ms": round(ms, 3), "build_gitems_s": round(n / ms / 1e6, 2),
+                     **table_error_gpu(w, table)}
+        torch.cuda.empty_cache()
+    assert wrs.alias_build(w, table, scratch, wrs.build_opts()) == 0
+    del scratch
+    torch.cuda.empty_cache()
+    out = torch.empty(m, dtype=torch.int32, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    assert wrs.alias_sample(table, n, m, SEED_SAMPLES, out, 0) == 0
+    e0.record()
+    assert wrs.alias_sample(table, n, m, SEED_SAMPLES, out, m) == 0
+    e1.record()
+    torch.cuda.synchronize()
+    res["sample_ms"] = round(e0.elapsed_time(e1), 3)
+    return res
+
+
+def side_configs(dev) -> dict:
+    """Compact summaries of the other configurations, measured in the same run: the plain
+    single table (n = 2^20, L2-resident), the precision comparison at n = 2^28, and the mixed
+    batch (alias or rejection per size class, autotuned)."""
+    import torch
+
+    out = {"config1": single_table_summary(dev, CONFIGS["1"])}
+    torch.cuda.empty_cache()
+    out["config3"] = precision_summary(dev)
+    torch.cuda.empty_cache()
+    b = batched_phase(dev, batch_config5, mixed=True)
+    out["config5"] = {k: b[k] for k in ("workload", "items", "samples", "batched_ms", "batched_g_items_plus_samples_s",
+                                        "per_table_ms", "speedup", "e2e") if k in b}
+    if "mixed" in b:
+        out["config5"]["mixed"] = b["mixed"]
+    return out
 
 
 def zipf_sizes(num: int, s: float, lo: int, hi: int, seed: int) -> np.ndarray:
@@ -898,6 +1011,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-tables measurement")
+    ap.add_argument("--no-side", action="store_true",
+                    help="skip the summaries of configurations 1, 3 and 5 in the default line")
     ap.add_argument("--log2-samples", type=int, default=0,
                     help="samples per step (2^k, 0 = the configuration's); for profiler captures only")
     ap.add_argument("--config", default="2", choices=sorted(CONFIGS) + ["4", "5"],

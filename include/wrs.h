@@ -51,7 +51,7 @@ extern "C" {
 #endif
 
 #define WRS_VERSION_MAJOR 0
-#define WRS_VERSION_MINOR 1
+#define WRS_VERSION_MINOR 2
 
 typedef enum wrs_status {
     WRS_SUCCESS = 0,
@@ -84,12 +84,25 @@ typedef enum wrs_build_method {
 
 #define WRS_FLAG_SYNC 1u      /* synchronise the stream and return the device status */
 
+/* Arithmetic of the split build's deficit and excess lines. MIXED (the default) keeps them in
+ * exact fixed point with a compensated weight total, and only the stored probabilities in
+ * FP32: per-item probability error about 2^-23. FP64 and FP32 are comparison builds that run
+ * the same merge with every quantity (weight total, W/N, deficits, excesses and their prefix
+ * sums) rounded to that type at each operation, as the reference's build does in FP64
+ * (AliasTableSplitGpu.cu:406-432); their error grows with n and the weights' spread. */
+typedef enum wrs_precision {
+    WRS_PRECISION_MIXED = 0,
+    WRS_PRECISION_FP64 = 1,
+    WRS_PRECISION_FP32 = 2
+} wrs_precision;
+
 typedef struct wrs_build_opts {
     uint32_t method;            /* wrs_build_method */
     uint32_t tile_items;        /* 0 = default (2048; 1024 for PSA+); 1024, 2048 or 4096 */
     uint32_t flags;             /* WRS_FLAG_* */
     uint32_t small_table_items; /* batched builds: tables of at most this many items are built
                                    one per warp (0 = default 128; 32, 64, 128, 256 or 512) */
+    uint32_t precision;         /* wrs_precision (single-table split builds only; 0 = MIXED) */
 } wrs_build_opts;
 
 typedef enum wrs_sample_mode {
@@ -176,6 +189,13 @@ WRS_API wrs_status wrs_alias_sample(const wrs_alias_row* d_table, int64_t n, uin
 WRS_API wrs_status wrs_alias_sample_to_host(const wrs_alias_row* d_table, int64_t n, uint64_t num_samples,
                                             uint64_t seed, uint64_t counter_base, uint64_t chunk_samples,
                                             uint32_t* d_out, uint32_t* h_out, void* stream);
+
+/* Diagnostic: num_gathers random 8-byte row gathers from the table (rows from an integer hash
+ * of seed and position; the plain sampler's load form, eight in flight per thread), XOR-folded
+ * into *d_sink (device u32). Its rate is the random-access ceiling of the plain sampler on that
+ * table. No counterpart in the reference. */
+WRS_API wrs_status wrs_random_gather_probe(const wrs_alias_row* d_table, int64_t n, uint64_t num_gathers,
+                                           uint64_t seed, uint32_t* d_sink, void* stream);
 
 /* ---- rejection sampling ------------------------------------------------- */
 

@@ -51,6 +51,7 @@ def oracle() -> ctypes.CDLL:
             "or_exact_build": (_I, [_P, _I64, _D, _P]),
             "or_sample_plain": (None, [_P, _I64, _U64, _U64, _U64, _P]),
             "or_plain_replay_uniforms": (None, [_I64, _U64, _U64, _U64, _P, _P, _P]),
+            "or_prec_build": (_I, [_P, _I64, _I, _P, _P]),
             "or_binomial": (_U64, [_U64, _D, _U32, _U32, _U64, _U32]),
             "or_section_counts": (None, [_I64, _U32, _U64, _U64, _U64, _P]),
             "or_sample_sectioned": (None, [_P, _I64, _U64, _U32, _U64, _U64, _P, _P]),
@@ -218,6 +219,16 @@ def sample_plain(rows: np.ndarray, m: int, seed: int, cbase: int = 0) -> np.ndar
     out = np.zeros(m, dtype=np.uint32)
     oracle().or_sample_plain(_p(rows), rows.shape[0], m, seed, cbase, _p(out))
     return out
+
+
+def prec_build(w: np.ndarray, fp64: bool):
+    """The library's all-FP64 / all-FP32 comparison build (rows, W); rows None for invalid
+    weights or a zero total."""
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    rows = np.zeros((w.size, 2), dtype=np.uint32)
+    W = np.zeros(1, dtype=np.float64)
+    rc = oracle().or_prec_build(_p(w), w.size, 1 if fp64 else 0, _p(rows), _p(W))
+    return (None if rc else rows), float(W[0])
 
 
 def plain_replay_uniforms(n: int, m: int, seed: int, cbase: int = 0):

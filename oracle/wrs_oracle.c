@@ -834,6 +834,160 @@ int or_batched_build(const float* w, const int64_t* off, int64_t num_tables, uin
     return bad;
 }
 
+
+/* ------------------------------------------------------------------ precision comparison builds */
+/* The library's all-FP64 / all-FP32 builds (precision_kernels.cuh): the merge of the deficit
+ * and excess lines with every quantity in one floating-point type R, in the kernels' summation
+ * order. The weight total: tiles of 256 threads x 8 items; a thread sums its items in order,
+ * each warp's 32 thread sums in lane order, the 8 warp sums in order; tiles in 1024 chunks of
+ * K = ceil(tiles / 1024) consecutive tiles, each chunk in order, the chunk sums in order. The
+ * lines: each tile's deficits (excesses) summed in item order, the tile bases in tile order,
+ * an item's position = tile base + its tile-local prefix. Bit-exact with the GPU. */
+#define PREC_NT 256
+#define PREC_IPT 8
+#define PREC_TILE (PREC_NT * PREC_IPT)
+#define PREC_CHUNKS 1024
+
+#define DEFINE_PREC_BUILD(R, NAME)                                                                           \
+    /* exclusive prefixes of v[0..255] in the CTA order; returns the total */                               \
+    static R NAME##_block_scan(const R* v, R* ex) {                                                         \
+        R wtot[PREC_NT / 32];                                                                               \
+        for (int wp = 0; wp < PREC_NT / 32; ++wp) {                                                         \
+            R acc = (R)0;                                                                                   \
+            for (int l = 0; l < 32; ++l) {                                                                  \
+                ex[wp * 32 + l] = acc;                                                                      \
+                acc = acc + v[wp * 32 + l];                                                                 \
+            }                                                                                               \
+            wtot[wp] = acc;                                                                                 \
+        }                                                                                                   \
+        R base[PREC_NT / 32];                                                                               \
+        R acc = (R)0;                                                                                       \
+        for (int wp = 0; wp < PREC_NT / 32; ++wp) {                                                         \
+            base[wp] = acc;                                                                                 \
+            acc = acc + wtot[wp];                                                                           \
+        }                                                                                                   \
+        for (int t = 0; t < PREC_NT; ++t) ex[t] = base[t / 32] + ex[t];                                     \
+        return acc;                                                                                         \
+    }                                                                                                       \
+    /* exclusive prefixes of per-tile values in the chunked order; returns the total */                    \
+    static R NAME##_tile_scan(const R* v, int64_t nt, R* pre) {                                             \
+        const int64_t K = (nt + PREC_CHUNKS - 1) / PREC_CHUNKS;                                             \
+        R chunk[PREC_CHUNKS];                                                                               \
+        for (int c = 0; c < PREC_CHUNKS; ++c) {                                                             \
+            R acc = (R)0;                                                                                   \
+            for (int64_t t = c * K; t < nt && t < (c + 1) * K; ++t) acc = acc + v[t];                       \
+            chunk[c] = acc;                                                                                 \
+        }                                                                                                   \
+        R b = (R)0;                                                                                         \
+        for (int c = 0; c < PREC_CHUNKS; ++c) {                                                             \
+            const R t = chunk[c];                                                                           \
+            chunk[c] = b;                                                                                   \
+            b = b + t;                                                                                      \
+        }                                                                                                   \
+        if (pre) {                                                                                          \
+            for (int c = 0; c < PREC_CHUNKS; ++c) {                                                         \
+                R p = chunk[c];                                                                             \
+                for (int64_t t = c * K; t < nt && t < (c + 1) * K; ++t) {                                   \
+                    pre[t] = p;                                                                             \
+                    p = p + v[t];                                                                           \
+                }                                                                                           \
+            }                                                                                               \
+        }                                                                                                   \
+        return b;                                                                                           \
+    }                                                                                                       \
+    static int NAME(const float* w, int64_t n, uint32_t* rows, double* W_out) {                             \
+        const int64_t nt = (n + PREC_TILE - 1) / PREC_TILE;                                                 \
+        R* tv = (R*)malloc(sizeof(R) * nt);                                                                 \
+        R* th = (R*)malloc(sizeof(R) * nt);                                                                 \
+        R* pl = (R*)malloc(sizeof(R) * nt);                                                                 \
+        R* ph = (R*)malloc(sizeof(R) * nt);                                                                 \
+        int64_t* cl = (int64_t*)calloc(nt + 1, sizeof(int64_t));                                            \
+        int64_t* ch = (int64_t*)calloc(nt + 1, sizeof(int64_t));                                            \
+        R* Lkey = (R*)malloc(sizeof(R) * (n + 1));                                                          \
+        R* Hkey = (R*)malloc(sizeof(R) * (n + 1));                                                          \
+        uint32_t* Litem = (uint32_t*)malloc(4 * (n + 1));                                                   \
+        uint32_t* Hitem = (uint32_t*)malloc(4 * (n + 1));                                                   \
+        float* Lprob = (float*)malloc(4 * (n + 1));                                                         \
+        R v[PREC_NT], ex[PREC_NT];                                                                          \
+        int bad = 0;                                                                                        \
+        for (int64_t t = 0; t < nt; ++t) {                                                                  \
+            for (int thr = 0; thr < PREC_NT; ++thr) {                                                       \
+                R acc = (R)0;                                                                               \
+                for (int k = 0; k < PREC_IPT; ++k) {                                                        \
+                    const int64_t i = t * PREC_TILE + thr * PREC_IPT + k;                                   \
+                    if (i < n) {                                                                            \
+                        if (!(w[i] >= 0.0f) || isinf(w[i])) bad = 1;                                        \
+                        acc = acc + (R)w[i];                                                                \
+                    }                                                                                       \
+                }                                                                                           \
+                v[thr] = acc;                                                                               \
+            }                                                                                               \
+            tv[t] = NAME##_block_scan(v, ex);                                                               \
+        }                                                                                                   \
+        const R W = NAME##_tile_scan(tv, nt, NULL);                                                         \
+        if (W_out) *W_out = (double)W;                                                                      \
+        if (bad || !(W > (R)0) || isinf((double)W)) {                                                       \
+            free(tv); free(th); free(pl); free(ph); free(cl); free(ch);                                     \
+            free(Lkey); free(Hkey); free(Litem); free(Hitem); free(Lprob);                                  \
+            return 1;                                                                                       \
+        }                                                                                                   \
+        const R W_N = W / (R)(double)n;                                                                     \
+        /* the lines: per tile, sums in item order; tile bases in tile order; positions b + local */       \
+        int64_t nL = 0, nH = 0;                                                                             \
+        R bl = (R)0, bh = (R)0;                                                                             \
+        for (int64_t t = 0; t < nt; ++t) {                                                                  \
+            R sl = (R)0, sh = (R)0;                                                                         \
+            for (int64_t i = t * PREC_TILE; i < n && i < (t + 1) * PREC_TILE; ++i) {                        \
+                const R wr = (R)w[i];                                                                       \
+                if (wr > W_N) {                                                                             \
+                    sh = sh + (wr - W_N);                                                                   \
+                    Hkey[nH] = bh + sh;                                                                     \
+                    Hitem[nH] = (uint32_t)i;                                                                \
+                    ++nH;                                                                                   \
+                } else {                                                                                    \
+                    Lkey[nL] = bl + sl;                                                                     \
+                    Litem[nL] = (uint32_t)i;                                                                \
+                    const R q = wr / W_N;                                                                   \
+                    Lprob[nL] = (float)(q < (R)1 ? q : (R)1);                                               \
+                    sl = sl + (W_N - wr);                                                                   \
+                    ++nL;                                                                                   \
+                }                                                                                           \
+            }                                                                                               \
+            bl = bl + sl;                                                                                   \
+            bh = bh + sh;                                                                                   \
+        }                                                                                                   \
+        const R A_total = bl;                                                                               \
+        /* the merge: heavy j before light i iff Hkey[j] <= Lkey[i] */                                      \
+        int64_t i = 0, j = 0;                                                                               \
+        while (i < nL || j < nH) {                                                                          \
+            if (j < nH && (i >= nL || Hkey[j] <= Lkey[i])) {                                                \
+                const R A_next = i < nL ? Lkey[i] : A_total;                                                \
+                R rr = (W_N + Hkey[j] - A_next) / W_N;                                                      \
+                if (rr > (R)1) rr = (R)1;                                                                   \
+                if (!(rr > (R)0)) rr = (R)0;                                                                \
+                const uint32_t item = Hitem[j];                                                             \
+                rows[2 * (int64_t)item] = f_bits((float)rr);                                                \
+                rows[2 * (int64_t)item + 1] = Hitem[j + 1 < nH ? j + 1 : j];                                \
+                ++j;                                                                                        \
+            } else {                                                                                        \
+                const uint32_t item = Litem[i];                                                             \
+                rows[2 * (int64_t)item] = f_bits(Lprob[i]);                                                 \
+                rows[2 * (int64_t)item + 1] = nH ? Hitem[j < nH ? j : nH - 1] : item;                       \
+                ++i;                                                                                        \
+            }                                                                                               \
+        }                                                                                                   \
+        free(tv); free(th); free(pl); free(ph); free(cl); free(ch);                                         \
+        free(Lkey); free(Hkey); free(Litem); free(Hitem); free(Lprob);                                      \
+        return 0;                                                                                           \
+    }
+
+DEFINE_PREC_BUILD(double, prec_build_f64)
+DEFINE_PREC_BUILD(float, prec_build_f32)
+
+int or_prec_build(const float* w, int64_t n, int fp64, uint32_t* rows, double* W_out) {
+    return fp64 ? prec_build_f64(w, n, rows, W_out) : prec_build_f32(w, n, rows, W_out);
+}
+
 /* ------------------------------------------------------------------ sampling */
 /* doSample (sampling/aliasTable/SamplerGpuBasic.cu:28-69) with frac := coin and
  * weight := prob * W/N: result = coin < prob ? row : alias (a full row keeps itself). */

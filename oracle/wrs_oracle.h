@@ -55,6 +55,9 @@ int or_check_ref_table_w(const float* w, int64_t n, const double* weight, const 
 
 /* the library's exact merge build, sequentially; W = the weight total the build uses */
 int or_exact_build(const float* w, int64_t n, double W, uint32_t* rows);
+/* The library's all-FP64 (fp64 = 1) or all-FP32 (fp64 = 0) comparison build
+ * (precision_kernels.cuh), bit-exact; returns 1 for invalid weights or a zero total. */
+int or_prec_build(const float* w, int64_t n, int fp64, uint32_t* rows, double* W_out);
 
 /* sampling contract */
 void or_sample_plain(const uint32_t* rows, int64_t n, uint64_t m, uint64_t seed, uint64_t cbase, uint32_t* out);

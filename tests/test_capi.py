@@ -46,7 +46,7 @@ def test_status_strings():
 
 
 def test_version():
-    assert wrs.lib().wrs_version() == 1
+    assert wrs.lib().wrs_version() == 2
 
 
 def test_scratch_sizes_are_host_only_and_monotone():
@@ -150,3 +150,12 @@ def test_wait_limit_setters_check_their_arguments():
     assert wrs.debug_hold_lookback(-2) == wrs.WRS_ERR_INVALID_ARGUMENT
     assert wrs.debug_hold_lookback(3) == wrs.WRS_SUCCESS
     assert wrs.debug_hold_lookback(-1) == wrs.WRS_SUCCESS
+
+
+def test_precision_options_are_checked_on_the_host():
+    n = 1 << 20
+    assert wrs.alias_build_scratch_bytes(n, wrs.build_opts(precision=wrs.WRS_PRECISION_FP64)) > 24 * n
+    assert wrs.alias_build_scratch_bytes(n, wrs.build_opts(precision=wrs.WRS_PRECISION_FP32)) > 16 * n
+    assert wrs.alias_build_scratch_bytes(n, wrs.build_opts(precision=3)) == 0
+    assert wrs.alias_build_scratch_bytes(
+        n, wrs.build_opts(method=wrs.WRS_METHOD_PSA_PLUS, precision=wrs.WRS_PRECISION_FP64)) == 0

@@ -126,3 +126,17 @@ def test_reference_verifier_accepts_the_tables(name, n):
         bad = weight.copy()
         bad[j] *= 0.75
         assert not po.ref_verify(w.astype(np.float64), bad, alias, W)
+
+
+def test_precision_comparison_builds_in_the_oracle():
+    """The oracle's all-FP64 / all-FP32 restatements give valid tables; the FP32 lines lose
+    accuracy on spread weights, the FP64 lines stay near the stored FP32 rounding."""
+    w = gen("loguniform", 1 << 16)
+    r64, W64 = po.prec_build(w, True)
+    r32, W32 = po.prec_build(w, False)
+    assert r64 is not None and r32 is not None
+    assert np.all(r64[:, 1] < w.size) and np.all(r32[:, 1] < w.size)
+    e64 = po.check_table(w, r64)["max_rel"]
+    e32 = po.check_table(w, r32)["max_rel"]
+    assert e64 < 1e-6 < e32
+    assert po.prec_build(np.zeros(10, np.float32), True)[0] is None
