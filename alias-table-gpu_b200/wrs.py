@@ -94,6 +94,11 @@ _SIGNATURES = {
     "wrs_batched_autotune_kinds": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _SZ,
                                                   _P, _P, _P, _P]),
     "wrs_scratch_status": (ctypes.c_int, [_P, _P]),
+    "wrs_table_file_write": (ctypes.c_int, [ctypes.c_char_p, _P, _I64, ctypes.c_double, _P]),
+    "wrs_batched_table_file_write": (ctypes.c_int, [ctypes.c_char_p, _P, _P, _I64, _P]),
+    "wrs_table_file_info": (ctypes.c_int, [ctypes.c_char_p, _P, _P, _P]),
+    "wrs_table_file_read": (ctypes.c_int, [ctypes.c_char_p, _P, _I64, _P, _I64, _P]),
+    "wrs_shard_tables": (ctypes.c_int, [_P, _I64, ctypes.c_int32, _I64, _P]),
     "wrs_static_scratch_status": (ctypes.c_int, [_P]),
     "wrs_set_device_wait_limit": (ctypes.c_int, [_U64]),
     "wrs_debug_hold_lookback": (ctypes.c_int, [_I64]),
@@ -169,6 +174,42 @@ def alias_build_static_scratch(w, table, opts: Optional[BuildOpts] = None, W_out
     memory; the scratch is a fixed array inside the library, shared by all calls on a device."""
     return lib().wrs_alias_build_f32_static_scratch(_ptr(w), w.numel(), ctypes.byref(opts) if opts else None,
                                                     _ptr(table), _ptr(W_out), _stream(stream))
+
+
+def table_file_write(path: str, table, W: float, stream=None) -> int:
+    return lib().wrs_table_file_write(path.encode(), _ptr(table), table.numel(), W, _stream(stream))
+
+
+def batched_table_file_write(path: str, table, h_offsets, stream=None) -> int:
+    import numpy as np
+    off = np.ascontiguousarray(h_offsets, dtype=np.int64)
+    return lib().wrs_batched_table_file_write(path.encode(), _ptr(table), off.ctypes.data, off.size - 1,
+                                              _stream(stream))
+
+
+def table_file_info(path: str):
+    """(status, n, num_tables, W) of a table file."""
+    n, t, W = ctypes.c_int64(0), ctypes.c_int64(0), ctypes.c_double(0.0)
+    st = lib().wrs_table_file_info(path.encode(), ctypes.byref(n), ctypes.byref(t), ctypes.byref(W))
+    return st, n.value, t.value, W.value
+
+
+def table_file_read(path: str, table, num_tables: int = 1, stream=None):
+    """(status, offsets) after reading a table file's rows into `table`."""
+    import numpy as np
+    off = np.zeros(num_tables + 1, dtype=np.int64)
+    st = lib().wrs_table_file_read(path.encode(), _ptr(table), table.numel(), off.ctypes.data, num_tables,
+                                   _stream(stream))
+    return st, off
+
+
+def shard_tables(h_offsets, num_shards: int, table_cost: int = 16):
+    """(status, bounds): contiguous table ranges [bounds[s], bounds[s+1]) per shard."""
+    import numpy as np
+    off = np.ascontiguousarray(h_offsets, dtype=np.int64)
+    bounds = np.zeros(num_shards + 1, dtype=np.int64)
+    st = lib().wrs_shard_tables(off.ctypes.data, off.size - 1, num_shards, table_cost, bounds.ctypes.data)
+    return st, bounds
 
 
 def set_device_wait_limit(limit_ns: int) -> int:

@@ -322,6 +322,36 @@ WRS_API wrs_status wrs_batched_autotune_kinds(const float* d_w, const int64_t* d
 WRS_API wrs_status wrs_export_reference_table(const wrs_alias_row* d_table, int64_t n, double W,
                                               double* d_weight, int32_t* d_alias, void* stream);
 
+/* ---- table files -------------------------------------------------------- */
+
+/* A table saved to a file and read back, so that a table built once is sampled later by another
+ * process or on another device (the reference keeps its tables in memory only,
+ * construction/aliasTable/TableStorage.cuh:6-128). The file holds a 64-byte header (magic
+ * "WRSTABLE", version, row size, n, number of tables, W, an FNV-1a checksum of offsets and rows),
+ * the CSR offsets (num_tables + 1 int64) and the n rows. The calls copy through host memory in
+ * chunks, synchronising `stream`. */
+WRS_API wrs_status wrs_table_file_write(const char* path, const wrs_alias_row* d_table, int64_t n, double W,
+                                        void* stream);
+WRS_API wrs_status wrs_batched_table_file_write(const char* path, const wrs_alias_row* d_table,
+                                                const int64_t* h_offsets, int64_t num_tables, void* stream);
+/* Rows, tables and W (0 for a batch) of a table file; WRS_ERR_INVALID_ARGUMENT if it is not one. */
+WRS_API wrs_status wrs_table_file_info(const char* path, int64_t* n, int64_t* num_tables, double* W);
+/* Reads the rows into d_table (n rows; n and num_tables must match the file, else
+ * WRS_ERR_CAPACITY) and the offsets into h_offsets (optional, num_tables + 1); a checksum
+ * mismatch gives WRS_ERR_INVALID_ARGUMENT. */
+WRS_API wrs_status wrs_table_file_read(const char* path, wrs_alias_row* d_table, int64_t n, int64_t* h_offsets,
+                                       int64_t num_tables, void* stream);
+
+/* ---- sharding a batch over devices ------------------------------------- */
+
+/* Tables are independent, so a batch spreads over devices by contiguous table ranges with no
+ * exchange between them: shard s builds and samples tables [h_bounds[s], h_bounds[s+1]) with
+ * the batched calls on its own device. The ranges balance items + table_cost per table
+ * (table_cost: the items one table's fixed costs are worth, e.g. 16). Host only; no counterpart
+ * in the reference (one GPU). */
+WRS_API wrs_status wrs_shard_tables(const int64_t* h_offsets, int64_t num_tables, int32_t num_shards,
+                                    int64_t table_cost, int64_t* h_bounds);
+
 /* ---- status / misc ------------------------------------------------------ */
 
 /* Bounded device waits. Every device-side wait of the library (the decoupled look-back scans
