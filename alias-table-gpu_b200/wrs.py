@@ -99,6 +99,11 @@ _SIGNATURES = {
     "wrs_table_file_info": (ctypes.c_int, [ctypes.c_char_p, _P, _P, _P]),
     "wrs_table_file_read": (ctypes.c_int, [ctypes.c_char_p, _P, _I64, _P, _I64, _P]),
     "wrs_shard_tables": (ctypes.c_int, [_P, _I64, ctypes.c_int32, _I64, _P]),
+    "wrs_autotune_build": (ctypes.c_int, [_P, _I64, _P, _P, _SZ, _P, _P]),
+    "wrs_autotune_sections": (ctypes.c_int, [_P, _I64, _U64, _P, _P, _P]),
+    "wrs_autotune_lookup": (ctypes.c_int, [_I64, _P, _P]),
+    "wrs_autotune_cache_save": (ctypes.c_int, [ctypes.c_char_p]),
+    "wrs_autotune_cache_load": (ctypes.c_int, [ctypes.c_char_p]),
     "wrs_static_scratch_status": (ctypes.c_int, [_P]),
     "wrs_set_device_wait_limit": (ctypes.c_int, [_U64]),
     "wrs_debug_hold_lookback": (ctypes.c_int, [_I64]),
@@ -210,6 +215,36 @@ def shard_tables(h_offsets, num_shards: int, table_cost: int = 16):
     bounds = np.zeros(num_shards + 1, dtype=np.int64)
     st = lib().wrs_shard_tables(off.ctypes.data, off.size - 1, num_shards, table_cost, bounds.ctypes.data)
     return st, bounds
+
+
+def autotune_build(w, table, scratch, opts: Optional[BuildOpts] = None, stream=None):
+    """(status, opts) with opts.tile_items the fastest tile size for these weights."""
+    opts = opts if opts is not None else build_opts()
+    st = lib().wrs_autotune_build(_ptr(w), w.numel(), _ptr(table), _ptr(scratch),
+                                  scratch.numel() * scratch.element_size(), ctypes.byref(opts), _stream(stream))
+    return st, opts
+
+
+def autotune_sections(table, n: int, num_samples: int, out, stream=None):
+    """(status, section_items): the fastest section size for sectioned sampling of this table."""
+    S = ctypes.c_uint32(0)
+    st = lib().wrs_autotune_sections(_ptr(table), n, num_samples, _ptr(out), ctypes.byref(S), _stream(stream))
+    return st, S.value
+
+
+def autotune_lookup(n: int):
+    """(status, tile_items, section_items) recorded for this GPU and ceil(log2 n)."""
+    t, S = ctypes.c_uint32(0), ctypes.c_uint32(0)
+    st = lib().wrs_autotune_lookup(n, ctypes.byref(t), ctypes.byref(S))
+    return st, t.value, S.value
+
+
+def autotune_cache_save(path: str) -> int:
+    return lib().wrs_autotune_cache_save(path.encode())
+
+
+def autotune_cache_load(path: str) -> int:
+    return lib().wrs_autotune_cache_load(path.encode())
 
 
 def set_device_wait_limit(limit_ns: int) -> int:

@@ -554,8 +554,20 @@ def single_table_summary(dev, cfg: dict, steps: int = 20) -> dict:
         raise RuntimeError("build failed on the device")
     b = statistics.median([ev[3 * r].elapsed_time(ev[3 * r + 1]) for r in range(steps)])
     smp = statistics.median([ev[3 * r + 1].elapsed_time(ev[3 * r + 2]) for r in range(steps)])
+    # sectioned sampling with the section size the autotuner picks for this table
+    st, S = wrs.autotune_sections(table, n, m, out)
+    if st:
+        raise wrs.WrsError(st, "autotune_sections")
+    for r in range(steps):
+        ev[3 * r].record()
+        assert wrs.alias_sample(table, n, m, SEED_SAMPLES, out, r * m, mode=wrs.WRS_SAMPLE_SECTIONED,
+                                section_items=S) == 0
+        ev[3 * r + 1].record()
+    torch.cuda.synchronize()
+    sec = statistics.median([ev[3 * r].elapsed_time(ev[3 * r + 1]) for r in range(steps)])
     return {"workload": cfg["workload"], "build_ms": round(b, 4), "build_gitems_s": round(n / b / 1e6, 2),
             "sample_ms": round(smp, 4), "sample_gsamples_s": round(m / smp / 1e6, 2),
+            "sectioned_sample_ms": round(sec, 4), "sectioned_section_items": S,
             "value": round((n + m) / (b + smp) / 1e6, 3), "unit": UNIT, "prob_error": table_error_gpu(w, table)}
 
 

@@ -313,6 +313,29 @@ WRS_API wrs_status wrs_batched_autotune_kinds(const float* d_w, const int64_t* d
                                               void* d_scratch, size_t scratch_bytes, uint8_t* h_kinds_out,
                                               uint8_t* class_kinds, float* class_ms, void* stream);
 
+/* ---- autotuning of the single-table build and the sectioned sampler --- */
+
+/* Times the split build of these weights at every tile size (1024, 2048, 4096; those whose
+ * scratch fits scratch_bytes) and writes the fastest into opts->tile_items (method SPLIT,
+ * precision MIXED). Synchronous; it builds into d_table. Replaces the reference's compile-time
+ * launch shapes and its fixed rule for the split count (AliasTableSplitGpu.cuh:60-94,
+ * AliasTableSplitGpu.cu:53-75). The choice is recorded for this GPU and ceil(log2 n). */
+WRS_API wrs_status wrs_autotune_build(const float* d_w, int64_t n, wrs_alias_row* d_table, void* d_scratch,
+                                      size_t scratch_bytes, wrs_build_opts* opts, void* stream);
+/* Times WRS_SAMPLE_SECTIONED sampling of num_samples from this table at section sizes 512 ..
+ * 65536 and writes the fastest into *section_items (recorded like wrs_autotune_build's choice).
+ * Synchronous; d_out holds num_samples. The reference takes the section size as an argument
+ * (SamplerGpuSectioned.cu:7-9). */
+WRS_API wrs_status wrs_autotune_sections(const wrs_alias_row* d_table, int64_t n, uint64_t num_samples,
+                                         uint32_t* d_out, uint32_t* section_items, void* stream);
+/* The recorded choices for this GPU and ceil(log2 n) (0 where not tuned); WRS_ERR_INVALID_ARGUMENT
+ * when nothing is recorded for that size. */
+WRS_API wrs_status wrs_autotune_lookup(int64_t n, uint32_t* tile_items, uint32_t* section_items);
+/* The recorded choices as JSON, {"entries": [{"gpu", "log2n", "tile_items", "section_items"}]},
+ * written to / merged from a file. */
+WRS_API wrs_status wrs_autotune_cache_save(const char* path);
+WRS_API wrs_status wrs_autotune_cache_load(const char* path);
+
 /* ---- reference table format -------------------------------------------- */
 
 /* Writes the table in the reference's format (TableStorage, construction/aliasTable/
