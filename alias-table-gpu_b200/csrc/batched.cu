@@ -62,8 +62,12 @@ bool shape_of(const wrs_build_opts* opts, Shape* sh) {
 }
 
 // The host's view of the batch for one shape (from h_offsets and h_kinds).
+// Tables of at most this many items are built by 8-lane groups, four per warp.
+constexpr uint32_t kTinyMax = 16;
+
 struct HostPlan {
     uint32_t small_tables;  // alias tables with 1 <= n <= small_max
+    uint32_t tiny_tables;   // ... of them with n <= kTinyMax
     uint32_t big_tables;    // alias tables with n > small_max
     uint32_t tiles;         // tiles of the big tables
     uint64_t big_items;
@@ -73,7 +77,7 @@ struct HostPlan {
 };
 
 HostPlan host_plan(const int64_t* h_offsets, int64_t num_tables, const Shape& sh, const uint8_t* h_kinds = nullptr) {
-    HostPlan p{0, 0, 0, 0, 0, 0, true};
+    HostPlan p{0, 0, 0, 0, 0, 0, 0, true};
     if (!h_offsets || num_tables < 1 || h_offsets[0] != 0) {
         p.valid = false;
         return p;
@@ -94,6 +98,7 @@ HostPlan host_plan(const int64_t* h_offsets, int64_t num_tables, const Shape& sh
         if (kind != WRS_TABLE_ALIAS) continue;
         if (n <= (int64_t)sh.small_max) {
             ++small;
+            if (n <= (int64_t)kTinyMax) ++p.tiny_tables;
         } else {
             ++tables;
             tiles += (uint64_t)((n + sh.tile - 1) / sh.tile);
@@ -146,25 +151,41 @@ BatchLayout carve_batch(void* scratch, int64_t num_tables, const HostPlan& p, ui
     return L;
 }
 
-template <int SPL>
-wrs_status launch_small(const float* d_w, const int64_t* d_offsets, const uint8_t* d_kinds, int64_t num_tables,
-                        wrs_alias_row* d_table, double* d_W, uint32_t* status, uint32_t small_tables,
-                        cudaStream_t stream) {
-    const size_t smem = sizeof(SmallSmem<SPL>) * kSmallWarps;
-    cudaError_t e = cudaFuncSetAttribute(small_tables_kernel<SPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+// One group of GW lanes per table of min_n <= n <= max_n items (persistent groups over all
+// tables, each skipping the others), `count` such tables.
+template <int SPL, int GW>
+wrs_status launch_small_groups(const float* d_w, const int64_t* d_offsets, const uint8_t* d_kinds, int64_t num_tables,
+                               uint32_t min_n, uint32_t max_n, wrs_alias_row* d_table, double* d_W, uint32_t* status,
+                               uint32_t count, cudaStream_t stream) {
+    if (count == 0) return WRS_SUCCESS;
+    constexpr int GPW = 32 / GW;
+    const size_t smem = sizeof(SmallSmem<SPL, GW>) * kSmallWarps * GPW;
+    cudaError_t e = cudaFuncSetAttribute(small_tables_kernel<SPL, GW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return WRS_ERR_CUDA;
-    // persistent warps over all tables (each warp skips the large and empty ones)
     const DeviceInfo d = device_info();
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, small_tables_kernel<SPL>, 32 * kSmallWarps, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, small_tables_kernel<SPL, GW>, 32 * kSmallWarps, smem);
     if (e != cudaSuccess || per_sm < 1) per_sm = 1;
-    const uint64_t want = ((uint64_t)small_tables + kSmallWarps - 1) / kSmallWarps;
+    const uint64_t want = ((uint64_t)count + kSmallWarps * GPW - 1) / (kSmallWarps * GPW);
     const uint64_t cap = (uint64_t)d.sm_count * per_sm;
     const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min(want, cap));
-    small_tables_kernel<SPL><<<grid, 32 * kSmallWarps, smem, stream>>>(d_w, d_offsets, d_kinds, num_tables,
-                                                                        32u * SPL, d_table, d_W, status);
+    small_tables_kernel<SPL, GW><<<grid, 32 * kSmallWarps, smem, stream>>>(d_w, d_offsets, d_kinds, num_tables, min_n,
+                                                                            max_n, d_table, d_W, status);
     return launch_status();
+}
+
+// The small tables: those of at most kTinyMax items by 8-lane groups, the others by warps.
+template <int SPL>
+wrs_status launch_small(const float* d_w, const int64_t* d_offsets, const uint8_t* d_kinds, int64_t num_tables,
+                        wrs_alias_row* d_table, double* d_W, uint32_t* status, const HostPlan& p,
+                        cudaStream_t stream) {
+    static_assert(32 * SPL > (int)kTinyMax, "the warp kernel takes the tables above the tiny ones");
+    wrs_status st = launch_small_groups<2, 8>(d_w, d_offsets, d_kinds, num_tables, 1u, kTinyMax, d_table, d_W, status,
+                                              p.tiny_tables, stream);
+    if (st != WRS_SUCCESS) return st;
+    return launch_small_groups<SPL, 32>(d_w, d_offsets, d_kinds, num_tables, kTinyMax + 1, 32u * SPL, d_table, d_W,
+                                        status, p.small_tables - p.tiny_tables, stream);
 }
 
 template <int T>
@@ -256,11 +277,11 @@ wrs_status batched_build(const float* d_w, const int64_t* d_offsets, const int64
         uint32_t* status = &L.hdr0->status;
         const cudaStream_t ss = small_stream;
         switch (sh.small_max) {
-            case 32: st = launch_small<1>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p.small_tables, ss); break;
-            case 64: st = launch_small<2>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p.small_tables, ss); break;
-            case 128: st = launch_small<4>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p.small_tables, ss); break;
-            case 256: st = launch_small<8>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p.small_tables, ss); break;
-            default: st = launch_small<16>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p.small_tables, ss); break;
+            case 32: st = launch_small<1>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p, ss); break;
+            case 64: st = launch_small<2>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p, ss); break;
+            case 128: st = launch_small<4>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p, ss); break;
+            case 256: st = launch_small<8>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p, ss); break;
+            default: st = launch_small<16>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p, ss); break;
         }
     }
     if (st == WRS_SUCCESS && p.big_tables > 0) {

@@ -302,44 +302,77 @@ __global__ void batch_status_kernel(const BuildHeader* hdrs, uint32_t num_tables
     }
 }
 
-// ---------------------------------------------------------------- small tables: one warp each
-// The whole build of a table of n <= 32 * SPL items in one warp. Lane l holds the
-// ipl = ceil(n / 32) consecutive items l * ipl ..; the quantities are those of the tiled
-// passes for a one-tile table (A_before = 0, no dithering offset), so the rows equal a
-// single-table build's. Shared memory per warp: light keys from the front and heavy keys
-// from the back of one u64 array, and the heavies' corrected excess ends and items.
+// ---------------------------------------------------------------- small tables: a lane group each
+// The whole build of a table of n <= GW * SPL items in one group of GW lanes (GW = 32: a warp
+// per table; GW = 8: four tables per warp, for the tiny tables that dominate skewed batches).
+// Lane l of the group holds the ipl = ceil(n / GW) consecutive items l * ipl ..; the
+// quantities are those of the tiled passes for a one-tile table (A_before = 0, no dithering
+// offset), so the rows equal a single-table build's. Shared memory per group: light keys from
+// the front and heavy keys from the back of one u64 array, and the heavies' corrected excess
+// ends and items. The kernel takes the alias tables with min_n <= n <= small_max.
 constexpr int kSmallWarps = 4;
 
-template <int SPL>
+template <int SPL, int GW = 32>
 struct SmallSmem {
-    static constexpr int CAP = 32 * SPL;
+    static constexpr int CAP = GW * SPL;
     uint64_t key[CAP];
     uint64_t elo[CAP];
     uint32_t ehi[CAP];
     uint32_t item[CAP];
 };
 
-template <int SPL>
+// Exclusive scans over a group of GW lanes (width GW shuffles); `total` gets the group's sum.
+template <int GW>
+__device__ __forceinline__ uint32_t group_excl_scan_u32(uint32_t v, uint32_t mask, uint32_t& total) {
+    const int gl = threadIdx.x & (GW - 1);
+    uint32_t inc = v;
+#pragma unroll
+    for (int off = 1; off < GW; off <<= 1) {
+        const uint32_t o = __shfl_up_sync(mask, inc, off, GW);
+        if (gl >= off) inc += o;
+    }
+    total = __shfl_sync(mask, inc, GW - 1, GW);
+    return inc - v;
+}
+template <int GW>
+__device__ __forceinline__ uint64_t group_excl_scan_u64(uint64_t v, uint32_t mask, uint64_t& total) {
+    const int gl = threadIdx.x & (GW - 1);
+    uint64_t inc = v;
+#pragma unroll
+    for (int off = 1; off < GW; off <<= 1) {
+        const uint64_t o = __shfl_up_sync(mask, inc, off, GW);
+        if (gl >= off) inc += o;
+    }
+    total = __shfl_sync(mask, inc, GW - 1, GW);
+    return inc - v;
+}
+
+template <int SPL, int GW = 32>
 __global__ void __launch_bounds__(32 * kSmallWarps) small_tables_kernel(const float* __restrict__ w,
                                                                        const int64_t* __restrict__ offsets,
                                                                        const uint8_t* kinds, int64_t num_tables,
-                                                                       uint32_t small_max,
+                                                                       uint32_t min_n, uint32_t small_max,
                                                                        wrs_alias_row* __restrict__ table,
                                                                        double* W_out, uint32_t* status) {
-    constexpr int CAP = 32 * SPL;
+    static_assert(GW == 32 || GW == 16 || GW == 8, "lane group width");
+    constexpr int CAP = GW * SPL;
+    constexpr int GPW = 32 / GW;  // groups per warp
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    SmallSmem<SPL>& sm = reinterpret_cast<SmallSmem<SPL>*>(smem_raw)[warp];
-    const int64_t nwarps = (int64_t)gridDim.x * kSmallWarps;
-    for (int64_t t = (int64_t)blockIdx.x * kSmallWarps + warp; t < num_tables; t += nwarps) {
+    const int grp = lane / GW, gl = lane & (GW - 1);
+    const uint32_t mask = GW == 32 ? 0xffffffffu : (((1u << GW) - 1u) << (grp * GW));
+    SmallSmem<SPL, GW>& sm = reinterpret_cast<SmallSmem<SPL, GW>*>(smem_raw)[warp * GPW + grp];
+    const int64_t ngroups = (int64_t)gridDim.x * kSmallWarps * GPW;
+    for (int64_t t = ((int64_t)blockIdx.x * kSmallWarps + warp) * GPW + grp; t < num_tables; t += ngroups) {
         const int64_t off = offsets[t];
         const int64_t nn = offsets[t + 1] - off;
-        if (nn < 1 || nn > (int64_t)small_max || nn > CAP || !kind_is(kinds, t, WRS_TABLE_ALIAS)) continue;
+        if (nn < (int64_t)min_n || nn < 1 || nn > (int64_t)small_max || nn > CAP || !kind_is(kinds, t, WRS_TABLE_ALIAS))
+            continue;
         const uint32_t n = (uint32_t)nn;
-        const uint32_t ipl = (n + 31) / 32;
+        const uint32_t ipl = (n + GW - 1) / GW;
         const float* wt = w + off;
         wrs_alias_row* rows = table + off;
-        const uint32_t i0 = (uint32_t)lane * ipl;
+        const uint32_t i0 = (uint32_t)gl * ipl;
         float x[SPL];
         DD acc = {0.0, 0.0};
         bool bad = false;
@@ -355,20 +388,20 @@ __global__ void __launch_bounds__(32 * kSmallWarps) small_tables_kernel(const fl
         }
         acc = dd_norm(acc);
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
+        for (int o = GW / 2; o > 0; o >>= 1) {
             DD v;
-            v.hi = __shfl_down_sync(0xffffffffu, acc.hi, o);
-            v.lo = __shfl_down_sync(0xffffffffu, acc.lo, o);
+            v.hi = __shfl_down_sync(mask, acc.hi, o, GW);
+            v.lo = __shfl_down_sync(mask, acc.lo, o, GW);
             acc = dd_add(acc, v);
         }
         acc = dd_norm(acc);
-        const double W = __shfl_sync(0xffffffffu, acc.hi, 0);
-        const bool any_bad = __any_sync(0xffffffffu, bad);
+        const double W = __shfl_sync(mask, acc.hi, 0, GW);
+        const bool any_bad = __any_sync(mask, bad);
         if (any_bad || !(W > 0.0) || isinf(W)) {
-            if (lane == 0) record_status(status, (any_bad || isinf(W)) ? kErrInvalidWeight : kErrZeroTotal);
+            if (gl == 0) record_status(status, (any_bad || isinf(W)) ? kErrInvalidWeight : kErrZeroTotal);
             continue;
         }
-        if (lane == 0 && W_out) W_out[t] = W;
+        if (gl == 0 && W_out) W_out[t] = W;
         const double W_N = W / (double)n;
         const ClassParams cp = class_params(W_N, 1.0 / W_N);
         // classification and per-lane sums
@@ -391,12 +424,12 @@ __global__ void __launch_bounds__(32 * kSmallWarps) small_tables_kernel(const fl
             if (heavy) E += rare_q(wk, true, cp);
         }
         uint32_t nl_tot, nh_tot;
-        const uint32_t l0 = warp_excl_scan_u32((uint32_t)__popc(lbits), nl_tot);
-        const uint32_t h0 = warp_excl_scan_u32((uint32_t)__popc(hbits), nh_tot);
+        const uint32_t l0 = group_excl_scan_u32<GW>((uint32_t)__popc(lbits), mask, nl_tot);
+        const uint32_t h0 = group_excl_scan_u32<GW>((uint32_t)__popc(hbits), mask, nh_tot);
         uint64_t S_tot, L_tot, E_tot;
-        const uint64_t s0 = warp_excl_scan_u64(S, S_tot);
-        const uint64_t lq0 = warp_excl_scan_u64(L, L_tot);
-        const uint64_t e0 = warp_excl_scan_u64(E, E_tot);
+        const uint64_t s0 = group_excl_scan_u64<GW>(S, mask, S_tot);
+        const uint64_t lq0 = group_excl_scan_u64<GW>(L, mask, L_tot);
+        const uint64_t e0 = group_excl_scan_u64<GW>(E, mask, E_tot);
         const u128 A_tot = ((u128)S_tot << 16) + q_round24((u128)L_tot << 16);
         const int64_t nfix = excess_correction(A_tot, (u128)E_tot << 40);
         Dither dth;
@@ -432,10 +465,10 @@ __global__ void __launch_bounds__(32 * kSmallWarps) small_tables_kernel(const fl
                 }
             }
         }
-        __syncwarp();
+        __syncwarp(mask);
         const uint64_t* hkey = sm.key + (CAP - nh_tot);
         // heavy rows
-        for (uint32_t j = lane; j < nh_tot; j += 32) {
+        for (uint32_t j = gl; j < nh_tot; j += GW) {
             const uint64_t kh = hkey[j];
             uint32_t lo = 0, hi = nl_tot;  // rank: the first light whose key is not below kh
             while (lo < hi) {
@@ -474,7 +507,7 @@ __global__ void __launch_bounds__(32 * kSmallWarps) small_tables_kernel(const fl
                 ++li;
             }
         }
-        __syncwarp();  // the next table reuses this warp's shared memory
+        __syncwarp(mask);  // the next table reuses this group's shared memory
     }
 }
 
