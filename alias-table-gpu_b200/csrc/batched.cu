@@ -20,22 +20,63 @@ namespace {
 
 constexpr uint32_t kDefaultSmall = 128;
 
-// The library's side stream of the current device (created on first use): the one-warp
-// tables of a batch are built there while `stream` runs the tiled passes.
+// The library's side streams of the current device (created on first use): the small tables
+// of a batch are built there, by size class, while `stream` runs the tiled passes.
 constexpr int kMaxDevices = 64;
+constexpr int kSideStreams = 3;
 std::mutex g_side_mu;
-cudaStream_t g_side[kMaxDevices] = {};
-wrs_status side_stream(cudaStream_t* out) {
+cudaStream_t g_side[kMaxDevices][kSideStreams] = {};
+wrs_status side_streams(cudaStream_t (&out)[kSideStreams]) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return WRS_ERR_CUDA;
     std::lock_guard<std::mutex> lock(g_side_mu);
-    if (!g_side[dev] && cudaStreamCreateWithFlags(&g_side[dev], cudaStreamNonBlocking) != cudaSuccess) {
-        g_side[dev] = nullptr;
-        return WRS_ERR_CUDA;
+    for (int k = 0; k < kSideStreams; ++k) {
+        if (!g_side[dev][k] && cudaStreamCreateWithFlags(&g_side[dev][k], cudaStreamNonBlocking) != cudaSuccess) {
+            g_side[dev][k] = nullptr;
+            return WRS_ERR_CUDA;
+        }
+        out[k] = g_side[dev][k];
     }
-    *out = g_side[dev];
     return WRS_SUCCESS;
 }
+
+// Side streams forked from `stream` and joined back into it by events (which a stream capture
+// records as a fork and a join). `mid` orders work between the side streams.
+struct Fork {
+    cudaStream_t side[kSideStreams];
+    cudaEvent_t fork = nullptr, mid = nullptr, join[kSideStreams] = {};
+    bool open = false;
+
+    wrs_status begin(cudaStream_t stream) {
+        for (int k = 0; k < kSideStreams; ++k) side[k] = stream;
+        if (side_streams(side) != WRS_SUCCESS) return WRS_ERR_CUDA;
+        bool ok = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming) == cudaSuccess &&
+                  cudaEventCreateWithFlags(&mid, cudaEventDisableTiming) == cudaSuccess;
+        for (int k = 0; ok && k < kSideStreams; ++k)
+            ok = cudaEventCreateWithFlags(&join[k], cudaEventDisableTiming) == cudaSuccess;
+        ok = ok && cudaEventRecord(fork, stream) == cudaSuccess;
+        for (int k = 0; ok && k < kSideStreams; ++k) ok = cudaStreamWaitEvent(side[k], fork, 0) == cudaSuccess;
+        open = ok;
+        return ok ? WRS_SUCCESS : WRS_ERR_CUDA;
+    }
+    // joins every side stream that was forked, so that a capture stays well formed
+    wrs_status end(cudaStream_t stream) {
+        bool ok = true;
+        if (open)
+            for (int k = 0; k < kSideStreams; ++k)
+                ok = cudaEventRecord(join[k], side[k]) == cudaSuccess &&
+                     cudaStreamWaitEvent(stream, join[k], 0) == cudaSuccess && ok;
+        open = false;
+        return ok ? WRS_SUCCESS : WRS_ERR_CUDA;
+    }
+    ~Fork() {
+        if (fork) cudaEventDestroy(fork);
+        if (mid) cudaEventDestroy(mid);
+        for (int k = 0; k < kSideStreams; ++k)
+            if (join[k]) cudaEventDestroy(join[k]);
+    }
+};
+
 const uint32_t kSmallChoices[] = {32, 64, 128, 256, 512};
 const uint32_t kTileChoices[] = {1024, 2048, 4096};
 
@@ -62,12 +103,9 @@ bool shape_of(const wrs_build_opts* opts, Shape* sh) {
 }
 
 // The host's view of the batch for one shape (from h_offsets and h_kinds).
-// Tables of at most this many items are built by 8-lane groups, four per warp.
-constexpr uint32_t kTinyMax = 16;
-
 struct HostPlan {
     uint32_t small_tables;  // alias tables with 1 <= n <= small_max
-    uint32_t tiny_tables;   // ... of them with n <= kTinyMax
+    uint32_t small_class_tables[kSmallClasses];  // ... of them per size class (small_class)
     uint32_t big_tables;    // alias tables with n > small_max
     uint32_t tiles;         // tiles of the big tables
     uint64_t big_items;
@@ -77,7 +115,7 @@ struct HostPlan {
 };
 
 HostPlan host_plan(const int64_t* h_offsets, int64_t num_tables, const Shape& sh, const uint8_t* h_kinds = nullptr) {
-    HostPlan p{0, 0, 0, 0, 0, 0, 0, true};
+    HostPlan p{0, {0, 0, 0, 0, 0, 0}, 0, 0, 0, 0, 0, true};
     if (!h_offsets || num_tables < 1 || h_offsets[0] != 0) {
         p.valid = false;
         return p;
@@ -98,14 +136,16 @@ HostPlan host_plan(const int64_t* h_offsets, int64_t num_tables, const Shape& sh
         if (kind != WRS_TABLE_ALIAS) continue;
         if (n <= (int64_t)sh.small_max) {
             ++small;
-            if (n <= (int64_t)kTinyMax) ++p.tiny_tables;
+            ++p.small_class_tables[small_class(n)];
         } else {
             ++tables;
             tiles += (uint64_t)((n + sh.tile - 1) / sh.tile);
             p.big_items += (uint64_t)n;
         }
     }
-    if (tables > 0x7fffffffull || tiles > 0x7fffffffull || small > 0xffffffffull) p.valid = false;
+    // table ids of the small-table lists are 32-bit
+    if (tables > 0x7fffffffull || tiles > 0x7fffffffull || (small > 0 && num_tables > (int64_t)0xffffffffll))
+        p.valid = false;
     p.small_tables = (uint32_t)small;
     p.big_tables = (uint32_t)tables;
     p.tiles = (uint32_t)tiles;
@@ -126,6 +166,7 @@ struct BatchLayout {
     uint32_t* hmask;
     uint32_t* heavy_item;
     uint4* heavy_E;
+    uint32_t* small_list;  // the small tables' ids by size class
     size_t bytes;
 };
 
@@ -147,16 +188,16 @@ BatchLayout carve_batch(void* scratch, int64_t num_tables, const HostPlan& p, ui
     L.hmask = c.take<uint32_t>((size_t)p.tiles * (tile / 32));
     L.heavy_item = c.take<uint32_t>(p.big_items);
     L.heavy_E = c.take<uint4>(p.big_items);
+    L.small_list = c.take<uint32_t>(p.small_tables);
     L.bytes = c.off;
     return L;
 }
 
-// One group of GW lanes per table of min_n <= n <= max_n items (persistent groups over all
-// tables, each skipping the others), `count` such tables.
+// The tables of one size class's list, a group of GW lanes each.
 template <int SPL, int GW>
-wrs_status launch_small_groups(const float* d_w, const int64_t* d_offsets, const uint8_t* d_kinds, int64_t num_tables,
-                               uint32_t min_n, uint32_t max_n, wrs_alias_row* d_table, double* d_W, uint32_t* status,
-                               uint32_t count, cudaStream_t stream) {
+wrs_status launch_small_class(const float* d_w, const int64_t* d_offsets, const SmallLists& sl, int cls,
+                              wrs_alias_row* d_table, double* d_W, uint32_t* status, cudaStream_t stream) {
+    const uint32_t count = sl.cap[cls];
     if (count == 0) return WRS_SUCCESS;
     constexpr int GPW = 32 / GW;
     const size_t smem = sizeof(SmallSmem<SPL, GW>) * kSmallWarps * GPW;
@@ -170,22 +211,47 @@ wrs_status launch_small_groups(const float* d_w, const int64_t* d_offsets, const
     const uint64_t want = ((uint64_t)count + kSmallWarps * GPW - 1) / (kSmallWarps * GPW);
     const uint64_t cap = (uint64_t)d.sm_count * per_sm;
     const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min(want, cap));
-    small_tables_kernel<SPL, GW><<<grid, 32 * kSmallWarps, smem, stream>>>(d_w, d_offsets, d_kinds, num_tables, min_n,
-                                                                            max_n, d_table, d_W, status);
+    small_tables_kernel<SPL, GW><<<grid, 32 * kSmallWarps, smem, stream>>>(
+        d_w, d_offsets, sl.list + sl.base[cls], sl.fill + cls, count, d_table, d_W, status);
     return launch_status();
 }
 
-// The small tables: those of at most kTinyMax items by 8-lane groups, the others by warps.
+// The small tables (n <= 32 * SPL): the lists by size class on the first side stream, then one
+// launch per class, the classes spread over the side streams (the launches of a class wait for
+// its slowest table, so classes run side by side).
 template <int SPL>
 wrs_status launch_small(const float* d_w, const int64_t* d_offsets, const uint8_t* d_kinds, int64_t num_tables,
-                        wrs_alias_row* d_table, double* d_W, uint32_t* status, const HostPlan& p,
-                        cudaStream_t stream) {
-    static_assert(32 * SPL > (int)kTinyMax, "the warp kernel takes the tables above the tiny ones");
-    wrs_status st = launch_small_groups<2, 8>(d_w, d_offsets, d_kinds, num_tables, 1u, kTinyMax, d_table, d_W, status,
-                                              p.tiny_tables, stream);
+                        wrs_alias_row* d_table, double* d_W, const BatchLayout& L, const HostPlan& p, Fork& f) {
+    uint32_t* status = &L.hdr0->status;
+    SmallLists sl;
+    sl.fill = L.hdr0->small_fill;  // cleared with the headers
+    sl.list = L.small_list;
+    uint32_t base = 0;
+    for (int c = 0; c < kSmallClasses; ++c) {
+        sl.base[c] = base;
+        sl.cap[c] = p.small_class_tables[c];
+        base += sl.cap[c];
+    }
+    const uint64_t nblk = ((uint64_t)num_tables + kSmallPlanThreads - 1) / kSmallPlanThreads;
+    const cudaStream_t* ss = f.side;
+    small_plan_kernel<<<(uint32_t)nblk, kSmallPlanThreads, 0, ss[0]>>>(d_offsets, d_kinds, num_tables, 32u * SPL, sl,
+                                                                       status);
+    wrs_status st = launch_status();
     if (st != WRS_SUCCESS) return st;
-    return launch_small_groups<SPL, 32>(d_w, d_offsets, d_kinds, num_tables, kTinyMax + 1, 32u * SPL, d_table, d_W,
-                                        status, p.small_tables - p.tiny_tables, stream);
+    if (cudaEventRecord(f.mid, ss[0]) != cudaSuccess || cudaStreamWaitEvent(ss[1], f.mid, 0) != cudaSuccess ||
+        cudaStreamWaitEvent(ss[2], f.mid, 0) != cudaSuccess)
+        return WRS_ERR_CUDA;
+    if (st == WRS_SUCCESS) st = launch_small_class<2, 2>(d_w, d_offsets, sl, 0, d_table, d_W, status, ss[0]);
+    if (st == WRS_SUCCESS) st = launch_small_class<2, 4>(d_w, d_offsets, sl, 1, d_table, d_W, status, ss[1]);
+    if (st == WRS_SUCCESS) st = launch_small_class<2, 16>(d_w, d_offsets, sl, 3, d_table, d_W, status, ss[2]);
+    if (st == WRS_SUCCESS) st = launch_small_class<2, 8>(d_w, d_offsets, sl, 2, d_table, d_W, status, ss[1]);
+    if constexpr (SPL >= 2) {
+        if (st == WRS_SUCCESS) st = launch_small_class<2, 32>(d_w, d_offsets, sl, 4, d_table, d_W, status, ss[2]);
+    }
+    if constexpr (SPL > 2) {
+        if (st == WRS_SUCCESS) st = launch_small_class<SPL, 32>(d_w, d_offsets, sl, 5, d_table, d_W, status, ss[0]);
+    }
+    return st;
 }
 
 template <int T>
@@ -257,31 +323,19 @@ wrs_status batched_build(const float* d_w, const int64_t* d_offsets, const int64
     if (cudaMemsetAsync(L.hdr0, 0, sizeof(BuildHeader) * (2 + (size_t)p.big_tables), stream) != cudaSuccess)
         return WRS_ERR_CUDA;
     wrs_status st = WRS_SUCCESS;
-    // the one-warp tables and the tiled tables are independent: with both present the former
-    // run on the side stream, forked from `stream` and joined back into it by events (which a
-    // stream capture records as a fork and a join)
-    cudaStream_t small_stream = stream;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-    const bool fork = p.small_tables > 0 && p.big_tables > 0;
-    if (fork) {
-        if (side_stream(&small_stream) != WRS_SUCCESS ||
-            cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventRecord(ev_fork, stream) != cudaSuccess || cudaStreamWaitEvent(small_stream, ev_fork, 0) != cudaSuccess) {
-            if (ev_fork) cudaEventDestroy(ev_fork);
-            if (ev_join) cudaEventDestroy(ev_join);
-            return WRS_ERR_CUDA;
-        }
+    // the small tables and the tiled tables are independent: the former run on the side streams
+    Fork f;
+    if (p.small_tables > 0 && f.begin(stream) != WRS_SUCCESS) {
+        f.end(stream);
+        return WRS_ERR_CUDA;
     }
     if (p.small_tables > 0) {
-        uint32_t* status = &L.hdr0->status;
-        const cudaStream_t ss = small_stream;
         switch (sh.small_max) {
-            case 32: st = launch_small<1>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p, ss); break;
-            case 64: st = launch_small<2>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p, ss); break;
-            case 128: st = launch_small<4>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p, ss); break;
-            case 256: st = launch_small<8>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p, ss); break;
-            default: st = launch_small<16>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, status, p, ss); break;
+            case 32: st = launch_small<1>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f); break;
+            case 64: st = launch_small<2>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f); break;
+            case 128: st = launch_small<4>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f); break;
+            case 256: st = launch_small<8>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f); break;
+            default: st = launch_small<16>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f); break;
         }
     }
     if (st == WRS_SUCCESS && p.big_tables > 0) {
@@ -291,13 +345,7 @@ wrs_status batched_build(const float* d_w, const int64_t* d_offsets, const int64
             default: st = launch_big<2048>(d_w, d_offsets, d_kinds, num_tables, sh.small_max, d_table, d_W, L, p, stream); break;
         }
     }
-    if (fork) {  // joined whatever happened above, so that a capture stays well formed
-        if ((cudaEventRecord(ev_join, small_stream) != cudaSuccess ||
-             cudaStreamWaitEvent(stream, ev_join, 0) != cudaSuccess) && st == WRS_SUCCESS)
-            st = WRS_ERR_CUDA;
-        cudaEventDestroy(ev_fork);
-        cudaEventDestroy(ev_join);
-    }
+    if (f.end(stream) != WRS_SUCCESS && st == WRS_SUCCESS) st = WRS_ERR_CUDA;
     if (st != WRS_SUCCESS) return st;
     if (rej && (p.rej_warp_tables > 0 || p.rej_block_tables > 0))
         st = launch_rejection(d_w, d_offsets, d_kinds, num_tables, p, *rej, d_W, &L.hdr0->status, stream);

@@ -304,12 +304,70 @@ __global__ void batch_status_kernel(const BuildHeader* hdrs, uint32_t num_tables
 
 // ---------------------------------------------------------------- small tables: a lane group each
 // The whole build of a table of n <= GW * SPL items in one group of GW lanes (GW = 32: a warp
-// per table; GW = 8: four tables per warp, for the tiny tables that dominate skewed batches).
-// Lane l of the group holds the ipl = ceil(n / GW) consecutive items l * ipl ..; the
+// per table; GW = 2 .. 16: 32 / GW tables per warp, for the tiny tables that dominate skewed
+// batches). Lane l of the group holds the ipl = ceil(n / GW) consecutive items l * ipl ..; the
 // quantities are those of the tiled passes for a one-tile table (A_before = 0, no dithering
 // offset), so the rows equal a single-table build's. Shared memory per group: light keys from
 // the front and heavy keys from the back of one u64 array, and the heavies' corrected excess
-// ends and items. The kernel takes the alias tables with min_n <= n <= small_max.
+// ends and items.
+//
+// Size classes: n <= 4, 8, 16, 32 by groups of 2, 4, 8, 16 lanes with two items a lane; n <= 64
+// by a warp with two items a lane; the rest (up to small_max) by a warp with small_max / 32
+// items a lane. small_plan_kernel lists the batch's small tables per class (appending with one
+// atomic per warp and class: the order within a list is arbitrary, the rows do not depend on
+// it), and one launch per class builds its list.
+constexpr int kSmallClasses = 6;
+__host__ __device__ __forceinline__ int small_class(int64_t n) {
+    return n <= 4 ? 0 : n <= 8 ? 1 : n <= 16 ? 2 : n <= 32 ? 3 : n <= 64 ? 4 : 5;
+}
+
+struct SmallLists {
+    uint32_t* fill;                // kSmallClasses counters, zero at the start of the build
+    uint32_t* list;                // table ids; class c at [base[c], base[c] + cap[c])
+    uint32_t base[kSmallClasses];
+    uint32_t cap[kSmallClasses];   // the host's count of the class
+};
+
+// One thread per table; positions come from a shared-memory counter per class and CTA, then one
+// global atomic per class and CTA reserves the CTA's run of each list.
+constexpr int kSmallPlanThreads = 1024;
+__global__ void __launch_bounds__(kSmallPlanThreads) small_plan_kernel(const int64_t* __restrict__ offsets,
+                                                                      const uint8_t* kinds, int64_t num_tables,
+                                                                      uint32_t small_max, SmallLists L,
+                                                                      uint32_t* status) {
+    __shared__ uint32_t s_cnt[kSmallClasses], s_base[kSmallClasses];
+    const int64_t t = (int64_t)blockIdx.x * kSmallPlanThreads + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x < kSmallClasses) s_cnt[threadIdx.x] = 0;
+    __syncthreads();
+    int cls = -1;
+    if (t < num_tables && kind_is(kinds, t, WRS_TABLE_ALIAS)) {
+        const int64_t n = __ldg(offsets + t + 1) - __ldg(offsets + t);
+        if (n >= 1 && n <= (int64_t)small_max) cls = small_class(n);
+    }
+    uint32_t pos = 0;
+#pragma unroll
+    for (int c = 0; c < kSmallClasses; ++c) {
+        const uint32_t m = __ballot_sync(0xffffffffu, cls == c);
+        if (m == 0) continue;
+        const int leader = __ffs(m) - 1;
+        uint32_t b = 0;
+        if (lane == leader) b = atomicAdd(s_cnt + c, (uint32_t)__popc(m));
+        b = __shfl_sync(0xffffffffu, b, leader);
+        if (cls == c) pos = b + (uint32_t)__popc(m & ((1u << lane) - 1u));
+    }
+    __syncthreads();
+    if (threadIdx.x < kSmallClasses && s_cnt[threadIdx.x] > 0)
+        s_base[threadIdx.x] = atomicAdd(L.fill + threadIdx.x, s_cnt[threadIdx.x]);
+    __syncthreads();
+    if (cls >= 0) {
+        pos += s_base[cls];
+        // more tables of a class than the host counted: offsets differ from the host's
+        if (pos < L.cap[cls]) L.list[L.base[cls] + pos] = (uint32_t)t;
+        else record_status(status, WRS_ERR_INVALID_ARGUMENT);
+    }
+}
+
 constexpr int kSmallWarps = 4;
 
 template <int SPL, int GW = 32>
@@ -347,14 +405,164 @@ __device__ __forceinline__ uint64_t group_excl_scan_u64(uint64_t v, uint32_t mas
     return inc - v;
 }
 
+// One table of n items (1 <= n <= GW * SPL) by the group of GW lanes in `mask` (gl = the
+// lane's index in the group), with the group's shared memory `sm`.
+template <int SPL, int GW>
+__device__ __forceinline__ void small_table_build(const float* __restrict__ w, int64_t off, uint32_t n, int64_t t,
+                                                  uint32_t mask, int gl, SmallSmem<SPL, GW>& sm,
+                                                  wrs_alias_row* __restrict__ table, double* W_out,
+                                                  uint32_t* status) {
+    constexpr int CAP = GW * SPL;
+    const uint32_t ipl = (n + GW - 1) / GW;
+    const float* wt = w + off;
+    wrs_alias_row* rows = table + off;
+    const uint32_t i0 = (uint32_t)gl * ipl;
+    float x[SPL];
+    DD acc = {0.0, 0.0};
+    bool bad = false;
+#pragma unroll
+    for (int k = 0; k < SPL; ++k) {
+        const uint32_t i = i0 + k;
+        const bool in = (uint32_t)k < ipl && i < n;
+        x[k] = in ? __ldg(wt + i) : -1.0f;
+        if (in) {
+            bad |= weight_invalid(x[k]);
+            acc = dd_add_d(acc, (double)x[k]);
+        }
+    }
+    acc = dd_norm(acc);
+#pragma unroll
+    for (int o = GW / 2; o > 0; o >>= 1) {
+        DD v;
+        v.hi = __shfl_down_sync(mask, acc.hi, o, GW);
+        v.lo = __shfl_down_sync(mask, acc.lo, o, GW);
+        acc = dd_add(acc, v);
+    }
+    acc = dd_norm(acc);
+    const double W = __shfl_sync(mask, acc.hi, 0, GW);
+    const bool any_bad = __any_sync(mask, bad);
+    if (any_bad || !(W > 0.0) || isinf(W)) {
+        if (gl == 0) record_status(status, (any_bad || isinf(W)) ? kErrInvalidWeight : kErrZeroTotal);
+        return;
+    }
+    if (gl == 0 && W_out) W_out[t] = W;
+    const double W_N = W / (double)n;
+    const ClassParams cp = class_params(W_N, 1.0 / W_N);
+    // classification and per-lane sums
+    float pk[SPL];
+    uint32_t lbits = 0, hbits = 0, gbits = 0;
+    uint64_t S = 0, L = 0, E = 0;
+#pragma unroll
+    for (int k = 0; k < SPL; ++k) {
+        const float wk = x[k];
+        const bool heavy = wk > cp.H1;
+        const bool small = wk >= 0.0f && wk < cp.Hh;
+        const bool large = wk >= cp.Hh && !heavy;
+        const float p = __fmul_rn(wk, cp.R32);
+        pk[k] = p;
+        lbits |= (uint32_t)(small || large) << k;
+        hbits |= (uint32_t)heavy << k;
+        gbits |= (uint32_t)large << k;
+        if (small) S += small_deficit(p);
+        if (large) L += rare_q(wk, false, cp);
+        if (heavy) E += rare_q(wk, true, cp);
+    }
+    uint32_t nl_tot, nh_tot;
+    const uint32_t l0 = group_excl_scan_u32<GW>((uint32_t)__popc(lbits), mask, nl_tot);
+    const uint32_t h0 = group_excl_scan_u32<GW>((uint32_t)__popc(hbits), mask, nh_tot);
+    uint64_t S_tot, L_tot, E_tot;
+    const uint64_t s0 = group_excl_scan_u64<GW>(S, mask, S_tot);
+    const uint64_t lq0 = group_excl_scan_u64<GW>(L, mask, L_tot);
+    const uint64_t e0 = group_excl_scan_u64<GW>(E, mask, E_tot);
+    const u128 A_tot = ((u128)S_tot << 16) + q_round24((u128)L_tot << 16);
+    const int64_t nfix = excess_correction(A_tot, (u128)E_tot << 40);
+    Dither dth;
+    dth.c0 = 1ull << 23;
+    dth.c0h = 0;
+    // keys: lights from the front, heavies from the back (CAP - nh_tot + j)
+    {
+        uint64_t sr = s0, lr = lq0, er = e0;
+        uint64_t D = dither_at(dth, lr);
+        uint32_t li = l0, hj = h0;
+#pragma unroll
+        for (int k = 0; k < SPL; ++k) {
+            const float wk = x[k];
+            if ((lbits >> k) & 1u) {
+                sm.key[li++] = sr + D;
+                if ((gbits >> k) & 1u) {
+                    lr += rare_q(wk, false, cp);
+                    const uint64_t D1 = dither_at(dth, lr);
+                    pk[k] = dithered_prob(D1 - D);
+                    D = D1;
+                } else {
+                    sr += small_deficit(pk[k]);
+                }
+            } else if ((hbits >> k) & 1u) {
+                er += rare_q(wk, true, cp);
+                const u128 Et = q_scale_excess((u128)er << 40, nfix);
+                const u128 d = Et + 0xffff;
+                sm.key[CAP - nh_tot + hj] = (q_hi(d) >> 16) ? ~0ull : (uint64_t)(d >> 16);
+                sm.elo[hj] = q_lo(Et);
+                sm.ehi[hj] = (uint32_t)q_hi(Et);
+                sm.item[hj] = i0 + k;
+                ++hj;
+            }
+        }
+    }
+    __syncwarp(mask);
+    const uint64_t* hkey = sm.key + (CAP - nh_tot);
+    // heavy rows
+    for (uint32_t j = gl; j < nh_tot; j += GW) {
+        const uint64_t kh = hkey[j];
+        uint32_t lo = 0, hi = nl_tot;  // rank: the first light whose key is not below kh
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (sm.key[mid] < kh) lo = mid + 1; else hi = mid;
+        }
+        const u128 Et = q_make(sm.ehi[j], sm.elo[j]);
+        const u128 A_next = (lo < nl_tot) ? ((u128)sm.key[lo] << 16) : A_tot;
+        wrs_alias_row r;
+        r.prob = heavy_row_prob(q_one() + Et - A_next);
+        r.alias = (j + 1 < nh_tot) ? sm.item[j + 1] : sm.item[j];
+        rows[sm.item[j]] = r;
+    }
+    // light rows: alias = the first heavy whose key exceeds the light's (else the last heavy)
+    {
+        uint32_t li = l0;
+#pragma unroll
+        for (int k = 0; k < SPL; ++k) {
+            if (!((lbits >> k) & 1u)) continue;
+            uint32_t al;
+            if (nh_tot == 0) {
+                al = i0 + k;
+            } else {
+                const uint64_t kl = sm.key[li];
+                uint32_t lo = 0, hi = nh_tot;
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (hkey[mid] > kl) hi = mid; else lo = mid + 1;
+                }
+                al = sm.item[lo < nh_tot ? lo : nh_tot - 1];
+            }
+            wrs_alias_row r;
+            r.prob = pk[k];
+            r.alias = al;
+            rows[i0 + k] = r;
+            ++li;
+        }
+    }
+    __syncwarp(mask);  // the next table reuses this group's shared memory
+}
+
+// The tables of list[0 .. min(cap, *fill)), a group of GW lanes each.
 template <int SPL, int GW = 32>
 __global__ void __launch_bounds__(32 * kSmallWarps) small_tables_kernel(const float* __restrict__ w,
                                                                        const int64_t* __restrict__ offsets,
-                                                                       const uint8_t* kinds, int64_t num_tables,
-                                                                       uint32_t min_n, uint32_t small_max,
+                                                                       const uint32_t* __restrict__ list,
+                                                                       const uint32_t* fill, uint32_t cap,
                                                                        wrs_alias_row* __restrict__ table,
                                                                        double* W_out, uint32_t* status) {
-    static_assert(GW == 32 || GW == 16 || GW == 8, "lane group width");
+    static_assert(GW == 32 || GW == 16 || GW == 8 || GW == 4 || GW == 2, "lane group width");
     constexpr int CAP = GW * SPL;
     constexpr int GPW = 32 / GW;  // groups per warp
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -362,152 +570,14 @@ __global__ void __launch_bounds__(32 * kSmallWarps) small_tables_kernel(const fl
     const int grp = lane / GW, gl = lane & (GW - 1);
     const uint32_t mask = GW == 32 ? 0xffffffffu : (((1u << GW) - 1u) << (grp * GW));
     SmallSmem<SPL, GW>& sm = reinterpret_cast<SmallSmem<SPL, GW>*>(smem_raw)[warp * GPW + grp];
-    const int64_t ngroups = (int64_t)gridDim.x * kSmallWarps * GPW;
-    for (int64_t t = ((int64_t)blockIdx.x * kSmallWarps + warp) * GPW + grp; t < num_tables; t += ngroups) {
-        const int64_t off = offsets[t];
-        const int64_t nn = offsets[t + 1] - off;
-        if (nn < (int64_t)min_n || nn < 1 || nn > (int64_t)small_max || nn > CAP || !kind_is(kinds, t, WRS_TABLE_ALIAS))
-            continue;
-        const uint32_t n = (uint32_t)nn;
-        const uint32_t ipl = (n + GW - 1) / GW;
-        const float* wt = w + off;
-        wrs_alias_row* rows = table + off;
-        const uint32_t i0 = (uint32_t)gl * ipl;
-        float x[SPL];
-        DD acc = {0.0, 0.0};
-        bool bad = false;
-#pragma unroll
-        for (int k = 0; k < SPL; ++k) {
-            const uint32_t i = i0 + k;
-            const bool in = (uint32_t)k < ipl && i < n;
-            x[k] = in ? __ldg(wt + i) : -1.0f;
-            if (in) {
-                bad |= weight_invalid(x[k]);
-                acc = dd_add_d(acc, (double)x[k]);
-            }
-        }
-        acc = dd_norm(acc);
-#pragma unroll
-        for (int o = GW / 2; o > 0; o >>= 1) {
-            DD v;
-            v.hi = __shfl_down_sync(mask, acc.hi, o, GW);
-            v.lo = __shfl_down_sync(mask, acc.lo, o, GW);
-            acc = dd_add(acc, v);
-        }
-        acc = dd_norm(acc);
-        const double W = __shfl_sync(mask, acc.hi, 0, GW);
-        const bool any_bad = __any_sync(mask, bad);
-        if (any_bad || !(W > 0.0) || isinf(W)) {
-            if (gl == 0) record_status(status, (any_bad || isinf(W)) ? kErrInvalidWeight : kErrZeroTotal);
-            continue;
-        }
-        if (gl == 0 && W_out) W_out[t] = W;
-        const double W_N = W / (double)n;
-        const ClassParams cp = class_params(W_N, 1.0 / W_N);
-        // classification and per-lane sums
-        float pk[SPL];
-        uint32_t lbits = 0, hbits = 0, gbits = 0;
-        uint64_t S = 0, L = 0, E = 0;
-#pragma unroll
-        for (int k = 0; k < SPL; ++k) {
-            const float wk = x[k];
-            const bool heavy = wk > cp.H1;
-            const bool small = wk >= 0.0f && wk < cp.Hh;
-            const bool large = wk >= cp.Hh && !heavy;
-            const float p = __fmul_rn(wk, cp.R32);
-            pk[k] = p;
-            lbits |= (uint32_t)(small || large) << k;
-            hbits |= (uint32_t)heavy << k;
-            gbits |= (uint32_t)large << k;
-            if (small) S += small_deficit(p);
-            if (large) L += rare_q(wk, false, cp);
-            if (heavy) E += rare_q(wk, true, cp);
-        }
-        uint32_t nl_tot, nh_tot;
-        const uint32_t l0 = group_excl_scan_u32<GW>((uint32_t)__popc(lbits), mask, nl_tot);
-        const uint32_t h0 = group_excl_scan_u32<GW>((uint32_t)__popc(hbits), mask, nh_tot);
-        uint64_t S_tot, L_tot, E_tot;
-        const uint64_t s0 = group_excl_scan_u64<GW>(S, mask, S_tot);
-        const uint64_t lq0 = group_excl_scan_u64<GW>(L, mask, L_tot);
-        const uint64_t e0 = group_excl_scan_u64<GW>(E, mask, E_tot);
-        const u128 A_tot = ((u128)S_tot << 16) + q_round24((u128)L_tot << 16);
-        const int64_t nfix = excess_correction(A_tot, (u128)E_tot << 40);
-        Dither dth;
-        dth.c0 = 1ull << 23;
-        dth.c0h = 0;
-        // keys: lights from the front, heavies from the back (CAP - nh_tot + j)
-        {
-            uint64_t sr = s0, lr = lq0, er = e0;
-            uint64_t D = dither_at(dth, lr);
-            uint32_t li = l0, hj = h0;
-#pragma unroll
-            for (int k = 0; k < SPL; ++k) {
-                const float wk = x[k];
-                if ((lbits >> k) & 1u) {
-                    sm.key[li++] = sr + D;
-                    if ((gbits >> k) & 1u) {
-                        lr += rare_q(wk, false, cp);
-                        const uint64_t D1 = dither_at(dth, lr);
-                        pk[k] = dithered_prob(D1 - D);
-                        D = D1;
-                    } else {
-                        sr += small_deficit(pk[k]);
-                    }
-                } else if ((hbits >> k) & 1u) {
-                    er += rare_q(wk, true, cp);
-                    const u128 Et = q_scale_excess((u128)er << 40, nfix);
-                    const u128 d = Et + 0xffff;
-                    sm.key[CAP - nh_tot + hj] = (q_hi(d) >> 16) ? ~0ull : (uint64_t)(d >> 16);
-                    sm.elo[hj] = q_lo(Et);
-                    sm.ehi[hj] = (uint32_t)q_hi(Et);
-                    sm.item[hj] = i0 + k;
-                    ++hj;
-                }
-            }
-        }
-        __syncwarp(mask);
-        const uint64_t* hkey = sm.key + (CAP - nh_tot);
-        // heavy rows
-        for (uint32_t j = gl; j < nh_tot; j += GW) {
-            const uint64_t kh = hkey[j];
-            uint32_t lo = 0, hi = nl_tot;  // rank: the first light whose key is not below kh
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (sm.key[mid] < kh) lo = mid + 1; else hi = mid;
-            }
-            const u128 Et = q_make(sm.ehi[j], sm.elo[j]);
-            const u128 A_next = (lo < nl_tot) ? ((u128)sm.key[lo] << 16) : A_tot;
-            wrs_alias_row r;
-            r.prob = heavy_row_prob(q_one() + Et - A_next);
-            r.alias = (j + 1 < nh_tot) ? sm.item[j + 1] : sm.item[j];
-            rows[sm.item[j]] = r;
-        }
-        // light rows: alias = the first heavy whose key exceeds the light's (else the last heavy)
-        {
-            uint32_t li = l0;
-#pragma unroll
-            for (int k = 0; k < SPL; ++k) {
-                if (!((lbits >> k) & 1u)) continue;
-                uint32_t al;
-                if (nh_tot == 0) {
-                    al = i0 + k;
-                } else {
-                    const uint64_t kl = sm.key[li];
-                    uint32_t lo = 0, hi = nh_tot;
-                    while (lo < hi) {
-                        const uint32_t mid = (lo + hi) >> 1;
-                        if (hkey[mid] > kl) hi = mid; else lo = mid + 1;
-                    }
-                    al = sm.item[lo < nh_tot ? lo : nh_tot - 1];
-                }
-                wrs_alias_row r;
-                r.prob = pk[k];
-                r.alias = al;
-                rows[i0 + k] = r;
-                ++li;
-            }
-        }
-        __syncwarp(mask);  // the next table reuses this group's shared memory
+    const uint32_t count = min(cap, *fill);
+    const uint32_t ngroups = gridDim.x * (uint32_t)(kSmallWarps * GPW);
+    for (uint32_t e = (blockIdx.x * kSmallWarps + warp) * GPW + grp; e < count; e += ngroups) {
+        const int64_t t = __ldg(list + e);
+        const int64_t off = __ldg(offsets + t);
+        const int64_t n = __ldg(offsets + t + 1) - off;
+        if (n < 1 || n > CAP) continue;  // uniform over the group; never for a listed table
+        small_table_build<SPL, GW>(w, off, (uint32_t)n, t, mask, gl, sm, table, W_out, status);
     }
 }
 
@@ -515,9 +585,13 @@ __global__ void __launch_bounds__(32 * kSmallWarps) small_tables_kernel(const fl
 // Output position s of the batch belongs to table t with sample_offsets[t] <= s <
 // sample_offsets[t + 1] and follows the plain contract over the global position s:
 // Philox counter counter_base + s, row = floor((x1:x0) * n_t / 2^64) (table-local),
-// coin = (x2 >> 8) * 2^-24, result = coin < prob[row] ? row : alias[row]. Every thread
-// takes kBatchSamplePer consecutive positions: it finds the table of its first one by a
-// binary search of the sample offsets and walks forward from there.
+// coin = (x2 >> 8) * 2^-24, result = coin < prob[row] ? row : alias[row]. A warp takes
+// 32 * kBatchSamplePer consecutive positions, lane l the positions base + 32 k + l, so that every
+// store of the warp is one coalesced line. The warp finds the table of its first position by a
+// 32-way search of the sample offsets (one load per lane and level); every lane moves forward
+// from there (a few single steps, then a binary search over the rest). In an all-alias batch
+// the lane first resolves the tables of all its positions, then draws and reads all its rows,
+// so that its row reads are in flight together.
 // In a mixed batch (kinds not null) a rejection table's positions follow the rejection
 // contract instead (rejection_sample_kernel: b = counter_base + s, one try per Philox block,
 // a 64-bit slot uniform and the acceptance from the table's own slot range), and the positions of a
@@ -525,32 +599,114 @@ __global__ void __launch_bounds__(32 * kSmallWarps) small_tables_kernel(const fl
 constexpr int kBatchSampleThreads = 256;
 constexpr int kBatchSamplePer = 8;
 
+// The last table whose sample range starts at or before s, over tables [lo, hi].
+__device__ __forceinline__ int64_t batch_table_of(const int64_t* __restrict__ sample_offsets, uint64_t s, int64_t lo,
+                                                  int64_t hi) {
+    while (lo < hi) {
+        const int64_t mid = (lo + hi + 1) >> 1;
+        if ((uint64_t)__ldg(sample_offsets + mid) <= s) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// The same over all tables, by the whole warp for one position s (uniform over the warp): each
+// level splits the range into 32 parts and a ballot picks the last part that starts at or before s.
+__device__ __forceinline__ int64_t warp_table_of(const int64_t* __restrict__ sample_offsets, uint64_t s,
+                                                 int64_t num_tables, uint32_t lane) {
+    int64_t lo = 0, hi = num_tables - 1;
+    for (;;) {
+        const int64_t step = hi - lo >= 32 ? (hi - lo + 32) >> 5 : 1;
+        const int64_t idx = lo + (int64_t)lane * step;
+        const bool le = idx <= hi && (uint64_t)__ldg(sample_offsets + idx) <= s;
+        const uint32_t m = __ballot_sync(0xffffffffu, le);
+        const int j = m ? 31 - __clz(m) : 0;
+        lo += (int64_t)j * step;
+        if (step == 1) return lo;
+        hi = min(hi, lo + step - 1);
+    }
+}
+
+// Moves lane state (t, s_end_t) forward to the table of position s >= the previous position.
+__device__ __forceinline__ void batch_advance(const int64_t* __restrict__ sample_offsets, int64_t num_tables,
+                                              uint64_t s, int64_t& t, uint64_t& s_end_t) {
+    int steps = 0;
+    do {
+        ++t;
+        s_end_t = (uint64_t)__ldg(sample_offsets + t + 1);
+    } while (s >= s_end_t && t + 1 < num_tables && ++steps < 4);
+    if (s >= s_end_t && t + 1 < num_tables) {
+        t = batch_table_of(sample_offsets, s, t + 1, num_tables - 1);
+        s_end_t = (uint64_t)__ldg(sample_offsets + t + 1);
+    }
+}
+
 __global__ void __launch_bounds__(kBatchSampleThreads) batch_sample_kernel(
     const wrs_alias_row* __restrict__ table, const int64_t* __restrict__ offsets, int64_t num_tables,
     const int64_t* __restrict__ sample_offsets, uint64_t total, uint64_t seed, uint64_t counter_base,
     uint32_t* __restrict__ out, uint32_t* status, const uint8_t* kinds, const uint32_t* __restrict__ A,
     const float* __restrict__ frac, const uint64_t* __restrict__ a_size, uint32_t max_tries) {
-    const uint64_t s0 = ((uint64_t)blockIdx.x * kBatchSampleThreads + threadIdx.x) * kBatchSamplePer;
-    if (s0 >= total) return;
-    // the last table whose sample range starts at or before s0
-    int64_t lo = 0, hi = num_tables - 1;
-    while (lo < hi) {
-        const int64_t mid = (lo + hi + 1) >> 1;
-        if ((uint64_t)__ldg(sample_offsets + mid) <= s0) lo = mid; else hi = mid - 1;
-    }
-    int64_t t = lo;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t wbase = (((uint64_t)blockIdx.x * kBatchSampleThreads + threadIdx.x) >> 5) *
+                           (32ull * kBatchSamplePer);
+    if (wbase >= total) return;  // uniform over the warp
+    int64_t t = warp_table_of(sample_offsets, wbase, num_tables, lane);
     uint64_t s_end_t = (uint64_t)__ldg(sample_offsets + t + 1);
+    const uint64_t base = wbase + lane;
     const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
-    const uint64_t s1 = min(total, s0 + kBatchSamplePer);
-    for (uint64_t s = s0; s < s1; ++s) {
-        while (s >= s_end_t && t + 1 < num_tables) {
-            ++t;
-            s_end_t = (uint64_t)__ldg(sample_offsets + t + 1);
+    if (!kinds) {
+        int64_t offk[kBatchSamplePer];
+        uint32_t nk[kBatchSamplePer];
+        int64_t off = __ldg(offsets + t);
+        uint64_t n = (uint64_t)(__ldg(offsets + t + 1) - off);
+#pragma unroll
+        for (int k = 0; k < kBatchSamplePer; ++k) {
+            const uint64_t s = base + 32ull * k;
+            offk[k] = 0;
+            nk[k] = 0;  // 0: no sample at s (past the end) or an invalid one
+            if (s >= total) continue;
+            if (s >= s_end_t && t + 1 < num_tables) {
+                batch_advance(sample_offsets, num_tables, s, t, s_end_t);
+                off = __ldg(offsets + t);
+                n = (uint64_t)(__ldg(offsets + t + 1) - off);
+            }
+            if (n == 0 || n > 0xffffffffull || s >= s_end_t) {
+                out[s] = 0xffffffffu;
+                if (status) record_status(status, WRS_ERR_INVALID_ARGUMENT);
+                continue;
+            }
+            offk[k] = off;
+            nk[k] = (uint32_t)n;
         }
-        const uint8_t kind = kinds ? __ldg(kinds + t) : (uint8_t)WRS_TABLE_ALIAS;
+        uint32_t rowk[kBatchSamplePer];
+        float coink[kBatchSamplePer];
+        uint2 ek[kBatchSamplePer];
+#pragma unroll
+        for (int k = 0; k < kBatchSamplePer; ++k) {
+            const uint64_t b = counter_base + base + 32ull * k;
+            const Philox4 x = philox4x32_10((uint32_t)b, (uint32_t)(b >> 32), 0u, 0u, k0, k1);
+            rowk[k] = scale_u64(x.x[0], x.x[1], nk[k]);
+            coink[k] = coin24(x.x[2]);
+            if (nk[k]) ek[k] = __ldg(reinterpret_cast<const uint2*>(table + offk[k]) + rowk[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < kBatchSamplePer; ++k)
+            if (nk[k]) out[base + 32ull * k] = coink[k] < __uint_as_float(ek[k].x) ? rowk[k] : ek[k].y;
+        return;
+    }
+    int64_t off = __ldg(offsets + t);
+    uint64_t n = (uint64_t)(__ldg(offsets + t + 1) - off);
+    uint8_t kind = __ldg(kinds + t);
+    for (int k = 0; k < kBatchSamplePer; ++k) {
+        const uint64_t s = base + 32ull * k;
+        if (s >= total) break;
+        if (s >= s_end_t && t + 1 < num_tables) {
+            batch_advance(sample_offsets, num_tables, s, t, s_end_t);
+            off = __ldg(offsets + t);
+            n = (uint64_t)(__ldg(offsets + t + 1) - off);
+            kind = __ldg(kinds + t);
+        }
         if (kind != WRS_TABLE_ALIAS && s < s_end_t) {
             if (kind != WRS_TABLE_REJECTION) continue;  // a skipped table
-            const int64_t off = __ldg(offsets + t);
             const uint64_t asz = __ldg(a_size + t);
             if (asz == 0 || asz > 0xffffffffull) {
                 out[s] = 0xffffffffu;
@@ -574,15 +730,13 @@ __global__ void __launch_bounds__(kBatchSampleThreads) batch_sample_kernel(
             out[s] = res;
             continue;
         }
-        const uint64_t b = counter_base + s;
-        const Philox4 x = philox4x32_10((uint32_t)b, (uint32_t)(b >> 32), 0u, 0u, k0, k1);
-        const int64_t off = __ldg(offsets + t);
-        const uint64_t n = (uint64_t)(__ldg(offsets + t + 1) - off);
         if (n == 0 || n > 0xffffffffull || s >= s_end_t) {
             out[s] = 0xffffffffu;
             if (status) record_status(status, WRS_ERR_INVALID_ARGUMENT);
             continue;
         }
+        const uint64_t b = counter_base + s;
+        const Philox4 x = philox4x32_10((uint32_t)b, (uint32_t)(b >> 32), 0u, 0u, k0, k1);
         const uint32_t row = scale_u64(x.x[0], x.x[1], (uint32_t)n);
         const uint2 e = __ldg(reinterpret_cast<const uint2*>(table + off) + row);
         out[s] = coin24(x.x[2]) < __uint_as_float(e.x) ? row : e.y;
