@@ -23,7 +23,7 @@ constexpr uint32_t kDefaultSmall = 128;
 // The library's side streams of the current device (created on first use): the small tables
 // of a batch are built there, by size class, while `stream` runs the tiled passes.
 constexpr int kMaxDevices = 64;
-constexpr int kSideStreams = 3;
+constexpr int kSideStreams = 4;
 std::mutex g_side_mu;
 cudaStream_t g_side[kMaxDevices][kSideStreams] = {};
 wrs_status side_streams(cudaStream_t (&out)[kSideStreams]) {
@@ -104,23 +104,26 @@ bool shape_of(const wrs_build_opts* opts, Shape* sh) {
 
 // The host's view of the batch for one shape (from h_offsets and h_kinds).
 struct HostPlan {
-    uint32_t small_tables;  // alias tables with 1 <= n <= small_max
-    uint32_t small_class_tables[kSmallClasses];  // ... of them per size class (small_class)
-    uint32_t big_tables;    // alias tables with n > small_max
-    uint32_t tiles;         // tiles of the big tables
+    uint32_t listed_tables;          // alias tables with 1 <= n <= kMediumMax
+    uint32_t list_tables[kLists];    // ... of them per list (table_list)
+    uint64_t list_items[kLists];     // items of each list's tables
+    uint64_t table_sum;              // sum over listed tables of (t + 1) * n_t (mod 2^64)
+    uint32_t big_tables;             // alias tables with n > kMediumMax (tiled passes)
+    uint32_t tiles;                  // tiles of the big tables
     uint64_t big_items;
-    uint64_t rej_warp_tables;   // rejection tables with 1 <= n <= kRejWarpMax
-    uint64_t rej_block_tables;  // larger rejection tables
+    uint64_t rej_warp_tables;        // rejection tables with 1 <= n <= kRejWarpMax
+    uint64_t rej_block_tables;       // larger rejection tables
     bool valid;
 };
 
 HostPlan host_plan(const int64_t* h_offsets, int64_t num_tables, const Shape& sh, const uint8_t* h_kinds = nullptr) {
-    HostPlan p{0, {0, 0, 0, 0, 0, 0}, 0, 0, 0, 0, 0, true};
+    HostPlan p{};
+    p.valid = true;
     if (!h_offsets || num_tables < 1 || h_offsets[0] != 0) {
         p.valid = false;
         return p;
     }
-    uint64_t tiles = 0, tables = 0, small = 0;
+    uint64_t tiles = 0, tables = 0, listed = 0;
     for (int64_t t = 0; t < num_tables; ++t) {
         const int64_t n = h_offsets[t + 1] - h_offsets[t];
         if (n < 0 || n > (int64_t)0x7fffffff - 8192) {
@@ -134,19 +137,22 @@ HostPlan host_plan(const int64_t* h_offsets, int64_t num_tables, const Shape& sh
             continue;
         }
         if (kind != WRS_TABLE_ALIAS) continue;
-        if (n <= (int64_t)sh.small_max) {
-            ++small;
-            ++p.small_class_tables[small_class(n)];
+        const int c = table_list(n, sh.small_max);
+        if (c >= 0) {
+            ++listed;
+            ++p.list_tables[c];
+            p.list_items[c] += (uint64_t)n;
+            p.table_sum += (uint64_t)(t + 1) * (uint64_t)n;
         } else {
             ++tables;
             tiles += (uint64_t)((n + sh.tile - 1) / sh.tile);
             p.big_items += (uint64_t)n;
         }
     }
-    // table ids of the small-table lists are 32-bit
-    if (tables > 0x7fffffffull || tiles > 0x7fffffffull || (small > 0 && num_tables > (int64_t)0xffffffffll))
+    // table ids of the lists are 32-bit
+    if (tables > 0x7fffffffull || tiles > 0x7fffffffull || (listed > 0 && num_tables > (int64_t)0xffffffffll))
         p.valid = false;
-    p.small_tables = (uint32_t)small;
+    p.listed_tables = (uint32_t)listed;
     p.big_tables = (uint32_t)tables;
     p.tiles = (uint32_t)tiles;
     return p;
@@ -166,7 +172,7 @@ struct BatchLayout {
     uint32_t* hmask;
     uint32_t* heavy_item;
     uint4* heavy_E;
-    uint32_t* small_list;  // the small tables' ids by size class
+    uint32_t* list;        // the listed tables' ids by list
     size_t bytes;
 };
 
@@ -188,14 +194,14 @@ BatchLayout carve_batch(void* scratch, int64_t num_tables, const HostPlan& p, ui
     L.hmask = c.take<uint32_t>((size_t)p.tiles * (tile / 32));
     L.heavy_item = c.take<uint32_t>(p.big_items);
     L.heavy_E = c.take<uint4>(p.big_items);
-    L.small_list = c.take<uint32_t>(p.small_tables);
+    L.list = c.take<uint32_t>(p.listed_tables);
     L.bytes = c.off;
     return L;
 }
 
 // The tables of one size class's list, a group of GW lanes each.
 template <int SPL, int GW>
-wrs_status launch_small_class(const float* d_w, const int64_t* d_offsets, const SmallLists& sl, int cls,
+wrs_status launch_small_class(const float* d_w, const int64_t* d_offsets, const TableLists& sl, int cls,
                               wrs_alias_row* d_table, double* d_W, uint32_t* status, cudaStream_t stream) {
     const uint32_t count = sl.cap[cls];
     if (count == 0) return WRS_SUCCESS;
@@ -212,41 +218,67 @@ wrs_status launch_small_class(const float* d_w, const int64_t* d_offsets, const 
     const uint64_t cap = (uint64_t)d.sm_count * per_sm;
     const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min(want, cap));
     small_tables_kernel<SPL, GW><<<grid, 32 * kSmallWarps, smem, stream>>>(
-        d_w, d_offsets, sl.list + sl.base[cls], sl.fill + cls, count, d_table, d_W, status);
+        d_w, d_offsets, sl.list + sl.base[cls], sl.cnt->list_fill + cls, count, d_table, d_W, status);
     return launch_status();
 }
 
-// The small tables (n <= 32 * SPL): the lists by size class on the first side stream, then one
-// launch per class, the classes spread over the side streams (the launches of a class wait for
-// its slowest table, so classes run side by side).
+// The medium tables of list `cls`, a CTA of MT threads each.
+template <int MT>
+wrs_status launch_medium(const float* d_w, const int64_t* d_offsets, const TableLists& sl, int cls,
+                         wrs_alias_row* d_table, double* d_W, uint32_t* status, cudaStream_t stream) {
+    const uint32_t count = sl.cap[cls];
+    if (count == 0) return WRS_SUCCESS;
+    constexpr size_t smem = medium_smem_bytes<MT>();
+    cudaError_t e = cudaFuncSetAttribute(medium_tables_kernel<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return WRS_ERR_CUDA;
+    const DeviceInfo d = device_info();
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, medium_tables_kernel<MT>, MT, smem);
+    if (e != cudaSuccess || per_sm < 1) per_sm = 1;
+    const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(count, (uint64_t)d.sm_count * per_sm));
+    medium_tables_kernel<MT><<<grid, MT, smem, stream>>>(d_w, d_offsets, sl.list + sl.base[cls], sl.cnt->list_fill + cls,
+                                                         count, d_table, d_W, status);
+    return launch_status();
+}
+
+// The listed tables (n <= kMediumMax): the lists on the first side stream, then one
+// launch per list, the lists spread over the side streams (a launch waits for its slowest
+// table, so lists run side by side).
 template <int SPL>
-wrs_status launch_small(const float* d_w, const int64_t* d_offsets, const uint8_t* d_kinds, int64_t num_tables,
+wrs_status launch_lists(const float* d_w, const int64_t* d_offsets, const uint8_t* d_kinds, int64_t num_tables,
                         wrs_alias_row* d_table, double* d_W, const BatchLayout& L, const HostPlan& p, Fork& f) {
-    uint32_t* status = &L.hdr0->status;
-    SmallLists sl;
-    sl.fill = L.hdr0->small_fill;  // cleared with the headers
-    sl.list = L.small_list;
+    BatchCounters* bc = reinterpret_cast<BatchCounters*>(L.hdr0);  // cleared with the headers
+    uint32_t* status = &bc->status;
+    TableLists sl;
+    sl.cnt = bc;
+    sl.list = L.list;
     uint32_t base = 0;
-    for (int c = 0; c < kSmallClasses; ++c) {
+    for (int c = 0; c < kLists; ++c) {
         sl.base[c] = base;
-        sl.cap[c] = p.small_class_tables[c];
+        sl.cap[c] = p.list_tables[c];
+        sl.items[c] = p.list_items[c];
         base += sl.cap[c];
     }
-    const uint64_t nblk = ((uint64_t)num_tables + kSmallPlanThreads - 1) / kSmallPlanThreads;
+    sl.table_sum = p.table_sum;
+    const uint64_t nblk = ((uint64_t)num_tables + kListThreads - 1) / kListThreads;
     const cudaStream_t* ss = f.side;
-    small_plan_kernel<<<(uint32_t)nblk, kSmallPlanThreads, 0, ss[0]>>>(d_offsets, d_kinds, num_tables, 32u * SPL, sl,
-                                                                       status);
+    table_lists_kernel<<<(uint32_t)nblk, kListThreads, 0, ss[0]>>>(d_offsets, d_kinds, num_tables, 32u * SPL, sl,
+                                                                  status);
+    lists_check_kernel<<<1, 32, 0, ss[0]>>>(sl, status);
     wrs_status st = launch_status();
     if (st != WRS_SUCCESS) return st;
-    if (cudaEventRecord(f.mid, ss[0]) != cudaSuccess || cudaStreamWaitEvent(ss[1], f.mid, 0) != cudaSuccess ||
-        cudaStreamWaitEvent(ss[2], f.mid, 0) != cudaSuccess)
-        return WRS_ERR_CUDA;
+    if (cudaEventRecord(f.mid, ss[0]) != cudaSuccess) return WRS_ERR_CUDA;
+    for (int k = 1; k < kSideStreams; ++k)
+        if (cudaStreamWaitEvent(ss[k], f.mid, 0) != cudaSuccess) return WRS_ERR_CUDA;
+    if (st == WRS_SUCCESS) st = launch_medium<1024>(d_w, d_offsets, sl, 7, d_table, d_W, status, ss[3]);
     if (st == WRS_SUCCESS) st = launch_small_class<2, 2>(d_w, d_offsets, sl, 0, d_table, d_W, status, ss[0]);
-    if (st == WRS_SUCCESS) st = launch_small_class<2, 4>(d_w, d_offsets, sl, 1, d_table, d_W, status, ss[1]);
-    if (st == WRS_SUCCESS) st = launch_small_class<2, 16>(d_w, d_offsets, sl, 3, d_table, d_W, status, ss[2]);
-    if (st == WRS_SUCCESS) st = launch_small_class<2, 8>(d_w, d_offsets, sl, 2, d_table, d_W, status, ss[1]);
+    if (st == WRS_SUCCESS) st = launch_medium<256>(d_w, d_offsets, sl, 6, d_table, d_W, status, ss[1]);
+    if (st == WRS_SUCCESS) st = launch_small_class<2, 4>(d_w, d_offsets, sl, 1, d_table, d_W, status, ss[2]);
+    if (st == WRS_SUCCESS) st = launch_small_class<2, 8>(d_w, d_offsets, sl, 2, d_table, d_W, status, ss[2]);
+    if (st == WRS_SUCCESS) st = launch_small_class<2, 16>(d_w, d_offsets, sl, 3, d_table, d_W, status, ss[1]);
     if constexpr (SPL >= 2) {
-        if (st == WRS_SUCCESS) st = launch_small_class<2, 32>(d_w, d_offsets, sl, 4, d_table, d_W, status, ss[2]);
+        if (st == WRS_SUCCESS) st = launch_small_class<2, 32>(d_w, d_offsets, sl, 4, d_table, d_W, status, ss[3]);
     }
     if constexpr (SPL > 2) {
         if (st == WRS_SUCCESS) st = launch_small_class<SPL, 32>(d_w, d_offsets, sl, 5, d_table, d_W, status, ss[0]);
@@ -256,14 +288,15 @@ wrs_status launch_small(const float* d_w, const int64_t* d_offsets, const uint8_
 
 template <int T>
 wrs_status launch_big(const float* d_w, const int64_t* d_offsets, const uint8_t* d_kinds, int64_t num_tables,
-                      uint32_t small_max, wrs_alias_row* d_table, double* d_W, const BatchLayout& L,
-                      const HostPlan& p, cudaStream_t stream) {
+                      wrs_alias_row* d_table, double* d_W, const BatchLayout& L, const HostPlan& p,
+                      cudaStream_t stream) {
+    const uint32_t big_min = (uint32_t)kMediumMax;  // the tiled passes take the tables above it
     constexpr int NT = PackShape<T>::NT, IPT = PackShape<T>::IPT;
     const uint32_t nblk = (uint32_t)((num_tables + kPlanBlock - 1) / kPlanBlock);
     const PlanCounts cap{p.big_tables, p.tiles, p.big_items};
-    plan_count_kernel<<<nblk, kPlanBlock, 0, stream>>>(d_offsets, d_kinds, num_tables, small_max, T, L.blk);
+    plan_count_kernel<<<nblk, kPlanBlock, 0, stream>>>(d_offsets, d_kinds, num_tables, big_min, T, L.blk);
     plan_scan_kernel<<<1, kPlanBlock, 0, stream>>>(L.blk, nblk, cap, L.plan_status);
-    plan_fill_kernel<<<nblk, kPlanBlock, 0, stream>>>(d_offsets, d_kinds, num_tables, small_max, T, L.blk, cap,
+    plan_fill_kernel<<<nblk, kPlanBlock, 0, stream>>>(d_offsets, d_kinds, num_tables, big_min, T, L.blk, cap,
                                                       L.desc, L.tile_table);
     const TileMap map{L.tile_table, L.desc, L.plan_status, 0, 0};
     const uint32_t nt = p.tiles;
@@ -323,26 +356,26 @@ wrs_status batched_build(const float* d_w, const int64_t* d_offsets, const int64
     if (cudaMemsetAsync(L.hdr0, 0, sizeof(BuildHeader) * (2 + (size_t)p.big_tables), stream) != cudaSuccess)
         return WRS_ERR_CUDA;
     wrs_status st = WRS_SUCCESS;
-    // the small tables and the tiled tables are independent: the former run on the side streams
+    // the listed tables and the tiled tables are independent: the former run on the side streams
     Fork f;
-    if (p.small_tables > 0 && f.begin(stream) != WRS_SUCCESS) {
+    if (p.listed_tables > 0 && f.begin(stream) != WRS_SUCCESS) {
         f.end(stream);
         return WRS_ERR_CUDA;
     }
-    if (p.small_tables > 0) {
+    if (p.listed_tables > 0) {
         switch (sh.small_max) {
-            case 32: st = launch_small<1>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f); break;
-            case 64: st = launch_small<2>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f); break;
-            case 128: st = launch_small<4>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f); break;
-            case 256: st = launch_small<8>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f); break;
-            default: st = launch_small<16>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f); break;
+            case 32: st = launch_lists<1>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f); break;
+            case 64: st = launch_lists<2>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f); break;
+            case 128: st = launch_lists<4>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f); break;
+            case 256: st = launch_lists<8>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f); break;
+            default: st = launch_lists<16>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f); break;
         }
     }
     if (st == WRS_SUCCESS && p.big_tables > 0) {
         switch (sh.tile) {
-            case 1024: st = launch_big<1024>(d_w, d_offsets, d_kinds, num_tables, sh.small_max, d_table, d_W, L, p, stream); break;
-            case 4096: st = launch_big<4096>(d_w, d_offsets, d_kinds, num_tables, sh.small_max, d_table, d_W, L, p, stream); break;
-            default: st = launch_big<2048>(d_w, d_offsets, d_kinds, num_tables, sh.small_max, d_table, d_W, L, p, stream); break;
+            case 1024: st = launch_big<1024>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, stream); break;
+            case 4096: st = launch_big<4096>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, stream); break;
+            default: st = launch_big<2048>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, stream); break;
         }
     }
     if (f.end(stream) != WRS_SUCCESS && st == WRS_SUCCESS) st = WRS_ERR_CUDA;
@@ -520,7 +553,7 @@ extern "C" wrs_status wrs_batched_mixed_build_f32(const float* d_w, const int64_
     if (opts && opts->method != WRS_METHOD_SPLIT) return WRS_ERR_UNSUPPORTED;
     const HostPlan p = host_plan(h_offsets, num_tables, sh, h_kinds);
     if (!p.valid) return WRS_ERR_INVALID_ARGUMENT;
-    if ((p.small_tables > 0 || p.big_tables > 0) && !d_table) return WRS_ERR_INVALID_ARGUMENT;
+    if ((p.listed_tables > 0 || p.big_tables > 0) && !d_table) return WRS_ERR_INVALID_ARGUMENT;
     if ((p.rej_warp_tables > 0 || p.rej_block_tables > 0) && (!d_A || !d_frac || !d_a_size))
         return WRS_ERR_INVALID_ARGUMENT;
     cudaStream_t stream = static_cast<cudaStream_t>(stream_);

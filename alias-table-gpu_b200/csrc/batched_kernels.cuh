@@ -313,59 +313,113 @@ __global__ void batch_status_kernel(const BuildHeader* hdrs, uint32_t num_tables
 //
 // Size classes: n <= 4, 8, 16, 32 by groups of 2, 4, 8, 16 lanes with two items a lane; n <= 64
 // by a warp with two items a lane; the rest (up to small_max) by a warp with small_max / 32
-// items a lane. small_plan_kernel lists the batch's small tables per class (appending with one
-// atomic per warp and class: the order within a list is arbitrary, the rows do not depend on
-// it), and one launch per class builds its list.
+// items a lane. Tables above small_max and up to kMediumMax items are built by a CTA each in
+// shared memory (medium_tables_kernel; lists 6 and 7 by CTA size), larger ones by the tiled passes.
+// table_lists_kernel lists the batch's small and medium tables per class (appending with one
+// atomic per CTA and class: the order within a list is arbitrary, the rows do not depend on it),
+// and one launch per class builds its list.
 constexpr int kSmallClasses = 6;
+constexpr int kLists = 8;
+constexpr int64_t kMediumSplit = 2048;  // medium tables up to this size: CTAs of 256 threads
+constexpr int64_t kMediumMax = 8192;    // the rest: CTAs of 1024 threads
 __host__ __device__ __forceinline__ int small_class(int64_t n) {
     return n <= 4 ? 0 : n <= 8 ? 1 : n <= 16 ? 2 : n <= 32 ? 3 : n <= 64 ? 4 : 5;
 }
+// List of an alias table of n >= 1 items, or -1 for the tiled passes.
+__host__ __device__ __forceinline__ int table_list(int64_t n, uint32_t small_max) {
+    if (n <= (int64_t)small_max) return small_class(n);
+    if (n <= kMediumSplit) return 6;
+    if (n <= kMediumMax) return 7;
+    return -1;
+}
 
-struct SmallLists {
-    uint32_t* fill;                // kSmallClasses counters, zero at the start of the build
-    uint32_t* list;                // table ids; class c at [base[c], base[c] + cap[c])
-    uint32_t base[kSmallClasses];
-    uint32_t cap[kSmallClasses];   // the host's count of the class
+// The batch header (the first header of the batch scratch, zeroed before every build) seen as
+// the batch status word and the fill counters of the lists.
+struct BatchCounters {
+    uint32_t status;
+    uint32_t list_fill[kLists];
+    unsigned long long list_items[kLists];  // items of each list's tables
+    unsigned long long table_sum;           // sum over listed tables of (t + 1) * n_t (mod 2^64)
+};
+static_assert(sizeof(BatchCounters) <= sizeof(BuildHeader) && offsetof(BatchCounters, status) == 0,
+              "batch counters overlay the batch header");
+
+struct TableLists {
+    BatchCounters* cnt;        // fill counters and checks, zero at the start
+    uint32_t* list;            // table ids; list c at [base[c], base[c] + cap[c])
+    uint32_t base[kLists];
+    uint32_t cap[kLists];      // the host's count of the list
+    uint64_t items[kLists];    // the host's items of the list
+    uint64_t table_sum;        // the host's sum of (t + 1) * n_t over listed tables
 };
 
-// One thread per table; positions come from a shared-memory counter per class and CTA, then one
-// global atomic per class and CTA reserves the CTA's run of each list.
-constexpr int kSmallPlanThreads = 1024;
-__global__ void __launch_bounds__(kSmallPlanThreads) small_plan_kernel(const int64_t* __restrict__ offsets,
-                                                                      const uint8_t* kinds, int64_t num_tables,
-                                                                      uint32_t small_max, SmallLists L,
-                                                                      uint32_t* status) {
-    __shared__ uint32_t s_cnt[kSmallClasses], s_base[kSmallClasses];
-    const int64_t t = (int64_t)blockIdx.x * kSmallPlanThreads + threadIdx.x;
+// One thread per table; positions come from a shared-memory counter per list and CTA, then one
+// global atomic per list and CTA reserves the CTA's run of each list. The CTAs also add up the
+// items of each list and a position-weighted table sum, which lists_check_kernel compares with
+// the host's plan (offsets that differ from the host's copy are an error, as in the tiled passes).
+constexpr int kListThreads = 1024;
+__global__ void __launch_bounds__(kListThreads) table_lists_kernel(const int64_t* __restrict__ offsets,
+                                                                  const uint8_t* kinds, int64_t num_tables,
+                                                                  uint32_t small_max, TableLists L,
+                                                                  uint32_t* status) {
+    __shared__ uint32_t s_cnt[kLists], s_base[kLists], s_items[kLists];
+    __shared__ unsigned long long s_tsum;
+    const int64_t t = (int64_t)blockIdx.x * kListThreads + threadIdx.x;
     const int lane = threadIdx.x & 31;
-    if (threadIdx.x < kSmallClasses) s_cnt[threadIdx.x] = 0;
+    if (threadIdx.x < kLists) {
+        s_cnt[threadIdx.x] = 0;
+        s_items[threadIdx.x] = 0;
+    }
+    if (threadIdx.x == 0) s_tsum = 0;
     __syncthreads();
     int cls = -1;
+    uint32_t n32 = 0;
     if (t < num_tables && kind_is(kinds, t, WRS_TABLE_ALIAS)) {
         const int64_t n = __ldg(offsets + t + 1) - __ldg(offsets + t);
-        if (n >= 1 && n <= (int64_t)small_max) cls = small_class(n);
+        if (n >= 1) cls = table_list(n, small_max);
+        if (cls >= 0) n32 = (uint32_t)n;  // <= kMediumMax
     }
     uint32_t pos = 0;
 #pragma unroll
-    for (int c = 0; c < kSmallClasses; ++c) {
+    for (int c = 0; c < kLists; ++c) {
         const uint32_t m = __ballot_sync(0xffffffffu, cls == c);
         if (m == 0) continue;
+        const uint32_t items = __reduce_add_sync(0xffffffffu, cls == c ? n32 : 0u);
         const int leader = __ffs(m) - 1;
         uint32_t b = 0;
-        if (lane == leader) b = atomicAdd(s_cnt + c, (uint32_t)__popc(m));
+        if (lane == leader) {
+            b = atomicAdd(s_cnt + c, (uint32_t)__popc(m));
+            atomicAdd(s_items + c, items);
+        }
         b = __shfl_sync(0xffffffffu, b, leader);
         if (cls == c) pos = b + (uint32_t)__popc(m & ((1u << lane) - 1u));
     }
+    unsigned long long ts = cls >= 0 ? (unsigned long long)(t + 1) * n32 : 0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ts += __shfl_down_sync(0xffffffffu, ts, o);
+    if (lane == 0 && ts) atomicAdd(&s_tsum, ts);
     __syncthreads();
-    if (threadIdx.x < kSmallClasses && s_cnt[threadIdx.x] > 0)
-        s_base[threadIdx.x] = atomicAdd(L.fill + threadIdx.x, s_cnt[threadIdx.x]);
+    if (threadIdx.x < kLists && s_cnt[threadIdx.x] > 0) {
+        s_base[threadIdx.x] = atomicAdd(L.cnt->list_fill + threadIdx.x, s_cnt[threadIdx.x]);
+        atomicAdd(L.cnt->list_items + threadIdx.x, (unsigned long long)s_items[threadIdx.x]);
+    }
+    if (threadIdx.x == 0 && s_tsum) atomicAdd(&L.cnt->table_sum, s_tsum);
     __syncthreads();
     if (cls >= 0) {
         pos += s_base[cls];
-        // more tables of a class than the host counted: offsets differ from the host's
+        // more tables of a list than the host counted: offsets differ from the host's
         if (pos < L.cap[cls]) L.list[L.base[cls] + pos] = (uint32_t)t;
         else record_status(status, WRS_ERR_INVALID_ARGUMENT);
     }
+}
+
+// After table_lists_kernel: the lists against the host's plan.
+__global__ void lists_check_kernel(TableLists L, uint32_t* status) {
+    const int c = threadIdx.x;
+    bool bad = false;
+    if (c < kLists) bad = L.cnt->list_fill[c] != L.cap[c] || L.cnt->list_items[c] != L.items[c];
+    if (c == 0) bad |= L.cnt->table_sum != (unsigned long long)L.table_sum;
+    if (__any_sync(0xffffffffu, bad) && c == 0) record_status(status, WRS_ERR_INVALID_ARGUMENT);
 }
 
 constexpr int kSmallWarps = 4;
@@ -578,6 +632,240 @@ __global__ void __launch_bounds__(32 * kSmallWarps) small_tables_kernel(const fl
         const int64_t n = __ldg(offsets + t + 1) - off;
         if (n < 1 || n > CAP) continue;  // uniform over the group; never for a listed table
         small_table_build<SPL, GW>(w, off, (uint32_t)n, t, mask, gl, sm, table, W_out, status);
+    }
+}
+
+// ---------------------------------------------------------------- medium tables: a CTA each
+// A table of small_max < n <= NS items by one CTA of MT threads with the whole table in shared
+// memory (NS = 8 MT): the weights, then the light and heavy keys (lights from the front and
+// heavies from the back of one array, like the lane-group build), the heavies' inclusive excess
+// prefixes, the light and heavy items (one array, the same way round), the rows' probabilities
+// (over the weights) and aliases. Thread k holds the items [k * ipt, (k + 1) * ipt), ipt =
+// ceil(n / MT). The quantities are those of a one-tile table over the whole table (A_before = 0,
+// no dithering offset), so the rows equal a single-table build's:
+//   1. the weights are copied in (coalesced) and summed in double-double, W over the CTA;
+//   2. per-thread sums of small-light deficits (Q16.48), large-light deficits (Q16.48), heavy
+//      excess (Q40.24) and the light and heavy counts, scanned over the CTA;
+//   3. every thread walks its items again from its prefixes: light keys, heavy keys and excess
+//      prefixes, items, and the light probabilities;
+//   4. the merge of the light keys with the heavy keys (a heavy precedes a light of equal key),
+//      cut into equal runs of the merged order by a binary search per thread (merge path): a
+//      light's alias is the next heavy in that order (the last heavy when none follows); a
+//      heavy's probability is 1 + its corrected excess end - the next light's key (the total
+//      deficit when none follows), its alias the next heavy (itself for the last one);
+//   5. the rows are written out (coalesced).
+constexpr int kMediumItemsPerThread = 8;
+
+template <int MT>
+struct MediumRed {
+    DD dd[MT / 32];
+    uint64_t sc[4][MT / 32];
+    double W;
+};
+// dynamic shared memory of a CTA for tables of up to NS items
+template <int MT>
+constexpr size_t medium_smem_bytes() {
+    constexpr size_t NS = (size_t)MT * kMediumItemsPerThread;
+    return sizeof(MediumRed<MT>) + NS * (8 + 8 + 4 + 4 + 4);
+}
+
+// Exclusive scan of four u64 values per thread over the CTA; tot gets the CTA's totals.
+// Starts and ends with a barrier.
+template <int MT>
+__device__ __forceinline__ void cta_scan4(uint64_t (&v)[4], uint64_t (&tot)[4], uint64_t (&sc)[4][MT / 32]) {
+    constexpr int NW = MT / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint64_t inc[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        inc[q] = v[q];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t x = __shfl_up_sync(0xffffffffu, inc[q], o);
+            if (lane >= o) inc[q] += x;
+        }
+    }
+    __syncthreads();
+    if (lane == 31)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) sc[q][warp] = inc[q];
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const uint64_t wv = lane < NW ? sc[q][lane] : 0ull;
+        uint64_t wi = wv;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t x = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += x;
+        }
+        tot[q] = __shfl_sync(0xffffffffu, wi, 31);
+        const uint64_t wbase = __shfl_sync(0xffffffffu, wi - wv, warp);
+        v[q] = wbase + inc[q] - v[q];
+    }
+    __syncthreads();
+}
+
+template <int MT>
+__device__ __forceinline__ void medium_table_build(const float* __restrict__ w, int64_t off, uint32_t n, int64_t t,
+                                                   wrs_alias_row* __restrict__ table, double* W_out,
+                                                   uint32_t* status, unsigned char* smem) {
+    constexpr int NW = MT / 32;
+    constexpr uint32_t NS = (uint32_t)MT * kMediumItemsPerThread;
+    MediumRed<MT>& red = *reinterpret_cast<MediumRed<MT>*>(smem);
+    uint64_t* key = reinterpret_cast<uint64_t*>(smem + sizeof(MediumRed<MT>));  // lights front, heavies back
+    uint64_t* hE = key + NS;                                                    // heavy j: inclusive excess
+    float* wp = reinterpret_cast<float*>(hE + NS);                               // weight, then probability
+    uint32_t* item = reinterpret_cast<uint32_t*>(wp + NS);                       // lights front, heavies back
+    uint32_t* alias = item + NS;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const float* wt = w + off;
+    // 1. weights in, weight total
+    DD acc = {0.0, 0.0};
+    bool bad = false;
+    for (uint32_t i = tid; i < n; i += MT) {
+        const float x = __ldg(wt + i);
+        wp[i] = x;
+        bad |= weight_invalid(x);
+        acc = dd_add_d(acc, (double)x);
+    }
+    acc = dd_norm(acc);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        DD u;
+        u.hi = __shfl_down_sync(0xffffffffu, acc.hi, o);
+        u.lo = __shfl_down_sync(0xffffffffu, acc.lo, o);
+        acc = dd_add(acc, u);
+    }
+    if (lane == 0) red.dd[warp] = acc;
+    const int any_bad = __syncthreads_or(bad);
+    if (warp == 0) {
+        DD v = lane < NW ? red.dd[lane] : DD{0.0, 0.0};
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            DD u;
+            u.hi = __shfl_down_sync(0xffffffffu, v.hi, o);
+            u.lo = __shfl_down_sync(0xffffffffu, v.lo, o);
+            v = dd_add(v, u);
+        }
+        if (lane == 0) red.W = dd_norm(v).hi;
+    }
+    __syncthreads();
+    const double W = red.W;
+    if (any_bad || !(W > 0.0) || isinf(W)) {  // uniform over the CTA
+        if (tid == 0) record_status(status, (any_bad || isinf(W)) ? kErrInvalidWeight : kErrZeroTotal);
+        return;
+    }
+    if (tid == 0 && W_out) W_out[t] = W;
+    const double W_N = W / (double)n;
+    const ClassParams cp = class_params(W_N, 1.0 / W_N);
+    const uint32_t ipt = (n + MT - 1) / MT;
+    const uint32_t i0 = min(n, (uint32_t)tid * ipt), i1 = min(n, i0 + ipt);
+    // 2. per-thread sums, scanned: S, L, E, lights | heavies << 32
+    uint64_t v[4] = {0ull, 0ull, 0ull, 0ull};
+    for (uint32_t i = i0; i < i1; ++i) {
+        const float x = wp[i];
+        if (x > cp.H1) {
+            v[2] += rare_q(x, true, cp);
+            v[3] += 1ull << 32;
+        } else {
+            v[3] += 1ull;
+            if (x < cp.Hh) v[0] += small_deficit(__fmul_rn(x, cp.R32));
+            else v[1] += rare_q(x, false, cp);
+        }
+    }
+    uint64_t tot[4];
+    cta_scan4<MT>(v, tot, red.sc);
+    const uint32_t nl = (uint32_t)tot[3], nh = (uint32_t)(tot[3] >> 32);
+    const u128 A_tot = ((u128)tot[0] << 16) + q_round24((u128)tot[1] << 16);
+    const int64_t nfix = excess_correction(A_tot, (u128)tot[2] << 40);
+    Dither dth;
+    dth.c0 = 1ull << 23;
+    dth.c0h = 0;
+    uint64_t* hkey = key + (NS - nh);
+    uint32_t* hitem = item + (NS - nh);
+    // 3. keys, heavy excess prefixes, items, light probabilities
+    {
+        uint64_t sr = v[0], lr = v[1], er = v[2];
+        uint32_t li = (uint32_t)v[3], hj = (uint32_t)(v[3] >> 32);
+        uint64_t D = dither_at(dth, lr);
+        for (uint32_t i = i0; i < i1; ++i) {
+            const float x = wp[i];
+            if (x > cp.H1) {
+                er += rare_q(x, true, cp);
+                const u128 d = q_scale_excess((u128)er << 40, nfix) + 0xffff;
+                hkey[hj] = (q_hi(d) >> 16) ? ~0ull : (uint64_t)(d >> 16);
+                hE[hj] = er;
+                hitem[hj] = i;
+                ++hj;
+            } else {
+                key[li] = sr + D;
+                item[li] = i;
+                ++li;
+                float pk;
+                if (x >= cp.Hh) {
+                    lr += rare_q(x, false, cp);
+                    const uint64_t D1 = dither_at(dth, lr);
+                    pk = dithered_prob(D1 - D);
+                    D = D1;
+                } else {
+                    pk = __fmul_rn(x, cp.R32);
+                    sr += small_deficit(pk);
+                }
+                wp[i] = pk;
+            }
+        }
+    }
+    __syncthreads();
+    // 4. merge path
+    {
+        const uint32_t M = nl + nh;
+        const uint32_t mpt = (M + MT - 1) / MT;
+        const uint32_t d0 = min(M, (uint32_t)tid * mpt), d1 = min(M, d0 + mpt);
+        uint32_t lo = d0 > nh ? d0 - nh : 0u, hi = min(d0, nl);
+        while (lo < hi) {  // lights among the first d0 of the merged order
+            const uint32_t mid = (lo + hi) >> 1;
+            if (key[mid] < hkey[d0 - 1 - mid]) lo = mid + 1; else hi = mid;
+        }
+        uint32_t a = lo, b = d0 - lo;
+        for (uint32_t k = d0; k < d1; ++k) {
+            if (b < nh && (a >= nl || hkey[b] <= key[a])) {
+                const u128 Et = q_scale_excess((u128)hE[b] << 40, nfix);
+                const u128 A_next = a < nl ? ((u128)key[a] << 16) : A_tot;
+                const uint32_t it = hitem[b];
+                wp[it] = heavy_row_prob(q_one() + Et - A_next);
+                alias[it] = b + 1 < nh ? hitem[b + 1] : it;
+                ++b;
+            } else {
+                const uint32_t it = item[a];
+                alias[it] = nh == 0 ? it : hitem[b < nh ? b : nh - 1];
+                ++a;
+            }
+        }
+    }
+    __syncthreads();
+    // 5. rows out
+    uint2* rows = reinterpret_cast<uint2*>(table + off);
+    for (uint32_t i = tid; i < n; i += MT) rows[i] = make_uint2(__float_as_uint(wp[i]), alias[i]);
+}
+
+// The tables of list[0 .. min(cap, *fill)), a CTA each (persistent CTAs over the list).
+template <int MT>
+__global__ void __launch_bounds__(MT) medium_tables_kernel(const float* __restrict__ w,
+                                                         const int64_t* __restrict__ offsets,
+                                                         const uint32_t* __restrict__ list, const uint32_t* fill,
+                                                         uint32_t cap, wrs_alias_row* __restrict__ table,
+                                                         double* W_out, uint32_t* status) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int64_t NS = (int64_t)MT * kMediumItemsPerThread;
+    const uint32_t count = min(cap, *fill);
+    for (uint32_t e = blockIdx.x; e < count; e += gridDim.x) {
+        const int64_t t = __ldg(list + e);
+        const int64_t off = __ldg(offsets + t);
+        const int64_t n = __ldg(offsets + t + 1) - off;
+        if (n < 1 || n > NS) continue;  // uniform over the CTA; never for a listed table
+        medium_table_build<MT>(w, off, (uint32_t)n, t, table, W_out, status, smem_raw);
+        __syncthreads();  // shared memory is reused by the next table
     }
 }
 

@@ -106,7 +106,8 @@ struct __align__(16) BuildHeader {
     uint64_t huge_count; // rejection: number of deferred items filled by the whole grid
     uint32_t chunk_count; // split build: tiles pack_walk_kernel left to the chunked form
     uint32_t pad1;
-    uint32_t small_fill[6];  // batched build, batch header: fill counts of the small-table lists
+    uint32_t pad2;
+    uint64_t pad[2];
 };
 static_assert(sizeof(BuildHeader) == 128, "header layout");
 
