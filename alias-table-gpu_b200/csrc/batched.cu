@@ -105,6 +105,7 @@ bool shape_of(const wrs_build_opts* opts, Shape* sh) {
 // The host's view of the batch for one shape (from h_offsets and h_kinds).
 struct HostPlan {
     uint32_t listed_tables;          // alias tables with 1 <= n <= kMediumMax
+    uint32_t empty_tables;           // tables with n = 0
     uint32_t list_tables[kLists];    // ... of them per list (table_list)
     uint64_t list_items[kLists];     // items of each list's tables
     uint64_t table_sum;              // sum over listed tables of (t + 1) * n_t (mod 2^64)
@@ -130,7 +131,10 @@ HostPlan host_plan(const int64_t* h_offsets, int64_t num_tables, const Shape& sh
             p.valid = false;
             return p;
         }
-        if (n == 0) continue;
+        if (n == 0) {
+            ++p.empty_tables;
+            continue;
+        }
         const uint8_t kind = h_kinds ? h_kinds[t] : (uint8_t)WRS_TABLE_ALIAS;
         if (kind == WRS_TABLE_REJECTION) {
             if (n <= (int64_t)kRejWarpMax) ++p.rej_warp_tables; else ++p.rej_block_tables;
@@ -173,10 +177,16 @@ struct BatchLayout {
     uint32_t* heavy_item;
     uint4* heavy_E;
     uint32_t* list;        // the listed tables' ids by list
+    // build and sample only: the spill list, and the chunked sampler's tables and chunk prefix
+    uint32_t* spill;
+    uint32_t spill_cap;
+    uint32_t* gen;
+    uint64_t* gen_prefix;
     size_t bytes;
 };
 
-BatchLayout carve_batch(void* scratch, int64_t num_tables, const HostPlan& p, uint32_t tile) {
+BatchLayout carve_batch(void* scratch, int64_t num_tables, const HostPlan& p, uint32_t tile,
+                        bool sampling = false) {
     Carver c(scratch);
     BatchLayout L;
     // the batch header, the plan header and the per-table headers are contiguous: one memset
@@ -195,8 +205,36 @@ BatchLayout carve_batch(void* scratch, int64_t num_tables, const HostPlan& p, ui
     L.heavy_item = c.take<uint32_t>(p.big_items);
     L.heavy_E = c.take<uint4>(p.big_items);
     L.list = c.take<uint32_t>(p.listed_tables);
+    L.spill_cap = sampling ? p.listed_tables + p.empty_tables : 0u;
+    L.spill = c.take<uint32_t>(L.spill_cap);
+    const size_t ngen = sampling ? (size_t)p.big_tables + L.spill_cap : 0;
+    L.gen = c.take<uint32_t>(ngen);
+    L.gen_prefix = c.take<uint64_t>(sampling ? ngen + 1 : 0);
     L.bytes = c.off;
     return L;
+}
+
+// Build and sample: where the samples go (wrs_batched_build_sample).
+struct SampleArgs {
+    const int64_t* d_sample_offsets;
+    uint64_t total;
+    uint64_t seed;
+    uint64_t counter_base;
+    uint32_t* d_out;
+};
+
+// The samples of list `cls`'s tables (those with at most kListSampleMax), on the list's stream.
+wrs_status launch_list_sample(const wrs_alias_row* d_table, const int64_t* d_offsets, const TableLists& sl, int cls,
+                              const SampleArgs& sa, const BatchLayout& L, uint32_t* status, cudaStream_t stream) {
+    const uint32_t count = sl.cap[cls];
+    if (count == 0) return WRS_SUCCESS;
+    const DeviceInfo d = device_info();
+    const uint64_t want = (count + kListSampleWarps - 1) / kListSampleWarps;
+    const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)d.sm_count * 8));
+    list_sample_kernel<<<grid, 32 * kListSampleWarps, 0, stream>>>(
+        d_table, d_offsets, sa.d_sample_offsets, sl.list + sl.base[cls], sl.cnt->list_fill + cls, count, sa.seed,
+        sa.counter_base, sa.d_out, L.spill, &sl.cnt->spill_fill, L.spill_cap, status);
+    return launch_status();
 }
 
 // The tables of one size class's list, a group of GW lanes each.
@@ -247,7 +285,8 @@ wrs_status launch_medium(const float* d_w, const int64_t* d_offsets, const Table
 // table, so lists run side by side).
 template <int SPL>
 wrs_status launch_lists(const float* d_w, const int64_t* d_offsets, const uint8_t* d_kinds, int64_t num_tables,
-                        wrs_alias_row* d_table, double* d_W, const BatchLayout& L, const HostPlan& p, Fork& f) {
+                        wrs_alias_row* d_table, double* d_W, const BatchLayout& L, const HostPlan& p, Fork& f,
+                        const SampleArgs* sa) {
     BatchCounters* bc = reinterpret_cast<BatchCounters*>(L.hdr0);  // cleared with the headers
     uint32_t* status = &bc->status;
     TableLists sl;
@@ -264,24 +303,38 @@ wrs_status launch_lists(const float* d_w, const int64_t* d_offsets, const uint8_
     const uint64_t nblk = ((uint64_t)num_tables + kListThreads - 1) / kListThreads;
     const cudaStream_t* ss = f.side;
     table_lists_kernel<<<(uint32_t)nblk, kListThreads, 0, ss[0]>>>(d_offsets, d_kinds, num_tables, 32u * SPL, sl,
-                                                                  status);
+                                                                  status, sa ? sa->d_sample_offsets : nullptr,
+                                                                  L.spill, L.spill_cap);
     lists_check_kernel<<<1, 32, 0, ss[0]>>>(sl, status);
     wrs_status st = launch_status();
     if (st != WRS_SUCCESS) return st;
     if (cudaEventRecord(f.mid, ss[0]) != cudaSuccess) return WRS_ERR_CUDA;
     for (int k = 1; k < kSideStreams; ++k)
         if (cudaStreamWaitEvent(ss[k], f.mid, 0) != cudaSuccess) return WRS_ERR_CUDA;
-    if (st == WRS_SUCCESS) st = launch_medium<1024>(d_w, d_offsets, sl, 7, d_table, d_W, status, ss[3]);
-    if (st == WRS_SUCCESS) st = launch_small_class<2, 2>(d_w, d_offsets, sl, 0, d_table, d_W, status, ss[0]);
-    if (st == WRS_SUCCESS) st = launch_medium<256>(d_w, d_offsets, sl, 6, d_table, d_W, status, ss[1]);
-    if (st == WRS_SUCCESS) st = launch_small_class<2, 4>(d_w, d_offsets, sl, 1, d_table, d_W, status, ss[2]);
-    if (st == WRS_SUCCESS) st = launch_small_class<2, 8>(d_w, d_offsets, sl, 2, d_table, d_W, status, ss[2]);
-    if (st == WRS_SUCCESS) st = launch_small_class<2, 16>(d_w, d_offsets, sl, 3, d_table, d_W, status, ss[1]);
+    // each list's samples (build and sample) right after the list, on the same stream
+    auto sampled = [&](wrs_status s2, int cls, cudaStream_t strm) {
+        if (s2 != WRS_SUCCESS || !sa) return s2;
+        return launch_list_sample(d_table, d_offsets, sl, cls, *sa, L, status, strm);
+    };
+    if (st == WRS_SUCCESS)
+        st = sampled(launch_medium<1024>(d_w, d_offsets, sl, 7, d_table, d_W, status, ss[3]), 7, ss[3]);
+    if (st == WRS_SUCCESS)
+        st = sampled(launch_small_class<2, 2>(d_w, d_offsets, sl, 0, d_table, d_W, status, ss[0]), 0, ss[0]);
+    if (st == WRS_SUCCESS)
+        st = sampled(launch_medium<256>(d_w, d_offsets, sl, 6, d_table, d_W, status, ss[1]), 6, ss[1]);
+    if (st == WRS_SUCCESS)
+        st = sampled(launch_small_class<2, 4>(d_w, d_offsets, sl, 1, d_table, d_W, status, ss[2]), 1, ss[2]);
+    if (st == WRS_SUCCESS)
+        st = sampled(launch_small_class<2, 8>(d_w, d_offsets, sl, 2, d_table, d_W, status, ss[2]), 2, ss[2]);
+    if (st == WRS_SUCCESS)
+        st = sampled(launch_small_class<2, 16>(d_w, d_offsets, sl, 3, d_table, d_W, status, ss[1]), 3, ss[1]);
     if constexpr (SPL >= 2) {
-        if (st == WRS_SUCCESS) st = launch_small_class<2, 32>(d_w, d_offsets, sl, 4, d_table, d_W, status, ss[3]);
+        if (st == WRS_SUCCESS)
+            st = sampled(launch_small_class<2, 32>(d_w, d_offsets, sl, 4, d_table, d_W, status, ss[3]), 4, ss[3]);
     }
     if constexpr (SPL > 2) {
-        if (st == WRS_SUCCESS) st = launch_small_class<SPL, 32>(d_w, d_offsets, sl, 5, d_table, d_W, status, ss[0]);
+        if (st == WRS_SUCCESS)
+            st = sampled(launch_small_class<SPL, 32>(d_w, d_offsets, sl, 5, d_table, d_W, status, ss[0]), 5, ss[0]);
     }
     return st;
 }
@@ -347,28 +400,31 @@ wrs_status launch_rejection(const float* d_w, const int64_t* d_offsets, const ui
 wrs_status batched_build(const float* d_w, const int64_t* d_offsets, const int64_t* h_offsets, int64_t num_tables,
                          const Shape& sh, wrs_alias_row* d_table, double* d_W, void* d_scratch, size_t scratch_bytes,
                          cudaStream_t stream, BatchLayout* out_layout, const uint8_t* d_kinds = nullptr,
-                         const uint8_t* h_kinds = nullptr, const RejOut* rej = nullptr) {
+                         const uint8_t* h_kinds = nullptr, const RejOut* rej = nullptr,
+                         const SampleArgs* sa = nullptr) {
     const HostPlan p = host_plan(h_offsets, num_tables, sh, h_kinds);
     if (!p.valid) return WRS_ERR_INVALID_ARGUMENT;
-    const BatchLayout L = carve_batch(d_scratch, num_tables, p, sh.tile);
+    const BatchLayout L = carve_batch(d_scratch, num_tables, p, sh.tile, sa != nullptr);
     if (scratch_bytes < L.bytes) return WRS_ERR_SCRATCH_TOO_SMALL;
     if (out_layout) *out_layout = L;
     if (cudaMemsetAsync(L.hdr0, 0, sizeof(BuildHeader) * (2 + (size_t)p.big_tables), stream) != cudaSuccess)
         return WRS_ERR_CUDA;
     wrs_status st = WRS_SUCCESS;
     // the listed tables and the tiled tables are independent: the former run on the side streams
+    // (with samples, the lists pass also finds the empty tables that have samples)
+    const bool lists = p.listed_tables > 0 || (sa && p.empty_tables > 0);
     Fork f;
-    if (p.listed_tables > 0 && f.begin(stream) != WRS_SUCCESS) {
+    if (lists && f.begin(stream) != WRS_SUCCESS) {
         f.end(stream);
         return WRS_ERR_CUDA;
     }
-    if (p.listed_tables > 0) {
+    if (lists) {
         switch (sh.small_max) {
-            case 32: st = launch_lists<1>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f); break;
-            case 64: st = launch_lists<2>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f); break;
-            case 128: st = launch_lists<4>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f); break;
-            case 256: st = launch_lists<8>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f); break;
-            default: st = launch_lists<16>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f); break;
+            case 32: st = launch_lists<1>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f, sa); break;
+            case 64: st = launch_lists<2>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f, sa); break;
+            case 128: st = launch_lists<4>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f, sa); break;
+            case 256: st = launch_lists<8>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f, sa); break;
+            default: st = launch_lists<16>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, f, sa); break;
         }
     }
     if (st == WRS_SUCCESS && p.big_tables > 0) {
@@ -380,6 +436,18 @@ wrs_status batched_build(const float* d_w, const int64_t* d_offsets, const int64
     }
     if (f.end(stream) != WRS_SUCCESS && st == WRS_SUCCESS) st = WRS_ERR_CUDA;
     if (st != WRS_SUCCESS) return st;
+    if (sa) {  // the tiled tables' samples and the spilled ones, after every build
+        BatchCounters* bc = reinterpret_cast<BatchCounters*>(L.hdr0);
+        const uint32_t* plan_status = p.big_tables > 0 ? L.plan_status : nullptr;
+        chunks_plan_kernel<<<1, 1024, 0, stream>>>(L.desc, p.big_tables, plan_status, L.spill, &bc->spill_fill,
+                                                   L.spill_cap, sa->d_sample_offsets, num_tables, sa->total, L.gen,
+                                                   L.gen_prefix, &bc->chunks, &bc->status);
+        const DeviceInfo d = device_info();
+        chunk_sample_kernel<<<d.sm_count * 8, kChunkThreads, 0, stream>>>(
+            d_table, d_offsets, sa->d_sample_offsets, L.gen, L.gen_prefix, &bc->spill_fill, L.spill_cap, plan_status,
+            p.big_tables, &bc->chunks, sa->seed, sa->counter_base, sa->d_out, &bc->status);
+        st = launch_status();
+    }
     if (rej && (p.rej_warp_tables > 0 || p.rej_block_tables > 0))
         st = launch_rejection(d_w, d_offsets, d_kinds, num_tables, p, *rej, d_W, &L.hdr0->status, stream);
     return st;
@@ -440,6 +508,47 @@ extern "C" wrs_status wrs_batched_sample(const wrs_alias_row* d_table, const int
     return launch_status();
 }
 
+extern "C" size_t wrs_batched_build_sample_scratch_bytes(const int64_t* h_offsets, int64_t num_tables,
+                                                         const wrs_build_opts* opts) {
+    auto bytes = [&](const Shape& sh) -> size_t {
+        const HostPlan p = host_plan(h_offsets, num_tables, sh);
+        return p.valid ? carve_batch(nullptr, num_tables, p, sh.tile, true).bytes : 0;
+    };
+    if (opts) {
+        Shape sh;
+        return shape_of(opts, &sh) ? bytes(sh) : 0;
+    }
+    size_t best = 0;
+    for (uint32_t s : kSmallChoices)
+        for (uint32_t t : kTileChoices) {
+            const size_t b = bytes(Shape{s, t});
+            if (b == 0) return 0;
+            best = std::max(best, b);
+        }
+    return best;
+}
+
+extern "C" wrs_status wrs_batched_build_sample(const float* d_w, const int64_t* d_offsets, const int64_t* h_offsets,
+                                               int64_t num_tables, const wrs_build_opts* opts, wrs_alias_row* d_table,
+                                               double* d_W, const int64_t* d_sample_offsets, uint64_t total_samples,
+                                               uint64_t seed, uint64_t counter_base, uint32_t* d_out, void* d_scratch,
+                                               size_t scratch_bytes, void* stream_) {
+    if (!d_w || !d_offsets || !h_offsets || !d_table || !d_scratch || !d_sample_offsets || num_tables < 1 ||
+        (total_samples > 0 && !d_out))
+        return WRS_ERR_INVALID_ARGUMENT;
+    Shape sh;
+    if (!shape_of(opts, &sh)) return WRS_ERR_INVALID_ARGUMENT;
+    if (opts && opts->method != WRS_METHOD_SPLIT) return WRS_ERR_UNSUPPORTED;
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+    const SampleArgs sa{d_sample_offsets, total_samples, seed, counter_base, d_out};
+    BatchLayout L;
+    const wrs_status st = batched_build(d_w, d_offsets, h_offsets, num_tables, sh, d_table, d_W, d_scratch,
+                                        scratch_bytes, stream, &L, nullptr, nullptr, nullptr, &sa);
+    if (st != WRS_SUCCESS) return st;
+    if (opts && (opts->flags & WRS_FLAG_SYNC)) return read_device_status(&L.hdr0->status, stream);
+    return WRS_SUCCESS;
+}
+
 extern "C" wrs_status wrs_batched_autotune(const float* d_w, const int64_t* d_offsets, const int64_t* h_offsets,
                                            int64_t num_tables, wrs_alias_row* d_table, void* d_scratch,
                                            size_t scratch_bytes, wrs_build_opts* opts, void* stream_) {
@@ -453,35 +562,56 @@ extern "C" wrs_status wrs_batched_autotune(const float* d_w, const int64_t* d_of
         cudaEventDestroy(e0);
         return WRS_ERR_CUDA;
     }
+    // every shape is captured into a graph and its launches timed, so that the host's planning
+    // (a pass over the offsets per call) stays out of the device time
     float best_ms = 1e30f;
     Shape best{kDefaultSmall, 2048};
     wrs_status result = WRS_SUCCESS;
+    cudaStream_t cap = nullptr;  // the capture stream, ordered after the caller's stream
+    if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess || cudaEventRecord(e0, stream) != cudaSuccess ||
+        cudaStreamWaitEvent(cap, e0, 0) != cudaSuccess)
+        result = WRS_ERR_CUDA;
     for (uint32_t s : kSmallChoices) {
         for (uint32_t t : kTileChoices) {
+            if (result != WRS_SUCCESS) break;
             const Shape sh{s, t};
+            BatchLayout L;
+            cudaGraph_t graph = nullptr;
+            cudaGraphExec_t exec = nullptr;
+            wrs_status st = WRS_SUCCESS;
+            if (cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+                result = WRS_ERR_CUDA;
+                break;
+            }
+            st = batched_build(d_w, d_offsets, h_offsets, num_tables, sh, d_table, nullptr, d_scratch, scratch_bytes,
+                               cap, &L);
+            if (cudaStreamEndCapture(cap, &graph) != cudaSuccess && st == WRS_SUCCESS) st = WRS_ERR_CUDA;
+            if (st == WRS_SUCCESS && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) st = WRS_ERR_CUDA;
             float ms_min = 1e30f;
-            for (int rep = 0; rep < 3; ++rep) {  // the first run warms up
-                BatchLayout L;
-                cudaEventRecord(e0, stream);
-                wrs_status st = batched_build(d_w, d_offsets, h_offsets, num_tables, sh, d_table, nullptr, d_scratch,
-                                              scratch_bytes, stream, &L);
-                cudaEventRecord(e1, stream);
-                if (st == WRS_SUCCESS) st = read_device_status(&L.hdr0->status, stream);
-                if (st != WRS_SUCCESS) {
-                    result = st;
-                    break;
-                }
+            for (int rep = 0; st == WRS_SUCCESS && rep < 4; ++rep) {  // the first launch warms up
+                cudaEventRecord(e0, cap);
+                if (cudaGraphLaunch(exec, cap) != cudaSuccess) st = WRS_ERR_CUDA;
+                cudaEventRecord(e1, cap);
+                if (st == WRS_SUCCESS) st = read_device_status(&L.hdr0->status, cap);
                 float ms = 0.0f;
                 cudaEventElapsedTime(&ms, e0, e1);
                 if (rep > 0) ms_min = std::min(ms_min, ms);
             }
-            if (result != WRS_SUCCESS) break;
+            if (exec) cudaGraphExecDestroy(exec);
+            if (graph) cudaGraphDestroy(graph);
+            if (st != WRS_SUCCESS) {
+                result = st;
+                break;
+            }
             if (ms_min < best_ms) {
                 best_ms = ms_min;
                 best = sh;
             }
         }
-        if (result != WRS_SUCCESS) break;
+    }
+    if (cap) {
+        cudaStreamSynchronize(cap);
+        cudaStreamDestroy(cap);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -338,8 +338,10 @@ __host__ __device__ __forceinline__ int table_list(int64_t n, uint32_t small_max
 struct BatchCounters {
     uint32_t status;
     uint32_t list_fill[kLists];
+    uint32_t spill_fill;                    // build and sample: tables left to the chunked sampler
     unsigned long long list_items[kLists];  // items of each list's tables
     unsigned long long table_sum;           // sum over listed tables of (t + 1) * n_t (mod 2^64)
+    unsigned long long chunks;              // build and sample: chunks of the chunked sampler
 };
 static_assert(sizeof(BatchCounters) <= sizeof(BuildHeader) && offsetof(BatchCounters, status) == 0,
               "batch counters overlay the batch header");
@@ -361,7 +363,9 @@ constexpr int kListThreads = 1024;
 __global__ void __launch_bounds__(kListThreads) table_lists_kernel(const int64_t* __restrict__ offsets,
                                                                   const uint8_t* kinds, int64_t num_tables,
                                                                   uint32_t small_max, TableLists L,
-                                                                  uint32_t* status) {
+                                                                  uint32_t* status,
+                                                                  const int64_t* __restrict__ sample_offsets,
+                                                                  uint32_t* spill, uint32_t spill_cap) {
     __shared__ uint32_t s_cnt[kLists], s_base[kLists], s_items[kLists];
     __shared__ unsigned long long s_tsum;
     const int64_t t = (int64_t)blockIdx.x * kListThreads + threadIdx.x;
@@ -378,6 +382,13 @@ __global__ void __launch_bounds__(kListThreads) table_lists_kernel(const int64_t
         const int64_t n = __ldg(offsets + t + 1) - __ldg(offsets + t);
         if (n >= 1) cls = table_list(n, small_max);
         if (cls >= 0) n32 = (uint32_t)n;  // <= kMediumMax
+        // build and sample: an empty table with samples goes to the chunked sampler (which
+        // reports it)
+        if (n == 0 && sample_offsets && __ldg(sample_offsets + t + 1) != __ldg(sample_offsets + t)) {
+            const uint32_t k = atomicAdd(&L.cnt->spill_fill, 1u);
+            if (k < spill_cap) spill[k] = (uint32_t)t;
+            else record_status(status, WRS_ERR_INVALID_ARGUMENT);
+        }
     }
     uint32_t pos = 0;
 #pragma unroll
@@ -1028,6 +1039,154 @@ __global__ void __launch_bounds__(kBatchSampleThreads) batch_sample_kernel(
         const uint32_t row = scale_u64(x.x[0], x.x[1], (uint32_t)n);
         const uint2 e = __ldg(reinterpret_cast<const uint2*>(table + off) + row);
         out[s] = coin24(x.x[2]) < __uint_as_float(e.x) ? row : e.y;
+    }
+}
+
+// ---------------------------------------------------------------- build and sample
+// wrs_batched_build_sample draws the samples of each list's tables right after the list is
+// built, on the list's stream, while the tiled passes still run: list_sample_kernel gives a
+// warp to each table of a list (positions so[t] + lane + 32 j, the plain contract over the
+// global position, exactly as batch_sample_kernel). A table with more than kListSampleMax
+// samples is put on the spill list instead; after all builds, chunks_plan_kernel cuts the
+// tiled tables and the spilled ones into chunks of kChunkSamples positions and
+// chunk_sample_kernel draws them.
+constexpr uint32_t kListSampleMax = 2048;
+constexpr uint32_t kChunkSamples = 2048;
+constexpr int kChunkThreads = 256;
+constexpr int kListSampleWarps = 8;
+
+__device__ __forceinline__ uint32_t alias_sample_at(const uint2* __restrict__ rows, uint32_t n, uint64_t b,
+                                                    uint32_t k0, uint32_t k1) {
+    const Philox4 x = philox4x32_10((uint32_t)b, (uint32_t)(b >> 32), 0u, 0u, k0, k1);
+    const uint32_t row = scale_u64(x.x[0], x.x[1], n);
+    const uint2 e = __ldg(rows + row);
+    return coin24(x.x[2]) < __uint_as_float(e.x) ? row : e.y;
+}
+
+__global__ void __launch_bounds__(32 * kListSampleWarps) list_sample_kernel(
+    const wrs_alias_row* __restrict__ table, const int64_t* __restrict__ offsets,
+    const int64_t* __restrict__ sample_offsets, const uint32_t* __restrict__ list, const uint32_t* fill,
+    uint32_t cap, uint64_t seed, uint64_t counter_base, uint32_t* __restrict__ out, uint32_t* spill,
+    uint32_t* spill_fill, uint32_t spill_cap, uint32_t* status) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t count = min(cap, *fill);
+    const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+    const uint32_t nwarps = gridDim.x * kListSampleWarps;
+    for (uint32_t e = blockIdx.x * kListSampleWarps + (threadIdx.x >> 5); e < count; e += nwarps) {
+        const int64_t t = __ldg(list + e);
+        const int64_t s0 = __ldg(sample_offsets + t), s1 = __ldg(sample_offsets + t + 1);
+        if (s1 <= s0) {
+            if (s1 < s0 && lane == 0) record_status(status, WRS_ERR_INVALID_ARGUMENT);
+            continue;
+        }
+        if (s1 - s0 > (int64_t)kListSampleMax) {  // uniform over the warp
+            if (lane == 0) {
+                const uint32_t k = atomicAdd(spill_fill, 1u);
+                if (k < spill_cap) spill[k] = (uint32_t)t;
+                else record_status(status, WRS_ERR_INVALID_ARGUMENT);
+            }
+            continue;
+        }
+        const int64_t off = __ldg(offsets + t);
+        const uint32_t n = (uint32_t)(__ldg(offsets + t + 1) - off);  // 1 <= n <= kMediumMax: a listed table
+        const uint2* rows = reinterpret_cast<const uint2*>(table + off);
+        for (int64_t s = s0 + lane; s < s1; s += 32) out[s] = alias_sample_at(rows, n, counter_base + (uint64_t)s, k0, k1);
+    }
+}
+
+// One CTA: the tiled tables (desc[0 .. num_big)) and the spilled ones (spill[0 .. *spill_fill))
+// as one list gen[] with the exclusive prefix of their chunk counts; the total in *chunks. Also
+// checks sample_offsets[num_tables] == total.
+__global__ void __launch_bounds__(1024) chunks_plan_kernel(const TableDesc* desc, uint32_t num_big,
+                                                          const uint32_t* plan_status, const uint32_t* spill,
+                                                          const uint32_t* spill_fill, uint32_t spill_cap,
+                                                          const int64_t* __restrict__ sample_offsets,
+                                                          int64_t num_tables, uint64_t total, uint32_t* gen,
+                                                          uint64_t* gen_prefix, unsigned long long* chunks,
+                                                          uint32_t* status) {
+    __shared__ uint64_t s_warp[32];
+    __shared__ uint64_t s_carry;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // the tiled tables are listed only if their plan held
+    const uint32_t nbig = (plan_status && *plan_status) ? 0u : num_big;
+    const uint32_t nsp = min(spill_cap, *spill_fill);
+    const uint32_t m = nbig + nsp;
+    if (threadIdx.x == 0) {
+        s_carry = 0;
+        if ((uint64_t)__ldg(sample_offsets + num_tables) != total || __ldg(sample_offsets) != 0)
+            record_status(status, WRS_ERR_INVALID_ARGUMENT);
+    }
+    __syncthreads();
+    for (uint32_t c0 = 0; c0 < m; c0 += 1024) {
+        const uint32_t j = c0 + threadIdx.x;
+        uint64_t v = 0;
+        if (j < m) {
+            const uint32_t t = j < nbig ? desc[j].id : spill[j - nbig];
+            gen[j] = t;
+            const int64_t cnt = __ldg(sample_offsets + t + 1) - __ldg(sample_offsets + t);
+            v = cnt > 0 ? ((uint64_t)cnt + kChunkSamples - 1) / kChunkSamples : 0ull;
+        }
+        uint64_t inc = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t x = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += x;
+        }
+        if (lane == 31) s_warp[warp] = inc;
+        __syncthreads();
+        if (warp == 0) {
+            uint64_t wv = s_warp[lane], wi = wv;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint64_t x = __shfl_up_sync(0xffffffffu, wi, o);
+                if (lane >= o) wi += x;
+            }
+            s_warp[lane] = wi - wv;
+        }
+        __syncthreads();
+        if (j < m) gen_prefix[j] = s_carry + s_warp[warp] + inc - v;
+        __syncthreads();
+        if (threadIdx.x == 1023) s_carry += s_warp[31] + inc;  // the last thread's inclusive value
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        gen_prefix[m] = s_carry;
+        *chunks = s_carry;
+    }
+}
+
+// Persistent CTAs over the chunks: chunk c belongs to gen entry j (the last with gen_prefix[j]
+// <= c) and covers its positions so[t] + (c - gen_prefix[j]) * kChunkSamples + [0, kChunkSamples).
+__global__ void __launch_bounds__(kChunkThreads) chunk_sample_kernel(
+    const wrs_alias_row* __restrict__ table, const int64_t* __restrict__ offsets,
+    const int64_t* __restrict__ sample_offsets, const uint32_t* __restrict__ gen,
+    const uint64_t* __restrict__ gen_prefix, const uint32_t* spill_fill, uint32_t spill_cap,
+    const uint32_t* plan_status, uint32_t num_big, const unsigned long long* chunks, uint64_t seed,
+    uint64_t counter_base, uint32_t* __restrict__ out, uint32_t* status) {
+    const uint32_t nbig = (plan_status && *plan_status) ? 0u : num_big;
+    const uint32_t m = nbig + min(spill_cap, *spill_fill);
+    const uint64_t nchunks = *chunks;
+    const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+    for (uint64_t c = blockIdx.x; c < nchunks; c += gridDim.x) {
+        uint32_t lo = 0, hi = m - 1;  // m >= 1 when there are chunks
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (__ldg(gen_prefix + mid) <= c) lo = mid; else hi = mid - 1;
+        }
+        const int64_t t = __ldg(gen + lo);
+        const int64_t s1 = __ldg(sample_offsets + t + 1);
+        const int64_t sb = __ldg(sample_offsets + t) + (int64_t)(c - __ldg(gen_prefix + lo)) * kChunkSamples;
+        const int64_t se = min(s1, sb + (int64_t)kChunkSamples);
+        const int64_t off = __ldg(offsets + t);
+        const int64_t n = __ldg(offsets + t + 1) - off;
+        if (n <= 0 || n > 0xffffffffll) {  // an empty table with samples
+            for (int64_t s = sb + threadIdx.x; s < se; s += kChunkThreads) out[s] = 0xffffffffu;
+            if (threadIdx.x == 0) record_status(status, WRS_ERR_INVALID_ARGUMENT);
+            continue;
+        }
+        const uint2* rows = reinterpret_cast<const uint2*>(table + off);
+        for (int64_t s = sb + threadIdx.x; s < se; s += kChunkThreads)
+            out[s] = alias_sample_at(rows, (uint32_t)n, counter_base + (uint64_t)s, k0, k1);
     }
 }
 

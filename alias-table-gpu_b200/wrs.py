@@ -86,6 +86,9 @@ _SIGNATURES = {
     "wrs_batched_build_scratch_bytes": (_SZ, [_P, _I64, _P]),
     "wrs_batched_build_f32": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P, _SZ, _P]),
     "wrs_batched_sample": (ctypes.c_int, [_P, _P, _I64, _P, _U64, _U64, _U64, _P, _P]),
+    "wrs_batched_build_sample_scratch_bytes": (_SZ, [_P, _I64, _P]),
+    "wrs_batched_build_sample": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P, _U64, _U64, _U64, _P, _P, _SZ,
+                                                _P]),
     "wrs_batched_autotune": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _SZ, _P, _P]),
     "wrs_batched_mixed_build_scratch_bytes": (_SZ, [_P, _P, _I64, _P]),
     "wrs_batched_mixed_build_f32": (ctypes.c_int, [_P, _P, _P, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _SZ, _P]),
@@ -331,6 +334,25 @@ def batched_sample(table, d_offsets, num_tables: int, d_sample_offsets, total: i
                    counter_base: int = 0, stream=None) -> int:
     return lib().wrs_batched_sample(_ptr(table), _ptr(d_offsets), num_tables, _ptr(d_sample_offsets), total,
                                     seed & (2**64 - 1), counter_base & (2**64 - 1), _ptr(out), _stream(stream))
+
+
+def batched_build_sample_scratch_bytes(h_offsets, opts: Optional[BuildOpts] = None) -> int:
+    """Scratch of wrs_batched_build_sample (opts None: enough for every launch shape)."""
+    h = _host_i64(h_offsets)
+    return lib().wrs_batched_build_sample_scratch_bytes(h.ctypes.data, h.shape[0] - 1,
+                                                        ctypes.byref(opts) if opts else None)
+
+
+def batched_build_sample(w, d_offsets, h_offsets, table, d_sample_offsets, total: int, seed: int, out, scratch,
+                         opts: Optional[BuildOpts] = None, counter_base: int = 0, W_out=None, stream=None) -> int:
+    """batched_build followed by batched_sample in one call: each size class's samples are drawn
+    as soon as it is built, while the larger tables are still being built."""
+    h = _host_i64(h_offsets)
+    return lib().wrs_batched_build_sample(_ptr(w), _ptr(d_offsets), h.ctypes.data, h.shape[0] - 1,
+                                          ctypes.byref(opts) if opts else None, _ptr(table), _ptr(W_out),
+                                          _ptr(d_sample_offsets), total, seed & (2**64 - 1),
+                                          counter_base & (2**64 - 1), _ptr(out), _ptr(scratch),
+                                          scratch.numel() * scratch.element_size(), _stream(stream))
 
 
 def batched_autotune(w, d_offsets, h_offsets, table, scratch, opts: BuildOpts, stream=None) -> int:

@@ -50,11 +50,30 @@ FALLBACK_HBM_GBS = 6650.0
 # kernels one step launches: wsum, scan, tile_prefix, link, pack_walk, split_pack (the chunked
 # form over the tiles pack_walk listed; an empty list costs one short launch) and the sampler
 KERNELS_PER_STEP = 7
-# kernels one replay of the batched graph launches when the batch has both one-warp tables
-# and tiled tables: plan_count, plan_scan, plan_fill, batch_wsum, tile_reduce, batch_prefix,
-# heavy_list, tile_link, split_pack, batch_status, small_tables (the build) and batch_sample;
-# a mixed batch with rejection tables adds one or two rejection kernels
-BATCHED_KERNELS_PER_REPLAY = 12
+
+def batched_kernels_per_replay(sizes, small_max: int, fused: bool, kinds=None) -> int:
+    """Kernels one replay of a batched graph launches: table_lists and lists_check, one build
+    launch per non-empty list (size classes n <= 4, 8, 16, 32, 64, <= small_max by lane groups;
+    n <= 2048 and <= 8192 by CTAs), with `fused` one list sampler per such list plus
+    chunks_plan and chunk_sample, else batch_sample; the ten tiled passes (plan_count,
+    plan_scan, plan_fill, batch_wsum, tile_reduce, batch_prefix, heavy_list, tile_link,
+    split_pack, batch_status) when tables above 8192 items are present; a mixed batch (kinds)
+    adds one or two rejection kernels."""
+    sizes = np.asarray(sizes)
+    alias = sizes[(sizes > 0) & ((np.asarray(kinds) == 0) if kinds is not None else True)]
+    lists = 0
+    for lo, hi in [(1, 4), (5, 8), (9, 16), (17, 32), (33, 64), (65, small_max)]:
+        hi = min(hi, small_max)
+        if lo <= hi:
+            lists += int(np.any((alias >= lo) & (alias <= hi)))
+    lists += int(np.any((alias > small_max) & (alias <= 2048))) + int(np.any((alias > 2048) & (alias <= 8192)))
+    k = 2 + lists * (2 if fused else 1) + (2 if fused else 1)
+    if np.any(alias > 8192):
+        k += 10
+    if kinds is not None:
+        rej = sizes[(sizes > 0) & (np.asarray(kinds) == 1)]
+        k += int(np.any(rej <= 4096)) + int(np.any(rej > 4096))
+    return k
 BATCH_TABLES = 1 << 17
 BATCH_SAMPLES_PER_TABLE = 64
 BATCH_PER_TABLE_SAMPLE = 4096  # tables timed one call at a time (the per-table baseline)
@@ -688,7 +707,8 @@ def batched_phase(dev, make=batch_config4, mixed: bool = False, shape: str = "")
     w = torch.from_numpy(w_np).to(dev)
     d_off = torch.from_numpy(off).to(dev)
     table = torch.empty(items, dtype=torch.int64, device=dev)
-    scratch = torch.empty(wrs.batched_build_scratch_bytes(off), dtype=torch.uint8, device=dev)
+    scratch = torch.empty(max(wrs.batched_build_scratch_bytes(off), wrs.batched_build_sample_scratch_bytes(off)),
+                          dtype=torch.uint8, device=dev)
     soff = np.zeros(nt + 1, dtype=np.int64)
     np.cumsum(counts, out=soff[1:])
     total = int(soff[-1])
@@ -719,18 +739,29 @@ def batched_phase(dev, make=batch_config4, mixed: bool = False, shape: str = "")
             raise RuntimeError("single-table build failed")
         exact &= bool(np.array_equal(rows[off[t]:off[t + 1]], t1.cpu().numpy().view(np.uint32).reshape(-1, 2)))
 
+    # the step: wrs_batched_build_sample (each size class sampled as soon as it is built); the
+    # separate build and sample calls are timed beside it, and must give the same samples
     s = torch.cuda.Stream(dev)
     s.wait_stream(torch.cuda.current_stream(dev))
     g = torch.cuda.CUDAGraph()
     with torch.cuda.stream(s):
         g.capture_begin()
-        wrs.batched_build(w, d_off, off, table, scratch, opts, stream=s)
-        wrs.batched_sample(table, d_off, nt, d_soff, total, SEED_SAMPLES, out, 0, stream=s)
+        wrs.batched_build_sample(w, d_off, off, table, d_soff, total, SEED_SAMPLES, out, scratch, opts, stream=s)
         g.capture_end()
+    g_sep = torch.cuda.CUDAGraph()
+    out_sep = torch.empty_like(out)
+    with torch.cuda.stream(s):
+        g_sep.capture_begin()
+        wrs.batched_build(w, d_off, off, table, scratch, opts, stream=s)
+        wrs.batched_sample(table, d_off, nt, d_soff, total, SEED_SAMPLES, out_sep, 0, stream=s)
+        g_sep.capture_end()
     torch.cuda.current_stream(dev).wait_stream(s)
     for _ in range(3):
         g.replay()
+        g_sep.replay()
     torch.cuda.synchronize()
+    if wrs.scratch_status(scratch) or not torch.equal(out, out_sep):
+        raise RuntimeError("build and sample differs from the separate build and sample calls")
     reps = 20
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     # the batch (weights, offsets, rows, samples) fits in L2: every replay is timed on its own
@@ -746,6 +777,13 @@ def batched_phase(dev, make=batch_config4, mixed: bool = False, shape: str = "")
     torch.cuda.synchronize()
     batched_ms = sum(ev[2 * i].elapsed_time(ev[2 * i + 1]) for i in range(reps)) / reps
     batched_wall_ms = (time.perf_counter() - t0) * 1e3 / reps
+    for i in range(reps):
+        flush.zero_()
+        ev[2 * i].record()
+        g_sep.replay()
+        ev[2 * i + 1].record()
+    torch.cuda.synchronize()
+    separate_ms = sum(ev[2 * i].elapsed_time(ev[2 * i + 1]) for i in range(reps)) / reps
     # end to end: the weights and both offset arrays copied up from pinned host memory, the
     # graph replayed, the samples copied down
     w_h = torch.from_numpy(w_np).pin_memory()
@@ -807,7 +845,9 @@ def batched_phase(dev, make=batch_config4, mixed: bool = False, shape: str = "")
                       "kinds_by_size_class": {f"n<=2^{c}": names.get(int(cls[c]), "skip") for c in present},
                       "class_ms_alias_vs_rejection": {f"n<=2^{c}": [round(float(cms[c, 0]), 3),
                                                                      round(float(cms[c, 1]), 3)] for c in present},
-                      "rejection_tables": int((kinds == wrs.WRS_TABLE_REJECTION).sum())}
+                      "rejection_tables": int((kinds == wrs.WRS_TABLE_REJECTION).sum()),
+                      "kernels_per_replay": batched_kernels_per_replay(sizes, int(opts.small_table_items), False,
+                                                                       kinds)}
         batched_ms = e0.elapsed_time(e1) / reps
         batched_wall_ms = (time.perf_counter() - t0) * 1e3 / reps
 
@@ -846,6 +886,10 @@ def batched_phase(dev, make=batch_config4, mixed: bool = False, shape: str = "")
         "workload": what, "items": items, "samples": total,
         "autotuned": {"small_table_items": int(opts.small_table_items), "tile_items": int(opts.tile_items)},
         "batched_ms": round(batched_ms, 4), "batched_wall_ms": round(batched_wall_ms, 4),
+        "step": "wrs_batched_build_sample (one call, captured in a CUDA graph)",
+        "kernels_per_replay": (mixed_info["kernels_per_replay"] if mixed_info else
+                               batched_kernels_per_replay(sizes, int(opts.small_table_items), True)),
+        "separate_build_then_sample_ms": round(separate_ms, 4),
         "l2": ("mixed graph: inputs larger than L2, replays back to back; all-alias graph: L2 flushed "
                "before every replay" if mixed else "L2 flushed (256 MiB write) before every replay"),
         "e2e": {"value": round((items + total) / (batched_e2e_ms * 1e-3) / 1e9, 3), "unit": UNIT,
@@ -922,7 +966,7 @@ def run_batched_only(args, rank: int, world: int, local_rank: int):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": b["workload"], "items": b["items"], "samples": b["samples"]},
                 "batched": b,
-                "gpu_launches": (BATCHED_KERNELS_PER_REPLAY + (2 if b.get("mixed", {}).get("rejection_tables") else 0)) * 20,
+                "gpu_launches": b["kernels_per_replay"] * 20,
                 "e2e": b["e2e"], "note": f"{items_samples} items+samples per graph replay"}
     b = batched_phase(dev, shard_of(make, rank, world), mixed=args.config == "5", shape=args.shape)
     slowest = max_over_ranks(b["batched_ms"], dev)
@@ -937,7 +981,7 @@ def run_batched_only(args, rank: int, world: int, local_rank: int):
             "config": {"workload": b["workload"].split("; shard")[0] + f"; sharded over {world} devices by table ranges",
                        "items_plus_samples": total, "parallelism": f"table shards x{world}"},
             "batched_rank0": b,
-            "gpu_launches": (BATCHED_KERNELS_PER_REPLAY + (2 if b.get("mixed", {}).get("rejection_tables") else 0)) * 20,
+            "gpu_launches": b["kernels_per_replay"] * 20,
             "e2e": b["e2e"]}
 
 

@@ -246,6 +246,22 @@ WRS_API wrs_status wrs_batched_sample(const wrs_alias_row* d_table, const int64_
                               int64_t num_tables, const int64_t* d_sample_offsets,
                               uint64_t total_samples, uint64_t seed, uint64_t counter_base,
                               uint32_t* d_out, void* stream);
+/* The batched build and the batched sampler in one call, with the same rows and the same
+ * samples as wrs_batched_build_f32 followed by wrs_batched_sample. The samples of each table of
+ * at most 8192 items (with at most 2048 samples) are drawn as soon as its size class is built,
+ * on the side stream that built it, while the larger tables are still being built; the other
+ * tables' samples follow the last build. d_sample_offsets must start at 0 and end at
+ * total_samples; an empty table with samples gets 0xFFFFFFFF at its positions and the status
+ * WRS_ERR_INVALID_ARGUMENT. Can be captured in a CUDA graph. */
+WRS_API size_t     wrs_batched_build_sample_scratch_bytes(const int64_t* h_offsets, int64_t num_tables,
+                                                  const wrs_build_opts* opts);
+WRS_API wrs_status wrs_batched_build_sample(const float* d_w, const int64_t* d_offsets,
+                                    const int64_t* h_offsets, int64_t num_tables,
+                                    const wrs_build_opts* opts, wrs_alias_row* d_table,
+                                    double* d_W /* num_tables, optional */,
+                                    const int64_t* d_sample_offsets, uint64_t total_samples,
+                                    uint64_t seed, uint64_t counter_base, uint32_t* d_out,
+                                    void* d_scratch, size_t scratch_bytes, void* stream);
 /* Times the batched build of this batch for every launch shape (small_table_items in
  * {32, 64, 128, 256, 512} x tile_items in {1024, 2048, 4096}) and writes the fastest into
  * *opts (method and flags are kept). Synchronous; it builds into d_table (the same rows every
