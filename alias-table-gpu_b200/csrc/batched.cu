@@ -549,6 +549,28 @@ extern "C" wrs_status wrs_batched_build_sample(const float* d_w, const int64_t* 
     return WRS_SUCCESS;
 }
 
+extern "C" wrs_status wrs_batched_per_table(const float* d_w, const int64_t* h_offsets,
+                                            const int64_t* h_sample_offsets, const int64_t* h_tables, int64_t num_ids,
+                                            const wrs_build_opts* opts, wrs_alias_row* d_table, uint64_t seed,
+                                            uint64_t counter_base, uint32_t* d_out, void* d_scratch,
+                                            size_t scratch_bytes, void* stream) {
+    if (!d_w || !h_offsets || !h_sample_offsets || !h_tables || num_ids < 0 || !d_table || !d_scratch)
+        return WRS_ERR_INVALID_ARGUMENT;
+    for (int64_t i = 0; i < num_ids; ++i) {
+        const int64_t t = h_tables[i];
+        const int64_t off = h_offsets[t], n = h_offsets[t + 1] - off;
+        const int64_t s0 = h_sample_offsets[t], cnt = h_sample_offsets[t + 1] - s0;
+        if (n < 0 || cnt < 0) return WRS_ERR_INVALID_ARGUMENT;
+        if (n == 0) continue;
+        wrs_status st = wrs_alias_build_f32(d_w + off, n, opts, d_table + off, nullptr, d_scratch, scratch_bytes, stream);
+        if (st == WRS_SUCCESS && cnt > 0)
+            st = wrs_alias_sample(d_table + off, n, (uint64_t)cnt, seed, counter_base + (uint64_t)s0, nullptr,
+                                  d_out + s0, nullptr, stream);
+        if (st != WRS_SUCCESS) return st;
+    }
+    return WRS_SUCCESS;
+}
+
 extern "C" wrs_status wrs_batched_autotune(const float* d_w, const int64_t* d_offsets, const int64_t* h_offsets,
                                            int64_t num_tables, wrs_alias_row* d_table, void* d_scratch,
                                            size_t scratch_bytes, wrs_build_opts* opts, void* stream_) {

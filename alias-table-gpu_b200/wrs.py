@@ -87,6 +87,7 @@ _SIGNATURES = {
     "wrs_batched_build_f32": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P, _SZ, _P]),
     "wrs_batched_sample": (ctypes.c_int, [_P, _P, _I64, _P, _U64, _U64, _U64, _P, _P]),
     "wrs_batched_build_sample_scratch_bytes": (_SZ, [_P, _I64, _P]),
+    "wrs_batched_per_table": (ctypes.c_int, [_P, _P, _P, _P, _I64, _P, _P, _U64, _U64, _P, _P, _SZ, _P]),
     "wrs_batched_build_sample": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P, _U64, _U64, _U64, _P, _P, _SZ,
                                                 _P]),
     "wrs_batched_autotune": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _SZ, _P, _P]),
@@ -353,6 +354,19 @@ def batched_build_sample(w, d_offsets, h_offsets, table, d_sample_offsets, total
                                           _ptr(d_sample_offsets), total, seed & (2**64 - 1),
                                           counter_base & (2**64 - 1), _ptr(out), _ptr(scratch),
                                           scratch.numel() * scratch.element_size(), _stream(stream))
+
+
+def batched_per_table(w, h_offsets, h_sample_offsets, tables, table, seed: int, out, scratch,
+                      opts: Optional[BuildOpts] = None, counter_base: int = 0, stream=None) -> int:
+    """The one-table-per-launch form of a batch (a native loop of single-table build and
+    sample calls over the table ids `tables`), for comparison with the batched calls."""
+    h = _host_i64(h_offsets)
+    hs = _host_i64(h_sample_offsets)
+    ids = _host_i64(tables)
+    return lib().wrs_batched_per_table(_ptr(w), h.ctypes.data, hs.ctypes.data, ids.ctypes.data, ids.size,
+                                       ctypes.byref(opts) if opts else None, _ptr(table), seed & (2**64 - 1),
+                                       counter_base & (2**64 - 1), _ptr(out), _ptr(scratch),
+                                       scratch.numel() * scratch.element_size(), _stream(stream))
 
 
 def batched_autotune(w, d_offsets, h_offsets, table, scratch, opts: BuildOpts, stream=None) -> int:

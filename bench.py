@@ -852,24 +852,19 @@ def batched_phase(dev, make=batch_config4, mixed: bool = False, shape: str = "")
         batched_wall_ms = (time.perf_counter() - t0) * 1e3 / reps
 
     # per-table launches: build + the table's samples, one call each, per size class
-    L = wrs.lib()
-    sp = torch.cuda.current_stream(dev).cuda_stream
     per_ms = per_wall_ms = 0.0
     timed = []
+    per_equal = True
     for grp, cls in per_table_groups:
         big = int(sizes[grp].max())
-        cmax = int(counts[grp].max())
-        tbl1 = torch.empty(big, dtype=torch.int64, device=dev)
         scr1 = torch.empty(wrs.alias_build_scratch_bytes(big), dtype=torch.uint8, device=dev)
-        out1 = torch.empty(max(1, cmax), dtype=torch.int32, device=dev)
-        wp, tp, sc, op = w.data_ptr(), tbl1.data_ptr(), scr1.data_ptr(), out1.data_ptr()
-        nbytes = scr1.numel()
+        tbl_p = torch.zeros_like(table)
+        out_p = torch.zeros_like(out)
 
-        def per_table(ts):
-            for t in ts:
-                n_t = int(sizes[t])
-                L.wrs_alias_build_f32(wp + 4 * int(off[t]), n_t, None, tp, None, sc, nbytes, sp)
-                L.wrs_alias_sample(tp, n_t, int(counts[t]), SEED_SAMPLES, 0, None, op, None, sp)
+        def per_table(ts):  # wrs_batched_per_table: a native loop of one build and one sample call per table
+            st = wrs.batched_per_table(w, off, soff, ts, tbl_p, SEED_SAMPLES, out_p, scr1)
+            if st:
+                raise wrs.WrsError(st, "per-table loop")
 
         per_table(grp[:8])
         torch.cuda.synchronize()
@@ -878,6 +873,13 @@ def batched_phase(dev, make=batch_config4, mixed: bool = False, shape: str = "")
         per_table(grp)
         e1.record()
         torch.cuda.synchronize()
+        # the per-table launches give the batch's rows and samples for these tables
+        if not mixed:
+            rows_p = tbl_p.cpu().numpy().view(np.uint32).reshape(-1, 2)
+            out_pn, out_bn = out_p.cpu().numpy(), out.cpu().numpy()
+            for t in grp[:256]:
+                per_equal &= bool(np.array_equal(rows_p[off[t]:off[t + 1]], rows[off[t]:off[t + 1]]))
+                per_equal &= bool(np.array_equal(out_pn[soff[t]:soff[t + 1]], out_bn[soff[t]:soff[t + 1]]))
         scale = int(cls.sum()) / grp.size
         per_ms += e0.elapsed_time(e1) * scale
         per_wall_ms += (time.perf_counter() - t0) * 1e3 * scale
@@ -898,6 +900,8 @@ def batched_phase(dev, make=batch_config4, mixed: bool = False, shape: str = "")
         "batched_g_items_plus_samples_s": round((items + total) / (batched_ms * 1e-3) / 1e9, 3),
         "per_table_ms": round(per_ms, 2), "per_table_wall_ms": round(per_wall_ms, 2),
         "per_table_sample": "timed on " + ", ".join(timed) + " per size class, scaled by table count",
+        "per_table_path": "wrs_batched_per_table (native loop: wrs_alias_build_f32 + wrs_alias_sample per table)",
+        **({} if mixed else {"per_table_equal_to_batched": per_equal}),
         "speedup": round(per_ms / batched_ms, 1) if per_ms else None,
         "tables_equal_to_single_builds": f"{int(check.size) if exact else 0} of {int(check.size)} checked",
         **({"mixed": mixed_info} if mixed_info else {}),

@@ -262,6 +262,16 @@ WRS_API wrs_status wrs_batched_build_sample(const float* d_w, const int64_t* d_o
                                     const int64_t* d_sample_offsets, uint64_t total_samples,
                                     uint64_t seed, uint64_t counter_base, uint32_t* d_out,
                                     void* d_scratch, size_t scratch_bytes, void* stream);
+/* The one-table-per-launch form of a batch, for comparison with the batched calls: for each
+ * table t in h_tables[0 .. num_ids), one wrs_alias_build_f32 of its weights into its rows and
+ * one wrs_alias_sample of its h_sample_offsets[t+1] - h_sample_offsets[t] samples with
+ * counter_base + h_sample_offsets[t] (the same samples as the batched sampler), in order on
+ * `stream`. d_scratch must hold the single-table scratch of the largest of these tables. */
+WRS_API wrs_status wrs_batched_per_table(const float* d_w, const int64_t* h_offsets,
+                                 const int64_t* h_sample_offsets, const int64_t* h_tables,
+                                 int64_t num_ids, const wrs_build_opts* opts, wrs_alias_row* d_table,
+                                 uint64_t seed, uint64_t counter_base, uint32_t* d_out,
+                                 void* d_scratch, size_t scratch_bytes, void* stream);
 /* Times the batched build of this batch for every launch shape (small_table_items in
  * {32, 64, 128, 256, 512} x tile_items in {1024, 2048, 4096}) and writes the fastest into
  * *opts (method and flags are kept). Synchronous; it builds into d_table (the same rows every
