@@ -334,7 +334,7 @@ wrs_status launch_lists(const float* d_w, const int64_t* d_offsets, const uint8_
     }
     if constexpr (SPL > 2) {
         if (st == WRS_SUCCESS)
-            st = sampled(launch_small_class<SPL, 32>(d_w, d_offsets, sl, 5, d_table, d_W, status, ss[0]), 5, ss[0]);
+            st = sampled(launch_small_class<SPL, 32>(d_w, d_offsets, sl, 5, d_table, d_W, status, ss[2]), 5, ss[2]);
     }
     return st;
 }
@@ -571,21 +571,21 @@ extern "C" wrs_status wrs_batched_per_table(const float* d_w, const int64_t* h_o
     return WRS_SUCCESS;
 }
 
-extern "C" wrs_status wrs_batched_autotune(const float* d_w, const int64_t* d_offsets, const int64_t* h_offsets,
-                                           int64_t num_tables, wrs_alias_row* d_table, void* d_scratch,
-                                           size_t scratch_bytes, wrs_build_opts* opts, void* stream_) {
-    if (!opts || !d_w || !d_offsets || !h_offsets || !d_table || !d_scratch) return WRS_ERR_INVALID_ARGUMENT;
-    if (scratch_bytes < wrs_batched_build_scratch_bytes(h_offsets, num_tables, nullptr))
-        return WRS_ERR_SCRATCH_TOO_SMALL;
-    cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+namespace wrs {
+namespace {
+
+// Times every launch shape of this batch's build (with `sa`, of its build and sample) and writes
+// the fastest into *opts. Every shape is captured into a graph and its launches timed, so that
+// the host's planning (a pass over the offsets per call) stays out of the device time.
+wrs_status autotune_shapes(const float* d_w, const int64_t* d_offsets, const int64_t* h_offsets, int64_t num_tables,
+                           wrs_alias_row* d_table, void* d_scratch, size_t scratch_bytes, wrs_build_opts* opts,
+                           cudaStream_t stream, const SampleArgs* sa) {
     cudaEvent_t e0, e1;
     if (cudaEventCreate(&e0) != cudaSuccess) return WRS_ERR_CUDA;
     if (cudaEventCreate(&e1) != cudaSuccess) {
         cudaEventDestroy(e0);
         return WRS_ERR_CUDA;
     }
-    // every shape is captured into a graph and its launches timed, so that the host's planning
-    // (a pass over the offsets per call) stays out of the device time
     float best_ms = 1e30f;
     Shape best{kDefaultSmall, 2048};
     wrs_status result = WRS_SUCCESS;
@@ -606,7 +606,7 @@ extern "C" wrs_status wrs_batched_autotune(const float* d_w, const int64_t* d_of
                 break;
             }
             st = batched_build(d_w, d_offsets, h_offsets, num_tables, sh, d_table, nullptr, d_scratch, scratch_bytes,
-                               cap, &L);
+                               cap, &L, nullptr, nullptr, nullptr, sa);
             if (cudaStreamEndCapture(cap, &graph) != cudaSuccess && st == WRS_SUCCESS) st = WRS_ERR_CUDA;
             if (st == WRS_SUCCESS && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) st = WRS_ERR_CUDA;
             float ms_min = 1e30f;
@@ -641,6 +641,34 @@ extern "C" wrs_status wrs_batched_autotune(const float* d_w, const int64_t* d_of
     opts->small_table_items = best.small_max;
     opts->tile_items = best.tile;
     return WRS_SUCCESS;
+}
+
+}  // namespace
+}  // namespace wrs
+
+extern "C" wrs_status wrs_batched_autotune(const float* d_w, const int64_t* d_offsets, const int64_t* h_offsets,
+                                           int64_t num_tables, wrs_alias_row* d_table, void* d_scratch,
+                                           size_t scratch_bytes, wrs_build_opts* opts, void* stream_) {
+    if (!opts || !d_w || !d_offsets || !h_offsets || !d_table || !d_scratch) return WRS_ERR_INVALID_ARGUMENT;
+    if (scratch_bytes < wrs_batched_build_scratch_bytes(h_offsets, num_tables, nullptr))
+        return WRS_ERR_SCRATCH_TOO_SMALL;
+    return autotune_shapes(d_w, d_offsets, h_offsets, num_tables, d_table, d_scratch, scratch_bytes, opts,
+                           static_cast<cudaStream_t>(stream_), nullptr);
+}
+
+extern "C" wrs_status wrs_batched_autotune_build_sample(const float* d_w, const int64_t* d_offsets,
+                                                        const int64_t* h_offsets, int64_t num_tables,
+                                                        wrs_alias_row* d_table, const int64_t* d_sample_offsets,
+                                                        uint64_t total_samples, uint32_t* d_out, void* d_scratch,
+                                                        size_t scratch_bytes, wrs_build_opts* opts, void* stream_) {
+    if (!opts || !d_w || !d_offsets || !h_offsets || !d_table || !d_scratch || !d_sample_offsets ||
+        (total_samples > 0 && !d_out))
+        return WRS_ERR_INVALID_ARGUMENT;
+    if (scratch_bytes < wrs_batched_build_sample_scratch_bytes(h_offsets, num_tables, nullptr))
+        return WRS_ERR_SCRATCH_TOO_SMALL;
+    const SampleArgs sa{d_sample_offsets, total_samples, 0, 0, d_out};
+    return autotune_shapes(d_w, d_offsets, h_offsets, num_tables, d_table, d_scratch, scratch_bytes, opts,
+                           static_cast<cudaStream_t>(stream_), &sa);
 }
 
 // ---------------------------------------------------------------- mixed batches

@@ -88,6 +88,7 @@ _SIGNATURES = {
     "wrs_batched_sample": (ctypes.c_int, [_P, _P, _I64, _P, _U64, _U64, _U64, _P, _P]),
     "wrs_batched_build_sample_scratch_bytes": (_SZ, [_P, _I64, _P]),
     "wrs_batched_per_table": (ctypes.c_int, [_P, _P, _P, _P, _I64, _P, _P, _U64, _U64, _P, _P, _SZ, _P]),
+    "wrs_batched_autotune_build_sample": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _U64, _P, _P, _SZ, _P, _P]),
     "wrs_batched_build_sample": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P, _U64, _U64, _U64, _P, _P, _SZ,
                                                 _P]),
     "wrs_batched_autotune": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _SZ, _P, _P]),
@@ -367,6 +368,16 @@ def batched_per_table(w, h_offsets, h_sample_offsets, tables, table, seed: int, 
                                        ctypes.byref(opts) if opts else None, _ptr(table), seed & (2**64 - 1),
                                        counter_base & (2**64 - 1), _ptr(out), _ptr(scratch),
                                        scratch.numel() * scratch.element_size(), _stream(stream))
+
+
+def batched_autotune_build_sample(w, d_offsets, h_offsets, table, d_sample_offsets, total: int, out, scratch,
+                                  opts: BuildOpts, stream=None) -> int:
+    """Times every launch shape of batched_build_sample on this batch and stores the fastest in `opts`."""
+    h = _host_i64(h_offsets)
+    return lib().wrs_batched_autotune_build_sample(_ptr(w), _ptr(d_offsets), h.ctypes.data, h.shape[0] - 1,
+                                                   _ptr(table), _ptr(d_sample_offsets), total, _ptr(out),
+                                                   _ptr(scratch), scratch.numel() * scratch.element_size(),
+                                                   ctypes.byref(opts), _stream(stream))
 
 
 def batched_autotune(w, d_offsets, h_offsets, table, scratch, opts: BuildOpts, stream=None) -> int:

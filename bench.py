@@ -719,7 +719,8 @@ def batched_phase(dev, make=batch_config4, mixed: bool = False, shape: str = "")
         opts = wrs.build_opts(0, tile, False, small)
     else:
         opts = wrs.build_opts()
-        st = wrs.batched_autotune(w, d_off, off, table, scratch, opts)
+        st = (wrs.batched_autotune(w, d_off, off, table, scratch, opts) if mixed else
+              wrs.batched_autotune_build_sample(w, d_off, off, table, d_soff, total, out, scratch, opts))
         if st:
             raise wrs.WrsError(st, "batched autotune")
     # the batch's rows equal single-table builds of the same weights (a sample of tables,

@@ -280,6 +280,15 @@ WRS_API wrs_status wrs_batched_autotune(const float* d_w, const int64_t* d_offse
                                 int64_t num_tables, wrs_alias_row* d_table, void* d_scratch,
                                 size_t scratch_bytes, wrs_build_opts* opts, void* stream);
 
+/* The same search for wrs_batched_build_sample: every shape's build and sample call is timed
+ * (samples with seed 0 into d_out). d_scratch must hold the opts == NULL scratch query of
+ * wrs_batched_build_sample_scratch_bytes. */
+WRS_API wrs_status wrs_batched_autotune_build_sample(const float* d_w, const int64_t* d_offsets,
+                                             const int64_t* h_offsets, int64_t num_tables,
+                                             wrs_alias_row* d_table, const int64_t* d_sample_offsets,
+                                             uint64_t total_samples, uint32_t* d_out, void* d_scratch,
+                                             size_t scratch_bytes, wrs_build_opts* opts, void* stream);
+
 /* ---- mixed batches: alias or rejection per table ----------------------- */
 
 /* Method of each table of a mixed batch, one byte per table (d_kinds in device memory,

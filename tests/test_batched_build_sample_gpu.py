@@ -125,3 +125,23 @@ def test_build_sample_reports_bad_total(cuda):
     scratch = alloc_scratch(wrs.batched_build_sample_scratch_bytes(off, opts))
     st = wrs.batched_build_sample(to_dev(w), to_dev(off), off, table, to_dev(soff), 40, 5, out, scratch, opts)
     assert st == wrs.WRS_ERR_INVALID_ARGUMENT
+
+
+def test_build_sample_autotune(cuda):
+    sizes = zipf_sizes(2048, 2.0, 2, 1 << 14, seed=81)
+    w, off = make_batch(sizes, seed=82, kinds=("uniform",))
+    counts = counts_for(off[1:] - off[:-1], "fixed64", seed=83)
+    soff = np.zeros(counts.size + 1, dtype=np.int64)
+    np.cumsum(counts, out=soff[1:])
+    total = int(soff[-1])
+    table = torch.empty(w.size, dtype=torch.int64, device="cuda")
+    out = torch.empty(total, dtype=torch.int32, device="cuda")
+    scratch = alloc_scratch(wrs.batched_build_sample_scratch_bytes(off, None))
+    opts = wrs.build_opts()
+    st = wrs.batched_autotune_build_sample(to_dev(w), to_dev(off), off, table, to_dev(soff), total, out, scratch, opts)
+    assert st == wrs.WRS_SUCCESS, wrs.status_string(st)
+    assert opts.small_table_items in (32, 64, 128, 256, 512) and opts.tile_items in (1024, 2048, 4096)
+    st, rows, rows2, got, soff2, seed, cbase = run_both(w, off, counts, opts.small_table_items, opts.tile_items)
+    assert st == wrs.WRS_SUCCESS
+    assert np.array_equal(rows, rows2)
+    assert np.array_equal(got, po.batched_sample(rows, off, soff2, seed, cbase))
