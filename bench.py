@@ -926,8 +926,8 @@ def batched_phase(dev, make=batch_config4, mixed: bool = False, shape: str = "")
 
 
 def batched_once(args, dev) -> dict:
-    """One batched build and one batched sampling call of configuration 4 or 5 with a fixed
-    launch shape (alias tables only), for profiler captures."""
+    """One wrs_batched_build_sample call (the config 4 step) of configuration 4 or 5 with a
+    fixed launch shape (alias tables only), for profiler captures."""
     import torch
     import wrs
     sizes, w_np, counts, what, _ = (batch_config5 if args.config == "5" else batch_config4)()
@@ -942,9 +942,8 @@ def batched_once(args, dev) -> dict:
     d_off, d_soff = torch.from_numpy(off).to(dev), torch.from_numpy(soff).to(dev)
     table = torch.empty(int(off[-1]), dtype=torch.int64, device=dev)
     out = torch.empty(int(soff[-1]), dtype=torch.int32, device=dev)
-    scratch = torch.empty(wrs.batched_build_scratch_bytes(off, opts), dtype=torch.uint8, device=dev)
-    st = wrs.batched_build(w, d_off, off, table, scratch, opts)
-    st = st or wrs.batched_sample(table, d_off, nt, d_soff, int(soff[-1]), SEED_SAMPLES, out, 0)
+    scratch = torch.empty(wrs.batched_build_sample_scratch_bytes(off, opts), dtype=torch.uint8, device=dev)
+    st = wrs.batched_build_sample(w, d_off, off, table, d_soff, int(soff[-1]), SEED_SAMPLES, out, scratch, opts)
     torch.cuda.synchronize()
     if st:
         raise wrs.WrsError(st, "batched once")
