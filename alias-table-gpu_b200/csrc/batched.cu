@@ -20,18 +20,23 @@ namespace {
 
 constexpr uint32_t kDefaultSmall = 128;
 
-// The library's side streams of the current device (created on first use): the small tables
-// of a batch are built there, by size class, while `stream` runs the tiled passes.
+// The library's side streams of the current device (created on first use): the listed tables
+// of a batch are built and sampled on the first kSideStreams - 1, by size class, at the lowest
+// stream priority; the tiled passes run on the last one, at the highest priority, so that their
+// short grids (the longest chain of the call) get SMs first as the list kernels' CTAs retire.
 constexpr int kMaxDevices = 64;
-constexpr int kSideStreams = 4;
+constexpr int kSideStreams = 5;
 std::mutex g_side_mu;
 cudaStream_t g_side[kMaxDevices][kSideStreams] = {};
 wrs_status side_streams(cudaStream_t (&out)[kSideStreams]) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return WRS_ERR_CUDA;
     std::lock_guard<std::mutex> lock(g_side_mu);
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
     for (int k = 0; k < kSideStreams; ++k) {
-        if (!g_side[dev][k] && cudaStreamCreateWithFlags(&g_side[dev][k], cudaStreamNonBlocking) != cudaSuccess) {
+        if (!g_side[dev][k] && cudaStreamCreateWithPriority(&g_side[dev][k], cudaStreamNonBlocking,
+                                                            k == kSideStreams - 1 ? greatest : least) != cudaSuccess) {
             g_side[dev][k] = nullptr;
             return WRS_ERR_CUDA;
         }
@@ -309,7 +314,7 @@ wrs_status launch_lists(const float* d_w, const int64_t* d_offsets, const uint8_
     wrs_status st = launch_status();
     if (st != WRS_SUCCESS) return st;
     if (cudaEventRecord(f.mid, ss[0]) != cudaSuccess) return WRS_ERR_CUDA;
-    for (int k = 1; k < kSideStreams; ++k)
+    for (int k = 1; k < kSideStreams - 1; ++k)  // the list streams (the last one runs the tiled passes)
         if (cudaStreamWaitEvent(ss[k], f.mid, 0) != cudaSuccess) return WRS_ERR_CUDA;
     // each list's samples (build and sample) right after the list, on the same stream
     auto sampled = [&](wrs_status s2, int cls, cudaStream_t strm) {
@@ -428,10 +433,11 @@ wrs_status batched_build(const float* d_w, const int64_t* d_offsets, const int64
         }
     }
     if (st == WRS_SUCCESS && p.big_tables > 0) {
+        const cudaStream_t bs = lists ? f.side[kSideStreams - 1] : stream;
         switch (sh.tile) {
-            case 1024: st = launch_big<1024>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, stream); break;
-            case 4096: st = launch_big<4096>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, stream); break;
-            default: st = launch_big<2048>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, stream); break;
+            case 1024: st = launch_big<1024>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, bs); break;
+            case 4096: st = launch_big<4096>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, bs); break;
+            default: st = launch_big<2048>(d_w, d_offsets, d_kinds, num_tables, d_table, d_W, L, p, bs); break;
         }
     }
     if (f.end(stream) != WRS_SUCCESS && st == WRS_SUCCESS) st = WRS_ERR_CUDA;
