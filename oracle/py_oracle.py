@@ -112,6 +112,7 @@ def ref_gpu() -> ctypes.CDLL:
             "ref_gpu_do_sample_soa": (_I, [_P, _P, _I, _D, _P, _P, _I]),
             "ref_gpu_rejection_build": (_I, [_P, _I, _D, _P, ctypes.c_longlong, _P]),
             "ref_gpu_rejection_fraction": (_I, [_P, _I, _D, _P]),
+            "ref_gpu_sample_timed": (_I, [_P, _P, _I, _D, _I, _I, ctypes.c_longlong, ctypes.c_ulonglong, _P, _P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)

@@ -17,6 +17,12 @@
  *    through cub::DeviceScan::InclusiveSum) and fillABinarySearch
  *    (RejectionSamplingBinarySearch.cu:12-37), with the weight total W given by the caller
  *    (the reference's build() sums it on the host first, SamplingAlgorithm.cu:14-19).
+ *  - ref_gpu_sample_timed: the reference's plain GPU sampling as its benchmark kernel draws it
+ *    (sampleBenchmarkBasic, SamplerGpuBasic.cu:77-101): a curand XORWOW generator per thread
+ *    (XorWowPrng, utils/Prng.cuh:58-94, seeded with a fixed seed and the thread number) and
+ *    doSample<ArrayOfStructs> on the reference's 16-byte rows, in a harness loop of a fixed
+ *    trip count. The benchmark kernel itself is not run: its closing `while (dummy == 0)` loop
+ *    never ends in a thread that drew no sample once the asserts are compiled out.
  *  - ref_gpu_rejection_fraction: the first-slot acceptance expression of
  *    SamplerRejection::sample (sampling/rejectionSampling/SamplerRejection.cu:27), with the
  *    reference's own fracf, for every item; the sampler itself (an unbounded retry loop) is
@@ -66,6 +72,16 @@ __global__ void rejection_fraction(const double* __restrict__ weights, int N, do
 
 int blocks_for(int count, int threads) { return count / threads + 1; }
 
+__global__ void harness_sample(ArrayOfStructs table, int N, double W_N, long long per_thread,
+                               unsigned long long seed, unsigned int* sink) {
+    XorWowPrng random;
+    random.initGpu(blockIdx.x * blockDim.x + threadIdx.x, (long)seed);
+    unsigned int acc = 0;
+    for (long long i = 0; i < per_thread; ++i)
+        acc ^= (unsigned int)doSample<ArrayOfStructs>(table, W_N, N, random.next());
+    atomicXor(sink, acc);
+}
+
 }  // namespace
 
 extern "C" {
@@ -81,6 +97,39 @@ int ref_gpu_do_sample_aos(const double* d_weight, const int* d_alias, int n, dou
     if (m > 0) replay_do_sample<ArrayOfStructs><<<blocks_for(m, 256), 256>>>(table, W_N, n, d_u, d_out, m);
     cudaError_t e = cudaDeviceSynchronize();
     if (e == cudaSuccess) e = cudaGetLastError();
+    table.free();
+    return (int)e;
+}
+
+/* The reference's plain GPU sampling (see above) of blocks x threads x per_thread samples on a
+ * table given as device arrays (absolute row weight, alias; packed into its 16-byte AoS rows
+ * first), timed with CUDA events around the sampling kernel alone (generator set-up included, as
+ * in the reference's benchmark). *ms gets the time, *checksum the XOR of all samples. */
+int ref_gpu_sample_timed(const double* d_weight, const int* d_alias, int n, double W_N, int blocks, int threads,
+                         long long per_thread, unsigned long long seed, float* ms, unsigned int* checksum) {
+    if (n < 1 || blocks < 1 || threads < 1 || threads > 1024 || per_thread < 0 || !ms || !checksum)
+        return (int)cudaErrorInvalidValue;
+    ArrayOfStructs table(DEVICE);
+    table.malloc((size_t)n);
+    fill_aos<<<blocks_for(n, 256), 256>>>(table, d_weight, d_alias, n);
+    unsigned int* sink = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaMalloc(&sink, sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMemset(sink, 0, sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e == cudaSuccess) {
+        cudaEventRecord(e0);
+        harness_sample<<<blocks, threads>>>(table, n, W_N, per_thread, seed, sink);
+        cudaEventRecord(e1);
+        e = cudaEventSynchronize(e1);
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaEventElapsedTime(ms, e0, e1);
+    if (e == cudaSuccess) e = cudaMemcpy(checksum, sink, sizeof(unsigned int), cudaMemcpyDeviceToHost);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (sink) cudaFree(sink);
     table.free();
     return (int)e;
 }

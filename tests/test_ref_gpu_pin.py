@@ -181,3 +181,22 @@ def check_fractions(w, W, frac, frac_ref):
     near_int = np.abs(x - np.round(x)) <= tol
     assert np.all(d[~wrapped] <= tol[~wrapped]), f"max excess {np.max(d[~wrapped] - tol[~wrapped]):.3g}"
     assert np.all(near_int[wrapped])
+
+
+def test_reference_sampling_harness_runs(ref_gpu):
+    """The timing harness over the reference's XORWOW generator and doSample (used by
+    oracle/ref_gpu_bench.py) runs on an exported table and returns only row indices (their XOR
+    stays below n = 2^12)."""
+    n = 1 << 12
+    st, rows, W = gpu_build(gen("uniform", n))
+    assert st == 0
+    table = torch.from_numpy(rows.view(np.int64).reshape(-1)).cuda()
+    weight = torch.zeros(n, dtype=torch.float64, device="cuda")
+    alias = torch.zeros(n, dtype=torch.int32, device="cuda")
+    assert wrs.export_reference_table(table, float(n), weight, alias) == wrs.WRS_SUCCESS
+    torch.cuda.synchronize()
+    ms, chk = np.zeros(1, np.float32), np.zeros(1, np.uint32)
+    rc = ref_gpu.ref_gpu_sample_timed(weight.data_ptr(), alias.data_ptr(), n, 1.0, 4, 64, 16, 7,
+                                      ms.ctypes.data, chk.ctypes.data)
+    assert rc == 0 and ms[0] > 0
+    assert int(chk[0]) < (1 << 12)  # an XOR of row indices below 2^12
