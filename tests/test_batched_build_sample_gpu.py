@@ -145,3 +145,33 @@ def test_build_sample_autotune(cuda):
     assert st == wrs.WRS_SUCCESS
     assert np.array_equal(rows, rows2)
     assert np.array_equal(got, po.batched_sample(rows, off, soff2, seed, cbase))
+
+
+# every size-class boundary of the lists: lane groups of 2/4/8/16 lanes, a warp with two items
+# a lane, a warp up to small_max, CTAs of 256 / 1024 threads, the tiled passes
+LIST_EDGES = [1, 2, 4, 5, 8, 9, 16, 17, 32, 33, 64, 65, 128, 129, 256, 257, 512, 513, 2047, 2048, 2049,
+              8191, 8192, 8193, 16385]
+
+
+@pytest.mark.parametrize("small", [32, 64, 256, 512])
+def test_build_sample_list_boundaries(cuda, small):
+    w, off = make_batch(LIST_EDGES + LIST_EDGES[::-1], seed=91)
+    counts = counts_for(off[1:] - off[:-1], "few", seed=92)
+    st, rows, rows2, got, soff, seed, cbase = run_both(w, off, counts, small, 1024)
+    assert st == wrs.WRS_SUCCESS, wrs.status_string(st)
+    assert np.array_equal(rows, rows2)
+    ref, _, _ = po.batched_build(w, off)
+    assert np.array_equal(rows, ref)
+    assert np.array_equal(got, po.batched_sample(rows, off, soff, seed, cbase))
+
+
+def test_build_sample_single_table_and_all_spilled(cuda):
+    """One table with many samples (spilled to the chunked sampler), and a batch whose every
+    table has more samples than a list sampler takes."""
+    for sizes, cnt in (([700], 100_000), ([3, 40, 500, 3000], 3000)):
+        w, off = make_batch(sizes, seed=93)
+        counts = np.full(len(sizes), cnt, dtype=np.int64)
+        st, rows, rows2, got, soff, seed, cbase = run_both(w, off, counts, 128, 2048)
+        assert st == wrs.WRS_SUCCESS, wrs.status_string(st)
+        assert np.array_equal(rows, rows2)
+        assert np.array_equal(got, po.batched_sample(rows, off, soff, seed, cbase))
