@@ -353,26 +353,42 @@ wrs_status launch_big(const float* d_w, const int64_t* d_offsets, const uint8_t*
     const uint32_t nblk = (uint32_t)((num_tables + kPlanBlock - 1) / kPlanBlock);
     const PlanCounts cap{p.big_tables, p.tiles, p.big_items};
     plan_count_kernel<<<nblk, kPlanBlock, 0, stream>>>(d_offsets, d_kinds, num_tables, big_min, T, L.blk);
-    plan_scan_kernel<<<1, kPlanBlock, 0, stream>>>(L.blk, nblk, cap, L.plan_status);
-    plan_fill_kernel<<<nblk, kPlanBlock, 0, stream>>>(d_offsets, d_kinds, num_tables, big_min, T, L.blk, cap,
-                                                      L.desc, L.tile_table);
+    // the kernels after plan_count are launched as programmatic dependents: each starts while its
+    // predecessor's last wave runs and waits for the predecessor's completion on entry
+    const auto ok = [](cudaError_t e) { return e == cudaSuccess; };
+    if (!ok(launch_pdl(plan_scan_kernel, dim3(1), dim3(kPlanBlock), 0, stream, L.blk, nblk, cap, L.plan_status)))
+        return WRS_ERR_CUDA;
+    if (!ok(launch_pdl(plan_fill_kernel, dim3(nblk), dim3(kPlanBlock), 0, stream, d_offsets, d_kinds, num_tables,
+                       big_min, (uint32_t)T, L.blk, cap, L.desc, L.tile_table)))
+        return WRS_ERR_CUDA;
     const TileMap map{L.tile_table, L.desc, L.plan_status, 0, 0};
     const uint32_t nt = p.tiles;
-    batch_wsum_kernel<T><<<nt, kBatchWsumThreads, 0, stream>>>(d_w, L.hdrs, L.partials, map, d_W);
-    tile_reduce_kernel<T, true><<<nt, kReduceThreads, 0, stream>>>(d_w, L.hdrs, L.agg, L.hmask, map);
-    batch_prefix_kernel<<<p.big_tables, kPrefixThreads, 0, stream>>>(L.hdrs, L.agg, L.incl, L.desc, L.plan_status);
-    heavy_list_kernel<T, true><<<(nt + heavy_warps(T) - 1) / heavy_warps(T), 32 * heavy_warps(T), 0, stream>>>(
-        d_w, L.hdrs, L.agg, L.incl, L.hmask, nt, L.heavy_item, L.heavy_E, map);
-    tile_link_kernel<true><<<(nt + p.big_tables + 255) / 256, 256, 0, stream>>>(L.hdrs, L.incl, nt, p.big_tables,
-                                                                               L.heavy_E, L.starts, map);
+    if (!ok(launch_pdl(batch_wsum_kernel<T>, dim3(nt), dim3(kBatchWsumThreads), 0, stream, d_w, L.hdrs, L.partials,
+                       map, d_W)))
+        return WRS_ERR_CUDA;
+    if (!ok(launch_pdl(tile_reduce_kernel<T, true>, dim3(nt), dim3(kReduceThreads), 0, stream, d_w, L.hdrs, L.agg,
+                       L.hmask, map)))
+        return WRS_ERR_CUDA;
+    if (!ok(launch_pdl(batch_prefix_kernel, dim3(p.big_tables), dim3(kPrefixThreads), 0, stream, L.hdrs, L.agg,
+                       L.incl, L.desc, L.plan_status)))
+        return WRS_ERR_CUDA;
+    if (!ok(launch_pdl(heavy_list_kernel<T, true>, dim3((nt + heavy_warps(T) - 1) / heavy_warps(T)),
+                       dim3(32 * heavy_warps(T)), 0, stream, d_w, L.hdrs, L.agg, L.incl, L.hmask, nt, L.heavy_item,
+                       L.heavy_E, map)))
+        return WRS_ERR_CUDA;
+    if (!ok(launch_pdl(tile_link_kernel<true>, dim3((nt + p.big_tables + 255) / 256), dim3(256), 0, stream, L.hdrs,
+                       L.incl, nt, p.big_tables, L.heavy_E, L.starts, map)))
+        return WRS_ERR_CUDA;
     const size_t smem = pack_smem_bytes(T);
     const cudaError_t e = cudaFuncSetAttribute(split_pack_kernel<NT, IPT, true, false>,
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return WRS_ERR_CUDA;
-    split_pack_kernel<NT, IPT, true, false><<<nt, NT, smem, stream>>>(d_w, L.hdrs, L.incl, L.starts, L.heavy_item,
-                                                                L.heavy_E, nt, d_table, map, nullptr, nullptr);
-    batch_status_kernel<<<(p.big_tables + 1 + 255) / 256, 256, 0, stream>>>(L.hdr0 + 1, p.big_tables + 1,
-                                                                           &L.hdr0->status);
+    if (!ok(launch_pdl(split_pack_kernel<NT, IPT, true, false>, dim3(nt), dim3(NT), smem, stream, d_w, L.hdrs, L.incl,
+                       L.starts, L.heavy_item, L.heavy_E, nt, d_table, map, nullptr, nullptr)))
+        return WRS_ERR_CUDA;
+    if (!ok(launch_pdl(batch_status_kernel, dim3((p.big_tables + 1 + 255) / 256), dim3(256), 0, stream, L.hdr0 + 1,
+                       p.big_tables + 1, &L.hdr0->status)))
+        return WRS_ERR_CUDA;
     return launch_status();
 }
 

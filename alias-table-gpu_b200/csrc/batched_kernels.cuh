@@ -95,6 +95,7 @@ __global__ void __launch_bounds__(kPlanBlock) plan_count_kernel(const int64_t* _
                                                                const uint8_t* kinds, int64_t num_tables,
                                                                uint32_t small_max,
                                                                uint32_t tile_items, PlanCounts* blk) {
+    pdl_enter();
     __shared__ PlanCounts s[32];
     int64_t n;
     const PlanCounts c =
@@ -108,6 +109,7 @@ __global__ void __launch_bounds__(kPlanBlock) plan_count_kernel(const int64_t* _
 // the totals against the host's plan.
 __global__ void __launch_bounds__(kPlanBlock) plan_scan_kernel(PlanCounts* blk, uint32_t num_blk, PlanCounts cap,
                                                               uint32_t* plan_status) {
+    pdl_enter();
     __shared__ PlanCounts s[32];
     PlanCounts carry{0u, 0u, 0ull};
     for (uint32_t c = 0; c < num_blk; c += kPlanBlock) {
@@ -127,6 +129,7 @@ __global__ void __launch_bounds__(kPlanBlock) plan_fill_kernel(const int64_t* __
                                                               uint32_t small_max,
                                                               uint32_t tile_items, const PlanCounts* blk,
                                                               PlanCounts cap, TableDesc* desc, uint32_t* tile_table) {
+    pdl_enter();
     __shared__ PlanCounts s[32];
     const int64_t t = (int64_t)blockIdx.x * kPlanBlock + threadIdx.x;
     int64_t n;
@@ -158,6 +161,7 @@ template <int T>
 __global__ void __launch_bounds__(kBatchWsumThreads) batch_wsum_kernel(const float* __restrict__ w,
                                                                        BuildHeader* hdrs, double2* partials,
                                                                        TileMap map, double* W_out) {
+    pdl_enter();
     constexpr int NT = kBatchWsumThreads;
     const uint32_t g = blockIdx.x;
     if (plan_failed<true>(map)) return;
@@ -237,6 +241,7 @@ __global__ void __launch_bounds__(kBatchWsumThreads) batch_wsum_kernel(const flo
 __global__ void __launch_bounds__(kPrefixThreads) batch_prefix_kernel(BuildHeader* hdrs, const TileVals* agg,
                                                                      TileVals* incl, const TableDesc* desc,
                                                                      const uint32_t* plan_status) {
+    pdl_enter();
     __shared__ PVals s_warp[kPrefixThreads / 32];
     if (__ldg(plan_status) != 0) return;
     const TableDesc d = desc[blockIdx.x];
@@ -296,6 +301,7 @@ __global__ void __launch_bounds__(kPrefixThreads) batch_prefix_kernel(BuildHeade
 
 // The first error of any large table's build (or of the plan) goes to the batch status word.
 __global__ void batch_status_kernel(const BuildHeader* hdrs, uint32_t num_tables, uint32_t* status) {
+    pdl_enter();
     for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < num_tables; b += gridDim.x * blockDim.x) {
         const uint32_t st = hdrs[b].status;
         if (st != 0) record_status(status, st);

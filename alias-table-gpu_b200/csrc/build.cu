@@ -152,17 +152,25 @@ wrs_status launch_split(const float* d_w, uint64_t n, wrs_alias_row* d_table, do
                                                                      reinterpret_cast<uint32_t*>(L.lb), zero_words,
                                                                      d_W);
     const WaitCfg wc = current_wait_cfg();
-    scan_kernel<S::SCAN_IPT><<<(uint32_t)L.num_groups, kScanThreads, 0, stream>>>(d_w, n, L.hdr, L.lb, nt, L.agg,
-                                                                                   L.heavy_item, L.heavy_E, wc);
-    tile_prefix_kernel<<<(uint32_t)L.num_blocks, kPrefixThreads, 0, stream>>>(L.hdr, L.agg, L.incl, L.blocks, nt, wc);
-    link_kernel<<<(nt + 1 + 255) / 256, 256, 0, stream>>>(L.hdr, L.incl, nt, L.heavy_E, L.starts);
+    // the kernels after wsum are launched as programmatic dependents: each starts while its
+    // predecessor's last wave runs and waits for the predecessor's completion on entry
+    if (launch_pdl(scan_kernel<S::SCAN_IPT>, dim3((uint32_t)L.num_groups), dim3(kScanThreads), 0, stream, d_w, n,
+                   L.hdr, L.lb, nt, L.agg, L.heavy_item, L.heavy_E, wc) != cudaSuccess)
+        return WRS_ERR_CUDA;
+    if (launch_pdl(tile_prefix_kernel, dim3((uint32_t)L.num_blocks), dim3(kPrefixThreads), 0, stream, L.hdr, L.agg,
+                   L.incl, L.blocks, nt, wc) != cudaSuccess)
+        return WRS_ERR_CUDA;
+    if (launch_pdl(link_kernel, dim3((nt + 1 + 255) / 256), dim3(256), 0, stream, L.hdr, L.incl, nt, L.heavy_E,
+                   L.starts) != cudaSuccess)
+        return WRS_ERR_CUDA;
     {
         const size_t smem = pack_walk_smem_bytes(T, S::IPT);
         if (cudaFuncSetAttribute(pack_walk_kernel<S::NT, S::IPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem) != cudaSuccess)
             return WRS_ERR_CUDA;
-        pack_walk_kernel<S::NT, S::IPT><<<nt, S::NT, smem, stream>>>(d_w, n, L.hdr, L.starts, L.heavy_item,
-                                                                      L.heavy_E, nt, d_table, L.chunk_list);
+        if (launch_pdl(pack_walk_kernel<S::NT, S::IPT>, dim3(nt), dim3(S::NT), smem, stream, d_w, n, L.hdr,
+                       L.starts, L.heavy_item, L.heavy_E, nt, d_table, L.chunk_list) != cudaSuccess)
+            return WRS_ERR_CUDA;
     }
     {
         constexpr int NT = PackShape<T>::NT, IPT = PackShape<T>::IPT;
@@ -173,8 +181,10 @@ wrs_status launch_split(const float* d_w, uint64_t n, wrs_alias_row* d_table, do
         const TileMap map{nullptr, nullptr, nullptr, n, nt};
         // the tiles pack_walk listed; a small grid, so that an empty list costs one short launch
         const uint32_t grid = std::min<uint32_t>(nt, (uint32_t)device_info().sm_count * 2u);
-        split_pack_kernel<NT, IPT, false, false, true><<<grid, NT, smem, stream>>>(
-            d_w, L.hdr, nullptr, L.starts, L.heavy_item, L.heavy_E, nt, d_table, map, nullptr, L.chunk_list);
+        if (launch_pdl(split_pack_kernel<NT, IPT, false, false, true>, dim3(grid), dim3(NT), smem, stream, d_w,
+                       L.hdr, nullptr, L.starts, L.heavy_item, L.heavy_E, nt, d_table, map, nullptr,
+                       L.chunk_list) != cudaSuccess)
+            return WRS_ERR_CUDA;
     }
     return launch_status();
 }
@@ -286,32 +296,43 @@ wrs_status launch_psa(const float* d_w, uint64_t n, wrs_alias_row* d_table, doub
                                                                      reinterpret_cast<uint32_t*>(L.blocks), zero_words,
                                                                      d_W);
     const TileMap map{nullptr, nullptr, nullptr, n, nt};
-    tile_reduce_kernel<T, false><<<nt, kReduceThreads, 0, stream>>>(d_w, L.hdr, L.agg, L.hmask, map);
+    // the kernels after wsum are programmatic dependents (launch_pdl)
+    const auto ok = [](cudaError_t e) { return e == cudaSuccess; };
+    if (!ok(launch_pdl(tile_reduce_kernel<T, false>, dim3(nt), dim3(kReduceThreads), 0, stream, d_w, L.hdr, L.agg,
+                       L.hmask, map)))
+        return WRS_ERR_CUDA;
     const WaitCfg wc = current_wait_cfg();
-    tile_prefix_kernel<<<(uint32_t)L.num_blocks, kPrefixThreads, 0, stream>>>(L.hdr, L.agg, L.incl, L.blocks, nt, wc);
+    if (!ok(launch_pdl(tile_prefix_kernel, dim3((uint32_t)L.num_blocks), dim3(kPrefixThreads), 0, stream, L.hdr, L.agg,
+                       L.incl, L.blocks, nt, wc)))
+        return WRS_ERR_CUDA;
     {
         const size_t smem = psa_local_smem_bytes(T);
         if (cudaFuncSetAttribute(psa_local_kernel<NT, IPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
             cudaSuccess)
             return WRS_ERR_CUDA;
-        psa_local_kernel<NT, IPT><<<nt, NT, smem, stream>>>(d_w, n, L.hdr, L.incl, d_table, L.slots, L.agg2, L.hdr2);
+        if (!ok(launch_pdl(psa_local_kernel<NT, IPT>, dim3(nt), dim3(NT), smem, stream, d_w, n, L.hdr, L.incl, d_table,
+                           L.slots, L.agg2, L.hdr2)))
+            return WRS_ERR_CUDA;
     }
-    tile_prefix_kernel<<<(uint32_t)L.num_blocks, kPrefixThreads, 0, stream>>>(L.hdr2, L.agg2, L.incl2, L.blocks2, nt,
-                                                                               wc);
-    psa_heavy_list_kernel<T><<<(nt + 3) / 4, 128, 0, stream>>>(L.hdr2, L.agg2, L.incl2, L.slots, nt, L.heavy_item2,
-                                                               L.heavy_E2);
-    tile_link_kernel<false><<<(nt + 1 + 255) / 256, 256, 0, stream>>>(L.hdr2, L.incl2, nt, 1u, L.heavy_E2, L.starts2,
-                                                                     map);
+    if (!ok(launch_pdl(tile_prefix_kernel, dim3((uint32_t)L.num_blocks), dim3(kPrefixThreads), 0, stream, L.hdr2,
+                       L.agg2, L.incl2, L.blocks2, nt, wc)))
+        return WRS_ERR_CUDA;
+    if (!ok(launch_pdl(psa_heavy_list_kernel<T>, dim3((nt + 3) / 4), dim3(128), 0, stream, L.hdr2, L.agg2, L.incl2,
+                       L.slots, nt, L.heavy_item2, L.heavy_E2)))
+        return WRS_ERR_CUDA;
+    if (!ok(launch_pdl(tile_link_kernel<false>, dim3((nt + 1 + 255) / 256), dim3(256), 0, stream, L.hdr2, L.incl2, nt,
+                       1u, L.heavy_E2, L.starts2, map)))
+        return WRS_ERR_CUDA;
     {
         const size_t smem = pack_smem_bytes(T);
         if (cudaFuncSetAttribute(split_pack_kernel<NT, IPT, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem) != cudaSuccess)
             return WRS_ERR_CUDA;
-        split_pack_kernel<NT, IPT, false, true><<<nt, NT, smem, stream>>>(d_w, L.hdr2, L.incl2, L.starts2,
-                                                                          L.heavy_item2, L.heavy_E2, nt, d_table, map,
-                                                                          L.slots, nullptr);
+        if (!ok(launch_pdl(split_pack_kernel<NT, IPT, false, true>, dim3(nt), dim3(NT), smem, stream, d_w, L.hdr2,
+                           L.incl2, L.starts2, L.heavy_item2, L.heavy_E2, nt, d_table, map, L.slots, nullptr)))
+            return WRS_ERR_CUDA;
     }
-    copy_status_kernel<<<1, 1, 0, stream>>>(L.hdr2, L.hdr);
+    if (!ok(launch_pdl(copy_status_kernel, dim3(1), dim3(1), 0, stream, L.hdr2, L.hdr))) return WRS_ERR_CUDA;
     return launch_status();
 }
 

@@ -254,6 +254,7 @@ __global__ void __launch_bounds__(BLOCK) wsum_kernel(const float* __restrict__ w
                                                      BuildHeader* hdr, double2* partials,
                                                      uint32_t* zero_words, uint64_t num_zero_words,
                                                      double* W_out) {
+    pdl_enter();
     const uint64_t gtid = (uint64_t)blockIdx.x * BLOCK + threadIdx.x;
     const uint64_t gsize = (uint64_t)gridDim.x * BLOCK;
     for (uint64_t i = gtid; i < num_zero_words; i += gsize) zero_words[i] = 0u;
@@ -612,6 +613,7 @@ template <int T, bool BATCH>
 __global__ void __launch_bounds__(kReduceThreads) tile_reduce_kernel(const float* __restrict__ w,
                                                                      const BuildHeader* hdr, TileVals* agg,
                                                                      uint32_t* __restrict__ hmask, TileMap map) {
+    pdl_enter();
     constexpr int IPT = T / kReduceThreads;
     constexpr int NW = kReduceThreads / 32;
     static_assert(IPT >= 4 && IPT <= 32 && (IPT & (IPT - 1)) == 0, "items per thread");
@@ -802,6 +804,7 @@ struct __align__(16) BlockWord {  // look-back record of one prefix CTA
 static __global__ void __launch_bounds__(kPrefixThreads) tile_prefix_kernel(BuildHeader* hdr, const TileVals* agg,
                                                                      TileVals* incl, BlockWord* blocks,
                                                                      uint32_t num_tiles, WaitCfg wc) {
+    pdl_enter();
     __shared__ uint32_t s_blk;
     __shared__ PVals s_warp[kPrefixThreads / 32 + 1];
     __shared__ PVals s_base;
@@ -1000,6 +1003,7 @@ __global__ void __launch_bounds__(32 * heavy_warps(T)) heavy_list_kernel(const f
                                                                       const uint32_t* __restrict__ hmask,
                                                                       uint32_t num_tiles, uint32_t* heavy_item,
                                                                       uint4* heavy_E, TileMap map) {
+    pdl_enter();
     constexpr int WPT = T / 32;    // mask words per tile
     constexpr int WPL = WPT / 32;  // sparse form: lane l owns tile items [l*32*WPL, (l+1)*32*WPL)
     static_assert(WPL >= 1 && WPL <= 4, "mask words per lane");
@@ -1142,6 +1146,7 @@ template <bool BATCH>
 __global__ void __launch_bounds__(256) tile_link_kernel(const BuildHeader* hdr, const TileVals* incl,
                                                         uint32_t num_tiles, uint32_t num_tables,
                                                         const uint4* heavy_E, TileStart* starts, TileMap map) {
+    pdl_enter();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (plan_failed<BATCH>(map)) return;
     TileRef tr;
@@ -1647,6 +1652,7 @@ __global__ void __launch_bounds__(NT, (NT == 256 && IPT == 8) ? 4 : 1) split_pac
                                                         wrs_alias_row* __restrict__ table, TileMap map,
                                                         const LeftSlot* __restrict__ left,
                                                         const uint32_t* __restrict__ tile_list) {
+    pdl_enter();
     if constexpr (E64) {
         const uint32_t count = min(__ldg(&hdr->chunk_count), num_tiles);
         for (uint32_t i = blockIdx.x; i < count; i += gridDim.x) {

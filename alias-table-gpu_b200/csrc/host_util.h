@@ -5,6 +5,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <utility>
+
 #include "wrs.h"
 #include "wrs_common.cuh"
 
@@ -29,6 +31,24 @@ inline wrs_status cuda_status(cudaError_t e) { return e == cudaSuccess ? WRS_SUC
 
 // Launch-error check after a kernel launch.
 inline wrs_status launch_status() { return cuda_status(cudaGetLastError()); }
+
+// A launch with programmatic stream serialisation (see pdl_enter): the kernel may be scheduled
+// before the previous kernel on `stream` has completed, and waits for it on the device.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                       Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // Synchronise `stream` and read a device status word.
 wrs_status read_device_status(const uint32_t* d_status, cudaStream_t stream);

@@ -42,6 +42,7 @@ __global__ void __launch_bounds__(NT) psa_local_kernel(const float* __restrict__
                                                        const BuildHeader* hdr, const TileVals* incl,
                                                        wrs_alias_row* __restrict__ table, LeftSlot* slots,
                                                        TileVals* agg2, BuildHeader* hdr2) {
+    pdl_enter();
     constexpr int T = NT * IPT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     u128* sHe = reinterpret_cast<u128*>(smem_raw);
@@ -286,6 +287,7 @@ __global__ void __launch_bounds__(128) psa_heavy_list_kernel(const BuildHeader* 
                                                              const TileVals* incl2, const LeftSlot* slots,
                                                              uint32_t num_tiles, uint32_t* heavy_item,
                                                              uint4* heavy_E) {
+    pdl_enter();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t u = blockIdx.x * 4 + warp;
     if (u >= num_tiles || earlier_status(hdr2) != 0) return;
@@ -310,6 +312,7 @@ __global__ void __launch_bounds__(128) psa_heavy_list_kernel(const BuildHeader* 
 
 // Copies the leftover passes' status into the build's header (read by wrs_scratch_status).
 __global__ void copy_status_kernel(const BuildHeader* from, BuildHeader* to) {
+    pdl_enter();
     const uint32_t st = from->status;
     if (st != 0) record_status(&to->status, st);
 }

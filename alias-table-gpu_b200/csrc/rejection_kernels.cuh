@@ -41,6 +41,7 @@ __global__ void __launch_bounds__(kBuildThreads) rejection_tile_kernel(
     const float* __restrict__ w, uint64_t n, BuildHeader* hdr, uint64_t* tile_words, uint32_t num_tiles,
     uint32_t* __restrict__ A, uint64_t a_capacity, float* __restrict__ frac, RejBigEntry* big_list,
     uint64_t big_capacity, uint64_t* a_size_out, WaitCfg wc) {
+    pdl_enter();
     constexpr int T = kBuildThreads * IPT;
     __shared__ uint32_t s_tile;
     __shared__ int s_abort;
@@ -248,6 +249,7 @@ __global__ void __launch_bounds__(256) rejection_big_kernel(BuildHeader* hdr, co
                                                             uint64_t big_capacity, uint32_t* __restrict__ A,
                                                             uint64_t a_capacity, uint32_t* huge_idx,
                                                             uint64_t huge_capacity) {
+    pdl_enter();
     const uint64_t cnt_raw = hdr->big_count;
     const uint64_t cnt = cnt_raw < big_capacity ? cnt_raw : big_capacity;
     if (cnt == 0) return;
@@ -276,6 +278,7 @@ constexpr uint32_t kRejChunk = 4096;
 __global__ void __launch_bounds__(256) rejection_huge_kernel(const BuildHeader* hdr, const RejBigEntry* big_list,
                                                              const uint32_t* huge_idx, uint64_t huge_capacity,
                                                              uint32_t* __restrict__ A, uint64_t a_capacity) {
+    pdl_enter();
     const uint64_t cnt_raw = hdr->huge_count;
     const uint64_t cnt = cnt_raw < huge_capacity ? cnt_raw : huge_capacity;
     for (uint64_t h = 0; h < cnt; ++h) {

@@ -182,14 +182,18 @@ extern "C" wrs_status wrs_rejection_build_f32(const float* d_w, int64_t n, uint3
     if (cudaMemsetAsync(L.hdr, 0, sizeof(BuildHeader), stream) != cudaSuccess) return WRS_ERR_CUDA;
     wsum_kernel<kWsumBlock><<<wsum_grid((uint64_t)n), kWsumBlock, 0, stream>>>(
         d_w, (uint64_t)n, L.hdr, L.partials, reinterpret_cast<uint32_t*>(L.tile_words), 2 * nt, d_W);
-    rejection_tile_kernel<kRejIpt><<<(uint32_t)nt, kBuildThreads, 0, stream>>>(
-        d_w, (uint64_t)n, L.hdr, L.tile_words, (uint32_t)nt, d_A, a_capacity, d_frac, L.big, L.big_capacity, d_A_size,
-        current_wait_cfg());
+    // the kernels after wsum are programmatic dependents (launch_pdl)
+    if (launch_pdl(rejection_tile_kernel<kRejIpt>, dim3((uint32_t)nt), dim3(kBuildThreads), 0, stream, d_w,
+                   (uint64_t)n, L.hdr, L.tile_words, (uint32_t)nt, d_A, a_capacity, d_frac, L.big, L.big_capacity,
+                   d_A_size, current_wait_cfg()) != cudaSuccess)
+        return WRS_ERR_CUDA;
     const DeviceInfo dev = device_info();
-    rejection_big_kernel<<<(uint32_t)dev.sm_count * 4, 256, 0, stream>>>(L.hdr, L.big, L.big_capacity, d_A, a_capacity,
-                                                                      L.huge, L.huge_capacity);
-    rejection_huge_kernel<<<(uint32_t)dev.sm_count * 4, 256, 0, stream>>>(L.hdr, L.big, L.huge, L.huge_capacity, d_A,
-                                                                       a_capacity);
+    if (launch_pdl(rejection_big_kernel, dim3((uint32_t)dev.sm_count * 4), dim3(256), 0, stream, L.hdr, L.big,
+                   L.big_capacity, d_A, a_capacity, L.huge, L.huge_capacity) != cudaSuccess)
+        return WRS_ERR_CUDA;
+    if (launch_pdl(rejection_huge_kernel, dim3((uint32_t)dev.sm_count * 4), dim3(256), 0, stream, L.hdr, L.big,
+                   L.huge, L.huge_capacity, d_A, a_capacity) != cudaSuccess)
+        return WRS_ERR_CUDA;
     const wrs_status st = launch_status();
     if (st != WRS_SUCCESS) return st;
     if (flags & WRS_FLAG_SYNC) return read_device_status(&L.hdr->status, stream);

@@ -176,6 +176,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(const float* __restr
                                                             LbWord* lb, uint32_t num_tiles, TileVals* agg,
                                                             uint32_t* __restrict__ heavy_item,
                                                             uint64_t* __restrict__ heavy_E, WaitCfg wc) {
+    pdl_enter();
     constexpr int NT = kScanThreads;
     constexpr int NW = NT / 32;
     constexpr int T = NT * IPT;
@@ -418,6 +419,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(const float* __restr
 // bound = 0 at b = 0 and the heavy count at b = num_tiles (which also goes to the header).
 __global__ void __launch_bounds__(256) link_kernel(BuildHeader* hdr, const TileVals* incl, uint32_t num_tiles,
                                                    const uint64_t* __restrict__ heavy_E, TileStart* starts) {
+    pdl_enter();
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b > num_tiles) return;
     if (earlier_status(hdr) != 0) return;
@@ -484,6 +486,7 @@ __global__ void __launch_bounds__(NT) pack_walk_kernel(const float* __restrict__
                                                        const uint32_t* __restrict__ heavy_item,
                                                        const uint64_t* __restrict__ heavy_E, uint32_t num_tiles,
                                                        wrs_alias_row* __restrict__ table, uint32_t* chunk_list) {
+    pdl_enter();
     constexpr int T = NT * IPT;
     constexpr int TS = T + T / IPT;
     constexpr int CW = walk_cap(T);

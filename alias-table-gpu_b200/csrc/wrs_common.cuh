@@ -233,6 +233,17 @@ __device__ __forceinline__ u128 shfl_xor_u128(u128 v, int mask) {
     return q_make(hi, lo);
 }
 
+// ---------------------------------------------------------------- programmatic dependent launch
+// A kernel of a build's chain is launched with programmatic stream serialisation (launch_pdl):
+// the launch is staged while the previous kernel runs, and the kernel's CTAs are scheduled as
+// the previous kernel's CTAs exit (no explicit trigger: one at the start of each kernel let the
+// dependents' CTAs sit on the SMs early and cost more than it saved). Every such kernel starts
+// with pdl_enter(), which waits until the previous kernel has completed and its writes are
+// visible (griddepcontrol.wait; immediate for a kernel launched without the attribute). Every
+// kernel of a chain waits before anything else, early exits included, so that the completion of
+// a kernel implies the completion of all kernels before it.
+__device__ __forceinline__ void pdl_enter() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // ---------------------------------------------------------------- bounded waits
 __device__ __forceinline__ uint64_t global_ns() {
     uint64_t t;
