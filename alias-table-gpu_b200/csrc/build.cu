@@ -42,6 +42,10 @@ DeviceInfo device_info() {
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
         d.smem_optin = (size_t)optin;
         if (d.sm_count <= 0) d.sm_count = 148;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.wsum_blocks_per_sm, wsum_kernel<kWsumBlock>, kWsumBlock,
+                                                          0) != cudaSuccess ||
+            d.wsum_blocks_per_sm < 1)
+            d.wsum_blocks_per_sm = 1;
         cache[dev] = d;
         have[dev] = true;
     }
@@ -60,7 +64,8 @@ wrs_status read_device_status(const uint32_t* d_status, cudaStream_t stream) {
 uint32_t wsum_grid(uint64_t n) {
     const DeviceInfo d = device_info();
     uint64_t g = (n + 2047) / 2048;
-    const uint64_t cap = (uint64_t)d.sm_count * 8;
+    // one wave: a second, partial wave of CTAs would run the tail at low occupancy
+    const uint64_t cap = (uint64_t)d.sm_count * (uint64_t)d.wsum_blocks_per_sm;
     if (g > cap) g = cap;
     if (g > kWsumMaxGrid) g = kWsumMaxGrid;
     if (g < 1) g = 1;

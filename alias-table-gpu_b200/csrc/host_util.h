@@ -22,6 +22,7 @@ struct DeviceInfo {
     int major;
     int minor;
     size_t smem_optin;
+    int wsum_blocks_per_sm;  // resident CTAs of the weight-total kernel per SM
 };
 
 // Cached per device ordinal.

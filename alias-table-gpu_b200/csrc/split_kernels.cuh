@@ -165,6 +165,12 @@ __device__ __forceinline__ void warp_scan_ce(uint32_t& c, uint64_t& e) {
         }
     }
 }
+// Warp sum of values below 2^51 by two 32-bit reductions (25-bit low parts, 26-bit high parts).
+__device__ __forceinline__ uint64_t warp_sum_u51(uint64_t v) {
+    const uint32_t lo = __reduce_add_sync(0xffffffffu, (uint32_t)v & ((1u << 25) - 1u));
+    const uint32_t hi = __reduce_add_sync(0xffffffffu, (uint32_t)(v >> 25));
+    return ((uint64_t)hi << 25) + lo;
+}
 __device__ __forceinline__ uint64_t warp_sum_u64x(uint64_t v) {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
@@ -189,8 +195,8 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(const float* __restr
     __shared__ uint64_t s_ws[U][NW];     // ... small-light deficits (Q16.48)
     __shared__ uint64_t s_wl[U][NW];     // ... large-light true deficits (Q16.48)
     __shared__ uint32_t s_hbits[U][NT];  // per tile and thread: heavy bits of its IPT items
-    __shared__ uint32_t s_hc[U][NT];     // ... exclusive heavy count within its warp
-    __shared__ uint64_t s_he[U][NT];     // ... exclusive heavy excess within its warp (Q40.24)
+    __shared__ uint32_t s_hc[U][NT];     // ... inclusive heavy count within its warp
+    __shared__ uint64_t s_he[U][NT];     // ... inclusive heavy excess within its warp (Q40.24)
     __shared__ uint32_t s_tc0[U + 1][NW];  // heavies before (tile, warp) within the group
     __shared__ uint64_t s_te0[U + 1][NW];  // ... their excess
     __shared__ uint64_t s_base_c, s_base_e;
@@ -277,10 +283,10 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(const float* __restr
         uint64_t ei = E;
         warp_scan_ce(ci, ei);
         s_hbits[u][threadIdx.x] = hbits;
-        s_hc[u][threadIdx.x] = ci - c;
-        s_he[u][threadIdx.x] = ei - E;
-        S = warp_sum_u64x(S);
-        L = warp_sum_u64x(L);
+        s_hc[u][threadIdx.x] = ci;
+        s_he[u][threadIdx.x] = ei;
+        S = warp_sum_u51(S);  // at most IPT deficits of at most 2^48 each
+        L = warp_sum_u51(L);
         if (lane == 31) {
             s_wc[u][warp] = ci;
             s_we[u][warp] = ei;
@@ -390,22 +396,26 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(const float* __restr
         }
     }
     __syncthreads();
-    // the heavies of the group's tiles at their global heavy index
+    // the heavies of the group's tiles at their global heavy index, each thread's from its last
+    // one back: the last one's excess end is the thread's inclusive prefix, an earlier one's the
+    // later one's minus the later one's excess (gathered again only for a thread with several)
     const uint64_t base_c = s_base_c, base_e = s_base_e;
     for (uint32_t u = 0; u < ntl; ++u) {
         const uint32_t hbits = s_hbits[u][threadIdx.x];
         if (hbits) {
             const uint64_t item0 = (uint64_t)(tile0 + u) * T + (uint64_t)threadIdx.x * IPT;
-            uint64_t g = base_c + s_tc0[u][warp] + s_hc[u][threadIdx.x];
+            uint64_t g = base_c + s_tc0[u][warp] + s_hc[u][threadIdx.x];  // one past the thread's last
             uint64_t er = base_e + s_te0[u][warp] + s_he[u][threadIdx.x];
-            for (uint32_t bits = hbits; bits; bits &= bits - 1) {
-                const int k = __ffs(bits) - 1;
-                er += rare_q(__ldg(w + item0 + k), true, cp);
+            for (uint32_t bits = hbits;;) {
+                const int k = 31 - __clz(bits);
+                --g;
                 if (g < n) {
                     heavy_item[g] = (uint32_t)(item0 + k);
                     heavy_E[g] = er;
                 }
-                ++g;
+                bits &= ~(1u << k);
+                if (!bits) break;
+                er -= rare_q(__ldg(w + item0 + k), true, cp);
             }
         }
     }
