@@ -21,6 +21,7 @@ namespace {
 constexpr int64_t kMaxItems = (int64_t)0x7fffffff - 8192;
 constexpr uint32_t kDefaultSection = 65536;
 constexpr size_t kStageMaxBytes = 96 * 1024;  // sections up to this size are staged in smem
+constexpr uint32_t kSectLargeRows = 32768;    // L2-form sections from this size draw 4 positions a step
 
 inline uint32_t seed_k0(uint64_t seed) { return (uint32_t)seed; }
 inline uint32_t seed_k1(uint64_t seed) { return (uint32_t)(seed >> 32); }
@@ -58,24 +59,29 @@ extern "C" wrs_status wrs_alias_sample(const wrs_alias_row* d_table, int64_t n, 
         const uint64_t K = ((uint64_t)n + S - 1) / S;
         const size_t sec_bytes = (size_t)S * sizeof(uint2);
         const bool stage = sec_bytes <= kStageMaxBytes && ((uintptr_t)d_table & 15u) == 0;
-        const uint32_t threads = 512;
+        const uint32_t threads = kSectThreads;
         if (stage) {
             const int per_sm = (int)(200 * 1024 / sec_bytes) < 4 ? (int)(200 * 1024 / sec_bytes) : 4;
             uint64_t grid = (uint64_t)dev.sm_count * (per_sm > 0 ? per_sm : 1);
             if (grid > K) grid = K;
-            cudaError_t e = cudaFuncSetAttribute(sample_sectioned_kernel<true>,
+            cudaError_t e = cudaFuncSetAttribute(sample_sectioned_kernel<true, 8>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sec_bytes);
             if (e != cudaSuccess) return WRS_ERR_CUDA;
-            sample_sectioned_kernel<true><<<(uint32_t)grid, threads, sec_bytes, stream>>>(
+            sample_sectioned_kernel<true, 8><<<(uint32_t)grid, threads, sec_bytes, stream>>>(
                 table, (uint32_t)n, num_samples, S, (uint32_t)K, seed_k0(seed), seed_k1(seed), counter_base, d_out,
                 d_section_counts);
         } else {
             // one CTA per SM: the sections in flight (SMs x section bytes) stay L2-resident
             uint64_t grid = (uint64_t)dev.sm_count;
             if (grid > K) grid = K;
-            sample_sectioned_kernel<false><<<(uint32_t)grid, threads, 0, stream>>>(
-                table, (uint32_t)n, num_samples, S, (uint32_t)K, seed_k0(seed), seed_k1(seed), counter_base, d_out,
-                d_section_counts);
+            if (S >= kSectLargeRows)
+                sample_sectioned_kernel<false, 4><<<(uint32_t)grid, threads, 0, stream>>>(
+                    table, (uint32_t)n, num_samples, S, (uint32_t)K, seed_k0(seed), seed_k1(seed), counter_base,
+                    d_out, d_section_counts);
+            else
+                sample_sectioned_kernel<false, 8><<<(uint32_t)grid, threads, 0, stream>>>(
+                    table, (uint32_t)n, num_samples, S, (uint32_t)K, seed_k0(seed), seed_k1(seed), counter_base,
+                    d_out, d_section_counts);
         }
     } else {
         return WRS_ERR_INVALID_ARGUMENT;
