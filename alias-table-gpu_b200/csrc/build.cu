@@ -165,7 +165,7 @@ wrs_status launch_split(const float* d_w, uint64_t n, wrs_alias_row* d_table, do
     if (launch_pdl(tile_prefix_kernel, dim3((uint32_t)L.num_blocks), dim3(kPrefixThreads), 0, stream, L.hdr, L.agg,
                    L.incl, L.blocks, nt, wc) != cudaSuccess)
         return WRS_ERR_CUDA;
-    if (launch_pdl(link_kernel, dim3((nt + 1 + 255) / 256), dim3(256), 0, stream, L.hdr, L.incl, nt, L.heavy_E,
+    if (launch_pdl(link_kernel, dim3(((nt + 1) * (uint32_t)kLinkLanes + 255) / 256), dim3(256), 0, stream, L.hdr, L.incl, nt, L.heavy_E,
                    L.starts) != cudaSuccess)
         return WRS_ERR_CUDA;
     {

@@ -422,40 +422,60 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(const float* __restr
 }
 
 // ---------------------------------------------------------------- link
-// One thread per tile boundary b (0 .. num_tiles): the start of the deficit line A_before(b)
-// and the base of its dithering from the tile prefixes (incl, tile_prefix_kernel), and
-// bound = #{heavies with corrected excess end <= A_before(b)} by a binary search of the heavy
-// list (the reference's split search at tile granularity, SplitMethodBasic.cu:14-50), with
-// bound = 0 at b = 0 and the heavy count at b = num_tiles (which also goes to the header).
+// A group of kLinkLanes lanes per tile boundary b (0 .. num_tiles): the start of the deficit
+// line A_before(b) and the base of its dithering from the tile prefixes (incl, tile_prefix_kernel),
+// and bound = #{heavies with corrected excess end <= A_before(b)} by a (kLinkLanes + 1)-ary search
+// of the heavy list (the reference's split search at tile granularity, SplitMethodBasic.cu:14-50):
+// each step tests kLinkLanes pivots at once, one L2 round trip, so a search over 2^21 heavies takes
+// 7 round trips instead of 21. bound = 0 at b = 0 and the heavy count at b = num_tiles (which also
+// goes to the header). The interval shrinks at every step whatever the list holds, so the loop ends
+// on any input.
+constexpr int kLinkLanes = 8;
 __global__ void __launch_bounds__(256) link_kernel(BuildHeader* hdr, const TileVals* incl, uint32_t num_tiles,
                                                    const uint64_t* __restrict__ heavy_E, TileStart* starts) {
     pdl_enter();
-    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b > num_tiles) return;
-    if (earlier_status(hdr) != 0) return;
+    constexpr uint32_t G = kLinkLanes;
+    static_assert(32 % G == 0, "lane groups");
+    if (earlier_status(hdr) != 0) return;  // the same for every thread
+    const uint32_t b = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const uint32_t j = threadIdx.x % G;
+    const uint32_t gfirst = (threadIdx.x & 31u) & ~(G - 1);  // the group's first lane in the warp
+    const bool active = b <= num_tiles;
     const uint32_t nH = __ldg(&incl[num_tiles - 1].nH);
     const int64_t nfix = __ldg(&hdr->nfix);
-    const TileVals pv = b ? ldcg_tilevals(incl + b - 1) : tv_zero();
+    const TileVals pv = (active && b) ? ldcg_tilevals(incl + b - 1) : tv_zero();
     const u128 X = deficit_line(pv);
-    uint32_t g;
-    if (b == 0) {
-        g = 0;
-    } else if (b == num_tiles) {
-        g = nH;
-        hdr->nH_total = nH;
-    } else {
-        uint32_t lo = 0, hi = nH;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (corrected_end(__ldg(heavy_E + mid), nfix) <= X) lo = mid + 1; else hi = mid;
+    // the bound lies in [lo, hi]: every heavy before lo ends at or below X, every one from hi on above
+    uint32_t lo = 0, hi = 0;
+    if (active && b == num_tiles) lo = hi = nH;
+    else if (active && b > 0) hi = nH;
+    while (__any_sync(0xffffffffu, lo < hi)) {
+        const uint32_t len = hi - lo;
+        bool pred = false;
+        if (lo < hi) {
+            const bool small = len <= G;
+            const uint32_t p = small ? lo + j : lo + (uint32_t)(((uint64_t)(j + 1) * len) / (G + 1));
+            if (!small || j < len) pred = corrected_end(__ldg(heavy_E + p), nfix) <= X;
         }
-        g = lo;
+        const uint32_t m = (__ballot_sync(0xffffffffu, pred) >> gfirst) & ((1u << G) - 1u);
+        if (lo < hi) {
+            const uint32_t c = (uint32_t)__popc(m);  // the ends ascend: the first c pivots are at or below X
+            if (len <= G) {
+                lo = hi = lo + c;
+            } else {
+                const uint32_t lo0 = lo;
+                if (c > 0) lo = lo0 + (uint32_t)(((uint64_t)c * len) / (G + 1)) + 1;
+                if (c < G) hi = lo0 + (uint32_t)(((uint64_t)(c + 1) * len) / (G + 1));
+            }
+        }
     }
+    if (!active || j != 0) return;
+    if (b == num_tiles) hdr->nH_total = nH;
     TileStart ts;
     ts.A_lo = q_lo(X);
     ts.A_hi = q_hi(X);
     ts.c0 = make_dither(pv.L).c0;
-    ts.bound = g;
+    ts.bound = lo;
     ts.pad = 0;
     starts[b] = ts;
 }
