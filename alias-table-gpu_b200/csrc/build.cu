@@ -114,7 +114,7 @@ SplitLayout carve_split(void* scratch, uint64_t n, uint64_t num_tiles) {
     SplitLayout L;
     L.hdr = c.take<BuildHeader>(1);
     L.partials = c.take<double2>(kWsumMaxGrid);
-    L.num_groups = (num_tiles + kScanGroup - 1) / kScanGroup;
+    L.num_groups = (num_tiles + scan_group_tiles(num_tiles) - 1) / scan_group_tiles(num_tiles);
     L.num_blocks = (num_tiles + kPrefixTiles - 1) / kPrefixTiles;
     L.lb = c.take<LbWord>(L.num_groups);
     L.blocks = c.take<BlockWord>(L.num_blocks);  // right after lb: one zeroing covers both
@@ -160,13 +160,13 @@ wrs_status launch_split(const float* d_w, uint64_t n, wrs_alias_row* d_table, do
     // the kernels after wsum are launched as programmatic dependents: each starts while its
     // predecessor's last wave runs and waits for the predecessor's completion on entry
     if (launch_pdl(scan_kernel<S::SCAN_IPT>, dim3((uint32_t)L.num_groups), dim3(kScanThreads), 0, stream, d_w, n,
-                   L.hdr, L.lb, nt, L.agg, L.heavy_item, L.heavy_E, wc) != cudaSuccess)
+                   L.hdr, L.lb, nt, L.agg, L.heavy_item, L.heavy_E, wc, scan_group_tiles(nt)) != cudaSuccess)
         return WRS_ERR_CUDA;
     if (launch_pdl(tile_prefix_kernel, dim3((uint32_t)L.num_blocks), dim3(kPrefixThreads), 0, stream, L.hdr, L.agg,
                    L.incl, L.blocks, nt, wc) != cudaSuccess)
         return WRS_ERR_CUDA;
-    if (launch_pdl(link_kernel, dim3(((nt + 1) * (uint32_t)kLinkLanes + 255) / 256), dim3(256), 0, stream, L.hdr, L.incl, nt, L.heavy_E,
-                   L.starts) != cudaSuccess)
+    if (launch_pdl(link_kernel, dim3(((nt + 1) * (uint32_t)kLinkLanes + 255) / 256), dim3(256), 0, stream, L.hdr,
+                   L.incl, nt, L.heavy_E, L.starts) != cudaSuccess)
         return WRS_ERR_CUDA;
     {
         const size_t smem = pack_walk_smem_bytes(T, S::IPT);

@@ -138,7 +138,16 @@ __device__ __forceinline__ Scan2 block_scan2(const Scan2 v, Scan2* s) {
 // Every wait is bounded (wc); heavy list writes are bounded by n whatever a failed look-back
 // left in the prefixes.
 constexpr int kScanThreads = 256;
-constexpr int kScanGroup = 8;  // tiles per look-back unit
+constexpr int kScanGroup = 8;  // most tiles per look-back unit
+// Tiles per look-back unit for a build of num_tiles tiles: kScanGroup, halved while that leaves
+// fewer than kScanMinGroups units, so that a small table's scan spreads over the SMs (2^20 items
+// in 2048-item tiles: 512 units of one tile instead of 64 of eight).
+constexpr uint64_t kScanMinGroups = 592;
+__host__ __device__ inline uint32_t scan_group_tiles(uint64_t num_tiles) {
+    uint32_t g = kScanGroup;
+    while (g > 1 && (num_tiles + g - 1) / g < kScanMinGroups) g >>= 1;
+    return g;
+}
 
 // Look-back word of a group: a = flag << 62 | heavy count, b = heavy excess (Q40.24); flag 1 =
 // the group's own sums, 2 = the sums of every group up to it.
@@ -181,7 +190,7 @@ template <int IPT>
 __global__ void __launch_bounds__(kScanThreads) scan_kernel(const float* __restrict__ w, uint64_t n, BuildHeader* hdr,
                                                             LbWord* lb, uint32_t num_tiles, TileVals* agg,
                                                             uint32_t* __restrict__ heavy_item,
-                                                            uint64_t* __restrict__ heavy_E, WaitCfg wc) {
+                                                            uint64_t* __restrict__ heavy_E, WaitCfg wc, uint32_t gt) {
     pdl_enter();
     constexpr int NT = kScanThreads;
     constexpr int NW = NT / 32;
@@ -201,7 +210,7 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(const float* __restr
     __shared__ uint64_t s_te0[U + 1][NW];  // ... their excess
     __shared__ uint64_t s_base_c, s_base_e;
 
-    const uint32_t num_groups = (num_tiles + U - 1) / U;
+    const uint32_t num_groups = (num_tiles + gt - 1) / gt;  // gt = scan_group_tiles(num_tiles) <= U
     if (threadIdx.x == 0) {
         s_group = atomicAdd(&hdr->tile_ticket, 1u);
         s_abort = load_relaxed(&hdr->status) != 0;
@@ -216,8 +225,8 @@ __global__ void __launch_bounds__(kScanThreads) scan_kernel(const float* __restr
     }
     const ClassParams cp = load_class_params(hdr);
     const float R48 = cp.R32 * 281474976710656.0f;
-    const uint32_t tile0 = group * U;
-    const uint32_t ntl = min((uint32_t)U, num_tiles - tile0);  // tiles of this group
+    const uint32_t tile0 = group * gt;
+    const uint32_t ntl = min(min(gt, (uint32_t)U), num_tiles - tile0);  // tiles of this group
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
     // one tile's sums from its weights in registers; warp-level only (no CTA barrier)
