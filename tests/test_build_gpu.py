@@ -46,6 +46,18 @@ def test_build_tile_sizes_give_identical_tables(cuda, tile, name):
     check_parity(w, rows, W)
 
 
+@pytest.mark.parametrize("num_tiles", [591, 592, 1182, 1184, 4728, 4729])
+def test_build_scan_group_boundaries(cuda, num_tiles):
+    # the scan groups fewer tiles per look-back unit while a table has fewer than 592 units of
+    # eight (1, 2, 4 or 8 tiles): tables on either side of each switch, with a ragged last tile
+    tile = 1024
+    n = num_tiles * tile - 7
+    w = gen("powerlaw_shuffled", n)
+    st, rows, W = gpu_build(w, tile_items=tile)
+    assert st == wrs.WRS_SUCCESS, wrs.status_string(st)
+    check_parity(w, rows, W)
+
+
 def test_build_reference_generators(cuda):
     g = np.load(GOLDEN)
     for case in ["sine", "bestworst", "ramp", "powerlaw1", "powerlaw2", "oneheavy", "onelight", "uniform_f32"]:
