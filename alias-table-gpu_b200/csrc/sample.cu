@@ -215,11 +215,52 @@ extern "C" wrs_status wrs_rejection_sample(const uint32_t* d_A, const uint64_t* 
     cudaStream_t stream = static_cast<cudaStream_t>(stream_);
     const DeviceInfo dev = device_info();
     const uint32_t tries = max_tries ? max_tries : 64u;
-    uint64_t grid = (num_samples + 255) / 256;
-    const uint64_t cap = (uint64_t)dev.sm_count * 16;
+    uint64_t grid = ((num_samples + kRejJ - 1) / kRejJ + 255) / 256;
+    const uint64_t cap = (uint64_t)dev.sm_count * 8;
     if (grid > cap) grid = cap;
     rejection_sample_kernel<<<(uint32_t)grid, 256, 0, stream>>>(d_A, d_A_size, d_frac, num_samples, seed_k0(seed),
                                                                seed_k1(seed), counter_base, tries, d_out, d_status);
+    const wrs_status st = launch_status();
+    if (st != WRS_SUCCESS) return st;
+    if (flags & WRS_FLAG_SYNC) {
+        if (d_status) return read_device_status(d_status, stream);
+        return cuda_status(cudaStreamSynchronize(stream));
+    }
+    return WRS_SUCCESS;
+}
+
+extern "C" wrs_status wrs_rejection_pack(const uint32_t* d_A, const uint64_t* d_A_size, const float* d_frac,
+                                         int64_t n, uint64_t a_capacity, uint64_t* d_slots, void* stream_) {
+    if (!d_A || !d_A_size || !d_frac || !d_slots || n < 1 || n > kMaxItems) return WRS_ERR_INVALID_ARGUMENT;
+    if (((uintptr_t)d_slots & 7u) != 0) return WRS_ERR_INVALID_ARGUMENT;
+    if (a_capacity == 0) return WRS_SUCCESS;
+    const DeviceInfo dev = device_info();
+    uint64_t grid = (a_capacity + 255) / 256;
+    const uint64_t cap = (uint64_t)dev.sm_count * 8;
+    if (grid > cap) grid = cap;
+    rejection_pack_kernel<<<(uint32_t)grid, 256, 0, static_cast<cudaStream_t>(stream_)>>>(
+        d_A, d_A_size, d_frac, (uint32_t)n, a_capacity, reinterpret_cast<uint2*>(d_slots));
+    return launch_status();
+}
+
+extern "C" wrs_status wrs_rejection_sample_packed(const uint64_t* d_slots, uint64_t slot_capacity,
+                                                  const uint64_t* d_A_size, int64_t n,
+                                                  uint64_t num_samples, uint64_t seed, uint64_t counter_base,
+                                                  uint32_t max_tries, uint32_t* d_out, uint32_t* d_status,
+                                                  uint32_t flags, void* stream_) {
+    if (!d_slots || !d_A_size || n < 1 || (num_samples > 0 && !d_out)) return WRS_ERR_INVALID_ARGUMENT;
+    if (((uintptr_t)d_slots & 7u) != 0) return WRS_ERR_INVALID_ARGUMENT;
+    if (num_samples == 0) return WRS_SUCCESS;
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_);
+    const DeviceInfo dev = device_info();
+    const uint32_t tries = max_tries ? max_tries : 64u;
+    const uint64_t per = (uint64_t)kRejPackedJ;
+    uint64_t grid = ((num_samples + per - 1) / per + 255) / 256;
+    const uint64_t cap = (uint64_t)dev.sm_count * 8;
+    if (grid > cap) grid = cap;
+    rejection_sample_packed_kernel<<<(uint32_t)grid, 256, 0, stream>>>(
+        reinterpret_cast<const uint2*>(d_slots), slot_capacity, d_A_size, num_samples, seed_k0(seed), seed_k1(seed), counter_base,
+        tries, d_out, d_status);
     const wrs_status st = launch_status();
     if (st != WRS_SUCCESS) return st;
     if (flags & WRS_FLAG_SYNC) {

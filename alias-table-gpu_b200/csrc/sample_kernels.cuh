@@ -260,36 +260,159 @@ __device__ __forceinline__ uint32_t slot_of(uint32_t x0, uint32_t x1, uint32_t a
 // slot is accepted with probability frac(n w / W). Try t of sample s uses Philox block
 // (counter_base + s, t, 0x52454a00): the slot from x0 and x1 (64 bits), the coin from x2. The first-slot test reads a flag bit in
 // the slot itself instead of comparing with A[index - 1].
+// J consecutive samples per thread with their tries interleaved: the J slot gathers of a try
+// are in flight together, then the fraction gathers of the first slots among them.
+constexpr int kRejJ = 4;
 __global__ void __launch_bounds__(256) rejection_sample_kernel(const uint32_t* __restrict__ A,
                                                                const uint64_t* __restrict__ a_size_ptr,
                                                                const float* __restrict__ frac, uint64_t m,
                                                                uint32_t k0, uint32_t k1, uint64_t cbase,
                                                                uint32_t max_tries, uint32_t* __restrict__ out,
                                                                uint32_t* status) {
+    constexpr int J = kRejJ;
+    static_assert(J % 4 == 0, "16-byte stores");
     const uint64_t asz64 = *a_size_ptr;
     const uint64_t gsize = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t g0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     bool failed = false;
     if (asz64 == 0 || asz64 > 0xffffffffull) {  // no (or an unusable) slot array: nothing to sample
-        for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < m; s += gsize) out[s] = 0xffffffffu;
+        for (uint64_t s = g0; s < m; s += gsize) out[s] = 0xffffffffu;
         if (status && blockIdx.x == 0 && threadIdx.x == 0) record_status(status, kErrCapacity);
         return;
     }
     const uint32_t asz = (uint32_t)asz64;
-    for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < m; s += gsize) {
-        const uint64_t b = cbase + s;
-        uint32_t res = 0xffffffffu;
-        for (uint32_t t = 0; t < max_tries; ++t) {
-            const Philox4 r = philox4x32_10((uint32_t)b, (uint32_t)(b >> 32), t, 0x52454a00u, k0, k1);
-            const uint32_t xc = r.x[2];
-            const uint32_t e = ld_u32_64B(A + slot_of(r.x[0], r.x[1], asz));
-            const uint32_t item = e & 0x7fffffffu;
-            if ((e >> 31) == 0u || coin24(xc) < ld_f32_64B(frac + item)) {
-                res = item;
-                break;
+    const bool out16 = ((uintptr_t)out & 15u) == 0;
+    for (uint64_t s0 = g0 * J; s0 < m; s0 += gsize * J) {
+        uint32_t res[J];
+        uint32_t open = 0;  // bit j: sample s0 + j still drawing
+#pragma unroll
+        for (int j = 0; j < J; ++j) {
+            res[j] = 0xffffffffu;
+            if (s0 + j < m) open |= 1u << j;
+        }
+        for (uint32_t t = 0; t < max_tries && open; ++t) {
+            uint32_t xc[J], e[J];
+#pragma unroll
+            for (int j = 0; j < J; ++j) {
+                if ((open >> j) & 1u) {
+                    const uint64_t b = cbase + s0 + j;
+                    const Philox4 r = philox4x32_10((uint32_t)b, (uint32_t)(b >> 32), t, 0x52454a00u, k0, k1);
+                    xc[j] = r.x[2];
+                    e[j] = ld_u32_64B(A + slot_of(r.x[0], r.x[1], asz));
+                }
+            }
+            float f[J];
+#pragma unroll
+            for (int j = 0; j < J; ++j)
+                if (((open >> j) & 1u) && (e[j] >> 31) != 0u) f[j] = ld_f32_64B(frac + (e[j] & 0x7fffffffu));
+#pragma unroll
+            for (int j = 0; j < J; ++j) {
+                if ((open >> j) & 1u) {
+                    if ((e[j] >> 31) == 0u || coin24(xc[j]) < f[j]) {
+                        res[j] = e[j] & 0x7fffffffu;
+                        open &= ~(1u << j);
+                    }
+                }
             }
         }
-        if (res == 0xffffffffu) failed = true;
-        out[s] = res;
+        if (open) failed = true;
+        if (out16 && s0 + J <= m) {
+#pragma unroll
+            for (int q = 0; q < J / 4; ++q)
+                reinterpret_cast<uint4*>(out + s0)[q] = make_uint4(res[4 * q], res[4 * q + 1], res[4 * q + 2], res[4 * q + 3]);
+        } else {
+#pragma unroll
+            for (int j = 0; j < J; ++j)
+                if (s0 + j < m) out[s0 + j] = res[j];
+        }
+    }
+    if (failed && status) record_status(status, kErrTooManyTries);
+}
+
+// ---------------------------------------------------------------- packed rejection slots
+// The slot array with each first slot's acceptance fraction beside it: slots[s] = {A[s], the
+// FP32 bits of frac[item] on the item's first slot, else 0}. A try then reads one 8-byte slot
+// (one random gather) where the unpacked form reads the slot and, on a first slot, the item's
+// fraction (a second random gather at another address).
+__global__ void __launch_bounds__(256) rejection_pack_kernel(const uint32_t* __restrict__ A,
+                                                             const uint64_t* __restrict__ a_size_ptr,
+                                                             const float* __restrict__ frac, uint32_t n,
+                                                             uint64_t a_capacity, uint2* __restrict__ slots) {
+    const uint64_t asz = min(*a_size_ptr, a_capacity);
+    const uint64_t gsize = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < asz; s += gsize) {
+        const uint32_t e = A[s];
+        const uint32_t item = e & 0x7fffffffu;
+        const float f = ((e >> 31) != 0u && item < n) ? __ldg(frac + item) : 0.0f;
+        slots[s] = make_uint2(e, __float_as_uint(f));
+    }
+}
+
+// Rejection sampling from packed slots: the tries and decisions of rejection_sample_kernel
+// (same Philox blocks, same slot, same comparison, so the same samples), eight consecutive
+// samples per thread with their tries interleaved, so that eight gathers are in flight (2^28
+// samples from 1.28e8 slots: 10.7 ms, 12.2 with four).
+constexpr int kRejPackedJ = 8;
+__global__ void __launch_bounds__(256) rejection_sample_packed_kernel(const uint2* __restrict__ slots,
+                                                                      uint64_t slot_capacity,
+                                                                      const uint64_t* __restrict__ a_size_ptr,
+                                                                      uint64_t m, uint32_t k0, uint32_t k1,
+                                                                      uint64_t cbase, uint32_t max_tries,
+                                                                      uint32_t* __restrict__ out, uint32_t* status) {
+    constexpr int J = kRejPackedJ;
+    static_assert(J % 4 == 0, "16-byte stores");
+    const uint64_t asz64 = *a_size_ptr;
+    const uint64_t gsize = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t g0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool failed = false;
+    if (asz64 == 0 || asz64 > 0xffffffffull || asz64 > slot_capacity) {  // no (or an unusable) slot array
+        for (uint64_t s = g0; s < m; s += gsize) out[s] = 0xffffffffu;
+        if (status && blockIdx.x == 0 && threadIdx.x == 0) record_status(status, kErrCapacity);
+        return;
+    }
+    const uint32_t asz = (uint32_t)asz64;
+    const bool out16 = ((uintptr_t)out & 15u) == 0;
+    for (uint64_t s0 = g0 * J; s0 < m; s0 += gsize * J) {
+        uint32_t res[J];
+        uint32_t open = 0;  // bit j: sample s0 + j still drawing
+#pragma unroll
+        for (int j = 0; j < J; ++j) {
+            res[j] = 0xffffffffu;
+            if (s0 + j < m) open |= 1u << j;
+        }
+        for (uint32_t t = 0; t < max_tries && open; ++t) {
+            uint32_t xc[J];
+            uint2 v[J];
+#pragma unroll
+            for (int j = 0; j < J; ++j) {
+                if ((open >> j) & 1u) {
+                    const uint64_t b = cbase + s0 + j;
+                    const Philox4 r = philox4x32_10((uint32_t)b, (uint32_t)(b >> 32), t, 0x52454a00u, k0, k1);
+                    xc[j] = r.x[2];
+                    v[j] = ld_row_64B(slots + slot_of(r.x[0], r.x[1], asz));
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < J; ++j) {
+                if ((open >> j) & 1u) {
+                    const uint32_t e = v[j].x;
+                    if ((e >> 31) == 0u || coin24(xc[j]) < __uint_as_float(v[j].y)) {
+                        res[j] = e & 0x7fffffffu;
+                        open &= ~(1u << j);
+                    }
+                }
+            }
+        }
+        if (open) failed = true;
+        if (out16 && s0 + J <= m) {
+#pragma unroll
+            for (int q = 0; q < J / 4; ++q)
+                reinterpret_cast<uint4*>(out + s0)[q] = make_uint4(res[4 * q], res[4 * q + 1], res[4 * q + 2], res[4 * q + 3]);
+        } else {
+#pragma unroll
+            for (int j = 0; j < J; ++j)
+                if (s0 + j < m) out[s0 + j] = res[j];
+        }
     }
     if (failed && status) record_status(status, kErrTooManyTries);
 }

@@ -83,6 +83,8 @@ _SIGNATURES = {
     "wrs_rejection_build_scratch_bytes": (_SZ, [_I64]),
     "wrs_rejection_build_f32": (ctypes.c_int, [_P, _I64, _P, _U64, _P, _P, _P, _P, _SZ, _U32, _P]),
     "wrs_rejection_sample": (ctypes.c_int, [_P, _P, _P, _I64, _U64, _U64, _U64, _U32, _P, _P, _U32, _P]),
+    "wrs_rejection_pack": (ctypes.c_int, [_P, _P, _P, _I64, _U64, _P, _P]),
+    "wrs_rejection_sample_packed": (ctypes.c_int, [_P, _U64, _P, _I64, _U64, _U64, _U64, _U32, _P, _P, _U32, _P]),
     "wrs_batched_build_scratch_bytes": (_SZ, [_P, _I64, _P]),
     "wrs_batched_build_f32": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P, _P, _SZ, _P]),
     "wrs_batched_sample": (ctypes.c_int, [_P, _P, _I64, _P, _U64, _U64, _U64, _P, _P]),
@@ -307,6 +309,19 @@ def rejection_sample(A, a_size, frac, n: int, num_samples: int, seed: int, out, 
     return lib().wrs_rejection_sample(_ptr(A), _ptr(a_size), _ptr(frac), n, num_samples, seed & (2**64 - 1),
                                       counter_base & (2**64 - 1), max_tries, _ptr(out), _ptr(status),
                                       WRS_FLAG_SYNC if sync else 0, _stream(stream))
+
+
+def rejection_pack(A, a_size, frac, n: int, slots, stream=None) -> int:
+    """Packs the slot array and the first slots' fractions into 8-byte slots (int64 tensor of at
+    least |A| entries)."""
+    return lib().wrs_rejection_pack(_ptr(A), _ptr(a_size), _ptr(frac), n, slots.numel(), _ptr(slots), _stream(stream))
+
+
+def rejection_sample_packed(slots, a_size, n: int, num_samples: int, seed: int, out, counter_base: int = 0,
+                            max_tries: int = 0, status=None, sync: bool = False, stream=None) -> int:
+    return lib().wrs_rejection_sample_packed(_ptr(slots), slots.numel(), _ptr(a_size), n, num_samples, seed & (2**64 - 1),
+                                             counter_base & (2**64 - 1), max_tries, _ptr(out), _ptr(status),
+                                             WRS_FLAG_SYNC if sync else 0, _stream(stream))
 
 
 def scratch_status(scratch, stream=None) -> int:

@@ -412,7 +412,29 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     if st or int(rstat.item()) or wrs.scratch_status(rscr, sp):
         raise wrs.WrsError(st or int(rstat.item()) or 1, "rejection")
     rej_slots = int(a_size.item())
-    del A, frac, rscr
+    # the same samples from packed slots (slot and fraction in one 8-byte gather per try)
+    slots = torch.empty(rej_slots, dtype=torch.int64, device=dev)
+    rout2 = torch.empty(rm, dtype=torch.int32, device=dev)
+    st = wrs.rejection_pack(A, a_size, frac, n, slots, stream=sp)
+    st |= wrs.rejection_sample_packed(slots, a_size, n, rm, SEED_SAMPLES, rout2, 0, 0, rstat, stream=sp)
+    torch.cuda.synchronize()
+    s0.record(stream)
+    for r in range(reps):
+        st |= wrs.rejection_pack(A, a_size, frac, n, slots, stream=sp)
+    s1.record(stream)
+    torch.cuda.synchronize()
+    rej_pack_ms = s0.elapsed_time(s1) / reps
+    s0.record(stream)
+    for r in range(reps):
+        st |= wrs.rejection_sample_packed(slots, a_size, n, rm, SEED_SAMPLES, rout2, (r + 1) * rm, 0, rstat, stream=sp)
+    s1.record(stream)
+    torch.cuda.synchronize()
+    rej_packed_ms = s0.elapsed_time(s1) / reps
+    if st or int(rstat.item()):
+        raise wrs.WrsError(st or int(rstat.item()), "packed rejection")
+    if not torch.equal(rout, rout2):
+        raise RuntimeError("packed rejection samples differ from the unpacked sampler's")
+    del A, frac, rscr, slots, rout2
     # the PSA+ build on the same weights (a table of its own; the headline table is the split one)
     popts = wrs.build_opts(wrs.WRS_METHOD_PSA_PLUS)
     ptable = torch.empty(n, dtype=torch.int64, device=dev)
@@ -530,6 +552,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                    "rejection_build_gitems_s": round(n / rej_build_ms / 1e6, 3),
                    "rejection_samples": rm, "rejection_sample_ms": round(rej_sample_ms, 4),
                    "rejection_gsamples_s": round(rm / rej_sample_ms / 1e6, 3),
+                   "rejection_pack_ms": round(rej_pack_ms, 4),
+                   "rejection_packed_sample_ms": round(rej_packed_ms, 4),
+                   "rejection_packed_gsamples_s": round(rm / rej_packed_ms / 1e6, 3),
                    "section_items": SECTION_ITEMS},
         "prob_error": err,
         "chi_square": chi2,

@@ -219,6 +219,25 @@ WRS_API wrs_status wrs_rejection_sample(const uint32_t* d_A, const uint64_t* d_A
                                 uint64_t counter_base, uint32_t max_tries, uint32_t* d_out,
                                 uint32_t* d_status, uint32_t flags, void* stream);
 
+/* The slot array packed with the first slots' acceptance fractions: d_slots[s] (u64, 8-byte
+ * aligned, a_capacity entries) = d_A[s] in the low 32 bits and, on an item's first slot, the
+ * FP32 bits of d_frac[item] in the high 32 bits (0 elsewhere), for s < |A| (read from
+ * d_A_size). Asynchronous. No counterpart in the reference: it is a layout of this library's
+ * rejection structure, for wrs_rejection_sample_packed. */
+WRS_API wrs_status wrs_rejection_pack(const uint32_t* d_A, const uint64_t* d_A_size, const float* d_frac,
+                                      int64_t n, uint64_t a_capacity, uint64_t* d_slots, void* stream);
+/* wrs_rejection_sample over packed slots: the same tries, slots and decisions, so the same
+ * samples and status, with one random 8-byte gather per try instead of a slot gather and, on a
+ * first slot, a second gather for the item's fraction. slot_capacity is the number of entries
+ * d_slots holds: a |A| above it samples nothing (outputs 0xFFFFFFFF, *d_status gets
+ * WRS_ERR_CAPACITY). The sampling side of SamplerRejection::sample
+ * (sampling/rejectionSampling/SamplerRejection.cu:17-35). */
+WRS_API wrs_status wrs_rejection_sample_packed(const uint64_t* d_slots, uint64_t slot_capacity,
+                                               const uint64_t* d_A_size, int64_t n,
+                                               uint64_t num_samples, uint64_t seed, uint64_t counter_base,
+                                               uint32_t max_tries, uint32_t* d_out, uint32_t* d_status,
+                                               uint32_t flags, void* stream);
+
 /* ---- batched (CSR) ------------------------------------------------------ */
 
 /* Tables t = 0..num_tables-1 own weights d_w[d_offsets[t] .. d_offsets[t+1]); their rows are

@@ -72,6 +72,55 @@ def test_rejection_sample_bit_exact(cuda, max_tries):
         assert st == 0
 
 
+def packed(A, asz, frac, n, capacity=None):
+    slots = torch.full((capacity if capacity is not None else int(asz.item()),), -1, dtype=torch.int64, device="cuda")
+    assert wrs.rejection_pack(A, asz, frac, n, slots) == wrs.WRS_SUCCESS
+    torch.cuda.synchronize()
+    return slots
+
+
+@pytest.mark.parametrize("maker", [lambda: gen("pareto", 20_000), lambda: big_items(70_001)])
+def test_rejection_pack_layout(cuda, maker):
+    w = maker()
+    st, A, frac, asz, W = gpu_rej_build(w)
+    assert st == 0
+    k = int(asz.item())
+    slots = packed(A, asz, frac, w.size).cpu().numpy().view(np.uint32).reshape(-1, 2)
+    a = A[:k].cpu().numpy().view(np.uint32)
+    f = frac.cpu().numpy()
+    np.testing.assert_array_equal(slots[:, 0], a)
+    first = (a >> 31) != 0
+    expect = np.where(first, f[a & 0x7FFFFFFF].view(np.uint32), 0).astype(np.uint32)
+    np.testing.assert_array_equal(slots[:, 1], expect)
+
+
+@pytest.mark.parametrize("m", [300_001, 4, 3, 1])
+@pytest.mark.parametrize("max_tries", [0, 1, 2])
+def test_rejection_sample_packed_equals_unpacked(cuda, max_tries, m):
+    # the same tries and decisions: bit for bit the oracle's samples, give-ups and status included
+    w = gen("pareto", 20_000)
+    st, A, frac, asz, W = gpu_rej_build(w)
+    slots = packed(A, asz, frac, w.size)
+    out = torch.empty(m, dtype=torch.int32, device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    st = wrs.rejection_sample_packed(slots, asz, w.size, m, SEED, out, 5, max_tries, status, sync=True)
+    A_ref, frac_ref = po.rejection_build(w, W)
+    ref, failed = po.rejection_sample(A_ref, frac_ref, m, SEED, 5, max_tries)
+    np.testing.assert_array_equal(out.cpu().numpy().view(np.uint32), ref)
+    assert st == (wrs.WRS_ERR_TOO_MANY_TRIES if failed else 0)
+
+
+def test_rejection_sample_packed_slot_capacity(cuda):
+    w = gen("uniform", 5_000)
+    st, A, frac, asz, W = gpu_rej_build(w)
+    slots = packed(A, asz, frac, w.size, capacity=int(asz.item()) - 1)
+    out = torch.zeros(1000, dtype=torch.int32, device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    st = wrs.rejection_sample_packed(slots, asz, w.size, 1000, SEED, out, 0, 0, status, sync=True)
+    assert st == wrs.WRS_ERR_CAPACITY
+    assert (out.cpu().numpy().view(np.uint32) == 0xFFFFFFFF).all()
+
+
 def test_rejection_distribution(cuda):
     w = gen("exp", 1 << 14)
     st, A, frac, asz, W = gpu_rej_build(w)
