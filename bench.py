@@ -1177,8 +1177,8 @@ def main():
     ap.add_argument("--log2-samples", type=int, default=0,
                     help="samples per step (2^k, 0 = the configuration's); for profiler captures only")
     ap.add_argument("--config", default="2", choices=sorted(CONFIGS) + ["4", "5"],
-                    help="BASELINE configuration: 2 (default, headline; includes the batched phase), 1, 3, "
-                         "or 4 / 5 (batched tables only)")
+                    help="workload: 2 (default, headline: n=2^26 table; includes the batched phase), 1 (n=2^20), 3 (n=2^28), "
+                         "or 4 / 5 (the batched-tables workloads only)")
     ap.add_argument("--shape", default="",
                     help="batched configurations: small_table_items,tile_items instead of the autotuner's")
     ap.add_argument("--once", action="store_true",
