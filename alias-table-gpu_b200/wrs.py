@@ -565,8 +565,12 @@ class RejectionSamplingGpu(SamplingAlgorithm):
                "rejection build")
 
     def postBuild(self) -> bool:
+        import torch
         _check(scratch_status(self.scratch), "rejection build (device)")
         self.W = float(self.W_dev.item())
+        # the slots packed with the first slots' fractions: one gather per try when sampling
+        self.slots = torch.empty(max(1, int(self.A_size.item())), dtype=torch.int64, device=self.device)
+        _check(rejection_pack(self.A, self.A_size, self.frac, self.N, self.slots), "rejection pack")
         return True
 
 
@@ -679,8 +683,8 @@ class SamplerRejection(Sampler):
         a = self.algorithm
         if out is None:
             out = torch.empty(numSamples, dtype=torch.int32, device=a.device)
-        _check(rejection_sample(a.A, a.A_size, a.frac, a.N, numSamples, self.seed, out, self.counter,
-                                self.max_tries), "rejection sample")
+        _check(rejection_sample_packed(a.slots, a.A_size, a.N, numSamples, self.seed, out, self.counter,
+                                       self.max_tries), "rejection sample")
         self.counter += numSamples
         return out
 

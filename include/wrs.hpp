@@ -192,14 +192,21 @@ public:
         check(wrs_scratch_status(scratch_.get(), stream_), "rejection build (device)");
         W = W_dev_.to_host(stream_)[0];
         slots = a_size_.to_host(stream_)[0];
+        // the slots packed with the first slots' fractions: one gather per try when sampling
+        packed_.resize(slots ? (size_t)slots : 1);
+        check(wrs_rejection_pack(A_.get(), a_size_.get(), frac_.get(), N, packed_.size(), packed_.get(), stream_),
+              "rejection pack");
         return true;
     }
     const uint32_t* deviceA() const { return A_.get(); }
     const float* deviceFrac() const { return frac_.get(); }
     const uint64_t* deviceASize() const { return a_size_.get(); }
+    const uint64_t* devicePacked() const { return packed_.get(); }
+    uint64_t packedCapacity() const { return packed_.size(); }
     uint64_t slots = 0;  // |A|
 
 private:
+    DeviceArray<uint64_t> packed_;
     DeviceArray<uint32_t> A_;
     DeviceArray<float> frac_;
     DeviceArray<uint64_t> a_size_{1};
@@ -318,8 +325,9 @@ public:
         : Sampler(seed), r_(r), tries_(maxTries) {}
     std::string name() override { return "SamplerRejection"; }
     void sample(uint64_t numSamples, uint32_t* d_out) override {
-        check(wrs_rejection_sample(r_.deviceA(), r_.deviceASize(), r_.deviceFrac(), r_.N, numSamples, seed_, counter,
-                                   tries_, d_out, nullptr, 0u, r_.stream()), "rejection sample");
+        check(wrs_rejection_sample_packed(r_.devicePacked(), r_.packedCapacity(), r_.deviceASize(), r_.N, numSamples,
+                                          seed_, counter, tries_, d_out, nullptr, 0u, r_.stream()),
+              "rejection sample");
         counter += numSamples;
     }
 
