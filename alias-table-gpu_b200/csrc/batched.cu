@@ -376,8 +376,9 @@ wrs_status launch_big(const float* d_w, const int64_t* d_offsets, const uint8_t*
                        dim3(32 * heavy_warps(T)), 0, stream, d_w, L.hdrs, L.agg, L.incl, L.hmask, nt, L.heavy_item,
                        L.heavy_E, map)))
         return WRS_ERR_CUDA;
-    if (!ok(launch_pdl(tile_link_kernel<true>, dim3((nt + p.big_tables + 255) / 256), dim3(256), 0, stream, L.hdrs,
-                       L.incl, nt, p.big_tables, L.heavy_E, L.starts, map)))
+    const uint32_t link_grid = ((nt + p.big_tables) * (uint32_t)kTileLinkLanes + 255) / 256;
+    if (!ok(launch_pdl(tile_link_kernel<true>, dim3(link_grid), dim3(256), 0, stream, L.hdrs, L.incl, nt,
+                       p.big_tables, L.heavy_E, L.starts, map)))
         return WRS_ERR_CUDA;
     const size_t smem = pack_smem_bytes(T);
     const cudaError_t e = cudaFuncSetAttribute(split_pack_kernel<NT, IPT, true, false>,

@@ -325,8 +325,9 @@ wrs_status launch_psa(const float* d_w, uint64_t n, wrs_alias_row* d_table, doub
     if (!ok(launch_pdl(psa_heavy_list_kernel<T>, dim3((nt + 3) / 4), dim3(128), 0, stream, L.hdr2, L.agg2, L.incl2,
                        L.slots, nt, L.heavy_item2, L.heavy_E2)))
         return WRS_ERR_CUDA;
-    if (!ok(launch_pdl(tile_link_kernel<false>, dim3((nt + 1 + 255) / 256), dim3(256), 0, stream, L.hdr2, L.incl2, nt,
-                       1u, L.heavy_E2, L.starts2, map)))
+    const uint32_t link_grid = ((nt + 1) * (uint32_t)kTileLinkLanes + 255) / 256;
+    if (!ok(launch_pdl(tile_link_kernel<false>, dim3(link_grid), dim3(256), 0, stream, L.hdr2, L.incl2, nt, 1u,
+                       L.heavy_E2, L.starts2, map)))
         return WRS_ERR_CUDA;
     {
         const size_t smem = pack_smem_bytes(T);

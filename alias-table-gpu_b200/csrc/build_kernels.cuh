@@ -1141,51 +1141,79 @@ struct __align__(16) TileStart {
 };
 static_assert(sizeof(TileStart) == 32, "TileStart layout");
 
-// One thread per start: the starts of the global tiles, then (batched) the end of each table.
+// A group of kTileLinkLanes lanes per start: the starts of the global tiles, then (batched) the
+// end of each table. The bound by a (kTileLinkLanes + 1)-ary search: each step tests
+// kTileLinkLanes pivots at once (one L2 round trip), and the interval shrinks at every step
+// whatever the list holds, so the loop ends on any input.
+constexpr int kTileLinkLanes = 8;
 template <bool BATCH>
 __global__ void __launch_bounds__(256) tile_link_kernel(const BuildHeader* hdr, const TileVals* incl,
                                                         uint32_t num_tiles, uint32_t num_tables,
                                                         const uint4* heavy_E, TileStart* starts, TileMap map) {
     pdl_enter();
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (plan_failed<BATCH>(map)) return;
+    constexpr uint32_t G = kTileLinkLanes;
+    static_assert(32 % G == 0, "lane groups");
+    if (plan_failed<BATCH>(map)) return;  // the same for every thread
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const uint32_t j = threadIdx.x % G;
+    const uint32_t gfirst = (threadIdx.x & 31u) & ~(G - 1);  // the group's first lane in the warp
+    bool active = true;
     TileRef tr;
     if (!BATCH) {
-        if (i > num_tiles) return;
-        tr = tile_ref<false>(map, 0);
-        tr.local = i;  // the boundary: i == num_tiles is the table's end
+        if (i > num_tiles) {
+            active = false;
+        } else {
+            tr = tile_ref<false>(map, 0);
+            tr.local = i;  // the boundary: i == num_tiles is the table's end
+        }
     } else if (i < num_tiles) {
         tr = tile_ref<true>(map, i);
-    } else {
-        if (i >= num_tiles + num_tables) return;
+    } else if (i < num_tiles + num_tables) {
         const uint32_t t = i - num_tiles;
         tr = table_ref(map.desc[t], t, map.desc[t].ntiles);
-    }
-    hdr += tr.table;
-    if (earlier_status(hdr) != 0) return;
-    heavy_E += tr.heavy_off;
-    const uint32_t b = tr.local;
-    const uint32_t nH = __ldg(&incl[tr.tile0 + tr.ntiles - 1].nH);
-    const TileVals pv = b ? ldcg_tilevals(incl + tr.tile0 + b - 1) : tv_zero();
-    const u128 X = deficit_line(pv);
-    uint32_t g;
-    if (b == 0) {
-        g = 0;
-    } else if (b == tr.ntiles) {
-        g = nH;
     } else {
-        uint32_t lo = 0, hi = nH;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (load_u128(heavy_E + mid) <= X) lo = mid + 1; else hi = mid;
-        }
-        g = lo;
+        active = false;
     }
+    if (active && earlier_status(hdr + tr.table) != 0) active = false;
+    uint32_t b = 0, nH = 0;
+    TileVals pv = tv_zero();
+    if (active) {
+        heavy_E += tr.heavy_off;
+        b = tr.local;
+        nH = __ldg(&incl[tr.tile0 + tr.ntiles - 1].nH);
+        if (b) pv = ldcg_tilevals(incl + tr.tile0 + b - 1);
+    }
+    const u128 X = deficit_line(pv);
+    // the bound lies in [lo, hi]: every heavy before lo ends at or below X, every one from hi on above
+    uint32_t lo = 0, hi = 0;
+    if (active && b == tr.ntiles) lo = hi = nH;
+    else if (active && b > 0) hi = nH;
+    while (__any_sync(0xffffffffu, lo < hi)) {
+        const uint32_t len = hi - lo;
+        bool pred = false;
+        if (lo < hi) {
+            const bool small = len <= G;
+            const uint32_t p = small ? lo + j : lo + (uint32_t)(((uint64_t)(j + 1) * len) / (G + 1));
+            if (!small || j < len) pred = load_u128(heavy_E + p) <= X;
+        }
+        const uint32_t m = (__ballot_sync(0xffffffffu, pred) >> gfirst) & ((1u << G) - 1u);
+        if (lo < hi) {
+            const uint32_t c = (uint32_t)__popc(m);  // the ends ascend: the first c pivots are at or below X
+            if (len <= G) {
+                lo = hi = lo + c;
+            } else {
+                const uint32_t lo0 = lo;
+                if (c > 0) lo = lo0 + (uint32_t)(((uint64_t)c * len) / (G + 1)) + 1;
+                if (c < G) hi = lo0 + (uint32_t)(((uint64_t)(c + 1) * len) / (G + 1));
+            }
+        }
+    }
+    if (!active || j != 0) return;
     TileStart ts;
     ts.A_lo = q_lo(X);
     ts.A_hi = q_hi(X);
     ts.c0 = make_dither(pv.L).c0;
-    ts.bound = g;
+    ts.bound = lo;
     ts.pad = 0;
     starts[tr.tile0 + tr.table + b] = ts;
 }
