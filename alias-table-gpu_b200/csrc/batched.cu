@@ -631,7 +631,11 @@ wrs_status autotune_shapes(const float* d_w, const int64_t* d_offsets, const int
             st = batched_build(d_w, d_offsets, h_offsets, num_tables, sh, d_table, nullptr, d_scratch, scratch_bytes,
                                cap, &L, nullptr, nullptr, nullptr, sa);
             if (cudaStreamEndCapture(cap, &graph) != cudaSuccess && st == WRS_SUCCESS) st = WRS_ERR_CUDA;
-            if (st == WRS_SUCCESS && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) st = WRS_ERR_CUDA;
+            // with node priorities, as a caller should instantiate it: the tiled passes' side stream
+            // keeps its higher priority in the replay
+            if (st == WRS_SUCCESS &&
+                cudaGraphInstantiate(&exec, graph, cudaGraphInstantiateFlagUseNodePriority) != cudaSuccess)
+                st = WRS_ERR_CUDA;
             float ms_min = 1e30f;
             for (int rep = 0; st == WRS_SUCCESS && rep < 4; ++rep) {  // the first launch warms up
                 cudaEventRecord(e0, cap);
