@@ -254,8 +254,8 @@ extern "C" wrs_status wrs_rejection_sample_packed(const uint64_t* d_slots, uint6
     cudaStream_t stream = static_cast<cudaStream_t>(stream_);
     const DeviceInfo dev = device_info();
     const uint32_t tries = max_tries ? max_tries : 64u;
-    const uint64_t per = (uint64_t)kRejPackedJ;
-    uint64_t grid = ((num_samples + per - 1) / per + 255) / 256;
+    const uint64_t per = (uint64_t)kRejPackedR * 256;  // samples per CTA and chunk
+    uint64_t grid = (num_samples + per - 1) / per;
     const uint64_t cap = (uint64_t)dev.sm_count * 8;
     if (grid > cap) grid = cap;
     rejection_sample_packed_kernel<<<(uint32_t)grid, 256, 0, stream>>>(

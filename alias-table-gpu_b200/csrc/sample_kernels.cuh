@@ -349,10 +349,13 @@ __global__ void __launch_bounds__(256) rejection_pack_kernel(const uint32_t* __r
 }
 
 // Rejection sampling from packed slots: the tries and decisions of rejection_sample_kernel
-// (same Philox blocks, same slot, same comparison, so the same samples), eight consecutive
-// samples per thread with their tries interleaved, so that eight gathers are in flight (2^28
-// samples from 1.28e8 slots: 10.7 ms, 12.2 with four).
-constexpr int kRejPackedJ = 8;
+// (same Philox blocks, same slot, same comparison, so the same samples). A thread owns R
+// consecutive samples of its CTA's chunk and keeps J of them in flight: a sample that is
+// accepted (or runs out of tries) writes its result to shared memory and its place is taken by
+// the thread's next sample, so that J gathers stay in flight until the thread's last samples;
+// the chunk's results then go out coalesced.
+constexpr int kRejPackedJ = 8;   // samples in flight per thread
+constexpr int kRejPackedR = 32;  // samples per thread and chunk
 __global__ void __launch_bounds__(256) rejection_sample_packed_kernel(const uint2* __restrict__ slots,
                                                                       uint64_t slot_capacity,
                                                                       const uint64_t* __restrict__ a_size_ptr,
@@ -360,59 +363,71 @@ __global__ void __launch_bounds__(256) rejection_sample_packed_kernel(const uint
                                                                       uint64_t cbase, uint32_t max_tries,
                                                                       uint32_t* __restrict__ out, uint32_t* status) {
     constexpr int J = kRejPackedJ;
-    static_assert(J % 4 == 0, "16-byte stores");
+    constexpr uint32_t R = kRejPackedR;
+    constexpr int NT = 256;
+    __shared__ uint32_t s_res[NT * (R + 1)];  // thread t's sample k at t * (R + 1) + k (no bank conflicts)
     const uint64_t asz64 = *a_size_ptr;
     const uint64_t gsize = (uint64_t)gridDim.x * blockDim.x;
-    const uint64_t g0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     bool failed = false;
     if (asz64 == 0 || asz64 > 0xffffffffull || asz64 > slot_capacity) {  // no (or an unusable) slot array
-        for (uint64_t s = g0; s < m; s += gsize) out[s] = 0xffffffffu;
+        for (uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; s < m; s += gsize) out[s] = 0xffffffffu;
         if (status && blockIdx.x == 0 && threadIdx.x == 0) record_status(status, kErrCapacity);
         return;
     }
     const uint32_t asz = (uint32_t)asz64;
-    const bool out16 = ((uintptr_t)out & 15u) == 0;
-    for (uint64_t s0 = g0 * J; s0 < m; s0 += gsize * J) {
-        uint32_t res[J];
-        uint32_t open = 0;  // bit j: sample s0 + j still drawing
+    const uint64_t chunk = (uint64_t)NT * R;
+    for (uint64_t c0 = (uint64_t)blockIdx.x * chunk; c0 < m; c0 += (uint64_t)gridDim.x * chunk) {
+        const uint64_t t0 = c0 + (uint64_t)threadIdx.x * R;  // the thread's first sample
+        const uint32_t cnt = t0 < m ? (uint32_t)min((uint64_t)R, m - t0) : 0u;
+        uint32_t* res = s_res + threadIdx.x * (R + 1);
+        uint32_t idx[J], tr[J];  // the sample (within the thread's R; R = none) and its next try
+        uint32_t next = 0;
 #pragma unroll
         for (int j = 0; j < J; ++j) {
-            res[j] = 0xffffffffu;
-            if (s0 + j < m) open |= 1u << j;
+            idx[j] = next < cnt ? next++ : R;
+            tr[j] = 0;
         }
-        for (uint32_t t = 0; t < max_tries && open; ++t) {
+        while (true) {
+            bool any = false;
             uint32_t xc[J];
             uint2 v[J];
 #pragma unroll
             for (int j = 0; j < J; ++j) {
-                if ((open >> j) & 1u) {
-                    const uint64_t b = cbase + s0 + j;
-                    const Philox4 r = philox4x32_10((uint32_t)b, (uint32_t)(b >> 32), t, 0x52454a00u, k0, k1);
+                if (idx[j] < R) {
+                    any = true;
+                    const uint64_t b = t0 + idx[j] + cbase;
+                    const Philox4 r = philox4x32_10((uint32_t)b, (uint32_t)(b >> 32), tr[j], 0x52454a00u, k0, k1);
                     xc[j] = r.x[2];
                     v[j] = ld_row_64B(slots + slot_of(r.x[0], r.x[1], asz));
                 }
             }
+            if (!any) break;
 #pragma unroll
             for (int j = 0; j < J; ++j) {
-                if ((open >> j) & 1u) {
+                if (idx[j] < R) {
                     const uint32_t e = v[j].x;
-                    if ((e >> 31) == 0u || coin24(xc[j]) < __uint_as_float(v[j].y)) {
-                        res[j] = e & 0x7fffffffu;
-                        open &= ~(1u << j);
+                    bool done = true;
+                    uint32_t val = e & 0x7fffffffu;
+                    if ((e >> 31) != 0u && !(coin24(xc[j]) < __uint_as_float(v[j].y))) {  // rejected
+                        if (++tr[j] < max_tries) {
+                            done = false;
+                        } else {
+                            val = 0xffffffffu;
+                            failed = true;
+                        }
+                    }
+                    if (done) {
+                        res[idx[j]] = val;
+                        idx[j] = next < cnt ? next++ : R;
+                        tr[j] = 0;
                     }
                 }
             }
         }
-        if (open) failed = true;
-        if (out16 && s0 + J <= m) {
-#pragma unroll
-            for (int q = 0; q < J / 4; ++q)
-                reinterpret_cast<uint4*>(out + s0)[q] = make_uint4(res[4 * q], res[4 * q + 1], res[4 * q + 2], res[4 * q + 3]);
-        } else {
-#pragma unroll
-            for (int j = 0; j < J; ++j)
-                if (s0 + j < m) out[s0 + j] = res[j];
-        }
+        __syncthreads();
+        const uint32_t n_out = (uint32_t)min(chunk, m - c0);
+        for (uint32_t i = threadIdx.x; i < n_out; i += NT) out[c0 + i] = s_res[i + i / R];
+        __syncthreads();  // before the next chunk's results
     }
     if (failed && status) record_status(status, kErrTooManyTries);
 }
