@@ -110,6 +110,23 @@ def test_rejection_sample_packed_equals_unpacked(cuda, max_tries, m):
     assert st == (wrs.WRS_ERR_TOO_MANY_TRIES if failed else 0)
 
 
+@pytest.mark.parametrize("maker", [lambda: big_items(70_001), lambda: many_huge_items(500_000)])
+def test_rejection_sample_packed_huge_items(cuda, maker):
+    # items of thousands and of more than 2^16 slots; more samples than one chunk per CTA
+    w = maker()
+    st, A, frac, asz, W = gpu_rej_build(w)
+    assert st == 0
+    slots = packed(A, asz, frac, w.size)
+    m = 1_000_003
+    out = torch.empty(m, dtype=torch.int32, device="cuda")
+    ref_out = torch.empty(m, dtype=torch.int32, device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    assert wrs.rejection_sample_packed(slots, asz, w.size, m, SEED, out, 11, 3, status, sync=True) in (0, wrs.WRS_ERR_TOO_MANY_TRIES)
+    st_ref = wrs.rejection_sample(A, asz, frac, w.size, m, SEED, ref_out, 11, 3, None, sync=True)
+    assert st_ref == 0
+    assert torch.equal(out, ref_out)
+
+
 def test_rejection_sample_packed_slot_capacity(cuda):
     w = gen("uniform", 5_000)
     st, A, frac, asz, W = gpu_rej_build(w)
